@@ -1,0 +1,228 @@
+"""Pins the CPU oracle against the reference's golden fixtures and hand cases (CPU only).
+
+The oracle (oracle/sssp_oracle.c) is the checker of the CUDA path; these tests establish that it
+reproduces the reference's bytes before anything is compared against it:
+  - cpp/tests/algorithms/sssp/sssp_fixture_test.cpp:110-190: compute() == the initial trees,
+    update() from the initial trees (imported without canonicalisation) == the updated trees,
+    `invalidated` == the recorded counter, for all 34 cases and every objective;
+  - cpp/tests/data/mosp_graph_io/*/applied: the applied CSR, its transpose and the
+    weight-increase mask of apply_batch_host;
+  - the README quickstart and hand cases of cpp/tests/algorithms/sssp/sssp_test.cpp:74-330.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import INF, fixture_case
+
+
+def _cases(z):
+    return [str(c) for c in z["cases"]]
+
+
+def test_fixture_count(fixtures):
+    assert len(_cases(fixtures)) == 34
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_fixtures_compute_and_update(fixtures, rule):
+    comparisons = 0
+    for name in _cases(fixtures):
+        c = fixture_case(fixtures, name)
+        for k in range(c["k"]):
+            g = O.Graph.from_csr(c["row_ptr"], c["col"], c["w"], c["k"], O.mosp_props())
+            t, _ = O.compute(g, 0, objective=k, rule=rule)
+            np.testing.assert_array_equal(t.distances, c["init_d"][k], err_msg=f"{name} k{k}")
+            np.testing.assert_array_equal(t.parents, c["init_p"][k], err_msg=f"{name} k{k}")
+            t = O.from_arrays(g, 0, c["init_d"][k], c["init_p"][k], canonicalize=False,
+                              objective=k, rule=rule)
+            st, _ = O.update(g, O.Batch(c["ins_src"], c["ins_dst"], c["ins_w"], c["del_src"],
+                                        c["del_dst"], c["k"]), t)
+            np.testing.assert_array_equal(t.distances, c["upd_d"][k], err_msg=f"{name} k{k}")
+            np.testing.assert_array_equal(t.parents, c["upd_p"][k], err_msg=f"{name} k{k}")
+            assert st["invalidated"] == c["invalidated"][k], name
+            comparisons += 1
+    assert comparisons > 34
+
+
+def test_fixtures_applied_csr(fixtures):
+    checked = 0
+    for name in _cases(fixtures):
+        c = fixture_case(fixtures, name)
+        if "applied_row_ptr" not in c:
+            continue
+        g = O.Graph.from_csr(c["row_ptr"], c["col"], c["w"], c["k"], O.mosp_props())
+        g.apply(O.Batch(c["ins_src"], c["ins_dst"], c["ins_w"], c["del_src"], c["del_dst"],
+                        c["k"]))
+        csr = g.to_csr()
+        np.testing.assert_array_equal(csr["row_ptr"], c["applied_row_ptr"], err_msg=name)
+        np.testing.assert_array_equal(csr["col"], c["applied_col"], err_msg=name)
+        np.testing.assert_array_equal(csr["w"], c["applied_w"], err_msg=name)
+        np.testing.assert_array_equal(csr["in_row_ptr"], c["applied_in_row_ptr"], err_msg=name)
+        np.testing.assert_array_equal(csr["in_col"], c["applied_in_col"], err_msg=name)
+        np.testing.assert_array_equal(csr["in_w"], c["applied_in_w"], err_msg=name)
+        np.testing.assert_array_equal(g.delta()["weight_increased"], c["applied_increase"],
+                                      err_msg=name)
+        checked += 1
+    assert checked == 27
+
+
+def _g(n, edges, props=None, k=1):
+    src = [e[0] for e in edges]
+    dst = [e[1] for e in edges]
+    w = [x for e in edges for x in e[2:]]
+    return O.Graph.from_edges(n, src, dst, w, k, props or O.mosp_props())
+
+
+def test_readme_quickstart():
+    # README.md:73-97: 0 4 1 2 | invalidated 2
+    g = _g(4, [(0, 1, 4), (0, 2, 1), (2, 1, 2), (1, 3, 1)], O.default_props())
+    t, _ = O.compute(g, 0)
+    assert t.distances.tolist() == [0, 3, 1, 4]
+    st, _ = O.update(g, O.Batch([2], [3], [1], [2], [1]), t)
+    assert t.distances.tolist() == [0, 4, 1, 2]
+    assert st["invalidated"] == 2
+
+
+def test_canonical_tree_and_tie_parent():
+    # sssp_test.cpp:74-99
+    g = _g(5, [(0, 1, 5), (0, 2, 1), (2, 3, 1), (1, 4, 2), (3, 4, 2)])
+    t, _ = O.compute(g, 0)
+    assert t.distances.tolist() == [0, 5, 1, 2, 4]
+    assert t.parents.tolist() == [-1, 0, 0, 2, 3]
+    st, sm = O.update(g, O.Batch([2], [1], [1]), t)
+    assert t.distances.tolist() == [0, 2, 1, 2, 4]
+    assert t.parents.tolist() == [-1, 2, 0, 2, 1]
+    assert st["invalidated"] == 0 and st["affected"] == 2
+    assert sm["inserted_edges"] == 1
+
+
+def test_no_count_to_infinity():
+    # sssp_test.cpp:101-112
+    g = _g(4, [(0, 1, 1), (0, 3, 50), (1, 2, 1), (2, 1, 1), (3, 1, 50)])
+    t, _ = O.compute(g, 0)
+    st, _ = O.update(g, O.Batch(delete_src=[0], delete_dst=[1]), t)
+    assert t.distances.tolist() == [0, 100, 101, 50]
+    assert t.parents.tolist() == [-1, 3, 1, 0]
+    assert st["invalidated"] == 2 and st["affected"] == 2
+
+
+def test_delete_all_then_reinsert():
+    # sssp_test.cpp:114-135
+    g = _g(5, [(0, 1, 3), (1, 2, 4), (0, 3, 2), (3, 4, 7)])
+    t, _ = O.compute(g, 0)
+    st, _ = O.update(g, O.Batch(delete_src=[0, 1, 0, 3], delete_dst=[1, 2, 3, 4]), t)
+    assert g.m == 0
+    assert t.distances.tolist() == [0, INF, INF, INF, INF]
+    assert t.parents.tolist() == [-1] * 5
+    assert st["invalidated"] == 4 and st["affected"] == 4
+    O.update(g, O.Batch([0, 4], [4, 2], [9, 1]), t)
+    assert t.distances.tolist() == [0, INF, 10, INF, 9]
+    assert t.parents.tolist() == [-1, -1, 4, -1, 0]
+
+
+def test_weight_increase_on_tree_edge():
+    # sssp_test.cpp:154-166
+    g = _g(3, [(0, 1, 1), (1, 2, 1), (0, 2, 5)])
+    t, _ = O.compute(g, 0)
+    st, sm = O.update(g, O.Batch([0], [1], [10]), t)
+    assert st["invalidated"] == 2 and sm["updated_edges"] == 1
+    assert t.distances.tolist() == [0, 10, 5]
+    assert t.parents.tolist() == [-1, 0, 0]
+
+
+def test_parallel_edges_and_self_loops():
+    # sssp_test.cpp:168-186
+    g = _g(3, [(0, 1, 7), (0, 1, 3), (1, 1, 1), (1, 2, 1)])
+    t, _ = O.compute(g, 0)
+    assert t.distances.tolist() == [0, 3, 4]
+    st, _ = O.update(g, O.Batch(delete_src=[0], delete_dst=[1]), t)
+    assert st["invalidated"] == 2
+    assert t.distances.tolist() == [0, 3, 4]
+    O.update(g, O.Batch(delete_src=[0], delete_dst=[1]), t)
+    assert t.distances.tolist() == [0, INF, INF]
+
+
+def test_vertex_growth():
+    # sssp_test.cpp:188-199
+    g = _g(3, [(0, 1, 2), (1, 2, 2)], O.default_props())
+    t, _ = O.compute(g, 0)
+    st, sm = O.update(g, O.Batch([2, 5], [5, 3], [1, 4]), t)
+    assert g.n == 6 and sm["num_vertices_after"] == 6
+    assert t.distances.tolist() == [0, 2, 4, 9, INF, 5]
+    assert t.parents.tolist() == [-1, 0, 1, 5, -1, 2]
+
+
+def test_undirected():
+    # sssp_test.cpp:201-212
+    g = _g(4, [(0, 1, 1), (1, 2, 1), (2, 3, 1)], O.mosp_props(directed=0))
+    t, _ = O.compute(g, 3)
+    assert t.distances.tolist() == [3, 2, 1, 0]
+    O.update(g, O.Batch([0], [3], [5], [1], [2]), t)
+    assert t.distances.tolist() == [5, 6, 1, 0]
+    assert t.parents.tolist() == [3, 0, 3, -1]
+
+
+def test_multi_objective_column():
+    # sssp_test.cpp:214-236
+    g = _g(3, [(0, 1, 1, 10), (1, 2, 1, 10), (0, 2, 5, 1)], k=2)
+    t1, _ = O.compute(g, 0, objective=1)
+    assert t1.distances.tolist() == [0, 10, 1]
+    st, _ = O.update(g, O.Batch([0], [2], [5, 30], num_weights=2), t1)
+    assert st["invalidated"] == 1
+    assert t1.distances.tolist() == [0, 10, 20]
+    assert t1.parents.tolist() == [-1, 0, 1]
+
+
+def test_non_canonical_tree_keeps_tie_parents():
+    # sssp_test.cpp:313-333
+    g = _g(5, [(0, 1, 1), (0, 2, 1), (1, 3, 1), (2, 3, 1), (0, 4, 5), (4, 3, 1)])
+    t = O.from_arrays(g, 0, [0, 1, 1, 2, 5], [-1, 0, 0, 2, 0], canonicalize=False)
+    st, _ = O.update(g, O.Batch([0], [4], [1]), t)
+    assert t.distances.tolist() == [0, 1, 1, 2, 1]
+    assert t.parents.tolist() == [-1, 0, 0, 2, 0]
+    assert st["affected"] == 1
+
+
+@pytest.mark.parametrize("side,dup", [(272, False), (64, True)])
+def test_distance_only_mode(side, dup):
+    # sssp_test.cpp:238-311: weights 2e9 so (n-1)*w does not fit next to the parent bits; the
+    # parents are recovered with the lowest-id rule.  Scaled down for the second case.
+    w = 2_000_000_000
+    v = np.arange(side * side)
+    x, y = v % side, v // side
+    r = v[x + 1 < side]
+    d = v[y + 1 < side]
+    src = np.concatenate([r, d] + ([r + 1, d + side] if dup else []))
+    dst = np.concatenate([r + 1, d + side] + ([r, d] if dup else []))
+    g = O.Graph.from_edges(side * side, src, dst, np.full(src.size, w), 1, O.mosp_props())
+    n = side * side
+    if not O.packs_parents(n, w, 0):
+        t, st = O.compute(g, 0)
+        assert st["packed_parents"] == 0
+        del_src = list(range(0, n - 1, 97))
+        st, _ = O.update(g, O.Batch([0], [n - 1], [w], del_src, [s + 1 for s in del_src]), t)
+        fresh, _ = O.compute(g, 0)
+        np.testing.assert_array_equal(t.distances, fresh.distances)
+        np.testing.assert_array_equal(t.parents, fresh.parents)
+
+
+def test_invalid_batches_raise():
+    g = _g(3, [(0, 1, 2), (1, 2, 2)], O.default_props())
+    t, _ = O.compute(g, 0)
+    with pytest.raises(O.OracleError):
+        O.update(g, O.Batch([0], [1], [0]), t)  # weight below 1
+    with pytest.raises(O.OracleError):
+        O.update(g, O.Batch([-1], [1], [3]), t)  # negative id
+    assert g.n == 3 and g.m == 2  # nothing changed
+
+
+def test_packing_rules():
+    # cuda.cu:225-234 vs sssp.cpp:153-165 (the packing window)
+    n = 1 << 17
+    bits = 18
+    maxd = ((2**64 - 1) >> bits) - 1
+    w = maxd // (n - 1)
+    assert O.packs_parents(n, w, 1)
+    assert not O.packs_parents(n, w, 0)
+    assert O.default_delta(100, 10, 1000) == 32
