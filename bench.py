@@ -1,0 +1,364 @@
+"""Benchmark: batch-dynamic SSSP update on one B200 (changed edges/s, p50/p99 update latency).
+
+Workload (the headline configuration): directed R-MAT, scale 22 (4,194,304 vertices), edge
+factor 16, (a, b, c) = (0.57, 0.19, 0.19), self-loops and duplicate pairs dropped, int32 weights
+uniform in [1, 1000], source 0; consecutive 100k-change batches, 75% insertions of uniform
+random pairs, 25% deletions (half current tree edges parent[v] -> v, half uniform other edges).
+Seeded synthetic data (the reference publishes no number for this configuration).
+
+A step is one sssp::update of one batch.  `value` times the update with the batch already in
+device memory (CUDA events on the library's stream); `e2e` times the public call with the batch
+in pinned host memory (the copy to the device and the read-back of the stats inside the timed
+region).  Every run checks the final tree against a from-scratch compute (distances and
+parents bit-exact).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch 100000] [--scale 22]
+    python bench.py --impl reference ...   # the reference algorithm's CPU restatement (oracle)
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "changed edges/s and p50/p99 update latency, learned vs plain schedule, 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=100_000)
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--schedule", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-verify", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_workload(args, device):
+    from dyng_b200 import generators as G
+    t0 = time.time()
+    edges = G.rmat(args.scale, 16, w_max=1000, seed=1, device=device)
+    return edges, time.time() - t0
+
+
+# Algorithmic bytes of the sssp kernel per counted unit (ints 4 B, packed words 8 B):
+#   per pushed vertex: list entry 4 + word 8 + row descriptor 8
+#   per scanned out-slot: column 4 + weight 4 + target word 8
+#   per successful atomicMin: 8;  per frontier append: 4
+#   per pulled in-slot: column 4 + weight 4 + source word 8
+#   per invalidation round: 12 per vertex (ancestor read + write, flag read)
+BYTES = {"pushes": 20, "edges": 16, "atomics": 8, "appends": 4, "pull_edges": 16,
+         "round_vertices": 12}
+
+
+def algorithmic_bytes(counters):
+    return sum(BYTES[k] * counters.get(k, 0) for k in BYTES)
+
+
+def cpu_baseline_sample(edges, tree_d, tree_p, batches, budget_s=20.0):
+    """The oracle (the reference's algorithm restated in C, one thread) on the same graph and
+    batches: time sssp::update per batch until the budget is spent."""
+    from oracle import oracle as O
+    rp, col, w = edges.csr()
+    og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
+    ot = O.from_arrays(og, 0, tree_d, tree_p, canonicalize=False, validate=False, rule=1)
+    done, changes, spent = 0, 0, 0.0
+    for b in batches:
+        t0 = time.perf_counter()
+        O.update(og, O.Batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                             b.delete_dst), ot)
+        spent += time.perf_counter() - t0
+        done += 1
+        changes += b.size
+        if spent > budget_s:
+            break
+    return changes / spent, done, spent
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU algorithm (the oracle port) on this workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    device = "cuda" if torch.cuda.is_available() else None
+    edges, _ = make_workload(args, device)
+    from dyng_b200 import generators as G
+    from oracle import oracle as O
+    rp, col, w = edges.csr()
+    og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
+    # initial tree: from the CUDA path when a GPU is present (a compute of the oracle at this
+    # scale is not part of the update path), else from the oracle
+    if device:
+        import dyng_b200 as D
+        g = D.Graph.from_csr(rp, col, w)
+        t = D.sssp.compute(g, 0)
+        d0, p0 = t.distances, t.parents
+        del t, g
+    else:
+        ot0, _ = O.compute(og, 0, rule=1)
+        d0, p0 = ot0.distances, ot0.parents
+    ot = O.from_arrays(og, 0, d0, p0, canonicalize=False, validate=False, rule=1)
+    stream = G.BatchStream(edges, seed=7)
+    times, sizes = [], []
+    for step in range(args.warmup + args.steps):
+        b = stream.next(args.batch, 0.75, 0.5, parents=ot.parents)
+        t0 = time.perf_counter()
+        O.update(og, O.Batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                             b.delete_dst), ot)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+            sizes.append(b.size)
+    total = sum(times)
+    value = sum(sizes) / total
+    line = {"metric": METRIC, "value": value, "unit": "changed edges/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"rmat-s{args.scale}-ef16-w1000-batch{args.batch}",
+                       "batch_changes": args.batch, "insert_fraction": 0.75,
+                       "p50_ms": 1000 * float(np.percentile(times, 50)),
+                       "p99_ms": 1000 * float(np.percentile(times, 99))},
+            "cpu_baseline": {"value": value, "unit": "changed edges/s", "cores": 1,
+                             "kind": "port",
+                             "sample": f"{len(times)} consecutive {args.batch}-change batches"},
+            "e2e": {"value": value, "unit": "changed edges/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import dyng_b200 as D
+    from dyng_b200 import generators as G
+    from dyng_b200 import _native as N
+
+    # replicas only: every rank runs the same independent workload on its own GPU
+    stream = torch.cuda.Stream()
+    res = D.Resources(local, stream.cuda_stream)
+    edges, gen_s = make_workload(args, "cuda")
+    rp, col, w = edges.csr()
+    t0 = time.time()
+    g = D.Graph.from_csr(rp, col, w, resources=res)
+    tree = D.sssp.compute(g, 0)
+    build_s = time.time() - t0
+    bs = G.BatchStream(edges, seed=7)
+
+    def device_batch(b):
+        ts = [torch.from_numpy(np.ascontiguousarray(x)).to(f"cuda:{local}") for x in
+              (b.insert_src, b.insert_dst, b.insert_weights, b.delete_src, b.delete_dst)]
+        return ts, D.EdgeBatch.device(ts[0].data_ptr(), ts[1].data_ptr(), ts[2].data_ptr(),
+                                      b.insert_src.size, ts[3].data_ptr(), ts[4].data_ptr(),
+                                      b.delete_src.size)
+
+    sched = None
+    timed_stats = []
+    lat = []
+    sizes = []
+    # warm-up + timed steps with device-resident batches
+    for step in range(args.warmup + args.steps):
+        b = bs.next(args.batch, 0.75, 0.5, parents=tree.parents)
+        keep, db = device_batch(b)
+        torch.cuda.synchronize()
+        if step == args.warmup:
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            sampler = ClockSampler(local)
+            sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = D.sssp.update(g, db, tree, schedule=sched)
+        e1.record(stream)
+        e1.synchronize()
+        if step >= args.warmup:
+            lat.append(e0.elapsed_time(e1))
+            sizes.append(b.size)
+            timed_stats.append(st)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = float(sum(lat))
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * sum(sizes) / (total_ms / 1000.0)
+
+    # end to end: batches in pinned host memory through the public call
+    e2e_lat, e2e_sizes = [], []
+    h2d = 0
+    for step in range(args.steps):
+        b = bs.next(args.batch, 0.75, 0.5, parents=tree.parents)
+        pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in
+                  (b.insert_src, b.insert_dst, b.insert_weights, b.delete_src, b.delete_dst)]
+        arrs = [p.numpy() for p in pinned]
+        hb = D.EdgeBatch.from_arrays(*arrs)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = D.sssp.update(g, hb, tree, schedule=sched)
+        e2e_lat.append(time.perf_counter() - t0)
+        e2e_sizes.append(b.size)
+        h2d = sum(a.nbytes for a in arrs)
+    e2e_value = world * sum(e2e_sizes) / sum(e2e_lat)
+
+    # correctness at full size: the updated tree equals a from-scratch compute on the new graph
+    verified = None
+    if not args.no_verify:
+        fresh = D.sssp.compute(g, 0)
+        verified = bool(np.array_equal(fresh.distances, tree.distances) and
+                        np.array_equal(fresh.parents, tree.parents))
+        del fresh
+
+    # roofline of the dominant kernel (the sssp persistent kernel)
+    sssp_ms = [s.sssp_ms for s in timed_stats]
+    apply_ms = [s.apply_ms for s in timed_stats]
+    peak, peak_kind = peaks()
+    counters = {}
+    for s in timed_stats:
+        for k, v in getattr(s, "counters", {}).items():
+            counters[k] = counters.get(k, 0) + v
+    alg = algorithmic_bytes(counters) / max(len(timed_stats), 1)
+    achieved = alg / (np.mean(sssp_ms) / 1000.0) / 1e9 if sssp_ms else 0.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cbs = G.BatchStream(edges, seed=7)
+            batches = [cbs.next(args.batch, 0.75, 0.5, parents=None) for _ in range(4)]
+            # the sample starts from the initial tree of the same graph
+            g0 = D.Graph.from_csr(rp, col, w, resources=res)
+            t_init = D.sssp.compute(g0, 0)
+            d0, p0 = t_init.distances, t_init.parents
+            del t_init, g0
+            v, done, spent = cpu_baseline_sample(edges, d0, p0, batches)
+            cpu = {"value": v, "unit": "changed edges/s", "cores": 1, "kind": "port",
+                   "sample": f"oracle sssp::update on {done} of the workload's {args.batch}-change "
+                             f"batches ({spent:.1f} s), same graph"}
+        except Exception as exc:  # noqa: BLE001
+            cpu = {"value": None, "unit": "changed edges/s", "cores": 1, "kind": "port",
+                   "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "changed edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic",
+            "config": {"workload": f"rmat-s{args.scale}-ef16-w1000-batch{args.batch}",
+                       "vertices": int(edges.num_vertices), "edges": int(edges.src.size),
+                       "batch_changes": args.batch, "insert_fraction": 0.75,
+                       "schedule": args.schedule, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (graph arenas ~1 GB)",
+                       "p50_ms": float(np.percentile(lat, 50)),
+                       "p99_ms": float(np.percentile(lat, 99)),
+                       "apply_ms_mean": float(np.mean(apply_ms)),
+                       "sssp_ms_mean": float(np.mean(sssp_ms)),
+                       "verified_vs_compute": verified,
+                       "setup_s": {"generate": round(gen_s, 1), "build_and_compute": round(build_s, 1)}},
+            "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 512,
+                    "p50_ms": 1000 * float(np.percentile(e2e_lat, 50)),
+                    "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
+            "gpu_launches": 14 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "peak_kind": peak_kind, "kernel": "k_sssp"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

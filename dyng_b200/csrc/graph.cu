@@ -1,0 +1,1568 @@
+// The device-resident slack-row graph and the batch applier.
+//
+// Layout in HBM (one graph):
+//   out_desc[v] = {start, len}   slack row of v in the out arena (len counts tombstones)
+//   out_cap[v], out_dead[v]      slots owned by the row, tombstones inside it
+//   out_col[arena], out_w[k][arena]   neighbour ids and k weight columns (objective-major);
+//                                      rows start on 16-byte boundaries (multiples of 4 slots)
+//   in_*                          the same for the in-edge mirror (source ids)
+// A deleted edge becomes a tombstone (column -1) in both rows; insertions append after the last
+// slot.  A row that runs out of slots moves to the top of its arena, compacted, with new slack.
+// Row order is the order of the reference's compact rows under row_order::append; under
+// row_order::sorted the export sorts (the sssp kernels do not depend on the order).
+//
+// The applier reproduces apply_batch_host (reference cpp/src/graph/apply_host.cpp:57-395):
+// Step 0 (self-loops, vertex growth, undirected expansion), deletions of the first alive match,
+// upserts of the first alive match or appends, and the weight-increase classification
+// (apply_host.cpp:348-393) -- restated per (u, v) pair: every outcome of a pair depends only on
+// its number of existing matches c, its deletions d and insertions t and the first / last
+// insertion, so the pairs are grouped by a hash table instead of rebuilding rows in batch order.
+#include "internal.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace dyngb200 {
+
+namespace {
+
+constexpr u64 kEmptyKey = ~0ULL;
+constexpr int kChunk = 2048;  // row entries scanned by one warp-sized work item
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ u64 mix64(u64 x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdULL;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ULL;
+  x ^= x >> 33;
+  return x;
+}
+
+__device__ __forceinline__ u64 pair_key(int32_t u, int32_t v) {
+  return (static_cast<u64>(static_cast<uint32_t>(u)) << 32) | static_cast<uint32_t>(v);
+}
+
+struct ApplyParams {
+  GraphView g;
+  const int32_t* ins_src;
+  const int32_t* ins_dst;
+  const int32_t* ins_w;
+  long long ni;
+  const int32_t* del_src;
+  const int32_t* del_dst;
+  long long nd;
+  int k;
+  int objective;
+  dyngb200_props props;
+  long long delta_opt;
+  // pair table
+  u64* key;
+  int mask;
+  int* d;
+  int* t;
+  int* first;
+  int* last;
+  int* out_pos;
+  int* in_pos;
+  int* out_pos2;
+  int* in_pos2;
+  int* flags;
+  int* out_rank;
+  int* in_rank;
+  int* out_count;  // matches in the out row (multi-edge graphs)
+  int* in_count;
+  int* list;
+  unsigned char* inc;
+  // touched rows
+  int* touch_out_stamp;
+  int* touch_in_stamp;
+  int* row_slot_out;
+  int* row_slot_in;
+  int touch_gen;
+  int* rows_out;
+  int* rows_in;
+  int* dels_out;
+  int* dels_in;
+  int* apps_out;
+  int* apps_in;
+  int* reloc_out;
+  int* reloc_in;
+  unsigned* new_start_out;
+  unsigned* new_start_in;
+  int* new_cap_out;
+  int* new_cap_in;
+  int* live_out;
+  int* live_in;
+  int2* chunks_out;
+  int2* chunks_in;
+  long long chunk_cap;
+  // column statistics deltas (k entries each)
+  long long* col_sum_delta;
+  long long* col_removed_at_max;
+  long long* col_written_max;
+  long long* col_written_at_max;
+  UpdateCtl* ctl;
+};
+
+// Pair flags.
+enum : int {
+  kPairDelete = 1,       // the batch deletes (u,v) at least once: a changed edge
+  kPairIncreased = 2,    // the objective's weight of (u,v) increased: a changed edge
+  kPairHead = 4,         // the batch inserts (u,v): v is an insertion head
+  kPairAppend = 8,       // a new slot is appended to both rows
+  kPairUpsert = 16,      // an existing slot receives the insertion's weights
+  kPairUseFirst = 32,    // the first insertion's weights (ignore semantics), else the last's
+};
+
+__device__ __forceinline__ int find_pair(const ApplyParams& p, u64 k) {
+  unsigned h = static_cast<unsigned>(mix64(k)) & static_cast<unsigned>(p.mask);
+  for (int probe = 0; probe <= p.mask; ++probe) {
+    const u64 cur = p.key[h];
+    if (cur == k) return static_cast<int>(h);
+    if (cur == kEmptyKey) return -1;
+    h = (h + 1) & static_cast<unsigned>(p.mask);
+  }
+  return -1;
+}
+
+// ---- A: Step 0 checks, vertex growth, largest insertion weight --------------------------------
+__global__ void k_validate(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  const long long total = p.ni + p.nd;
+  const long long n = c->n_old;
+  long long top = 0;
+  long long wmax = 1;
+  int dropped = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (i < p.ni) {
+      const int32_t u = p.ins_src[i], v = p.ins_dst[i];
+      if (p.objective >= 0) {
+        const long long w = p.ins_w[i * p.k + p.objective];
+        if (w < 1) {
+          set_error(&c->error, kErrInvalidBatch);
+          atomicMin(&c->err_index, i);
+        }
+        wmax = max(wmax, w);
+      }
+      if (u < 0 || v < 0 || (!p.props.allow_vertex_growth && (u >= n || v >= n)) ||
+          u == INT32_MAX || v == INT32_MAX) {
+        set_error(&c->error, kErrInvalidBatch);
+        atomicMin(&c->err_index, i);
+        continue;
+      }
+      if (u == v && p.props.on_self_loop != 0) {
+        if (p.props.on_self_loop == 2) {
+          set_error(&c->error, kErrInvalidBatch);
+          atomicMin(&c->err_index, i);
+        }
+        ++dropped;
+        continue;
+      }
+      top = max(top, static_cast<long long>(max(u, v)) + 1);
+    } else {
+      const long long j = i - p.ni;
+      const int32_t u = p.del_src[j], v = p.del_dst[j];
+      if (u < 0 || v < 0) {
+        set_error(&c->error, kErrInvalidBatch);
+        atomicMin(&c->err_index, p.ni + j);
+        continue;
+      }
+      if (u == v && p.props.on_self_loop != 0) {
+        if (p.props.on_self_loop == 2) {
+          set_error(&c->error, kErrInvalidBatch);
+          atomicMin(&c->err_index, p.ni + j);
+        }
+        ++dropped;
+      }
+    }
+  }
+  if (top > 0) atomicMax(&c->n_after, top);
+  if (p.objective >= 0 && wmax > 1) atomicMax(&c->batch_ins_max, wmax);
+  if (dropped) atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[5]),
+                         static_cast<unsigned long long>(dropped));
+}
+
+// ---- B: the plan (one thread): capacity, packing bound, near-far width ------------------------
+__global__ void k_plan(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  const GraphCounters* gc = p.g.counters;
+  c->n_after = max(c->n_after, c->n_old);
+  if (c->n_after > p.g.n_cap) {
+    set_error(&c->error, kErrCapacity);
+  }
+  c->top_out = gc->out_top;
+  c->top_in = gc->in_top;
+  if (p.objective >= 0) {
+    const ColumnStats cs = p.g.columns[p.objective];
+    c->max_w = max(cs.max_w, c->batch_ins_max);
+    if (!distances_fit(c->n_after, c->max_w)) {
+      set_error(&c->error, kErrInvalidBatch);
+      c->err_index = -2;  // distances do not fit in 62 bits
+    }
+    const long long m = gc->m;
+    c->delta = p.delta_opt > 0 ? p.delta_opt : default_delta(m > 1 ? m : 1, gc->n, cs.sum_w);
+    u64 bound = 0;
+    const Packing pk = choose_packing(c->n_after, c->max_w, &bound);
+    c->packing_bits = pk.bits;
+    c->max_distance = bound;
+  }
+}
+
+__device__ void touch_row(const ApplyParams& p, int side, int32_t r) {
+  int* stamp = side == 0 ? p.touch_out_stamp : p.touch_in_stamp;
+  if (atomicExch(&stamp[r], p.touch_gen) == p.touch_gen) return;
+  UpdateCtl* c = p.ctl;
+  const int slot = atomicAdd(side == 0 ? &c->rows_out : &c->rows_in, 1);
+  (side == 0 ? p.rows_out : p.rows_in)[slot] = r;
+  (side == 0 ? p.row_slot_out : p.row_slot_in)[r] = slot;
+  (side == 0 ? p.dels_out : p.dels_in)[slot] = 0;
+  (side == 0 ? p.apps_out : p.apps_in)[slot] = 0;
+  const int len = r < c->n_old ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r].len : 0;
+  if (len > 0 && !p.g.allow_multi) {
+    const int chunks = (len + kChunk - 1) / kChunk;
+    const int base = atomicAdd(side == 0 ? &c->chunks_out : &c->chunks_in, chunks);
+    int2* list = side == 0 ? p.chunks_out : p.chunks_in;
+    for (int i = 0; i < chunks && base + i < p.chunk_cap; ++i) list[base + i] = make_int2(r, i);
+    if (base + chunks > p.chunk_cap) set_error(&c->error, kErrInternal);
+  }
+}
+
+__device__ void add_op(const ApplyParams& p, int32_t u, int32_t v, int kind, int index) {
+  const u64 k = pair_key(u, v);
+  unsigned h = static_cast<unsigned>(mix64(k)) & static_cast<unsigned>(p.mask);
+  int slot = -1;
+  for (int probe = 0; probe <= p.mask; ++probe) {
+    const u64 prev = atomicCAS(&p.key[h], kEmptyKey, k);
+    if (prev == kEmptyKey) {
+      slot = static_cast<int>(h);
+      p.out_pos[slot] = -1;
+      p.in_pos[slot] = -1;
+      p.out_pos2[slot] = -1;
+      p.in_pos2[slot] = -1;
+      p.out_count[slot] = 0;
+      p.in_count[slot] = 0;
+      p.list[append_slot(&p.ctl->pairs)] = slot;
+      touch_row(p, 0, u);
+      touch_row(p, 1, v);
+      break;
+    }
+    if (prev == k) {
+      slot = static_cast<int>(h);
+      break;
+    }
+    h = (h + 1) & static_cast<unsigned>(p.mask);
+  }
+  if (slot < 0) {
+    set_error(&p.ctl->error, kErrInternal);
+    return;
+  }
+  if (kind == 0) {
+    atomicAdd(&p.d[slot], 1);
+  } else {
+    atomicAdd(&p.t[slot], 1);
+    atomicMin(&p.first[slot], index);
+    atomicMax(&p.last[slot], index);
+  }
+}
+
+// ---- C: group the effective operations by (u, v) pair ------------------------------------------
+__global__ void k_pairs(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const long long total = p.ni + p.nd;
+  const long long n_after = c->n_after;
+  long long missing = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (i < p.ni) {
+      const int32_t u = p.ins_src[i], v = p.ins_dst[i];
+      if (u == v && p.props.on_self_loop != 0) continue;
+      add_op(p, u, v, 1, static_cast<int>(i));
+      if (!p.props.directed && u != v) add_op(p, v, u, 1, static_cast<int>(i));
+    } else {
+      const long long j = i - p.ni;
+      const int32_t u = p.del_src[j], v = p.del_dst[j];
+      if (u == v && p.props.on_self_loop != 0) continue;
+      if (u >= n_after || v >= n_after) {
+        missing += (!p.props.directed && u != v) ? 2 : 1;
+        if (p.props.on_missing_delete == 1) {
+          set_error(&c->error, kErrInvalidBatch);
+          atomicMin(&c->err_index, p.ni + j);
+        }
+        continue;
+      }
+      add_op(p, u, v, 0, static_cast<int>(j));
+      if (!p.props.directed && u != v) add_op(p, v, u, 0, static_cast<int>(j));
+    }
+  }
+  if (missing)
+    atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[4]),
+              static_cast<unsigned long long>(missing));
+}
+
+// ---- D: match existing slots (simple graphs: at most one slot per pair) -------------------------
+// One warp per chunk of kChunk slots; each live slot probes the pair table.
+__global__ void k_scan(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int n_out = min(static_cast<long long>(c->chunks_out), p.chunk_cap);
+  const int n_in = min(static_cast<long long>(c->chunks_in), p.chunk_cap);
+  for (int item = warp; item < n_out + n_in; item += warps) {
+    const int side = item < n_out ? 0 : 1;
+    const int2 ch = side == 0 ? p.chunks_out[item] : p.chunks_in[item - n_out];
+    const int32_t r = ch.x;
+    const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
+    const int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
+    const int begin = ch.y * kChunk;
+    const int end = min(desc.len, begin + kChunk);
+    for (int e = begin + lane; e < end; e += 32) {
+      const int32_t x = col[desc.start + e];
+      if (x < 0) continue;
+      const int slot = find_pair(p, side == 0 ? pair_key(r, x) : pair_key(x, r));
+      if (slot >= 0) {
+        if (side == 0) {
+          p.out_pos[slot] = e;
+          atomicAdd(&p.out_count[slot], 1);
+        } else {
+          p.in_pos[slot] = e;
+          atomicAdd(&p.in_count[slot], 1);
+        }
+      }
+    }
+  }
+}
+
+// Multi-edge graphs: one thread per pair walks its rows in order (the first alive matches).
+// Records c, the first match and the match the insertions address (see resolve).
+__global__ void k_scan_multi(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int pairs = c->pairs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    const u64 key = p.key[slot];
+    const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
+    const int d = p.d[slot];
+    const int t = p.t[slot];
+    for (int side = 0; side < 2; ++side) {
+      const int32_t r = side == 0 ? u : v;
+      const int32_t want = side == 0 ? v : u;
+      if (r >= c->n_old) continue;
+      const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
+      const int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
+      // first match, and match number d (the first survivor of the deletions)
+      int count = 0, first = -1, target = -1;
+      for (int e = 0; e < desc.len; ++e) {
+        if (col[e] != want) continue;
+        if (count == 0) first = e;
+        if (count == d) target = e;
+        ++count;
+      }
+      (void)t;
+      if (side == 0) {
+        p.out_count[slot] = count;
+        p.out_pos[slot] = first;
+        p.out_pos2[slot] = target;
+      } else {
+        p.in_count[slot] = count;
+        p.in_pos[slot] = first;
+        p.in_pos2[slot] = target;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void add_summary(UpdateCtl* c, int field, long long v) {
+  if (v) atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[field]),
+                   static_cast<unsigned long long>(v));
+}
+
+// ---- E: resolve every pair (counts, policies, classification, per-row slot demand) -------------
+__global__ void k_resolve(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int pairs = c->pairs;
+  const bool del_first = p.props.deletions_first != 0;
+  const int policy = p.props.on_existing_insert;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    const u64 key = p.key[slot];
+    const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
+    const int d = p.d[slot];
+    const int t = p.t[slot];
+    const int cnt = p.out_count[slot];
+    if (cnt != p.in_count[slot]) {
+      set_error(&c->error, kErrInternal);  // the in-edge mirror disagrees with the out rows
+      continue;
+    }
+    // Positions in storage: orig[0] is out_pos / in_pos; the addressed match (multi-edge graphs)
+    // is out_pos2 / in_pos2 (simple graphs: cnt <= 1, so match 0 is the only one).
+    const bool appended = t >= 1 && (del_first ? cnt <= d : cnt == 0);
+    const int seq = cnt + (appended ? 1 : 0);  // S = original matches, then the appended slot
+    const int removed = del_first ? min(cnt, d) : min(seq, d);
+    // Which element of S receives the insertion's weights (-1 none).
+    int target = -1;
+    if (t >= 1) target = appended ? cnt : (del_first ? d : 0);
+    const bool target_survives = target >= removed;
+    int flags = 0;
+    if (d > 0) flags |= kPairDelete;
+    if (t > 0) flags |= kPairHead;
+    long long inserted = 0, updated = 0, ignored_ins = 0;
+    if (t >= 1) {
+      if (appended) {
+        inserted = 1;
+        if (policy == 0) updated = t - 1;
+        else if (policy == 2) ignored_ins = t - 1;
+        else if (t > 1) set_error(&c->error, kErrInvalidBatch);
+      } else {
+        if (policy == 0) updated = t;
+        else if (policy == 2) ignored_ins = t;
+        else set_error(&c->error, kErrInvalidBatch);
+      }
+    }
+    const long long deleted = removed;
+    const long long ignored_del = d - removed;
+    if (ignored_del > 0 && p.props.on_missing_delete == 1) set_error(&c->error, kErrInvalidBatch);
+    const bool writes_weights = t >= 1 && (appended || policy == 0);
+    const bool use_first = appended && policy == 2;
+    if (appended && target_survives) flags |= kPairAppend;
+    if (!appended && t >= 1 && policy == 0 && target_survives) flags |= kPairUpsert;
+    if (use_first) flags |= kPairUseFirst;
+    add_summary(c, 0, inserted);
+    add_summary(c, 1, deleted);
+    add_summary(c, 2, updated);
+    add_summary(c, 3, ignored_ins);
+    add_summary(c, 4, ignored_del);
+    // Weight-increase classification (apply_host.cpp:348-393): first (u,v) before vs after.
+    const int ins_index = use_first ? p.first[slot] : p.last[slot];
+    const int final_idx = removed;  // S[removed] is the first (u,v) after the batch
+    const bool final_exists = final_idx < seq;
+    const bool orig_exists = cnt >= 1 && u < c->n_old;
+    const int out_base = orig_exists ? static_cast<int>(p.g.out_desc[u].start) : 0;
+    // storage position of S[final_idx] when it is an original slot (final_idx is 0 or d)
+    int final_pos = -1;
+    if (final_exists && final_idx < cnt) {
+      final_pos = final_idx == 0 ? p.out_pos[slot] : p.out_pos2[slot];
+    }
+    for (int j = 0; j < p.k; ++j) {
+      unsigned char inc = 0;
+      if (orig_exists && final_exists) {
+        const long long w0 = p.g.out_w[j * p.g.arena_cap + out_base + p.out_pos[slot]];
+        long long wf;
+        if (final_idx == target && writes_weights) {
+          wf = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+        } else {
+          wf = p.g.out_w[j * p.g.arena_cap + out_base + final_pos];
+        }
+        inc = wf > w0 ? 1 : 0;
+      }
+      p.inc[static_cast<long long>(slot) * p.k + j] = inc;
+      if (j == p.objective && inc) flags |= kPairIncreased;
+    }
+    p.flags[slot] = flags;
+    // per-row demand: tombstones for removed originals, one slot per surviving append
+    const int tomb = min(removed, cnt);
+    const int app = (flags & kPairAppend) ? 1 : 0;
+    if (tomb || app) {
+      const int so = p.row_slot_out[u];
+      const int si = p.row_slot_in[v];
+      if (tomb) {
+        atomicAdd(&p.dels_out[so], tomb);
+        atomicAdd(&p.dels_in[si], tomb);
+      }
+      if (app) {
+        p.out_rank[slot] = atomicAdd(&p.apps_out[so], 1);
+        p.in_rank[slot] = atomicAdd(&p.apps_in[si], 1);
+      }
+    }
+  }
+}
+
+// ---- F: per touched row: stay in place or move to the top of the arena -------------------------
+__global__ void k_alloc(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int rows_out = c->rows_out, rows_in = c->rows_in;
+  const double headroom = p.props.headroom;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows_out + rows_in;
+       i += gridDim.x * blockDim.x) {
+    const int side = i < rows_out ? 0 : 1;
+    const int s = side == 0 ? i : i - rows_out;
+    const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
+    const bool existing = r < c->n_old;
+    const RowDesc desc = existing ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r] : RowDesc{0, 0};
+    const int cap = existing ? (side == 0 ? p.g.out_cap : p.g.in_cap)[r] : 0;
+    const int dead = existing ? (side == 0 ? p.g.out_dead : p.g.in_dead)[r] : 0;
+    const int dels = (side == 0 ? p.dels_out : p.dels_in)[s];
+    const int apps = (side == 0 ? p.apps_out : p.apps_in)[s];
+    const int live = desc.len - dead - dels;
+    const int tomb = dead + dels;
+    const bool compact = tomb > 8 && tomb * 4 > desc.len;
+    int reloc = 0;
+    unsigned start = desc.start;
+    int new_cap = cap;
+    if (desc.len + apps > cap || compact) {
+      reloc = 1;
+      const long long want = static_cast<long long>(live) + apps;
+      long long extra = static_cast<long long>(ceil(static_cast<double>(want) * headroom));
+      if (extra < 4) extra = 4;
+      new_cap = static_cast<int>((want + extra + 3) & ~3LL);
+      const u64 at = atomicAdd(side == 0 ? &c->top_out : &c->top_in, static_cast<u64>(new_cap));
+      if (at + new_cap > static_cast<u64>(p.g.arena_cap) || at + new_cap > 0xffffffffULL) {
+        set_error(&c->error, kErrCapacity);
+      }
+      start = static_cast<unsigned>(at);
+    }
+    (side == 0 ? p.reloc_out : p.reloc_in)[s] = reloc;
+    (side == 0 ? p.new_start_out : p.new_start_in)[s] = start;
+    (side == 0 ? p.new_cap_out : p.new_cap_in)[s] = new_cap;
+    (side == 0 ? p.live_out : p.live_in)[s] = live;
+    if (reloc) atomicAdd(side == 0 ? &c->relocated_out : &c->relocated_in, 1);
+  }
+}
+
+__device__ __forceinline__ void column_out(const ApplyParams& p, int j, long long w,
+                                           long long old_max) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_sum_delta[j]),
+            static_cast<unsigned long long>(-w));
+  if (w == old_max) atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_removed_at_max[j]), 1ULL);
+  if (w < 1) atomicSub(&p.g.columns[j].bad, 1);
+}
+__device__ __forceinline__ void column_in(const ApplyParams& p, int j, long long w) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_sum_delta[j]),
+            static_cast<unsigned long long>(w));
+  atomicMax(&p.col_written_max[j], w);
+  if (w < 1) atomicAdd(&p.g.columns[j].bad, 1);
+}
+
+// ---- G: tombstones and upserts in place -------------------------------------------------------
+__global__ void k_mutate(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int pairs = c->pairs;
+  const bool del_first = p.props.deletions_first != 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    const u64 key = p.key[slot];
+    const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
+    const int d = p.d[slot];
+    const int t = p.t[slot];
+    const int cnt = p.out_count[slot];
+    const int flags = p.flags[slot];
+    const bool appended = (flags & kPairAppend) || (t >= 1 && (del_first ? cnt <= d : cnt == 0));
+    const int seq = cnt + (appended ? 1 : 0);
+    const int removed = del_first ? min(cnt, d) : min(seq, d);
+    const int tomb = min(removed, cnt);
+    const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
+    if (!tomb && !(flags & kPairUpsert)) continue;
+    const int target = del_first ? d : 0;  // the original match an upsert addresses
+    for (int side = 0; side < 2; ++side) {
+      const int32_t r = side == 0 ? u : v;
+      const int32_t want = side == 0 ? v : u;
+      const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
+      int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
+      int32_t* w = (side == 0 ? p.g.out_w : p.g.in_w) + desc.start;
+      if (cnt <= 1 && !p.g.allow_multi) {
+        const int pos = side == 0 ? p.out_pos[slot] : p.in_pos[slot];
+        if (tomb) {
+          col[pos] = kDead;
+          if (side == 0)
+            for (int j = 0; j < p.k; ++j)
+              column_out(p, j, w[j * p.g.arena_cap + pos], p.g.columns[j].max_w);
+        } else {
+          for (int j = 0; j < p.k; ++j) {
+            const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+            if (side == 0) {
+              column_out(p, j, w[j * p.g.arena_cap + pos], p.g.columns[j].max_w);
+              column_in(p, j, nw);
+            }
+            w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
+          }
+        }
+        continue;
+      }
+      // multi-edge graphs: walk the row in order
+      int seen = 0;
+      for (int e = 0; e < desc.len && seen < cnt; ++e) {
+        if (col[e] != want) continue;
+        if (seen < tomb) {
+          col[e] = kDead;
+          if (side == 0)
+            for (int j = 0; j < p.k; ++j)
+              column_out(p, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
+        } else if ((flags & kPairUpsert) && seen == target) {
+          for (int j = 0; j < p.k; ++j) {
+            const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+            if (side == 0) {
+              column_out(p, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
+              column_in(p, j, nw);
+            }
+            w[j * p.g.arena_cap + e] = static_cast<int32_t>(nw);
+          }
+        }
+        ++seen;
+      }
+    }
+  }
+}
+
+// ---- H: move relocated rows (live slots, in order) ---------------------------------------------
+__global__ void k_move(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int rows_out = c->rows_out, rows_in = c->rows_in;
+  for (int i = warp; i < rows_out + rows_in; i += warps) {
+    const int side = i < rows_out ? 0 : 1;
+    const int s = side == 0 ? i : i - rows_out;
+    if (!(side == 0 ? p.reloc_out : p.reloc_in)[s]) continue;
+    const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
+    if (r >= c->n_old) continue;
+    const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
+    const unsigned dst = (side == 0 ? p.new_start_out : p.new_start_in)[s];
+    int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
+    int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
+    int written = 0;
+    for (int base = 0; base < desc.len; base += 32) {
+      const int e = base + lane;
+      const int32_t x = e < desc.len ? col[desc.start + e] : kDead;
+      const bool live = x >= 0;
+      const unsigned ballot = __ballot_sync(0xffffffffu, live);
+      const int pos = written + __popc(ballot & ((1u << lane) - 1));
+      if (live) {
+        col[dst + pos] = x;
+        for (int j = 0; j < p.k; ++j)
+          w[j * p.g.arena_cap + dst + pos] = w[j * p.g.arena_cap + desc.start + e];
+      }
+      written += __popc(ballot);
+    }
+  }
+}
+
+// ---- I: append the new slots ---------------------------------------------------------------------
+__global__ void k_append(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int pairs = c->pairs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    const int flags = p.flags[slot];
+    if (!(flags & kPairAppend)) continue;
+    const u64 key = p.key[slot];
+    const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
+    const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
+    for (int side = 0; side < 2; ++side) {
+      const int32_t r = side == 0 ? u : v;
+      const int s = (side == 0 ? p.row_slot_out : p.row_slot_in)[r];
+      const int reloc = (side == 0 ? p.reloc_out : p.reloc_in)[s];
+      const RowDesc desc = r < c->n_old ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r] : RowDesc{0, 0};
+      const unsigned base = reloc ? (side == 0 ? p.new_start_out : p.new_start_in)[s] +
+                                        (side == 0 ? p.live_out : p.live_in)[s]
+                                  : desc.start + desc.len;
+      const unsigned pos = base + (side == 0 ? p.out_rank : p.in_rank)[slot];
+      (side == 0 ? p.g.out_col : p.g.in_col)[pos] = side == 0 ? v : u;
+      int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
+      for (int j = 0; j < p.k; ++j) {
+        const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+        w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
+        if (side == 0) column_in(p, j, nw);
+      }
+    }
+  }
+}
+
+// ---- J: new row descriptors ----------------------------------------------------------------------
+__global__ void k_rows_final(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int rows_out = c->rows_out, rows_in = c->rows_in;
+  long long garbage_out = 0, garbage_in = 0, dead_delta_out = 0, dead_delta_in = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows_out + rows_in;
+       i += gridDim.x * blockDim.x) {
+    const int side = i < rows_out ? 0 : 1;
+    const int s = side == 0 ? i : i - rows_out;
+    const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
+    const bool existing = r < c->n_old;
+    RowDesc* descs = side == 0 ? p.g.out_desc : p.g.in_desc;
+    const RowDesc desc = existing ? descs[r] : RowDesc{0, 0};
+    int* caps = side == 0 ? p.g.out_cap : p.g.in_cap;
+    int* deads = side == 0 ? p.g.out_dead : p.g.in_dead;
+    const int old_cap = existing ? caps[r] : 0;
+    const int old_dead = existing ? deads[r] : 0;
+    const int dels = (side == 0 ? p.dels_out : p.dels_in)[s];
+    const int apps = (side == 0 ? p.apps_out : p.apps_in)[s];
+    RowDesc nd;
+    if ((side == 0 ? p.reloc_out : p.reloc_in)[s]) {
+      nd.start = (side == 0 ? p.new_start_out : p.new_start_in)[s];
+      nd.len = (side == 0 ? p.live_out : p.live_in)[s] + apps;
+      caps[r] = (side == 0 ? p.new_cap_out : p.new_cap_in)[s];
+      deads[r] = 0;
+      (side == 0 ? garbage_out : garbage_in) += old_cap;
+      (side == 0 ? dead_delta_out : dead_delta_in) -= old_dead;
+    } else {
+      nd.start = desc.start;
+      nd.len = desc.len + apps;
+      deads[r] = old_dead + dels;
+      (side == 0 ? dead_delta_out : dead_delta_in) += dels;
+    }
+    descs[r] = nd;
+  }
+  GraphCounters* gc = p.g.counters;
+  if (garbage_out) atomicAdd(&gc->out_garbage, static_cast<u64>(garbage_out));
+  if (garbage_in) atomicAdd(&gc->in_garbage, static_cast<u64>(garbage_in));
+  if (dead_delta_out)
+    atomicAdd(reinterpret_cast<unsigned long long*>(&gc->dead_out),
+              static_cast<unsigned long long>(dead_delta_out));
+  if (dead_delta_in)
+    atomicAdd(reinterpret_cast<unsigned long long*>(&gc->dead_in),
+              static_cast<unsigned long long>(dead_delta_in));
+}
+
+// Count the weights written by the batch that equal the new maximum (for count_at_max).
+__global__ void k_count_written_max(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int pairs = c->pairs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    const int flags = p.flags[slot];
+    if (!(flags & (kPairAppend | kPairUpsert))) continue;
+    const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
+    for (int j = 0; j < p.k; ++j) {
+      const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+      const long long target = max(p.col_written_max[j], p.g.columns[j].max_w);
+      if (nw == target)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_written_at_max[j]), 1ULL);
+    }
+  }
+}
+
+// One thread: graph counters and column statistics after the batch.
+__global__ void k_finalize(ApplyParams p) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  GraphCounters* gc = p.g.counters;
+  gc->n = c->n_after;
+  gc->m += c->summary[0] - c->summary[1];
+  gc->out_top = c->top_out;
+  gc->in_top = c->top_in;
+  c->summary[6] = c->n_after - c->n_old;
+  c->summary[7] = c->n_after;
+  for (int j = 0; j < p.k; ++j) {
+    ColumnStats cs = p.g.columns[j];
+    cs.sum_w += p.col_sum_delta[j];
+    const long long wmax = p.col_written_max[j];
+    if (wmax > cs.max_w) {
+      cs.max_w = wmax;
+      cs.count_at_max = p.col_written_at_max[j];
+    } else {
+      cs.count_at_max += p.col_written_at_max[j] - p.col_removed_at_max[j];
+      if (cs.count_at_max <= 0) cs.dirty = 1;
+    }
+    if (gc->m == 0) {
+      cs.max_w = 1;
+      cs.count_at_max = 0;
+      cs.sum_w = 0;
+      cs.dirty = 0;
+    }
+    cs.bad = p.g.columns[j].bad;  // maintained by atomics during the mutation
+    p.g.columns[j] = cs;
+  }
+}
+
+// Column statistics by a full pass over the live slots (after a maximum edge was deleted).
+__global__ void k_rescan_columns(GraphView g, long long n, long long* out) {
+  // out: per objective [max, count, sum]
+  for (int j = 0; j < g.k; ++j) {
+    long long mx = 0, sum = 0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n;
+         v += (long long)gridDim.x * blockDim.x) {
+      const RowDesc desc = g.out_desc[v];
+      for (int e = 0; e < desc.len; ++e) {
+        if (g.out_col[desc.start + e] < 0) continue;
+        const long long w = g.out_w[j * g.arena_cap + desc.start + e];
+        mx = max(mx, w);
+        sum += w;
+      }
+    }
+    atomicMax(&out[3 * j], mx);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&out[3 * j + 2]),
+              static_cast<unsigned long long>(sum));
+  }
+}
+
+__global__ void k_rescan_count(GraphView g, long long n, long long* out) {
+  for (int j = 0; j < g.k; ++j) {
+    const long long mx = out[3 * j];
+    long long cnt = 0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n;
+         v += (long long)gridDim.x * blockDim.x) {
+      const RowDesc desc = g.out_desc[v];
+      for (int e = 0; e < desc.len; ++e) {
+        if (g.out_col[desc.start + e] < 0) continue;
+        cnt += g.out_w[j * g.arena_cap + desc.start + e] == mx;
+      }
+    }
+    atomicAdd(reinterpret_cast<unsigned long long*>(&out[3 * j + 1]),
+              static_cast<unsigned long long>(cnt));
+  }
+}
+
+// Append order (row_order::append): the new slots of a row follow the batch order of their first
+// insertion, as the reference appends them (apply_host.cpp:214-246).  The atomic ranks of
+// k_resolve are replaced by the rank among the row's appended pairs ordered by first insertion.
+__global__ void k_row_offsets(ApplyParams p, int* offsets) {
+  // one block: exclusive scan of apps_out over the touched out rows
+  __shared__ int s_carry;
+  __shared__ int s_part[1024];
+  const int rows = p.ctl->rows_out;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < rows; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < rows ? p.apps_out[i] : 0;
+    s_part[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      const int add = threadIdx.x >= o ? s_part[threadIdx.x - o] : 0;
+      __syncthreads();
+      s_part[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (i < rows) offsets[i] = s_carry + s_part[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry += s_part[1023];
+    __syncthreads();
+  }
+}
+
+__global__ void k_fill_segments(ApplyParams p, const int* offsets, int* seg) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int pairs = c->pairs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    if (!(p.flags[slot] & kPairAppend)) continue;
+    const int32_t u = static_cast<int32_t>(p.key[slot] >> 32);
+    seg[offsets[p.row_slot_out[u]] + p.out_rank[slot]] = slot;
+  }
+}
+
+__global__ void k_sort_segments(ApplyParams p, const int* offsets, int* seg) {
+  UpdateCtl* c = p.ctl;
+  if (c->error) return;
+  const int rows = c->rows_out;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < rows; s += gridDim.x * blockDim.x) {
+    const int a = p.apps_out[s];
+    if (a <= 0) continue;
+    int* base = seg + offsets[s];
+    for (int i = 1; i < a; ++i) {
+      const int x = base[i];
+      const int key = p.first[x];
+      int j = i - 1;
+      while (j >= 0 && p.first[base[j]] > key) {
+        base[j + 1] = base[j];
+        --j;
+      }
+      base[j + 1] = x;
+    }
+    for (int i = 0; i < a; ++i) p.out_rank[base[i]] = i;
+  }
+}
+
+// The classification per batch insertion (the weight-increase mask of apply_host.cpp:348-393):
+// insertion i reads the flags of its pair (u, v).
+__global__ void k_insert_flags(ApplyParams p, unsigned char* out) {
+  UpdateCtl* c = p.ctl;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < p.ni;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int32_t u = p.ins_src[i], v = p.ins_dst[i];
+    int slot = -1;
+    if (!c->error && u >= 0 && v >= 0) slot = find_pair(p, pair_key(u, v));
+    for (int j = 0; j < p.k; ++j)
+      out[i * p.k + j] = slot >= 0 ? p.inc[static_cast<long long>(slot) * p.k + j] : 0;
+  }
+}
+
+int grid_for(long long work, int block, int sm_count) {
+  long long g = (work + block - 1) / block;
+  const long long cap = static_cast<long long>(sm_count) * 8;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return static_cast<int>(g);
+}
+
+long long round4(long long x) { return (x + 3) & ~3LL; }
+
+long long slack_cap(long long len, double headroom) {
+  if (len <= 0) return 0;
+  long long extra = static_cast<long long>(std::ceil(static_cast<double>(len) * headroom));
+  if (extra < 4) extra = 4;
+  return round4(len + extra);
+}
+
+ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int objective,
+                        long long delta_opt) {
+  Workspace& ws = ctx.ws;
+  ApplyParams p{};
+  p.g = g.view();
+  p.ins_src = b.ins_src;
+  p.ins_dst = b.ins_dst;
+  p.ins_w = b.ins_w;
+  p.ni = b.ni;
+  p.del_src = b.del_src;
+  p.del_dst = b.del_dst;
+  p.nd = b.nd;
+  p.k = g.k;
+  p.objective = objective;
+  p.props = g.props;
+  p.delta_opt = delta_opt;
+  p.key = ws.pair_key.ptr;
+  p.mask = static_cast<int>(ws.pairs_sized - 1);
+  p.d = ws.pair_d.ptr;
+  p.t = ws.pair_t.ptr;
+  p.first = ws.pair_first.ptr;
+  p.last = ws.pair_last.ptr;
+  p.out_pos = ws.pair_out_pos.ptr;
+  p.in_pos = ws.pair_in_pos.ptr;
+  p.out_pos2 = ws.pair_out_pos2.ptr;
+  p.in_pos2 = ws.pair_in_pos2.ptr;
+  p.flags = ws.pair_flags.ptr;
+  p.out_rank = ws.pair_out_rank.ptr;
+  p.in_rank = ws.pair_in_rank.ptr;
+  p.out_count = ws.pair_out_row.ptr;
+  p.in_count = ws.pair_in_row.ptr;
+  p.list = ws.pair_list.ptr;
+  p.inc = ws.pair_inc.ptr;
+  p.touch_out_stamp = ws.touch_out_stamp.ptr;
+  p.touch_in_stamp = ws.touch_in_stamp.ptr;
+  p.row_slot_out = ws.row_slot_out.ptr;
+  p.row_slot_in = ws.row_slot_in.ptr;
+  p.rows_out = ws.rows_out.ptr;
+  p.rows_in = ws.rows_in.ptr;
+  p.dels_out = ws.row_dels_out.ptr;
+  p.dels_in = ws.row_dels_in.ptr;
+  p.apps_out = ws.row_apps_out.ptr;
+  p.apps_in = ws.row_apps_in.ptr;
+  p.reloc_out = ws.row_reloc_out.ptr;
+  p.reloc_in = ws.row_reloc_in.ptr;
+  p.new_start_out = ws.row_new_start_out.ptr;
+  p.new_start_in = ws.row_new_start_in.ptr;
+  p.new_cap_out = ws.row_new_cap_out.ptr;
+  p.new_cap_in = ws.row_new_cap_in.ptr;
+  p.live_out = ws.row_live_out.ptr;
+  p.live_in = ws.row_live_in.ptr;
+  p.chunks_out = ws.chunks_out.ptr;
+  p.chunks_in = ws.chunks_in.ptr;
+  p.chunk_cap = static_cast<long long>(ws.chunks_out.count);
+  p.col_sum_delta = ws.col_sum_delta.ptr;
+  p.col_removed_at_max = ws.col_removed_at_max.ptr;
+  p.col_written_max = ws.col_written_max.ptr;
+  p.col_written_at_max = ws.col_written_at_max.ptr;
+  p.ctl = ws.ctl.ptr;
+  return p;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// Workspace
+// ------------------------------------------------------------------------------------------------
+void Workspace::reserve_vertices(long long n_cap, cudaStream_t s) {
+  if (n_cap <= n_sized) return;
+  const size_t n = static_cast<size_t>(n_cap);
+  for (DevBuf<int>* b : {&touch_out_stamp, &touch_in_stamp, &stamp, &touch_stamp}) {
+    b->release();
+    b->reserve(n, s);
+    DYNGB200_CUDA(cudaMemsetAsync(b->ptr, 0, n * sizeof(int), s));
+  }
+  for (DevBuf<int>* b : {&flag, &in_far}) {
+    b->release();
+    b->reserve(n, s);
+    DYNGB200_CUDA(cudaMemsetAsync(b->ptr, 0, n * sizeof(int), s));
+  }
+  for (DevBuf<int>* b : {&row_slot_out, &row_slot_in, &ancestor, &candidates, &frontier, &near_a,
+                         &near_b, &far_a, &far_b, &touched}) {
+    b->release();
+    b->reserve(n, s);
+  }
+  for (DevBuf<int>* b : {&heavy_a, &heavy_b}) {  // int2 entries
+    b->release();
+    b->reserve(2 * n, s);
+  }
+  generation = 0;
+  touch_generation = 0;
+  n_sized = n_cap;
+}
+
+void Workspace::reserve_batch(long long ops, int k, cudaStream_t s) {
+  // pair table: a power of two, at least twice the number of directed operations
+  long long cap = 1024;
+  while (cap < 2 * ops) cap <<= 1;
+  if (cap > pairs_sized) {
+    const size_t c = static_cast<size_t>(cap);
+    pair_key.release();
+    pair_key.reserve(c, s);
+    for (DevBuf<int>* b : {&pair_d, &pair_t, &pair_first, &pair_last, &pair_out_pos, &pair_in_pos,
+                           &pair_out_pos2, &pair_in_pos2, &pair_flags, &pair_out_row,
+                           &pair_in_row, &pair_out_rank, &pair_in_rank, &pair_list}) {
+      b->release();
+      b->reserve(c, s);
+    }
+    for (DevBuf<int>* b : {&rows_out, &rows_in, &row_dels_out, &row_dels_in, &row_apps_out,
+                           &row_apps_in, &row_reloc_out, &row_reloc_in, &row_new_cap_out,
+                           &row_new_cap_in, &row_live_out, &row_live_in}) {
+      b->release();
+      b->reserve(c, s);
+    }
+    row_new_start_out.release();
+    row_new_start_out.reserve(c, s);
+    row_new_start_in.release();
+    row_new_start_in.reserve(c, s);
+    pairs_sized = cap;
+  }
+  const size_t inc = static_cast<size_t>(pairs_sized) * static_cast<size_t>(k > 0 ? k : 1);
+  pair_inc.reserve(inc, s);
+  for (DevBuf<long long>* b : {&col_ins_max, &col_sum_delta, &col_removed_at_max,
+                               &col_written_max, &col_written_at_max}) {
+    b->reserve(static_cast<size_t>(k > 0 ? k : 1), s);
+  }
+  ctl.reserve(1, s);
+  host_ctl.reserve(1);
+}
+
+int Workspace::next_generation(int count, cudaStream_t s) {
+  if (generation > INT32_MAX / 2) {
+    DYNGB200_CUDA(cudaMemsetAsync(stamp.ptr, 0, stamp.count * sizeof(int), s));
+    DYNGB200_CUDA(cudaMemsetAsync(touch_stamp.ptr, 0, touch_stamp.count * sizeof(int), s));
+    generation = 0;
+  }
+  const int g = generation + 1;
+  generation += count;
+  return g;
+}
+
+int Workspace::next_touch_generation(cudaStream_t s) {
+  if (touch_generation > INT32_MAX / 2) {
+    DYNGB200_CUDA(cudaMemsetAsync(touch_out_stamp.ptr, 0, touch_out_stamp.count * sizeof(int), s));
+    DYNGB200_CUDA(cudaMemsetAsync(touch_in_stamp.ptr, 0, touch_in_stamp.count * sizeof(int), s));
+    touch_generation = 0;
+  }
+  return ++touch_generation;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Build, export, growth
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+// Host layout of one side: row descriptors, caps, the arena (col + k weight columns).
+struct HostSide {
+  std::vector<RowDesc> desc;
+  std::vector<int32_t> cap, dead;
+  std::vector<int32_t> col;
+  std::vector<int32_t> w;  // k x arena
+  long long top = 0;
+};
+
+void layout_side(long long n, long long n_cap, int k, const int64_t* row_ptr, const int32_t* col,
+                 const int32_t* w, long long m, double headroom, long long arena_cap,
+                 HostSide& out) {
+  out.desc.assign(static_cast<size_t>(n_cap), RowDesc{0, 0});
+  out.cap.assign(static_cast<size_t>(n_cap), 0);
+  out.dead.assign(static_cast<size_t>(n_cap), 0);
+  long long top = 0;
+  for (long long v = 0; v < n; ++v) {
+    const long long len = row_ptr[v + 1] - row_ptr[v];
+    const long long cap = slack_cap(len, headroom);
+    out.desc[v] = RowDesc{static_cast<uint32_t>(top), static_cast<int32_t>(len)};
+    out.cap[v] = static_cast<int32_t>(cap);
+    top += cap;
+  }
+  out.top = top;
+  out.col.assign(static_cast<size_t>(top), kDead);
+  out.w.assign(static_cast<size_t>(top) * static_cast<size_t>(k), 0);
+  for (long long v = 0; v < n; ++v) {
+    const long long len = row_ptr[v + 1] - row_ptr[v];
+    const long long s = out.desc[v].start;
+    std::memcpy(&out.col[s], col + row_ptr[v], static_cast<size_t>(len) * sizeof(int32_t));
+    for (int j = 0; j < k; ++j)
+      std::memcpy(&out.w[static_cast<size_t>(j) * top + s], w + static_cast<size_t>(j) * m + row_ptr[v],
+                  static_cast<size_t>(len) * sizeof(int32_t));
+  }
+  (void)arena_cap;
+}
+
+long long needed_top(long long n, const int64_t* row_ptr, double headroom) {
+  long long top = 0;
+  for (long long v = 0; v < n; ++v) top += slack_cap(row_ptr[v + 1] - row_ptr[v], headroom);
+  return top;
+}
+
+void upload_side(Context& ctx, const HostSide& h, long long n_cap, long long arena_cap, int k,
+                 DevBuf<RowDesc>& desc, DevBuf<int32_t>& cap, DevBuf<int32_t>& dead,
+                 DevBuf<int32_t>& col, DevBuf<int32_t>& w) {
+  cudaStream_t s = ctx.stream;
+  desc.release();
+  cap.release();
+  dead.release();
+  col.release();
+  w.release();
+  desc.reserve(static_cast<size_t>(n_cap));
+  cap.reserve(static_cast<size_t>(n_cap));
+  dead.reserve(static_cast<size_t>(n_cap));
+  col.reserve(static_cast<size_t>(arena_cap));
+  w.reserve(static_cast<size_t>(arena_cap) * static_cast<size_t>(k > 0 ? k : 1));
+  DYNGB200_CUDA(cudaMemcpyAsync(desc.ptr, h.desc.data(), n_cap * sizeof(RowDesc),
+                                cudaMemcpyHostToDevice, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(cap.ptr, h.cap.data(), n_cap * sizeof(int32_t),
+                                cudaMemcpyHostToDevice, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(dead.ptr, h.dead.data(), n_cap * sizeof(int32_t),
+                                cudaMemcpyHostToDevice, s));
+  if (h.top > 0) {
+    DYNGB200_CUDA(cudaMemcpyAsync(col.ptr, h.col.data(), h.top * sizeof(int32_t),
+                                  cudaMemcpyHostToDevice, s));
+    for (int j = 0; j < k; ++j)
+      DYNGB200_CUDA(cudaMemcpyAsync(w.ptr + static_cast<size_t>(j) * arena_cap,
+                                    h.w.data() + static_cast<size_t>(j) * h.top,
+                                    h.top * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  }
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+}
+
+// Transposition with the reference's order: inside an in-row the sources appear in out-edge
+// order (apply_host.cpp:470-518).
+void transpose_host(long long n, long long m, int k, const int64_t* row_ptr, const int32_t* col,
+                    const int32_t* w, std::vector<int64_t>& irp, std::vector<int32_t>& icol,
+                    std::vector<int32_t>& iw) {
+  irp.assign(static_cast<size_t>(n) + 1, 0);
+  for (long long e = 0; e < m; ++e) irp[static_cast<size_t>(col[e]) + 1]++;
+  for (long long v = 0; v < n; ++v) irp[v + 1] += irp[v];
+  icol.resize(static_cast<size_t>(m));
+  iw.resize(static_cast<size_t>(m) * static_cast<size_t>(k));
+  std::vector<int64_t> cursor(irp.begin(), irp.end() - 1);
+  for (long long u = 0; u < n; ++u) {
+    for (int64_t e = row_ptr[u]; e < row_ptr[u + 1]; ++e) {
+      const int64_t pos = cursor[col[e]]++;
+      icol[pos] = static_cast<int32_t>(u);
+      for (int j = 0; j < k; ++j)
+        iw[static_cast<size_t>(j) * m + pos] = w[static_cast<size_t>(j) * m + e];
+    }
+  }
+}
+
+}  // namespace
+
+void graph_build(Context& ctx, Graph& g, long long n, const int64_t* row_ptr, const int32_t* col,
+                 const int32_t* w, long long m) {
+  const int k = g.k;
+  const double headroom = g.props.headroom;
+  std::vector<int64_t> irp;
+  std::vector<int32_t> icol, iw;
+  transpose_host(n, m, k, row_ptr, col, w, irp, icol, iw);
+  const long long n_cap = n + 1024 + n / 16;
+  const long long top_out = needed_top(n, row_ptr, headroom);
+  const long long top_in = needed_top(n, irp.data(), headroom);
+  long long arena = std::max(top_out, top_in);
+  arena = round4(arena + std::max(arena / 2, 1LL << 16));
+  expects(arena < 0xffffffffLL, "graph: the slack arena exceeds 2^32 slots", DYNGB200_CAPACITY);
+  HostSide out, in;
+  layout_side(n, n_cap, k, row_ptr, col, w, m, headroom, arena, out);
+  layout_side(n, n_cap, k, irp.data(), icol.data(), iw.data(), m, headroom, arena, in);
+  g.n = n;
+  g.m = m;
+  g.n_cap = n_cap;
+  g.arena_cap = arena;
+  upload_side(ctx, out, n_cap, arena, k, g.out_desc, g.out_cap, g.out_dead, g.out_col, g.out_w);
+  upload_side(ctx, in, n_cap, arena, k, g.in_desc, g.in_cap, g.in_dead, g.in_col, g.in_w);
+  GraphCounters gc{};
+  gc.n = n;
+  gc.m = m;
+  gc.out_top = static_cast<u64>(out.top);
+  gc.in_top = static_cast<u64>(in.top);
+  g.counters.reserve(1);
+  g.host_columns.assign(static_cast<size_t>(k > 0 ? k : 1), ColumnStats{1, 0, 0, 0, 0});
+  for (int j = 0; j < k; ++j) {
+    ColumnStats cs{1, 0, 0, 0, 0};
+    long long mx = 0;
+    for (long long e = 0; e < m; ++e) mx = std::max<long long>(mx, w[static_cast<size_t>(j) * m + e]);
+    long long cnt = 0, sum = 0;
+    for (long long e = 0; e < m; ++e) {
+      const long long x = w[static_cast<size_t>(j) * m + e];
+      sum += x;
+      cnt += x == mx;
+    }
+    int bad = 0;
+    for (long long e = 0; e < m; ++e) bad += w[static_cast<size_t>(j) * m + e] < 1;
+    cs.max_w = m > 0 ? std::max<long long>(mx, 1) : 1;
+    cs.count_at_max = m > 0 ? cnt : 0;
+    cs.sum_w = sum;
+    cs.bad = bad;
+    g.host_columns[j] = cs;
+  }
+  g.columns.reserve(g.host_columns.size());
+  DYNGB200_CUDA(cudaMemcpyAsync(g.counters.ptr, &gc, sizeof(gc), cudaMemcpyHostToDevice, ctx.stream));
+  DYNGB200_CUDA(cudaMemcpyAsync(g.columns.ptr, g.host_columns.data(),
+                                g.host_columns.size() * sizeof(ColumnStats),
+                                cudaMemcpyHostToDevice, ctx.stream));
+  DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+  g.host_counters = gc;
+}
+
+void graph_refresh_host(Context& ctx, Graph& g) {
+  DYNGB200_CUDA(cudaMemcpyAsync(&g.host_counters, g.counters.ptr, sizeof(GraphCounters),
+                                cudaMemcpyDeviceToHost, ctx.stream));
+  DYNGB200_CUDA(cudaMemcpyAsync(g.host_columns.data(), g.columns.ptr,
+                                g.host_columns.size() * sizeof(ColumnStats),
+                                cudaMemcpyDeviceToHost, ctx.stream));
+  DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+  g.n = g.host_counters.n;
+  g.m = g.host_counters.m;
+}
+
+namespace {
+
+// Download one side as raw slack rows.
+void download_side(Context& ctx, Graph& g, int side, long long n, std::vector<RowDesc>& desc,
+                   std::vector<int32_t>& col, std::vector<int32_t>& w, long long& top) {
+  cudaStream_t s = ctx.stream;
+  top = static_cast<long long>(side == 0 ? g.host_counters.out_top : g.host_counters.in_top);
+  desc.resize(static_cast<size_t>(n));
+  col.resize(static_cast<size_t>(top));
+  w.resize(static_cast<size_t>(top) * static_cast<size_t>(g.k));
+  DYNGB200_CUDA(cudaMemcpyAsync(desc.data(), (side == 0 ? g.out_desc : g.in_desc).ptr,
+                                n * sizeof(RowDesc), cudaMemcpyDeviceToHost, s));
+  if (top > 0) {
+    DYNGB200_CUDA(cudaMemcpyAsync(col.data(), (side == 0 ? g.out_col : g.in_col).ptr,
+                                  top * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    for (int j = 0; j < g.k; ++j)
+      DYNGB200_CUDA(cudaMemcpyAsync(w.data() + static_cast<size_t>(j) * top,
+                                    (side == 0 ? g.out_w : g.in_w).ptr +
+                                        static_cast<size_t>(j) * g.arena_cap,
+                                    top * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  }
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+}
+
+// Compact CSR of one side: live slots per row, stably sorted by neighbour when `sort`.
+void side_to_csr(long long n, int k, const std::vector<RowDesc>& desc,
+                 const std::vector<int32_t>& col, const std::vector<int32_t>& w, long long top,
+                 bool sort, std::vector<int64_t>& rp, std::vector<int32_t>& ocol,
+                 std::vector<int32_t>& ow) {
+  rp.assign(static_cast<size_t>(n) + 1, 0);
+  for (long long v = 0; v < n; ++v) {
+    long long live = 0;
+    for (int e = 0; e < desc[v].len; ++e) live += col[desc[v].start + e] >= 0;
+    rp[v + 1] = rp[v] + live;
+  }
+  const long long m = rp[n];
+  ocol.resize(static_cast<size_t>(m));
+  ow.resize(static_cast<size_t>(m) * static_cast<size_t>(k));
+  std::vector<long long> idx;
+  for (long long v = 0; v < n; ++v) {
+    idx.clear();
+    for (int e = 0; e < desc[v].len; ++e)
+      if (col[desc[v].start + e] >= 0) idx.push_back(desc[v].start + e);
+    if (sort)
+      std::stable_sort(idx.begin(), idx.end(),
+                       [&](long long a, long long b) { return col[a] < col[b]; });
+    long long out = rp[v];
+    for (long long e : idx) {
+      ocol[out] = col[e];
+      for (int j = 0; j < k; ++j)
+        ow[static_cast<size_t>(j) * m + out] = w[static_cast<size_t>(j) * top + e];
+      ++out;
+    }
+  }
+}
+
+}  // namespace
+
+void graph_export(Context& ctx, Graph& g, int64_t* row_ptr, int32_t* col, int32_t* w,
+                  int64_t* in_row_ptr, int32_t* in_col, int32_t* in_w) {
+  graph_refresh_host(ctx, g);
+  const long long n = g.n;
+  for (int side = 0; side < 2; ++side) {
+    int64_t* rp_dst = side == 0 ? row_ptr : in_row_ptr;
+    int32_t* col_dst = side == 0 ? col : in_col;
+    int32_t* w_dst = side == 0 ? w : in_w;
+    if (!rp_dst && !col_dst && !w_dst) continue;
+    std::vector<RowDesc> desc;
+    std::vector<int32_t> c, ww;
+    long long top = 0;
+    download_side(ctx, g, side, n, desc, c, ww, top);
+    std::vector<int64_t> rp;
+    std::vector<int32_t> oc, ow;
+    // out rows: sorted by neighbour under row_order::sorted; in rows: always by source
+    side_to_csr(n, g.k, desc, c, ww, top, side == 1 || g.props.sorted, rp, oc, ow);
+    if (rp_dst) std::memcpy(rp_dst, rp.data(), rp.size() * sizeof(int64_t));
+    if (col_dst) std::memcpy(col_dst, oc.data(), oc.size() * sizeof(int32_t));
+    if (w_dst) std::memcpy(w_dst, ow.data(), ow.size() * sizeof(int32_t));
+  }
+}
+
+// Grow the vertex capacity and/or the arenas.  Heavily fragmented arenas are compacted instead
+// (a rebuild through the host layout).
+void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, long long need_in) {
+  graph_refresh_host(ctx, g);
+  const long long n = g.n;
+  const long long m = g.m;
+  const long long garbage = static_cast<long long>(
+      std::max(g.host_counters.out_garbage, g.host_counters.in_garbage));
+  const bool compact = garbage > m / 2 + 1024 || need_out > g.arena_cap || need_in > g.arena_cap;
+  if (compact) {
+    // rebuild from the exported CSR (append order is storage order, so it is kept)
+    std::vector<int64_t> rp(static_cast<size_t>(n) + 1);
+    std::vector<int32_t> col(static_cast<size_t>(m)), w(static_cast<size_t>(m) * g.k);
+    // export in storage order: temporarily pretend append order
+    const int sorted = g.props.sorted;
+    g.props.sorted = 0;
+    graph_export(ctx, g, rp.data(), col.data(), w.data(), nullptr, nullptr, nullptr);
+    g.props.sorted = sorted;
+    // keep the in-mirror's relative order: rebuild it by transposition (stable per source)
+    const long long keep_n = std::max(n, need_n);
+    std::vector<int64_t> rp2(static_cast<size_t>(keep_n) + 1, rp[n]);
+    std::copy(rp.begin(), rp.end(), rp2.begin());
+    graph_build(ctx, g, keep_n, rp2.data(), col.data(), w.data(), m);
+    g.n = n;
+    GraphCounters gc = g.host_counters;
+    gc.n = n;
+    DYNGB200_CUDA(cudaMemcpyAsync(g.counters.ptr, &gc, sizeof(gc), cudaMemcpyHostToDevice,
+                                  ctx.stream));
+    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+    g.host_counters = gc;
+    if (need_n > g.n_cap) {
+      // graph_build sized n_cap from keep_n already
+    }
+    return;
+  }
+  if (need_n > g.n_cap) {
+    const long long new_cap = std::max(need_n + 1024, g.n_cap * 2);
+    for (DevBuf<RowDesc>* d : {&g.out_desc, &g.in_desc}) {
+      DevBuf<RowDesc> fresh;
+      fresh.reserve(static_cast<size_t>(new_cap));
+      DYNGB200_CUDA(cudaMemsetAsync(fresh.ptr, 0, new_cap * sizeof(RowDesc), ctx.stream));
+      DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, g.n_cap * sizeof(RowDesc),
+                                    cudaMemcpyDeviceToDevice, ctx.stream));
+      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+      std::swap(d->ptr, fresh.ptr);
+      std::swap(d->count, fresh.count);
+    }
+    for (DevBuf<int32_t>* d : {&g.out_cap, &g.in_cap, &g.out_dead, &g.in_dead}) {
+      DevBuf<int32_t> fresh;
+      fresh.reserve(static_cast<size_t>(new_cap));
+      DYNGB200_CUDA(cudaMemsetAsync(fresh.ptr, 0, new_cap * sizeof(int32_t), ctx.stream));
+      DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, g.n_cap * sizeof(int32_t),
+                                    cudaMemcpyDeviceToDevice, ctx.stream));
+      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+      std::swap(d->ptr, fresh.ptr);
+      std::swap(d->count, fresh.count);
+    }
+    g.n_cap = new_cap;
+  }
+}
+
+void graph_rescan_columns(Context& ctx, Graph& g) {
+  DevBuf<long long> out;
+  const size_t k = static_cast<size_t>(g.k > 0 ? g.k : 1);
+  out.reserve(3 * k);
+  DYNGB200_CUDA(cudaMemsetAsync(out.ptr, 0, 3 * k * sizeof(long long), ctx.stream));
+  const int grid = grid_for(g.n, kBlock, ctx.sm_count);
+  k_rescan_columns<<<grid, kBlock, 0, ctx.stream>>>(g.view(), g.n, out.ptr);
+  k_rescan_count<<<grid, kBlock, 0, ctx.stream>>>(g.view(), g.n, out.ptr);
+  std::vector<long long> h(3 * k);
+  DYNGB200_CUDA(cudaMemcpyAsync(h.data(), out.ptr, 3 * k * sizeof(long long),
+                                cudaMemcpyDeviceToHost, ctx.stream));
+  DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+  for (int j = 0; j < g.k; ++j) {
+    ColumnStats cs{std::max<long long>(h[3 * j], 1), h[3 * j + 1], h[3 * j + 2], 0,
+                   g.host_columns[j].bad};
+    if (h[3 * j] == 0) cs.count_at_max = 0;
+    g.host_columns[j] = cs;
+  }
+  DYNGB200_CUDA(cudaMemcpyAsync(g.columns.ptr, g.host_columns.data(),
+                                g.host_columns.size() * sizeof(ColumnStats),
+                                cudaMemcpyHostToDevice, ctx.stream));
+  DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// ------------------------------------------------------------------------------------------------
+// The applier (queued on ctx.stream; the caller reads the control block once at the end)
+// ------------------------------------------------------------------------------------------------
+StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k) {
+  StagedBatch b{};
+  b.ni = batch.num_insertions;
+  b.nd = batch.num_deletions;
+  if (batch.memory == DYNGB200_DEVICE) {
+    b.ins_src = batch.insert_src;
+    b.ins_dst = batch.insert_dst;
+    b.ins_w = batch.insert_weights;
+    b.del_src = batch.delete_src;
+    b.del_dst = batch.delete_dst;
+    return b;
+  }
+  Workspace& ws = ctx.ws;
+  cudaStream_t s = ctx.stream;
+  const size_t ni = static_cast<size_t>(b.ni), nd = static_cast<size_t>(b.nd);
+  ws.b_ins_src.reserve(ni + 1);
+  ws.b_ins_dst.reserve(ni + 1);
+  ws.b_ins_w.reserve(ni * static_cast<size_t>(k > 0 ? k : 1) + 1);
+  ws.b_del_src.reserve(nd + 1);
+  ws.b_del_dst.reserve(nd + 1);
+  if (ni) {
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.b_ins_src.ptr, batch.insert_src, ni * 4, cudaMemcpyHostToDevice, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.b_ins_dst.ptr, batch.insert_dst, ni * 4, cudaMemcpyHostToDevice, s));
+    if (k > 0)
+      DYNGB200_CUDA(cudaMemcpyAsync(ws.b_ins_w.ptr, batch.insert_weights, ni * k * 4,
+                                    cudaMemcpyHostToDevice, s));
+  }
+  if (nd) {
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.b_del_src.ptr, batch.delete_src, nd * 4, cudaMemcpyHostToDevice, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.b_del_dst.ptr, batch.delete_dst, nd * 4, cudaMemcpyHostToDevice, s));
+  }
+  b.ins_src = ws.b_ins_src.ptr;
+  b.ins_dst = ws.b_ins_dst.ptr;
+  b.ins_w = ws.b_ins_w.ptr;
+  b.del_src = ws.b_del_src.ptr;
+  b.del_dst = ws.b_del_dst.ptr;
+  return b;
+}
+
+// Steps A-E (nothing in the graph changes): checks, plan, grouping, matching, resolution.
+void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
+                   long long delta_opt) {
+  Workspace& ws = ctx.ws;
+  cudaStream_t s = ctx.stream;
+  const long long dir = g.props.directed ? 1 : 2;
+  const long long ops = (b.ni + b.nd) * dir;
+  ws.reserve_vertices(g.n_cap, s);
+  ws.reserve_batch(ops, g.k, s);
+  // chunk lists: every touched row's slots in kChunk pieces (bounded by arena / kChunk + rows)
+  const long long chunk_cap = std::min<long long>(
+      2 * ops + g.arena_cap / kChunk + 64, 2 * ws.pairs_sized + g.arena_cap / kChunk + 64);
+  ws.chunks_out.reserve(static_cast<size_t>(chunk_cap));
+  ws.chunks_in.reserve(static_cast<size_t>(chunk_cap));
+  const int touch_gen = ws.next_touch_generation(s);
+  const size_t cap = static_cast<size_t>(ws.pairs_sized);
+  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_key.ptr, 0xff, cap * sizeof(u64), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_d.ptr, 0, cap * sizeof(int), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_t.ptr, 0, cap * sizeof(int), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_first.ptr, 0x7f, cap * sizeof(int), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_last.ptr, 0xff, cap * sizeof(int), s));
+  const size_t kk = static_cast<size_t>(g.k > 0 ? g.k : 1);
+  DYNGB200_CUDA(cudaMemsetAsync(ws.col_sum_delta.ptr, 0, kk * sizeof(long long), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.col_removed_at_max.ptr, 0, kk * sizeof(long long), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.col_written_max.ptr, 0, kk * sizeof(long long), s));
+  DYNGB200_CUDA(cudaMemsetAsync(ws.col_written_at_max.ptr, 0, kk * sizeof(long long), s));
+  UpdateCtl init{};
+  init.err_index = INT64_MAX;
+  init.n_old = g.n;
+  init.n_after = g.n;
+  init.batch_ins_max = 1;
+  init.minimum = kPackedInf;
+  *ws.host_ctl.ptr = init;
+  DYNGB200_CUDA(cudaMemcpyAsync(ws.ctl.ptr, ws.host_ctl.ptr, sizeof(UpdateCtl),
+                                cudaMemcpyHostToDevice, s));
+  ApplyParams p = make_params(ctx, g, b, objective, delta_opt);
+  p.touch_gen = touch_gen;
+  p.chunk_cap = chunk_cap;
+  const int grid_ops = grid_for(b.ni + b.nd, kBlock, ctx.sm_count);
+  k_validate<<<grid_ops, kBlock, 0, s>>>(p);
+  k_plan<<<1, 1, 0, s>>>(p);
+  k_pairs<<<grid_ops, kBlock, 0, s>>>(p);
+  const int grid_wide = ctx.sm_count * 4;
+  if (g.props.allow_multi) {
+    k_scan_multi<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
+  } else {
+    k_scan<<<grid_wide, kBlock, 0, s>>>(p);
+  }
+  k_resolve<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
+  if (!g.props.sorted) {
+    ws.row_seg_offsets.reserve(cap);
+    ws.row_seg.reserve(cap);
+    k_row_offsets<<<1, 1024, 0, s>>>(p, ws.row_seg_offsets.ptr);
+    k_fill_segments<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, ws.row_seg_offsets.ptr,
+                                                                           ws.row_seg.ptr);
+    k_sort_segments<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, ws.row_seg_offsets.ptr,
+                                                                           ws.row_seg.ptr);
+  }
+  DYNGB200_CUDA(cudaGetLastError());
+}
+
+// Steps F-J: allocation (the last point where a capacity error leaves the graph untouched), then
+// the mutation of the slack rows and the counters.
+void apply_commit(Context& ctx, Graph& g, const StagedBatch& b) {
+  cudaStream_t s = ctx.stream;
+  const long long dir = g.props.directed ? 1 : 2;
+  const long long ops = (b.ni + b.nd) * dir;
+  ApplyParams p = make_params(ctx, g, b, -1, 0);
+  p.chunk_cap = static_cast<long long>(ctx.ws.chunks_out.count);
+  const int grid = grid_for(2 * ops, kBlock, ctx.sm_count);
+  k_alloc<<<grid, kBlock, 0, s>>>(p);
+  k_mutate<<<grid, kBlock, 0, s>>>(p);
+  k_move<<<ctx.sm_count * 4, kBlock, 0, s>>>(p);
+  k_append<<<grid, kBlock, 0, s>>>(p);
+  k_rows_final<<<grid, kBlock, 0, s>>>(p);
+  k_count_written_max<<<grid, kBlock, 0, s>>>(p);
+  k_finalize<<<1, 1, 0, s>>>(p);
+  DYNGB200_CUDA(cudaGetLastError());
+}
+
+// graph::apply on its own (no tree): the applier, one read-back, growth and retry on capacity.
+void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
+                 dyngb200_apply_summary* summary, unsigned char* weight_increased) {
+  Workspace& ws = ctx.ws;
+  cudaStream_t s = ctx.stream;
+  const StagedBatch b = stage_batch(ctx, batch, g.k);
+  UpdateCtl r{};
+  DevBuf<unsigned char> flags;
+  for (int attempt = 0;; ++attempt) {
+    apply_prepare(ctx, g, b, -1, 0);
+    apply_commit(ctx, g, b);
+    if (weight_increased && b.ni > 0) {
+      flags.reserve(static_cast<size_t>(b.ni) * g.k);
+      ApplyParams p = make_params(ctx, g, b, -1, 0);
+      k_insert_flags<<<grid_for(b.ni, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, flags.ptr);
+      DYNGB200_CUDA(cudaGetLastError());
+      DYNGB200_CUDA(cudaMemcpyAsync(weight_increased, flags.ptr, static_cast<size_t>(b.ni) * g.k,
+                                    cudaMemcpyDeviceToHost, s));
+    }
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(&g.host_counters, g.counters.ptr, sizeof(GraphCounters),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(g.host_columns.data(), g.columns.ptr,
+                                  g.host_columns.size() * sizeof(ColumnStats),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    r = *ws.host_ctl.ptr;
+    if ((r.error & kErrCapacity) && attempt < 4) {
+      graph_grow(ctx, g, r.n_after > g.n_cap ? r.n_after : 0, static_cast<long long>(r.top_out),
+                 static_cast<long long>(r.top_in));
+      continue;
+    }
+    break;
+  }
+  if (r.error & kErrCapacity) throw Error(DYNGB200_CAPACITY, "graph::apply: capacity exceeded");
+  if (r.error & kErrInvalidBatch) {
+    std::string msg = "graph::apply: invalid batch";
+    if (r.err_index != INT64_MAX) msg += " (operation " + std::to_string(r.err_index) + ")";
+    throw Error(DYNGB200_INVALID_ARGUMENT, msg);
+  }
+  if (r.error) throw Error(DYNGB200_INTERNAL, "graph::apply: internal error");
+  g.version += 1;
+  g.n = g.host_counters.n;
+  g.m = g.host_counters.m;
+  if (summary) std::memcpy(summary, r.summary, sizeof(*summary));
+}
+
+}  // namespace dyngb200

@@ -1,0 +1,271 @@
+// Host-side objects of the dyng_b200 library: the execution context (resources::cuda()), the
+// device-resident slack-row graph and the shortest-path tree.  Not part of the public ABI.
+#pragma once
+
+#include "common.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dyngb200.h"
+
+namespace dyngb200 {
+
+// A library error carrying the C-ABI status it maps to.
+struct Error : std::runtime_error {
+  dyngb200_status status;
+  Error(dyngb200_status s, const std::string& msg) : std::runtime_error(msg), status(s) {}
+};
+
+#define DYNGB200_CUDA(call)                                                                     \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) {                                                                    \
+      if (e_ == cudaErrorMemoryAllocation) {                                                    \
+        cudaGetLastError();                                                                     \
+        throw ::dyngb200::Error(DYNGB200_OUT_OF_MEMORY,                                         \
+                                std::string("CUDA out of memory at ") + #call);                 \
+      }                                                                                         \
+      throw ::dyngb200::Error(DYNGB200_CUDA_ERROR, std::string(cudaGetErrorString(e_)) + " at " \
+                                                       + #call);                               \
+    }                                                                                           \
+  } while (0)
+
+inline void expects(bool ok, const std::string& msg,
+                    dyngb200_status s = DYNGB200_INVALID_ARGUMENT) {
+  if (!ok) throw Error(s, msg);
+}
+
+// A device buffer that grows on demand (contents are not preserved unless asked).
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  // Ensure room for n elements; keeps the first `keep` elements when it reallocates.
+  void reserve(size_t n, cudaStream_t stream = 0, size_t keep = 0) {
+    if (n <= count) return;
+    T* fresh = nullptr;
+    DYNGB200_CUDA(cudaMalloc(&fresh, (n ? n : 1) * sizeof(T)));
+    if (ptr && keep) {
+      DYNGB200_CUDA(cudaMemcpyAsync(fresh, ptr, keep * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+      DYNGB200_CUDA(cudaStreamSynchronize(stream));
+    }
+    if (ptr) cudaFree(ptr);
+    ptr = fresh;
+    count = n;
+  }
+};
+
+// Pinned host buffer.
+template <typename T>
+struct HostBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  ~HostBuf() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+  void reserve(size_t n) {
+    if (n <= count) return;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    DYNGB200_CUDA(cudaMallocHost(&ptr, (n ? n : 1) * sizeof(T)));
+    count = n;
+  }
+};
+
+// The control block of one update, written by the kernels and read back once at the end.
+struct UpdateCtl {
+  unsigned error;
+  int pad0;
+  long long err_index;
+  // Step 0 / applier
+  long long n_old, n_after;
+  long long batch_ins_max;  // largest insertion weight of the objective (at least 1)
+  long long max_w;          // max(column max before the batch, batch_ins_max)
+  long long delta;
+  int pairs;
+  int rows_out, rows_in;
+  int chunks_out, chunks_in;
+  int relocated_out, relocated_in;
+  int pad1;
+  u64 top_out, top_in;  // tentative arena tops
+  long long summary[8];  // apply_summary fields in dyngb200_apply_summary order
+  // sssp
+  int packing_bits;
+  int repacked;
+  u64 max_distance;
+  int list_count, frontier_count, near_count, next_count, far_count, far2_count;
+  int heavy_count, next_heavy_count;
+  int touched_count;
+  int active[3];
+  int rounds;
+  int iterations, epochs;
+  long long pushes;
+  long long invalidated;
+  long long affected;
+  u64 minimum;
+  int changed;         // the batch holds a deleted or weight-increased edge
+  int last_generation; // last stamp generation the kernel used
+  u64 heavy_counter[2];  // (slots << 40 | chunks) of the current and next heavy frontier lists
+  // grid barrier
+  unsigned bar_count;
+  unsigned bar_gen;
+};
+
+// Scratch memory of a context, sized on demand and reused (the reference's workspace pool).
+struct Workspace {
+  // applier
+  DevBuf<u64> pair_key;
+  DevBuf<int> pair_d, pair_t, pair_first, pair_last, pair_out_pos, pair_in_pos, pair_out_pos2,
+      pair_in_pos2, pair_flags, pair_out_row, pair_in_row, pair_out_rank, pair_in_rank, pair_list;
+  DevBuf<unsigned char> pair_inc;  // pairs x k weight-increase flags
+  DevBuf<int> touch_out_stamp, touch_in_stamp, row_slot_out, row_slot_in;
+  DevBuf<int> rows_out, rows_in;  // touched row ids
+  DevBuf<int> row_dels_out, row_dels_in, row_apps_out, row_apps_in, row_reloc_out, row_reloc_in;
+  DevBuf<unsigned> row_new_start_out, row_new_start_in;
+  DevBuf<int> row_new_cap_out, row_new_cap_in, row_live_out, row_live_in;
+  DevBuf<int2> chunks_out, chunks_in;
+  DevBuf<int> row_seg_offsets, row_seg;  // append order: appended pairs per row
+  DevBuf<long long> col_ins_max, col_sum_delta, col_removed_at_max, col_written_max,
+      col_written_at_max;
+  // batch staging
+  DevBuf<int32_t> b_ins_src, b_ins_dst, b_ins_w, b_del_src, b_del_dst;
+  // sssp
+  DevBuf<int> stamp, touch_stamp, flag, in_far, ancestor;
+  DevBuf<int> candidates, frontier, near_a, near_b, far_a, far_b, heavy_a, heavy_b, touched;
+  DevBuf<UpdateCtl> ctl;
+  HostBuf<UpdateCtl> host_ctl;
+  int generation = 0;     // stamp generations (sssp)
+  int touch_generation = 0;  // row-touch generations (applier)
+  long long n_sized = 0;
+  long long pairs_sized = 0;
+
+  void reserve_vertices(long long n_cap, cudaStream_t s);
+  void reserve_batch(long long ops, int k, cudaStream_t s);
+  int next_generation(int count, cudaStream_t s);  // reserves `count` sssp generations
+  int next_touch_generation(cudaStream_t s);
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 0;
+  int coop_supported = 0;
+  int update_blocks_per_sm = 0;
+  int compute_blocks_per_sm = 0;
+  Workspace ws;
+  // the learned scheduler's hook: when set, the next update runs with this schedule
+  dyngb200_schedule schedule{};
+  int schedule_set = 0;
+};
+
+struct Graph {
+  uint64_t id = 0;
+  uint64_t version = 0;
+  dyngb200_props props{};
+  int k = 1;
+  long long n = 0, m = 0;  // host mirrors after the last completed call
+  long long n_cap = 0, arena_cap = 0;
+  DevBuf<RowDesc> out_desc, in_desc;
+  DevBuf<int32_t> out_cap, in_cap, out_dead, in_dead;
+  DevBuf<int32_t> out_col, in_col;
+  DevBuf<int32_t> out_w, in_w;
+  DevBuf<GraphCounters> counters;
+  DevBuf<ColumnStats> columns;
+  GraphCounters host_counters{};
+  std::vector<ColumnStats> host_columns;
+  int device = 0;
+
+  GraphView view() {
+    GraphView v{};
+    v.out_desc = out_desc.ptr;
+    v.out_cap = out_cap.ptr;
+    v.out_dead = out_dead.ptr;
+    v.out_col = out_col.ptr;
+    v.out_w = out_w.ptr;
+    v.in_desc = in_desc.ptr;
+    v.in_cap = in_cap.ptr;
+    v.in_dead = in_dead.ptr;
+    v.in_col = in_col.ptr;
+    v.in_w = in_w.ptr;
+    v.arena_cap = arena_cap;
+    v.n_cap = n_cap;
+    v.k = k;
+    v.sorted = props.sorted;
+    v.allow_multi = props.allow_multi;
+    v.counters = counters.ptr;
+    v.columns = columns.ptr;
+    return v;
+  }
+};
+
+struct Tree {
+  uint64_t graph_id = 0;
+  uint64_t version = 0;
+  int32_t source = 0;
+  dyngb200_options opt{};
+  long long n = 0, cap = 0;
+  DevBuf<int64_t> dist;
+  DevBuf<int32_t> parent;
+  DevBuf<u64> packed;
+  int packed_bits = -1;  // format of `packed` (-1: not valid, repack before use)
+  bool trusted = true;   // built by compute() or validated: no parent cycle possible
+  bool poisoned = false;
+  int device = 0;
+};
+
+// graph.cu
+void graph_build(Context& ctx, Graph& g, long long n, const int64_t* row_ptr, const int32_t* col,
+                 const int32_t* w_objective_major, long long m);
+void graph_export(Context& ctx, Graph& g, int64_t* row_ptr, int32_t* col, int32_t* w,
+                  int64_t* in_row_ptr, int32_t* in_col, int32_t* in_w);
+void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_arena_out,
+                long long need_arena_in);
+void graph_rescan_columns(Context& ctx, Graph& g);
+void graph_refresh_host(Context& ctx, Graph& g);
+
+// Launches the batch applier (Step 0 checks, grouping, matching, resolution, allocation and the
+// mutation of the slack rows).  `objective` >= 0 also records the sssp change classification for
+// that weight column; tree arrays are not touched.  Work is queued on ctx.stream.
+struct StagedBatch {
+  const int32_t* ins_src;
+  const int32_t* ins_dst;
+  const int32_t* ins_w;
+  long long ni;
+  const int32_t* del_src;
+  const int32_t* del_dst;
+  long long nd;
+};
+void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
+                   long long delta_opt);
+void apply_commit(Context& ctx, Graph& g, const StagedBatch& b);
+StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k);
+
+// sssp.cu
+void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st);
+void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
+                 const dyngb200_schedule& sched, dyngb200_stats* st);
+void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
+                 dyngb200_apply_summary* summary, unsigned char* weight_increased);
+void tree_reserve(Context& ctx, Tree& t, long long n_cap);
+void tree_repack(Context& ctx, Tree& t, int bits);
+void tree_canonicalize(Context& ctx, Graph& g, Tree& t);
+
+}  // namespace dyngb200

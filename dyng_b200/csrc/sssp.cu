@@ -1,0 +1,867 @@
+// The sssp kernels: one persistent cooperative kernel per compute() / update() that runs subtree
+// invalidation, the pull pass, the near-far push loop and the commit, with every loop decision
+// taken on the device (the schedule of the reference's fused engine,
+// cpp/src/algorithms/sssp/fused.cuh:155-495), on the slack rows of the device graph.
+//
+// What differs from the reference's kernel (the results do not):
+//   - the packed (distance << b | parent) words persist between updates in the tree, so an update
+//     does not pack and unpack all n vertices: only the vertices whose word changed (the
+//     `touched` list) are unpacked and compared for `affected`;
+//   - frontier rows longer than `heavy_degree` are split into 1024-slot chunks spread over all
+//     warps (one 64-bit atomic reserves a list slot and its chunk range together), shorter rows
+//     of 32+ slots are scanned by a whole warp, the rest by one lane each;
+//   - the grid barrier is this file's own, with a time limit after which it records kErrTimeout
+//     and every block leaves the kernel (no unbounded spin).
+#include "internal.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace dyngb200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kHeavyChunk = 1024;
+constexpr unsigned long long kBarrierTimeoutNs = 5ULL * 1000 * 1000 * 1000;
+
+struct SsspParams {
+  GraphView g;
+  int objective;
+  int32_t source;
+  int from_scratch;
+  long long* dist;
+  int32_t* parent;
+  u64* packed;
+  int tree_bits;         // format of the persistent words (-1: none); another format is rebuilt
+  long long tree_n;      // vertices the tree held before this call (growth fills the rest)
+  // pairs of the applier (update only)
+  const u64* pair_key;
+  const int* pair_list;
+  const int* pair_flags;
+  // scratch
+  int* stamp;
+  int* touch_stamp;
+  int* flag;
+  int* in_far;
+  int* ancestor;
+  int* candidates;
+  int* frontier;
+  int* near_a;
+  int* near_b;
+  int* far_a;
+  int* far_b;
+  int2* heavy_a;
+  int2* heavy_b;
+  int* touched;
+  int generation;
+  int touch_gen;
+  int heavy_degree;
+  long long delta_override;
+  UpdateCtl* ctl;
+  u64* heavy_counter;  // ctl->heavy_counter: (slots << 40 | chunks), current and next lists
+};
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
+  return *reinterpret_cast<const volatile unsigned*>(p);
+}
+
+// Grid-wide barrier over co-resident blocks (cooperative launch).  Returns false once any block
+// has recorded a timeout; the caller then leaves the kernel.
+__device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    const unsigned target = gen + 1;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&c->bar_count, 1u) + 1u;
+    int ok = 1;
+    if (arrived == gridDim.x) {
+      atomicExch(&c->bar_count, 0u);
+      __threadfence();
+      atomicExch(&c->bar_gen, target);
+    } else {
+      unsigned long long start = 0;
+      unsigned spins = 0;
+      while (ld_volatile(&c->bar_gen) != target) {
+        __nanosleep(64);
+        if ((++spins & 255u) == 0) {
+          if (ld_volatile(&c->error) & kErrTimeout) {
+            ok = 0;
+            break;
+          }
+          const unsigned long long now = global_ns();
+          if (start == 0) {
+            start = now;
+          } else if (now - start > kBarrierTimeoutNs) {
+            atomicOr(&c->error, kErrTimeout);
+            ok = 0;
+            break;
+          }
+        }
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  ++gen;
+  return s_ok != 0;
+}
+
+__device__ __forceinline__ bool claim(int* stamp, int v, int generation) {
+  return atomicExch(&stamp[v], generation) != generation;
+}
+
+__device__ __forceinline__ void touch(const SsspParams& p, int v) {
+  if (atomicExch(&p.touch_stamp[v], p.touch_gen) != p.touch_gen) {
+    p.touched[append_slot(&p.ctl->touched_count)] = v;
+  }
+}
+
+__device__ __forceinline__ void warp_min_into(u64 v, u64* target) {
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v != kPackedInf) atomicMin(target, v);
+}
+
+template <typename T>
+__device__ __forceinline__ void warp_sum_into(T v, T* target) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(target, v);
+}
+
+__device__ __forceinline__ void warp_sum_into_ll(long long v, long long* target) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0)
+    atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(v));
+}
+
+// Put v on the next near frontier: the light list, or the heavy list with its chunk range.
+__device__ __forceinline__ void push_near(const SsspParams& p, int v, int* light, int* light_count,
+                                          int2* heavy, u64* heavy_counter) {
+  const int len = p.g.out_desc[v].len;
+  if (len > p.heavy_degree) {
+    const u64 chunks = static_cast<u64>((len + kHeavyChunk - 1) / kHeavyChunk);
+    const u64 prev = atomicAdd(heavy_counter, (1ULL << 40) | chunks);
+    const int slot = static_cast<int>(prev >> 40);
+    heavy[slot] = make_int2(v, static_cast<int>(prev & ((1ULL << 40) - 1)));
+  } else {
+    light[append_slot(light_count)] = v;
+  }
+}
+
+struct Loop {
+  u64 threshold;
+  int gen;
+};
+
+// One relaxation of edge (u, x) of weight w from distance du.
+__device__ __forceinline__ void relax_edge(const SsspParams& p, const Packing& pk, u64 maxd,
+                                           int u, u64 du, int x, int w, const Loop& L,
+                                           int* next_light, int2* next_heavy, int* far) {
+  if (x < 0 || x == p.source) return;
+  const u64 nd = du + static_cast<u64>(w);
+  if (nd > maxd) return;
+  const u64 cand = pk.pack(nd, u);
+  if (cand >= ld_cg(&p.packed[x])) return;
+  const u64 old = atomicMin(&p.packed[x], cand);
+  if (cand < old) touch(p, x);
+  if (nd < pk.dist(old)) {
+    if (nd < L.threshold) {
+      if (claim(p.stamp, x, L.gen))
+        push_near(p, x, next_light, &p.ctl->next_count, next_heavy, &p.heavy_counter[1]);
+    } else if (atomicExch(&p.in_far[x], 1) == 0) {
+      far[append_slot(&p.ctl->far_count)] = x;
+    }
+  }
+}
+
+// Scan slots [e0, e1) of a row with the 32 lanes of a warp: lane l takes the 4-slot groups
+// l, l + 32, ... with one 16-byte load of columns and one of weights (rows start on 4-slot
+// boundaries and own at least round_up(len, 4) slots, so a group never leaves its row).
+__device__ __forceinline__ void warp_row(const SsspParams& p, const Packing& pk, u64 maxd, int u,
+                                         u64 du, unsigned start, int e0, int e1, const Loop& L,
+                                         int* next_light, int2* next_heavy, int* far) {
+  const int lane = threadIdx.x & 31;
+  const int32_t* col = p.g.out_col + start;
+  const int32_t* wt = p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap + start;
+  const int g0 = e0 >> 2;
+  const int g1 = (e1 + 3) >> 2;
+  for (int grp = g0 + lane; grp < g1; grp += 32) {
+    const int e = grp << 2;
+    const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + e));
+    const int4 w4 = __ldg(reinterpret_cast<const int4*>(wt + e));
+    if (e + 0 < e1) relax_edge(p, pk, maxd, u, du, c4.x, w4.x, L, next_light, next_heavy, far);
+    if (e + 1 < e1) relax_edge(p, pk, maxd, u, du, c4.y, w4.y, L, next_light, next_heavy, far);
+    if (e + 2 < e1) relax_edge(p, pk, maxd, u, du, c4.z, w4.z, L, next_light, next_heavy, far);
+    if (e + 3 < e1) relax_edge(p, pk, maxd, u, du, c4.w, w4.w, L, next_light, next_heavy, far);
+  }
+}
+
+__device__ __forceinline__ int find_heavy(const int2* list, int count, long long chunk) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (static_cast<long long>(__ldcg(&list[mid].y)) <= chunk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
+  UpdateCtl* c = p.ctl;
+  if (ld_volatile(&c->error) != 0) return;
+  unsigned bar = 0;
+  const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long threads = static_cast<long long>(gridDim.x) * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const long long gwarp = tid >> 5;
+  const long long nwarps = threads >> 5;
+  const long long n = c->n_after;
+  Packing pk;
+  pk.bits = c->packing_bits;
+  pk.no_parent = pk.bits ? (1ULL << pk.bits) - 1 : 0;
+  const u64 maxd = c->max_distance;
+  const u64 delta = static_cast<u64>(p.delta_override > 0 ? p.delta_override : c->delta);
+  int gen = p.generation;
+  int frontier_count = 0;
+
+  if (p.from_scratch) {
+    for (long long v = tid; v < n; v += threads)
+      p.packed[v] = v == p.source ? pk.pack(0, -1) : kPackedInf;
+    if (tid == 0) p.frontier[0] = p.source;
+    frontier_count = 1;
+    if (!grid_barrier(c, bar)) return;
+  } else {
+    // ---- the persistent words in this update's format; growth -------------------------------
+    if (p.tree_bits != pk.bits) {
+      for (long long v = tid; v < n; v += threads) {
+        if (v >= p.tree_n) {
+          p.dist[v] = kInfinity;
+          p.parent[v] = -1;
+        }
+        const long long d = p.dist[v];
+        u64 word = kPackedInf;
+        if (d < kInfinity / 2) {
+          if (d < 0 || static_cast<u64>(d) > maxd) atomicOr(&c->error, kErrOverflow);
+          else word = pk.pack(static_cast<u64>(d), p.parent[v]);
+        }
+        p.packed[v] = word;
+      }
+    } else {
+      for (long long v = p.tree_n + tid; v < n; v += threads) {
+        p.dist[v] = kInfinity;
+        p.parent[v] = -1;
+        p.packed[v] = kPackedInf;
+      }
+    }
+    // ---- roots: heads v of changed edges (u,v) with parent[v] == u ---------------------------
+    const int pairs = c->pairs;
+    int changed = 0;
+    for (long long i = tid; i < pairs; i += threads) {
+      const int slot = p.pair_list[i];
+      const int f = p.pair_flags[slot];
+      if (f & 3) {  // deleted or weight increased in the objective
+        changed = 1;
+        const u64 key = p.pair_key[slot];
+        const int32_t u = static_cast<int32_t>(key >> 32);
+        const int32_t v = static_cast<int32_t>(key & 0xffffffffu);
+        if (v < p.tree_n && p.parent[v] == u) p.flag[v] = 1;
+      }
+    }
+    if (__any_sync(0xffffffffu, changed) && lane == 0) c->changed = 1;
+    for (long long v = tid; v < n; v += threads) p.ancestor[v] = p.parent[v];
+    if (!grid_barrier(c, bar)) return;
+    if (ld_volatile(&c->error)) return;
+    const bool any_changed = ld_cg(&c->changed) != 0;
+    // ---- subtree invalidation by pointer jumping (fused.cuh:199-234) --------------------------
+    int max_rounds = 0;
+    while ((1LL << max_rounds) < n) ++max_rounds;
+    ++max_rounds;
+    if (any_changed) {
+      for (int round = 0; round < max_rounds; ++round) {
+        if (tid == 0) {
+          c->active[(round + 1) % 3] = 0;
+          c->rounds = round + 1;
+        }
+        int jumping = 0;
+        for (long long v = tid; v < n; v += threads) {
+          const int a = ld_cg(&p.ancestor[v]);
+          if (a < 0 || ld_cg(&p.flag[v])) continue;
+          if (ld_cg(&p.flag[a])) {
+            p.flag[v] = 1;
+            continue;
+          }
+          const int next = ld_cg(&p.ancestor[a]);
+          p.ancestor[v] = next;
+          jumping |= next >= 0 ? 1 : 0;
+        }
+        if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
+        if (!grid_barrier(c, bar)) return;
+        if (ld_cg(&c->active[round % 3]) == 0) break;
+      }
+    }
+    // ---- invalidate; candidates = invalidated + insertion heads -------------------------------
+    ++gen;
+    long long invalidated = 0;
+    for (long long v = tid; v < n; v += threads) {
+      if (ld_cg(&p.flag[v])) {
+        p.flag[v] = 0;
+        p.packed[v] = kPackedInf;
+        p.stamp[v] = gen;
+        touch(p, static_cast<int>(v));
+        p.candidates[append_slot(&c->list_count)] = static_cast<int>(v);
+        ++invalidated;
+      }
+    }
+    warp_sum_into_ll(invalidated, &c->invalidated);
+    if (!grid_barrier(c, bar)) return;
+    for (long long i = tid; i < pairs; i += threads) {
+      const int slot = p.pair_list[i];
+      if (!(p.pair_flags[slot] & 4)) continue;
+      const int32_t v = static_cast<int32_t>(p.pair_key[slot] & 0xffffffffu);
+      if (v != p.source && claim(p.stamp, v, gen))
+        p.candidates[append_slot(&c->list_count)] = v;
+    }
+    if (!grid_barrier(c, bar)) return;
+    // ---- pull pass (fused.cuh:258-285) over the in-rows ------------------------------------
+    ++gen;
+    const int candidate_count = ld_cg(&c->list_count);
+    const int32_t* in_w = p.g.in_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+    for (long long i = tid; i < candidate_count; i += threads) {
+      const int v = ld_cg(&p.candidates[i]);
+      const u64 current = ld_cg(&p.packed[v]);
+      u64 best = current;
+      const RowDesc desc = p.g.in_desc[v];
+      for (int e = 0; e < desc.len; ++e) {
+        const int u = p.g.in_col[desc.start + e];
+        if (u < 0) continue;
+        const u64 word = ld_cg(&p.packed[u]);
+        if (word == kPackedInf) continue;
+        const u64 nd = pk.dist(word) + static_cast<u64>(in_w[desc.start + e]);
+        if (nd <= maxd) best = min(best, pk.pack(nd, u));
+      }
+      if (best < current) {
+        const u64 old = atomicMin(&p.packed[v], best);
+        if (best < old) touch(p, v);
+        if (pk.dist(best) < pk.dist(old) && claim(p.stamp, v, gen))
+          p.frontier[append_slot(&c->frontier_count)] = v;
+      }
+    }
+    if (!grid_barrier(c, bar)) return;
+    frontier_count = ld_cg(&c->frontier_count);
+  }
+
+  // ---- near-far propagation (fused.cuh:288-417) ------------------------------------------------
+  u64 local = kPackedInf;
+  for (long long i = tid; i < frontier_count; i += threads) {
+    const u64 word = ld_cg(&p.packed[ld_cg(&p.frontier[i])]);
+    if (word != kPackedInf) local = min(local, pk.dist(word));
+  }
+  warp_min_into(local, &c->minimum);
+  if (!grid_barrier(c, bar)) return;
+  const u64 smallest = ld_cg(reinterpret_cast<const u64*>(&c->minimum));
+  Loop L;
+  L.threshold = (smallest == kPackedInf ? 0 : smallest) + delta;
+  int* cur = p.near_a;
+  int* nxt = p.near_b;
+  int2* cur_h = p.heavy_a;
+  int2* nxt_h = p.heavy_b;
+  int* far = p.far_a;
+  int* far2 = p.far_b;
+  ++gen;
+  L.gen = gen;
+  for (long long i = tid; i < frontier_count; i += threads) {
+    const int v = ld_cg(&p.frontier[i]);
+    const u64 word = ld_cg(&p.packed[v]);
+    const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
+    if (d < L.threshold) {
+      if (claim(p.stamp, v, gen)) push_near(p, v, cur, &c->near_count, cur_h, &p.heavy_counter[0]);
+    } else if (atomicExch(&p.in_far[v], 1) == 0) {
+      far[append_slot(&c->far_count)] = v;
+    }
+  }
+  if (!grid_barrier(c, bar)) return;
+  if (tid == 0) c->minimum = kPackedInf;
+  if (!grid_barrier(c, bar)) return;
+  int iterations = 0, epochs = 0;
+  long long pushes = 0;
+  const long long iteration_cap = 4 * n + 64;
+  while (true) {
+    const int near_count = ld_cg(&c->near_count);
+    const u64 hc = ld_cg(&p.heavy_counter[0]);
+    const int heavy_count = static_cast<int>(hc >> 40);
+    const long long heavy_chunks = static_cast<long long>(hc & ((1ULL << 40) - 1));
+    if (near_count > 0 || heavy_count > 0) {
+      ++gen;
+      ++iterations;
+      if (iterations > iteration_cap) {
+        if (tid == 0) atomicOr(&c->error, kErrNotConverged);
+        break;
+      }
+      L.gen = gen;
+      pushes += near_count + heavy_count;
+      // light rows: 32 frontier entries per warp
+      for (long long base = gwarp * 32; base < near_count; base += nwarps * 32) {
+        const long long i = base + lane;
+        int u = -1;
+        u64 du = 0;
+        RowDesc desc{0, 0};
+        if (i < near_count) {
+          u = ld_cg(&cur[i]);
+          const u64 word = ld_cg(&p.packed[u]);
+          if (word != kPackedInf) {
+            du = pk.dist(word);
+            desc = p.g.out_desc[u];
+          }
+        }
+        unsigned big = __ballot_sync(0xffffffffu, desc.len >= 32);
+        while (big) {
+          const int leader = __ffs(big) - 1;
+          big &= big - 1;
+          const int U = __shfl_sync(0xffffffffu, u, leader);
+          const u64 DU = __shfl_sync(0xffffffffu, du, leader);
+          const unsigned S = __shfl_sync(0xffffffffu, desc.start, leader);
+          const int LEN = __shfl_sync(0xffffffffu, desc.len, leader);
+          warp_row(p, pk, maxd, U, DU, S, 0, LEN, L, nxt, nxt_h, far);
+        }
+        if (desc.len > 0 && desc.len < 32) {
+          const int32_t* col = p.g.out_col + desc.start;
+          const int32_t* wt =
+              p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap + desc.start;
+          for (int e = 0; e < desc.len; ++e)
+            relax_edge(p, pk, maxd, u, du, col[e], wt[e], L, nxt, nxt_h, far);
+        }
+      }
+      // heavy rows: 1024-slot chunks spread over all warps
+      for (long long ch = gwarp; ch < heavy_chunks; ch += nwarps) {
+        const int h = find_heavy(cur_h, heavy_count, ch);
+        const int2 entry = make_int2(__ldcg(&cur_h[h].x), __ldcg(&cur_h[h].y));
+        const int u = entry.x;
+        const u64 word = ld_cg(&p.packed[u]);
+        if (word == kPackedInf) continue;
+        const RowDesc desc = p.g.out_desc[u];
+        const int e0 = static_cast<int>(ch - entry.y) * kHeavyChunk;
+        const int e1 = min(desc.len, e0 + kHeavyChunk);
+        warp_row(p, pk, maxd, u, pk.dist(word), desc.start, e0, e1, L, nxt, nxt_h, far);
+      }
+      if (!grid_barrier(c, bar)) return;
+      if (tid == 0) {
+        c->near_count = ld_cg(&c->next_count);
+        c->next_count = 0;
+        p.heavy_counter[0] = ld_cg(&p.heavy_counter[1]);
+        p.heavy_counter[1] = 0;
+      }
+      if (!grid_barrier(c, bar)) return;
+      int* t = cur;
+      cur = nxt;
+      nxt = t;
+      int2* th = cur_h;
+      cur_h = nxt_h;
+      nxt_h = th;
+      continue;
+    }
+    // near frontier empty: raise the threshold past the far pile
+    const int far_count = ld_cg(&c->far_count);
+    if (far_count == 0) break;
+    ++epochs;
+    local = kPackedInf;
+    for (long long i = tid; i < far_count; i += threads) {
+      const u64 word = ld_cg(&p.packed[ld_cg(&far[i])]);
+      if (word != kPackedInf) local = min(local, pk.dist(word));
+    }
+    warp_min_into(local, &c->minimum);
+    if (!grid_barrier(c, bar)) return;
+    L.threshold = max(L.threshold, ld_cg(reinterpret_cast<const u64*>(&c->minimum))) + delta;
+    ++gen;
+    for (long long i = tid; i < far_count; i += threads) {
+      const int v = ld_cg(&far[i]);
+      const u64 word = ld_cg(&p.packed[v]);
+      const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
+      if (d < L.threshold) {
+        p.in_far[v] = 0;
+        if (claim(p.stamp, v, gen))
+          push_near(p, v, cur, &c->near_count, cur_h, &p.heavy_counter[0]);
+      } else {
+        far2[append_slot(&c->far2_count)] = v;
+      }
+    }
+    if (!grid_barrier(c, bar)) return;
+    if (tid == 0) {
+      c->far_count = ld_cg(&c->far2_count);
+      c->far2_count = 0;
+      c->minimum = kPackedInf;
+    }
+    if (!grid_barrier(c, bar)) return;
+    int* t = far;
+    far = far2;
+    far2 = t;
+  }
+
+  // ---- commit: unpack (fused.cuh:419-494) ------------------------------------------------------
+  long long affected = 0;
+  if (pk.bits > 0) {
+    if (p.from_scratch) {
+      for (long long v = tid; v < n; v += threads) {
+        const u64 word = ld_cg(&p.packed[v]);
+        p.dist[v] = word == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word));
+        p.parent[v] = word == kPackedInf ? -1 : pk.parent(word);
+      }
+    } else {
+      const int touched = ld_cg(&c->touched_count);
+      for (long long i = tid; i < touched; i += threads) {
+        const int v = ld_cg(&p.touched[i]);
+        const u64 word = ld_cg(&p.packed[v]);
+        const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word));
+        const int32_t par = word == kPackedInf ? -1 : pk.parent(word);
+        if (p.dist[v] != d || p.parent[v] != par) {
+          p.dist[v] = d;
+          p.parent[v] = par;
+          ++affected;
+        }
+      }
+    }
+  } else {
+    // distance-only words: recover the lowest-id tight parent of every vertex
+    for (long long v = tid; v < n; v += threads) {
+      const u64 word = ld_cg(&p.packed[v]);
+      const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(word);
+      if (!p.from_scratch) {
+        p.ancestor[v] = p.parent[v];
+        p.candidates[v] = d != p.dist[v] ? 1 : 0;
+      }
+      p.dist[v] = d;
+      p.parent[v] = (word == kPackedInf || v == p.source) ? -1 : INT32_MAX;
+    }
+    if (!grid_barrier(c, bar)) return;
+    const int32_t* wcol = p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+    for (long long u = tid; u < n; u += threads) {
+      const u64 du = ld_cg(&p.packed[u]);
+      if (du == kPackedInf) continue;
+      const RowDesc desc = p.g.out_desc[u];
+      for (int e = 0; e < desc.len; ++e) {
+        const int x = p.g.out_col[desc.start + e];
+        if (x < 0 || x == p.source) continue;
+        if (du + static_cast<u64>(wcol[desc.start + e]) == ld_cg(&p.packed[x]))
+          atomicMin(&p.parent[x], static_cast<int32_t>(u));
+      }
+    }
+    if (!grid_barrier(c, bar)) return;
+    if (!p.from_scratch) {
+      for (long long v = tid; v < n; v += threads)
+        affected += (ld_cg(&p.candidates[v]) != 0 || ld_cg(&p.ancestor[v]) != ld_cg(&p.parent[v]));
+    }
+  }
+  warp_sum_into_ll(affected, &c->affected);
+  if (tid == 0) {
+    c->iterations = iterations;
+    c->epochs = epochs;
+    c->pushes = pushes;
+    c->last_generation = gen;
+  }
+}
+
+// Canonicalise an imported tree (sssp.cpp:377-396): for every edge (u,v) with
+// dist[u] + w == dist[v] and u < parent[v], parent[v] becomes u.  Lowest id wins via atomicMin.
+__global__ void k_canonicalize(GraphView g, int objective, int32_t source, long long n,
+                               const long long* dist, int32_t* parent) {
+  const int32_t* wcol = g.out_w + static_cast<long long>(objective) * g.arena_cap;
+  for (long long u = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; u < n;
+       u += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long du = dist[u];
+    if (du >= kInfinity / 2) continue;
+    const RowDesc desc = g.out_desc[u];
+    for (int e = 0; e < desc.len; ++e) {
+      const int v = g.out_col[desc.start + e];
+      if (v < 0 || v == source) continue;
+      if (du + wcol[desc.start + e] == dist[v]) atomicMin(&parent[v], static_cast<int32_t>(u));
+    }
+  }
+}
+
+__global__ void k_pack(long long n, int bits, const long long* dist, const int32_t* parent,
+                       u64* packed) {
+  Packing pk;
+  pk.bits = bits;
+  pk.no_parent = bits ? (1ULL << bits) - 1 : 0;
+  for (long long v = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; v < n;
+       v += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long d = dist[v];
+    packed[v] = d >= kInfinity / 2 ? kPackedInf : pk.pack(static_cast<u64>(d), parent[v]);
+  }
+}
+
+}  // namespace
+
+// Blocks of the persistent kernel (co-resident: cooperative launch).
+static int persistent_blocks(Context& ctx, const dyngb200_schedule& sched) {
+  if (ctx.update_blocks_per_sm == 0) {
+    int per_sm = 0;
+    DYNGB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sssp, kThreads, 0));
+    expects(per_sm >= 1, "sssp: the persistent kernel does not fit on an SM", DYNGB200_NOT_SUPPORTED);
+    ctx.update_blocks_per_sm = per_sm;
+  }
+  const int max_blocks = ctx.update_blocks_per_sm * ctx.sm_count;
+  int blocks = sched.grid_blocks > 0 ? sched.grid_blocks : max_blocks;
+  if (blocks > max_blocks) blocks = max_blocks;
+  if (blocks < 1) blocks = 1;
+  return blocks;
+}
+
+
+static void launch(Context& ctx, SsspParams& p, int blocks) {
+  expects(ctx.coop_supported != 0, "sssp: the fused engine needs cooperative launch",
+          DYNGB200_NOT_SUPPORTED);
+  void* args[] = {&p};
+  DYNGB200_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_sssp), dim3(blocks),
+                                            dim3(kThreads), args, 0, ctx.stream));
+}
+
+static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
+  Workspace& ws = ctx.ws;
+  SsspParams p{};
+  p.g = g.view();
+  p.objective = t.opt.objective;
+  p.source = t.source;
+  p.dist = reinterpret_cast<long long*>(t.dist.ptr);
+  p.parent = t.parent.ptr;
+  p.packed = t.packed.ptr;
+  p.stamp = ws.stamp.ptr;
+  p.touch_stamp = ws.touch_stamp.ptr;
+  p.flag = ws.flag.ptr;
+  p.in_far = ws.in_far.ptr;
+  p.ancestor = ws.ancestor.ptr;
+  p.candidates = ws.candidates.ptr;
+  p.frontier = ws.frontier.ptr;
+  p.near_a = ws.near_a.ptr;
+  p.near_b = ws.near_b.ptr;
+  p.far_a = ws.far_a.ptr;
+  p.far_b = ws.far_b.ptr;
+  p.heavy_a = reinterpret_cast<int2*>(ws.heavy_a.ptr);
+  p.heavy_b = reinterpret_cast<int2*>(ws.heavy_b.ptr);
+  p.touched = ws.touched.ptr;
+  p.ctl = ws.ctl.ptr;
+  p.heavy_counter = ws.ctl.ptr->heavy_counter;
+  return p;
+}
+
+// compute(): the persistent kernel from the source (fused.cuh:167-176).
+void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
+  Workspace& ws = ctx.ws;
+  cudaStream_t s = ctx.stream;
+  ws.reserve_vertices(g.n_cap, s);
+  ws.reserve_batch(0, g.k, s);
+  // heavy lists hold int2 entries: sized 2 x n_cap ints each by reserve_vertices
+  const long long n = g.n;
+  if (g.host_columns[t.opt.objective].dirty) graph_rescan_columns(ctx, g);
+  const ColumnStats cs = g.host_columns[t.opt.objective];
+  expects(cs.bad == 0, "sssp::compute: an edge has a weight below 1 in objective " +
+                           std::to_string(t.opt.objective) + "; sssp needs weights in [1, 2^31 - 1]");
+  expects(distances_fit(n, cs.max_w), "sssp::compute: distances do not fit in 62 bits");
+  UpdateCtl init{};
+  init.err_index = INT64_MAX;
+  init.n_old = n;
+  init.n_after = n;
+  init.max_w = cs.max_w;
+  init.delta = t.opt.delta > 0 ? t.opt.delta
+                               : default_delta(g.m > 1 ? g.m : 1, n, cs.sum_w);
+  u64 bound = 0;
+  const Packing pk = choose_packing(n, cs.max_w, &bound);
+  init.packing_bits = pk.bits;
+  init.max_distance = bound;
+  init.minimum = kPackedInf;
+  *ws.host_ctl.ptr = init;
+  DYNGB200_CUDA(cudaMemcpyAsync(ws.ctl.ptr, ws.host_ctl.ptr, sizeof(UpdateCtl),
+                                cudaMemcpyHostToDevice, s));
+  tree_reserve(ctx, t, g.n_cap);
+  SsspParams p = base_params(ctx, g, t);
+  p.from_scratch = 1;
+  p.tree_bits = pk.bits;
+  p.tree_n = n;
+  p.generation = ws.next_generation(1, s);
+  p.touch_gen = 1;
+  p.heavy_degree = ctx.schedule_set && ctx.schedule.heavy_degree > 0 ? ctx.schedule.heavy_degree
+                                                                      : 2048;
+  p.delta_override = 0;
+  const dyngb200_schedule sched = ctx.schedule_set ? ctx.schedule : dyngb200_schedule{};
+  const int blocks = persistent_blocks(ctx, sched);
+  cudaEvent_t e0, e1;
+  DYNGB200_CUDA(cudaEventCreate(&e0));
+  DYNGB200_CUDA(cudaEventCreate(&e1));
+  DYNGB200_CUDA(cudaEventRecord(e0, s));
+  if (n > 0) launch(ctx, p, blocks);
+  DYNGB200_CUDA(cudaEventRecord(e1, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
+                                cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const UpdateCtl& r = *ws.host_ctl.ptr;
+  if (r.error & kErrTimeout) throw Error(DYNGB200_INTERNAL, "sssp: a grid barrier timed out");
+  if (r.error & kErrNotConverged)
+    throw Error(DYNGB200_INTERNAL, "sssp: the near-far loop did not converge");
+  ws.generation = std::max(ws.generation, r.last_generation);
+  t.packed_bits = pk.bits;
+  t.n = n;
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->iterations = r.iterations;
+    st->epochs = r.epochs;
+    st->pushes = r.pushes;
+    st->packed_parents = pk.bits > 0;
+    st->engine_used = DYNGB200_ENGINE_FUSED;
+    st->delta = init.delta;
+    st->max_weight = cs.max_w;
+    st->grid_blocks = blocks;
+    st->sssp_ms = ms;
+  }
+}
+
+// update(): the applier, then the persistent kernel, then one read-back of the control block.
+void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
+                 const dyngb200_schedule& sched, dyngb200_stats* st) {
+  Workspace& ws = ctx.ws;
+  cudaStream_t s = ctx.stream;
+  const int objective = t.opt.objective;
+  if (g.host_columns[objective].dirty) graph_rescan_columns(ctx, g);
+  const StagedBatch b = stage_batch(ctx, batch, g.k);
+  const int blocks = persistent_blocks(ctx, sched);
+  cudaEvent_t e0, e1, e2;
+  DYNGB200_CUDA(cudaEventCreate(&e0));
+  DYNGB200_CUDA(cudaEventCreate(&e1));
+  DYNGB200_CUDA(cudaEventCreate(&e2));
+  UpdateCtl r{};
+  for (int attempt = 0;; ++attempt) {
+    tree_reserve(ctx, t, g.n_cap);
+    DYNGB200_CUDA(cudaEventRecord(e0, s));
+    apply_prepare(ctx, g, b, objective, t.opt.delta);
+    apply_commit(ctx, g, b);
+    DYNGB200_CUDA(cudaEventRecord(e1, s));
+    SsspParams p = base_params(ctx, g, t);
+    p.from_scratch = 0;
+    p.tree_n = t.n;
+    p.tree_bits = t.packed_bits;
+    p.pair_key = ws.pair_key.ptr;
+    p.pair_list = ws.pair_list.ptr;
+    p.pair_flags = ws.pair_flags.ptr;
+    p.generation = ws.next_generation(1, s);
+    p.touch_gen = p.generation;
+    p.heavy_degree = sched.heavy_degree > 0 ? sched.heavy_degree : 2048;
+    p.delta_override = sched.delta;
+    launch(ctx, p, blocks);
+    DYNGB200_CUDA(cudaEventRecord(e2, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(&g.host_counters, g.counters.ptr, sizeof(GraphCounters),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(g.host_columns.data(), g.columns.ptr,
+                                  g.host_columns.size() * sizeof(ColumnStats),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    r = *ws.host_ctl.ptr;
+    ws.generation = std::max(ws.generation, r.last_generation);
+    if ((r.error & kErrCapacity) && attempt < 4) {
+      // nothing was changed: grow the vertex capacity or the arenas and run again
+      const long long need_n = std::max<long long>(r.n_after, g.n_cap);
+      graph_grow(ctx, g, r.n_after > g.n_cap ? r.n_after : 0,
+                 static_cast<long long>(r.top_out), static_cast<long long>(r.top_in));
+      (void)need_n;
+      continue;
+    }
+    break;
+  }
+  float apply_ms = 0, sssp_ms = 0;
+  cudaEventElapsedTime(&apply_ms, e0, e1);
+  cudaEventElapsedTime(&sssp_ms, e1, e2);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  if (r.error & (kErrInvalidBatch | kErrCapacity)) {
+    // found before the commit: the graph and the tree are unchanged
+    std::string msg = "sssp::update: invalid batch";
+    if (r.err_index == -2) msg = "sssp::update: distances do not fit in 62 bits";
+    else if (r.err_index != INT64_MAX) msg += " (operation " + std::to_string(r.err_index) + ")";
+    if (r.error & kErrCapacity) throw Error(DYNGB200_CAPACITY, "sssp::update: capacity exceeded");
+    throw Error(DYNGB200_INVALID_ARGUMENT, msg);
+  }
+  // the batch is committed from here on
+  g.version += 1;
+  g.n = g.host_counters.n;
+  g.m = g.host_counters.m;
+  t.version = g.version;
+  if (r.error & kErrInternal) {
+    t.poisoned = true;
+    throw Error(DYNGB200_INTERNAL, "sssp::update: the in-edge mirror disagrees with the rows");
+  }
+  if (r.error & kErrOverflow) {
+    t.poisoned = true;
+    throw Error(DYNGB200_INVALID_ARGUMENT,
+                "sssp::update: an input distance is negative or larger than (n - 1) * max "
+                "weight; the initial tree does not belong to this graph");
+  }
+  int max_rounds = 0;
+  while ((1LL << max_rounds) < r.n_after) ++max_rounds;
+  ++max_rounds;
+  if (r.rounds == max_rounds && r.rounds > 0 && r.active[(r.rounds - 1) % 3] != 0) {
+    t.poisoned = true;
+    throw Error(DYNGB200_INVALID_ARGUMENT,
+                "sssp: the input shortest-path tree has a parent cycle (pointer jumping did not "
+                "reach a root in ceil(log2 n) + 1 rounds)");
+  }
+  if (r.error & (kErrTimeout | kErrNotConverged)) {
+    t.poisoned = true;
+    throw Error(DYNGB200_INTERNAL, (r.error & kErrTimeout)
+                                       ? "sssp::update: a grid barrier timed out"
+                                       : "sssp::update: the near-far loop did not converge");
+  }
+  t.n = r.n_after;
+  t.packed_bits = r.packing_bits;
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    std::memcpy(&st->batch, r.summary, sizeof(st->batch));
+    st->invalidated = r.invalidated;
+    st->affected = r.affected;
+    st->iterations = r.iterations;
+    st->epochs = r.epochs;
+    st->pushes = r.pushes;
+    st->packed_parents = r.packing_bits > 0;
+    st->engine_used = DYNGB200_ENGINE_FUSED;
+    st->delta = sched.delta > 0 ? sched.delta : r.delta;
+    st->max_weight = r.max_w;
+    st->grid_blocks = blocks;
+    st->invalidation = 0;
+    st->apply_ms = apply_ms;
+    st->sssp_ms = sssp_ms;
+    st->rounds = r.rounds;
+    st->touched = r.touched_count;
+  }
+}
+
+// Tree arrays sized for the graph's vertex capacity (contents kept).
+void tree_reserve(Context& ctx, Tree& t, long long n_cap) {
+  if (t.cap >= n_cap) return;
+  const size_t keep = static_cast<size_t>(t.n);
+  t.dist.reserve(static_cast<size_t>(n_cap), ctx.stream, keep);
+  t.parent.reserve(static_cast<size_t>(n_cap), ctx.stream, keep);
+  t.packed.reserve(static_cast<size_t>(n_cap), ctx.stream, keep);
+  t.cap = n_cap;
+}
+void tree_canonicalize(Context& ctx, Graph& g, Tree& t) {
+  const int grid = ctx.sm_count * 8;
+  k_canonicalize<<<grid, kThreads, 0, ctx.stream>>>(g.view(), t.opt.objective, t.source, t.n,
+                                                    reinterpret_cast<const long long*>(t.dist.ptr),
+                                                    t.parent.ptr);
+  DYNGB200_CUDA(cudaGetLastError());
+}
+
+void tree_repack(Context& ctx, Tree& t, int bits) {
+  const int grid = ctx.sm_count * 8;
+  k_pack<<<grid, kThreads, 0, ctx.stream>>>(t.n, bits, reinterpret_cast<const long long*>(t.dist.ptr),
+                                            t.parent.ptr, t.packed.ptr);
+  DYNGB200_CUDA(cudaGetLastError());
+  t.packed_bits = bits;
+}
+
+}  // namespace dyngb200

@@ -1,0 +1,196 @@
+"""dyng_b200.sssp: dynamic single-source shortest paths on B200 (mirrors the reference's
+python/dyng/sssp.py: Options, Stats, Result, compute, update, INFINITE_DISTANCE).
+
+:func:`compute` builds the canonical shortest-path tree (ties to the lowest parent id);
+:func:`update` applies an edge batch to the device-resident graph and repairs the tree.  The
+distances, parents, ``invalidated`` and ``affected`` equal the reference's sequential backend bit
+for bit (cpp/include/dyng/sssp.hpp:23-73).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .graph import (DEVICE, HOST, ApplySummary, EdgeBatch, Graph, InvalidArgumentError, check,
+                    _ptr32, _ptr64)
+
+INFINITE_DISTANCE: int = (2**63 - 1) // 4
+
+_ENGINES = {"automatic": 0, "fused": 1, "operators": 2}
+
+
+@dataclass
+class Options:
+    """sssp::options (sssp.hpp:78-94)."""
+
+    delta: int = 0
+    objective: int = 0
+    cuda_engine: str = "automatic"
+    validate_inputs: bool = True
+
+    def _to_native(self) -> N.Options:
+        if self.cuda_engine not in _ENGINES:
+            raise InvalidArgumentError(f"unknown cuda_engine {self.cuda_engine!r}")
+        return N.Options(int(self.delta), int(self.objective), _ENGINES[self.cuda_engine],
+                         int(bool(self.validate_inputs)))
+
+
+@dataclass
+class Schedule:
+    """The schedule of one update (what the learned scheduler picks; never changes results)."""
+
+    delta: int = 0
+    grid_blocks: int = 0
+    invalidation: int = 0
+    small_frontier: int = 0
+    heavy_degree: int = 0
+
+    def _to_native(self) -> N.Schedule:
+        return N.Schedule(int(self.delta), int(self.grid_blocks), int(self.invalidation),
+                          int(self.small_frontier), int(self.heavy_degree))
+
+
+@dataclass(frozen=True)
+class Stats:
+    """sssp::stats (sssp.hpp:100-117) plus the schedule that ran and the device times."""
+
+    batch: ApplySummary = field(default_factory=ApplySummary)
+    invalidated: int = 0
+    affected: int = 0
+    iterations: int = 0
+    epochs: int = 0
+    pushes: int = 0
+    packed_parents: bool = True
+    engine_used: str = "fused"
+    delta: int = 0
+    max_weight: int = 0
+    grid_blocks: int = 0
+    invalidation: int = 0
+    apply_ms: float = 0.0
+    sssp_ms: float = 0.0
+    rounds: int = 0
+    touched: int = 0
+
+    @classmethod
+    def _from_native(cls, s: N.Stats) -> "Stats":
+        engines = {v: k for k, v in _ENGINES.items()}
+        return cls(ApplySummary._from_native(s.batch), s.invalidated, s.affected, s.iterations,
+                   s.epochs, s.pushes, bool(s.packed_parents), engines.get(s.engine_used, "fused"),
+                   s.delta, s.max_weight, s.grid_blocks, s.invalidation, float(s.apply_ms),
+                   float(s.sssp_ms), s.rounds, s.touched)
+
+
+class Result:
+    """sssp::result: int64 distances and int32 parents in device memory (sssp.hpp:153-310)."""
+
+    def __init__(self, handle, graph: Graph):
+        self._h = handle
+        self._graph = graph
+        self._res = graph._res
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None) and self._h.value:
+                N.lib().dyngb200_tree_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+    def _info(self):
+        src, n, ver, poisoned = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_uint64(), ctypes.c_int32()
+        opt = N.Options()
+        check(N.lib().dyngb200_tree_info(self._h, ctypes.byref(src), ctypes.byref(n),
+                                         ctypes.byref(ver), ctypes.byref(poisoned),
+                                         ctypes.byref(opt)))
+        return src.value, n.value, ver.value, bool(poisoned.value), opt
+
+    @property
+    def source(self) -> int:
+        return self._info()[0]
+
+    @property
+    def graph_version(self) -> int:
+        return self._info()[2]
+
+    @property
+    def poisoned(self) -> bool:
+        return self._info()[3]
+
+    @property
+    def distances(self) -> np.ndarray:
+        n = self._info()[1]
+        out = np.zeros(n, np.int64)
+        check(N.lib().dyngb200_tree_distances(self._res._h, self._h, _ptr64(out), HOST))
+        return out
+
+    @property
+    def parents(self) -> np.ndarray:
+        n = self._info()[1]
+        out = np.zeros(n, np.int32)
+        check(N.lib().dyngb200_tree_parents(self._res._h, self._h, _ptr32(out), HOST))
+        return out
+
+    def device_arrays(self):
+        """Raw device pointers (int64 distances, int32 parents), valid until the next update."""
+        d, p = N.c_i64p(), N.c_i32p()
+        check(N.lib().dyngb200_tree_device_arrays(self._h, ctypes.byref(d), ctypes.byref(p)))
+        return ctypes.cast(d, ctypes.c_void_p).value, ctypes.cast(p, ctypes.c_void_p).value
+
+    @property
+    def options(self) -> Options:
+        o = self._info()[4]
+        engines = {v: k for k, v in _ENGINES.items()}
+        return Options(o.delta, o.objective, engines.get(o.cuda_engine, "automatic"),
+                       bool(o.validate_inputs))
+
+    def set_options(self, options: Options) -> None:
+        o = options._to_native()
+        check(N.lib().dyngb200_tree_set_options(self._h, ctypes.byref(o)))
+
+    def clone(self) -> "Result":
+        h = ctypes.c_void_p()
+        check(N.lib().dyngb200_tree_clone(self._res._h, self._h, ctypes.byref(h)))
+        return Result(h, self._graph)
+
+    @classmethod
+    def from_arrays(cls, graph: Graph, source: int, distances, parents, canonicalize: bool = True,
+                    options: Options | None = None) -> "Result":
+        d = np.ascontiguousarray(np.asarray(distances, dtype=np.int64))
+        p = np.ascontiguousarray(np.asarray(parents, dtype=np.int32))
+        if d.size != p.size:
+            raise InvalidArgumentError("from_arrays: distances and parents differ in length")
+        o = (options or Options())._to_native()
+        h = ctypes.c_void_p()
+        check(N.lib().dyngb200_tree_from_arrays(graph._res._h, graph._h, source, _ptr64(d),
+                                                _ptr32(p), d.size, HOST, int(canonicalize),
+                                                ctypes.byref(o), ctypes.byref(h)))
+        return cls(h, graph)
+
+
+def compute(graph: Graph, source: int = 0, options: Options | None = None,
+            stats: bool = False):
+    """sssp::compute(resources::cuda(), g, source, opt) (sssp.hpp:415-421)."""
+    o = (options or Options())._to_native()
+    h = ctypes.c_void_p()
+    st = N.Stats()
+    check(N.lib().dyngb200_sssp_compute(graph._res._h, graph._h, int(source), ctypes.byref(o),
+                                        ctypes.byref(h), ctypes.byref(st)))
+    r = Result(h, graph)
+    return (r, Stats._from_native(st)) if stats else r
+
+
+def update(graph: Graph, batch: EdgeBatch, tree: Result, schedule: Schedule | None = None) -> Stats:
+    """sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489)."""
+    nb = batch._to_native()
+    st = N.Stats()
+    if schedule is None:
+        check(N.lib().dyngb200_sssp_update(graph._res._h, graph._h, ctypes.byref(nb), tree._h,
+                                           ctypes.byref(st)))
+    else:
+        sc = schedule._to_native()
+        check(N.lib().dyngb200_sssp_update_scheduled(graph._res._h, graph._h, ctypes.byref(nb),
+                                                     tree._h, ctypes.byref(sc), ctypes.byref(st)))
+    return Stats._from_native(st)

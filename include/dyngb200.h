@@ -1,0 +1,229 @@
+/*
+ * dyngb200.h -- the C ABI of dyng_b200: dynG's batch-dynamic single-source shortest-path update
+ * (dyng::sssp::compute / dyng::sssp::update on resources::cuda()) rebuilt for NVIDIA B200
+ * (sm_100a).  Plain pointers and sizes, no C++ or torch types.
+ *
+ * Every entry point returns a dyngb200_status; on failure dyngb200_last_error_message() holds a
+ * message for the calling thread.  The statuses mirror the reference's exception classes
+ * (cpp/include/dyng/core/error.hpp): invalid_argument_error, not_supported_error,
+ * stale_result_error, out_of_memory_error, cuda_error, capacity_error, internal_error.
+ *
+ * Memory: graphs and trees live in device memory.  Batch and array arguments name their memory
+ * space (DYNGB200_HOST or DYNGB200_DEVICE).  A call is complete on the host when it returns: the
+ * context's stream is synchronized once at the end of compute/update (the control block is
+ * read), as the reference's fused engine does (cpp/src/algorithms/sssp/cuda.cu:183-195).
+ *
+ * Threading: a context, graph or tree is not thread-safe; distinct graphs and trees may be used
+ * concurrently from different contexts (cpp/include/dyng/graph/graph.hpp:63-70).
+ */
+#ifndef DYNGB200_H
+#define DYNGB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DYNGB200_ABI_VERSION 1
+
+typedef enum dyngb200_status {
+  DYNGB200_OK = 0,
+  DYNGB200_INVALID_ARGUMENT = 1, /* invalid_argument_error */
+  DYNGB200_NOT_SUPPORTED = 2,    /* not_supported_error */
+  DYNGB200_STALE_RESULT = 3,     /* stale_result_error */
+  DYNGB200_OUT_OF_MEMORY = 4,    /* out_of_memory_error */
+  DYNGB200_CUDA_ERROR = 5,       /* cuda_error */
+  DYNGB200_CAPACITY = 6,         /* capacity_error */
+  DYNGB200_INTERNAL = 7          /* internal_error */
+} dyngb200_status;
+
+typedef enum dyngb200_memory { DYNGB200_HOST = 0, DYNGB200_DEVICE = 1 } dyngb200_memory;
+
+/* dyng::engine (cpp/include/dyng/core/types.hpp): a tunable that never changes the result. */
+typedef enum dyngb200_engine {
+  DYNGB200_ENGINE_AUTOMATIC = 0,
+  DYNGB200_ENGINE_FUSED = 1,
+  DYNGB200_ENGINE_OPERATORS = 2
+} dyngb200_engine;
+
+typedef struct dyngb200_context_s* dyngb200_context; /* resources::cuda() */
+typedef struct dyngb200_graph_s* dyngb200_graph;     /* graph<int32,int64,int32> on the device */
+typedef struct dyngb200_tree_s* dyngb200_tree;       /* sssp::result<int32> */
+
+/* graph_properties + batch_semantics (cpp/include/dyng/graph/graph_properties.hpp:67-241).
+ * dyngb200_props_default() gives the reference's defaults; mosp_compatible() is sorted = 0,
+ * allow_multi = 1. */
+typedef struct dyngb200_props {
+  int32_t directed;            /* 1: directed; 0: every batch edge (u,v) changes both directions */
+  int32_t sorted;              /* row_order::sorted (1) or append (0) */
+  int32_t allow_multi;         /* multi_edges::allow (1) or forbid (0) */
+  int32_t on_existing_insert;  /* 0 upsert, 1 error, 2 ignore */
+  int32_t on_missing_delete;   /* 0 ignore, 1 error */
+  int32_t on_self_loop;        /* 0 keep, 1 drop, 2 error */
+  int32_t deletions_first;     /* 1: deletions, then insertions */
+  int32_t allow_vertex_growth; /* 1: insertions may name new vertices */
+  double headroom;             /* spare slots per slack row, as a fraction of its degree */
+} dyngb200_props;
+
+/* edge_batch_view<int32, int32> (cpp/include/dyng/graph/edge_batch.hpp:38-76). Insertion weights
+ * are insertion-major: num_weights per insertion. */
+typedef struct dyngb200_batch {
+  const int32_t* insert_src;
+  const int32_t* insert_dst;
+  const int32_t* insert_weights;
+  int64_t num_insertions;
+  const int32_t* delete_src;
+  const int32_t* delete_dst;
+  int64_t num_deletions;
+  int32_t num_weights;
+  int32_t memory; /* dyngb200_memory of all five arrays */
+} dyngb200_batch;
+
+/* apply_summary (cpp/include/dyng/graph/apply_summary.hpp). */
+typedef struct dyngb200_apply_summary {
+  int64_t inserted_edges;
+  int64_t deleted_edges;
+  int64_t updated_edges;
+  int64_t ignored_insertions;
+  int64_t ignored_deletions;
+  int64_t dropped_self_loops;
+  int64_t inserted_vertices;
+  int64_t num_vertices_after;
+} dyngb200_apply_summary;
+
+/* sssp::stats (cpp/include/dyng/sssp.hpp:100-117) plus the schedule that ran and device times. */
+typedef struct dyngb200_stats {
+  dyngb200_apply_summary batch;
+  int64_t invalidated; /* deterministic */
+  int64_t affected;    /* deterministic: vertices whose distance or parent changed */
+  int64_t iterations;  /* schedule-dependent */
+  int64_t epochs;      /* schedule-dependent */
+  int64_t pushes;      /* schedule-dependent */
+  int32_t packed_parents;
+  int32_t engine_used;
+  int64_t delta;       /* near-far width that ran */
+  int64_t max_weight;  /* bound weight of the packing */
+  int32_t grid_blocks; /* persistent grid that ran */
+  int32_t invalidation; /* 0 pointer jumping, 1 subtree walk */
+  float apply_ms;      /* device time of the batch applier */
+  float sssp_ms;       /* device time of the sssp kernel */
+  int64_t rounds;      /* pointer-jumping rounds */
+  int64_t touched;     /* vertices whose packed word was written */
+} dyngb200_stats;
+
+/* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */
+typedef struct dyngb200_options {
+  int64_t delta;           /* near-far width; 0 = automatic (the reference's defaultDelta) */
+  int32_t objective;       /* weight column, fixed at compute() */
+  int32_t cuda_engine;     /* dyngb200_engine */
+  int32_t validate_inputs; /* O(n) checks of imported trees */
+} dyngb200_options;
+
+/* The schedule of one update: what the learned scheduler chooses.  A tunable only: every field
+ * changes the order of work, never the distances or parents.  Zero fields mean "the fixed
+ * heuristic": delta from the options, the occupancy grid, pointer-jumping invalidation. */
+typedef struct dyngb200_schedule {
+  int64_t delta;          /* near-far bucket width (0: heuristic) */
+  int32_t grid_blocks;    /* persistent grid size (0: occupancy x SMs) */
+  int32_t invalidation;   /* 0 heuristic/pointer jumping, 1 subtree walk */
+  int32_t small_frontier; /* frontiers up to this size run on one block between grid barriers (0 off) */
+  int32_t heavy_degree;   /* rows longer than this are split across warps (0: default) */
+} dyngb200_schedule;
+
+/* ---- errors ------------------------------------------------------------------------------ */
+const char* dyngb200_last_error_message(void);
+const char* dyngb200_status_name(dyngb200_status s);
+int dyngb200_abi_version(void);
+
+/* ---- context: resources::cuda(device) (cpp/include/dyng/core/resources.hpp) --------------- */
+/* stream: a cudaStream_t, or NULL for a stream owned by the context. */
+dyngb200_status dyngb200_context_create(int device, void* stream, dyngb200_context* out);
+dyngb200_status dyngb200_context_destroy(dyngb200_context ctx);
+dyngb200_status dyngb200_context_synchronize(dyngb200_context ctx);
+void dyngb200_props_default(dyngb200_props* props);
+void dyngb200_props_mosp_compatible(dyngb200_props* props);
+
+/* ---- graph (cpp/include/dyng/graph/graph.hpp:143-195, 332-487) ----------------------------- */
+/* graph<int32,int64,int32>::from_edges: weights insertion-major (num_weights per edge). */
+dyngb200_status dyngb200_graph_from_edges(dyngb200_context ctx, int64_t num_vertices,
+                                          const int32_t* src, const int32_t* dst,
+                                          const int32_t* weights, int64_t num_edges,
+                                          int32_t num_weights, int32_t memory,
+                                          const dyngb200_props* props, dyngb200_graph* out);
+/* graph::from_csr: row_ptr has num_vertices + 1 entries, weights objective-major. */
+dyngb200_status dyngb200_graph_from_csr(dyngb200_context ctx, int64_t num_vertices,
+                                        const int64_t* row_ptr, const int32_t* col,
+                                        const int32_t* weights, int32_t num_weights,
+                                        int32_t memory, const dyngb200_props* props,
+                                        dyngb200_graph* out);
+dyngb200_status dyngb200_graph_destroy(dyngb200_graph g);
+/* num_vertices / num_edges / num_weights / version (graph.hpp:332-354). */
+dyngb200_status dyngb200_graph_info(dyngb200_graph g, int64_t* num_vertices, int64_t* num_edges,
+                                    int32_t* num_weights, uint64_t* version);
+/* graph::apply (graph.hpp:474): the batch alone, on the device.  weight_increased (optional,
+ * host, num_effective_insertions x num_weights bytes) receives the classification. */
+dyngb200_status dyngb200_graph_apply(dyngb200_context ctx, dyngb200_graph g,
+                                     const dyngb200_batch* batch,
+                                     dyngb200_apply_summary* summary);
+/* graph::apply plus the weight-increase classification of apply_host.cpp:348-393: host buffer
+ * weight_increased receives num_insertions x num_weights bytes (1: the insertion raised that
+ * objective's weight of the first (u,v) of row u). */
+dyngb200_status dyngb200_graph_apply_classified(dyngb200_context ctx, dyngb200_graph g,
+                                                const dyngb200_batch* batch,
+                                                dyngb200_apply_summary* summary,
+                                                uint8_t* weight_increased);
+/* graph::to_csr (graph.hpp:487) plus the in-edge mirror; host buffers sized from
+ * dyngb200_graph_info (row_ptr n+1, col m, weights k*m objective-major); any pointer may be NULL. */
+dyngb200_status dyngb200_graph_to_csr(dyngb200_context ctx, dyngb200_graph g, int64_t* row_ptr,
+                                      int32_t* col, int32_t* weights, int64_t* in_row_ptr,
+                                      int32_t* in_col, int32_t* in_weights);
+/* Device memory held by the graph, in bytes. */
+dyngb200_status dyngb200_graph_device_bytes(dyngb200_graph g, int64_t* bytes);
+
+/* ---- sssp (cpp/include/dyng/sssp.hpp:415-489) -------------------------------------------- */
+/* sssp::compute(resources::cuda(), g, source, opt) (sssp.hpp:415-421). opt may be NULL. */
+dyngb200_status dyngb200_sssp_compute(dyngb200_context ctx, dyngb200_graph g, int32_t source,
+                                      const dyngb200_options* opt, dyngb200_tree* out,
+                                      dyngb200_stats* stats);
+/* sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489). */
+dyngb200_status dyngb200_sssp_update(dyngb200_context ctx, dyngb200_graph g,
+                                     const dyngb200_batch* batch, dyngb200_tree tree,
+                                     dyngb200_stats* stats);
+/* sssp::update with an explicit schedule (the learned scheduler's entry point; no reference
+ * counterpart beyond options::delta / options::cuda_engine, which are tunables the same way). */
+dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_graph g,
+                                               const dyngb200_batch* batch, dyngb200_tree tree,
+                                               const dyngb200_schedule* schedule,
+                                               dyngb200_stats* stats);
+
+/* ---- tree: sssp::result (sssp.hpp:153-310) ------------------------------------------------ */
+/* result::from_arrays (sssp.hpp:253-302): arrays in `memory`, n entries each. */
+dyngb200_status dyngb200_tree_from_arrays(dyngb200_context ctx, dyngb200_graph g, int32_t source,
+                                          const int64_t* distances, const int32_t* parents,
+                                          int64_t n, int32_t memory, int32_t canonicalize,
+                                          const dyngb200_options* opt, dyngb200_tree* out);
+/* result::clone (sssp.hpp:245). */
+dyngb200_status dyngb200_tree_clone(dyngb200_context ctx, dyngb200_tree t, dyngb200_tree* out);
+dyngb200_status dyngb200_tree_destroy(dyngb200_tree t);
+/* result::distances() / parents() copied into `dst` (n entries, in `memory`). */
+dyngb200_status dyngb200_tree_distances(dyngb200_context ctx, dyngb200_tree t, int64_t* dst,
+                                        int32_t memory);
+dyngb200_status dyngb200_tree_parents(dyngb200_context ctx, dyngb200_tree t, int32_t* dst,
+                                      int32_t memory);
+/* The device arrays themselves (valid until the next update of t). */
+dyngb200_status dyngb200_tree_device_arrays(dyngb200_tree t, const int64_t** distances,
+                                            const int32_t** parents);
+/* source(), num vertices, graph_version(), poisoned, get_options(). */
+dyngb200_status dyngb200_tree_info(dyngb200_tree t, int32_t* source, int64_t* num_vertices,
+                                   uint64_t* graph_version, int32_t* poisoned,
+                                   dyngb200_options* opt);
+/* result::set_options (sssp.hpp:214-222): objective must stay. */
+dyngb200_status dyngb200_tree_set_options(dyngb200_tree t, const dyngb200_options* opt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DYNGB200_H */
