@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--schedule", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--invalidation", type=int, default=0, help="0 pointer jumping, 1 subtree walk")
+    ap.add_argument("--delta", type=int, default=0)
+    ap.add_argument("--grid-blocks", type=int, default=0)
+    ap.add_argument("--heavy-degree", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
     return ap.parse_args()
@@ -115,20 +119,6 @@ def make_workload(args, device):
     t0 = time.time()
     edges = G.rmat(args.scale, 16, w_max=1000, seed=1, device=device)
     return edges, time.time() - t0
-
-
-# Algorithmic bytes of the sssp kernel per counted unit (ints 4 B, packed words 8 B):
-#   per pushed vertex: list entry 4 + word 8 + row descriptor 8
-#   per scanned out-slot: column 4 + weight 4 + target word 8
-#   per successful atomicMin: 8;  per frontier append: 4
-#   per pulled in-slot: column 4 + weight 4 + source word 8
-#   per invalidation round: 12 per vertex (ancestor read + write, flag read)
-BYTES = {"pushes": 20, "edges": 16, "atomics": 8, "appends": 4, "pull_edges": 16,
-         "round_vertices": 12}
-
-
-def algorithmic_bytes(counters):
-    return sum(BYTES[k] * counters.get(k, 0) for k in BYTES)
 
 
 def cpu_baseline_sample(edges, tree_d, tree_p, batches, budget_s=20.0):
@@ -240,6 +230,10 @@ def main():
                                       b.delete_src.size)
 
     sched = None
+    if args.invalidation or args.delta or args.grid_blocks or args.heavy_degree:
+        sched = D.sssp.Schedule(delta=args.delta, grid_blocks=args.grid_blocks,
+                                invalidation=args.invalidation, heavy_degree=args.heavy_degree)
+    host_lat = []
     timed_stats = []
     lat = []
     sizes = []
@@ -256,10 +250,12 @@ def main():
             sampler.start()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        h0 = time.perf_counter()
         e0.record(stream)
         st = D.sssp.update(g, db, tree, schedule=sched)
         e1.record(stream)
         e1.synchronize()
+        host_lat.append(time.perf_counter() - h0)
         if step >= args.warmup:
             lat.append(e0.elapsed_time(e1))
             sizes.append(b.size)
@@ -298,16 +294,20 @@ def main():
                         np.array_equal(fresh.parents, tree.parents))
         del fresh
 
-    # roofline of the dominant kernel (the sssp persistent kernel)
+    # roofline of the dominant kernel (the sssp persistent kernel): algorithmic bytes counted by
+    # the kernel (Stats.work x Stats.WORK_BYTES) over its CUDA-event time on the launching stream
     sssp_ms = [s.sssp_ms for s in timed_stats]
     apply_ms = [s.apply_ms for s in timed_stats]
     peak, peak_kind = peaks()
-    counters = {}
-    for s in timed_stats:
-        for k, v in getattr(s, "counters", {}).items():
-            counters[k] = counters.get(k, 0) + v
-    alg = algorithmic_bytes(counters) / max(len(timed_stats), 1)
-    achieved = alg / (np.mean(sssp_ms) / 1000.0) / 1e9 if sssp_ms else 0.0
+    alg = [s.algorithmic_bytes + 12 * s.affected for s in timed_stats]
+    achieved = float(np.sum(alg) / (np.sum(sssp_ms) / 1000.0) / 1e9) if sssp_ms else 0.0
+    work = {name: int(np.mean([s.work[i] for s in timed_stats]))
+            for i, name in enumerate(timed_stats[0].WORK_NAMES)}
+    phases = {name: round(float(np.mean([s.phase_ms[i] for s in timed_stats])), 3)
+              for i, name in enumerate(timed_stats[0].PHASES)}
+    shape = {k: float(np.mean([getattr(s, k) for s in timed_stats]))
+             for k in ("iterations", "epochs", "pushes", "invalidated", "affected", "rounds",
+                       "touched", "delta", "grid_blocks")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -342,6 +342,9 @@ def main():
                        "p99_ms": float(np.percentile(lat, 99)),
                        "apply_ms_mean": float(np.mean(apply_ms)),
                        "sssp_ms_mean": float(np.mean(sssp_ms)),
+                       "host_ms_p50": 1000 * float(np.percentile(host_lat[args.warmup:], 50)),
+                       "sssp_phases_ms": phases, "sssp_work": work, "update_shape": shape,
+                       "alg_bytes_per_update": float(np.mean(alg)),
                        "verified_vs_compute": verified,
                        "setup_s": {"generate": round(gen_s, 1), "build_and_compute": round(build_s, 1)}},
             "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,

@@ -50,7 +50,8 @@ class Stats(ctypes.Structure):
                 ("delta", ctypes.c_int64), ("max_weight", ctypes.c_int64),
                 ("grid_blocks", ctypes.c_int32), ("invalidation", ctypes.c_int32),
                 ("apply_ms", ctypes.c_float), ("sssp_ms", ctypes.c_float),
-                ("rounds", ctypes.c_int64), ("touched", ctypes.c_int64)]
+                ("rounds", ctypes.c_int64), ("touched", ctypes.c_int64),
+                ("work", ctypes.c_int64 * 12), ("phase_ms", ctypes.c_float * 7)]
 
 
 class Options(ctypes.Structure):

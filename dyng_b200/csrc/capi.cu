@@ -563,6 +563,7 @@ dyngb200_status dyngb200_tree_from_arrays(dyngb200_context ctx, dyngb200_graph g
       validate_tree(source, d, p, cs.max_w * std::max<long long>(n - 1, 1));
     }
     t.trusted = o.validate_inputs != 0;
+    t.canonical = canonicalize != 0;
     // the persistent packed words in the format of the graph's current bound
     u64 bound = 0;
     const Packing pk = choose_packing(n, cs.max_w, &bound);
@@ -590,6 +591,7 @@ dyngb200_status dyngb200_tree_clone(dyngb200_context ctx, dyngb200_tree tree, dy
     t.device = c.device;
     t.packed_bits = s.packed_bits;
     t.trusted = s.trusted;
+    t.canonical = s.canonical;
     tree_reserve(c, t, std::max(s.cap, s.n));
     if (s.n > 0) {
       DYNGB200_CUDA(cudaMemcpyPeerAsync(t.dist.ptr, c.device, s.dist.ptr, s.device,

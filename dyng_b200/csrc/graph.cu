@@ -995,7 +995,7 @@ void Workspace::reserve_vertices(long long n_cap, cudaStream_t s) {
     b->release();
     b->reserve(n, s);
   }
-  for (DevBuf<int>* b : {&heavy_a, &heavy_b}) {  // int2 entries
+  for (DevBuf<int>* b : {&heavy_a, &heavy_b, &pull_heavy}) {  // int2 entries
     b->release();
     b->reserve(2 * n, s);
   }

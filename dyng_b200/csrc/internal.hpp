@@ -110,19 +110,28 @@ struct UpdateCtl {
   int packing_bits;
   int repacked;
   u64 max_distance;
-  int list_count, frontier_count, near_count, next_count, far_count, far2_count;
-  int heavy_count, next_heavy_count;
+  int cand_count;       // light pull candidates
+  int frontier_count;   // vertices the pull (or the head offers) improved
+  int near_cnt[3];      // light near-frontier lists, triple-buffered counters
+  int walk_cnt[3];      // subtree-walk levels
+  int far_count, far2_count;
+  u64 heavy_cnt[3];     // (slots << 40 | chunks) of the heavy near-frontier lists
+  u64 walk_heavy[3];
+  u64 pull_heavy;       // heavy pull candidates
   int touched_count;
   int active[3];
   int rounds;
   int iterations, epochs;
+  int levels;
   long long pushes;
   long long invalidated;
   long long affected;
   u64 minimum;
   int changed;         // the batch holds a deleted or weight-increased edge
   int last_generation; // last stamp generation the kernel used
-  u64 heavy_counter[2];  // (slots << 40 | chunks) of the current and next heavy frontier lists
+  // work counters (algorithmic traffic) and phase timestamps of the sssp kernel
+  long long work[12];
+  unsigned long long phase_ns[8];
   // grid barrier
   unsigned bar_count;
   unsigned bar_gen;
@@ -148,7 +157,8 @@ struct Workspace {
   DevBuf<int32_t> b_ins_src, b_ins_dst, b_ins_w, b_del_src, b_del_dst;
   // sssp
   DevBuf<int> stamp, touch_stamp, flag, in_far, ancestor;
-  DevBuf<int> candidates, frontier, near_a, near_b, far_a, far_b, heavy_a, heavy_b, touched;
+  DevBuf<int> candidates, frontier, near_a, near_b, far_a, far_b, heavy_a, heavy_b, pull_heavy,
+      touched;
   DevBuf<UpdateCtl> ctl;
   HostBuf<UpdateCtl> host_ctl;
   int generation = 0;     // stamp generations (sssp)
@@ -217,6 +227,7 @@ struct Graph {
 };
 
 struct Tree {
+  bool canonical = true;  // every parent is the lowest-id tight in-neighbour (compute, canonicalize)
   uint64_t graph_id = 0;
   uint64_t version = 0;
   int32_t source = 0;

@@ -35,10 +35,16 @@ struct SsspParams {
   u64* packed;
   int tree_bits;         // format of the persistent words (-1: none); another format is rebuilt
   long long tree_n;      // vertices the tree held before this call (growth fills the rest)
-  // pairs of the applier (update only)
+  int walk;              // invalidation by a subtree walk instead of pointer jumping
+  int offer_heads;       // canonical tree: insertion heads take the inserted edge's offer
+  // pairs of the applier (update only) and the batch weights
   const u64* pair_key;
   const int* pair_list;
   const int* pair_flags;
+  const int* pair_first;
+  const int* pair_last;
+  const int32_t* ins_w;
+  int k;
   // scratch
   int* stamp;
   int* touch_stamp;
@@ -53,14 +59,20 @@ struct SsspParams {
   int* far_b;
   int2* heavy_a;
   int2* heavy_b;
+  int2* pull_heavy;
   int* touched;
   int generation;
   int touch_gen;
   int heavy_degree;
   long long delta_override;
   UpdateCtl* ctl;
-  u64* heavy_counter;  // ctl->heavy_counter: (slots << 40 | chunks), current and next lists
 };
+
+// Pair flags of the applier (graph.cu).
+constexpr int kPairDelete = 1, kPairIncreased = 2, kPairHead = 4, kPairAppend = 8,
+              kPairUpsert = 16, kPairUseFirst = 32;
+
+enum Mode { kPush = 0, kPull = 1, kWalk = 2 };
 
 __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
   return *reinterpret_cast<const volatile unsigned*>(p);
@@ -84,7 +96,7 @@ __device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
       unsigned long long start = 0;
       unsigned spins = 0;
       while (ld_volatile(&c->bar_gen) != target) {
-        __nanosleep(64);
+        __nanosleep(32);
         if ((++spins & 255u) == 0) {
           if (ld_volatile(&c->error) & kErrTimeout) {
             ok = 0;
@@ -124,77 +136,180 @@ __device__ __forceinline__ void warp_min_into(u64 v, u64* target) {
   if ((threadIdx.x & 31) == 0 && v != kPackedInf) atomicMin(target, v);
 }
 
-template <typename T>
-__device__ __forceinline__ void warp_sum_into(T v, T* target) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(target, v);
-}
-
 __device__ __forceinline__ void warp_sum_into_ll(long long v, long long* target) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0 && v != 0)
     atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(v));
 }
 
-// Put v on the next near frontier: the light list, or the heavy list with its chunk range.
-__device__ __forceinline__ void push_near(const SsspParams& p, int v, int* light, int* light_count,
-                                          int2* heavy, u64* heavy_counter) {
-  const int len = p.g.out_desc[v].len;
-  if (len > p.heavy_degree) {
+// Append v to a frontier: the light list, or (rows longer than heavy_degree) the heavy list with
+// its 1024-slot chunk range, reserved together with the slot by one 64-bit atomic so that chunk
+// bases grow with the slot index.
+__device__ __forceinline__ void list_append(int v, int len, int heavy_degree, int* light,
+                                            int* light_count, int2* heavy, u64* heavy_count) {
+  if (len > heavy_degree) {
     const u64 chunks = static_cast<u64>((len + kHeavyChunk - 1) / kHeavyChunk);
-    const u64 prev = atomicAdd(heavy_counter, (1ULL << 40) | chunks);
-    const int slot = static_cast<int>(prev >> 40);
-    heavy[slot] = make_int2(v, static_cast<int>(prev & ((1ULL << 40) - 1)));
+    const u64 prev = atomicAdd(heavy_count, (1ULL << 40) | chunks);
+    heavy[static_cast<int>(prev >> 40)] = make_int2(v, static_cast<int>(prev & ((1ULL << 40) - 1)));
   } else {
     light[append_slot(light_count)] = v;
   }
 }
 
-struct Loop {
+// A vertex to re-evaluate by the pull pass (light or heavy by in-degree).
+__device__ __forceinline__ void add_candidate(const SsspParams& p, int v) {
+  list_append(v, p.g.in_desc[v].len, p.heavy_degree, p.candidates, &p.ctl->cand_count,
+              p.pull_heavy, &p.ctl->pull_heavy);
+}
+
+// Per-thread state of one expansion: where improved vertices go, and work counters.
+struct Ctx {
+  Packing pk;
+  u64 maxd;
   u64 threshold;
-  int gen;
+  int gen;       // claim generation of the appends
+  int* next;     // next light list (push: near; pull: frontier; walk: next level)
+  int* next_cnt;
+  int2* next_heavy;
+  u64* next_heavy_cnt;
+  int* far;
+  int* far_cnt;
+  unsigned slots, words, atomics, appends, rows;
 };
 
-// One relaxation of edge (u, x) of weight w from distance du.
-__device__ __forceinline__ void relax_edge(const SsspParams& p, const Packing& pk, u64 maxd,
-                                           int u, u64 du, int x, int w, const Loop& L,
-                                           int* next_light, int2* next_heavy, int* far) {
-  if (x < 0 || x == p.source) return;
+// One slot of a row.  push: owner u relaxes (u -> y); pull: in-neighbour y offers to the owner;
+// walk: y is invalidated if its old parent is the owner.
+template <int MODE>
+__device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u64 odu, int y,
+                                      int w) {
+  ++X.slots;
+  if (y < 0) return;  // tombstone
+  if (MODE == kWalk) {
+    if (y < p.tree_n && p.parent[y] == owner && claim(p.stamp, y, X.gen)) {
+      p.packed[y] = kPackedInf;
+      touch(p, y);
+      add_candidate(p, y);
+      ++X.appends;
+      list_append(y, p.g.out_desc[y].len, p.heavy_degree, X.next, X.next_cnt, X.next_heavy,
+                  X.next_heavy_cnt);
+    }
+    return;
+  }
+  int src, dst;
+  u64 du;
+  if (MODE == kPush) {
+    if (y == p.source) return;
+    src = owner;
+    dst = y;
+    du = odu;
+  } else {
+    const u64 word = ld_cg(&p.packed[y]);
+    ++X.words;
+    if (word == kPackedInf) return;
+    src = y;
+    dst = owner;
+    du = X.pk.dist(word);
+  }
   const u64 nd = du + static_cast<u64>(w);
-  if (nd > maxd) return;
-  const u64 cand = pk.pack(nd, u);
-  if (cand >= ld_cg(&p.packed[x])) return;
-  const u64 old = atomicMin(&p.packed[x], cand);
-  if (cand < old) touch(p, x);
-  if (nd < pk.dist(old)) {
-    if (nd < L.threshold) {
-      if (claim(p.stamp, x, L.gen))
-        push_near(p, x, next_light, &p.ctl->next_count, next_heavy, &p.heavy_counter[1]);
-    } else if (atomicExch(&p.in_far[x], 1) == 0) {
-      far[append_slot(&p.ctl->far_count)] = x;
+  if (nd > X.maxd) return;
+  const u64 cand = X.pk.pack(nd, src);
+  if (MODE == kPush) ++X.words;
+  if (cand >= ld_cg(&p.packed[dst])) return;
+  const u64 old = atomicMin(&p.packed[dst], cand);
+  if (cand < old) {
+    ++X.atomics;
+    touch(p, dst);
+  }
+  if (nd < X.pk.dist(old)) {
+    if (MODE == kPull) {
+      if (claim(p.stamp, dst, X.gen)) {
+        ++X.appends;
+        X.next[append_slot(X.next_cnt)] = dst;
+      }
+    } else if (nd < X.threshold) {
+      if (claim(p.stamp, dst, X.gen)) {
+        ++X.appends;
+        list_append(dst, p.g.out_desc[dst].len, p.heavy_degree, X.next, X.next_cnt, X.next_heavy,
+                    X.next_heavy_cnt);
+      }
+    } else if (atomicExch(&p.in_far[dst], 1) == 0) {
+      ++X.appends;
+      X.far[append_slot(X.far_cnt)] = dst;
     }
   }
 }
 
-// Scan slots [e0, e1) of a row with the 32 lanes of a warp: lane l takes the 4-slot groups
-// l, l + 32, ... with one 16-byte load of columns and one of weights (rows start on 4-slot
-// boundaries and own at least round_up(len, 4) slots, so a group never leaves its row).
-__device__ __forceinline__ void warp_row(const SsspParams& p, const Packing& pk, u64 maxd, int u,
-                                         u64 du, unsigned start, int e0, int e1, const Loop& L,
-                                         int* next_light, int2* next_heavy, int* far) {
+template <int MODE>
+__device__ __forceinline__ const int32_t* row_col(const SsspParams& p) {
+  return MODE == kPull ? p.g.in_col : p.g.out_col;
+}
+template <int MODE>
+__device__ __forceinline__ const int32_t* row_w(const SsspParams& p) {
+  return (MODE == kPull ? p.g.in_w : p.g.out_w) + static_cast<long long>(p.objective) * p.g.arena_cap;
+}
+
+// Slots [e0, e1) of one row by the 32 lanes of a warp: lane l takes the 4-slot groups l, l+32, ...
+// with one 16-byte load of columns and one of weights (rows start on 4-slot boundaries and own at
+// least round_up(len, 4) slots, so a group never leaves its row).
+template <int MODE>
+__device__ __forceinline__ void warp_slots(const SsspParams& p, Ctx& X, int owner, u64 odu,
+                                           unsigned start, int e0, int e1) {
   const int lane = threadIdx.x & 31;
-  const int32_t* col = p.g.out_col + start;
-  const int32_t* wt = p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap + start;
-  const int g0 = e0 >> 2;
+  const int32_t* col = row_col<MODE>(p) + start;
+  const int32_t* wt = row_w<MODE>(p) + start;
   const int g1 = (e1 + 3) >> 2;
-  for (int grp = g0 + lane; grp < g1; grp += 32) {
+  for (int grp = (e0 >> 2) + lane; grp < g1; grp += 32) {
     const int e = grp << 2;
     const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + e));
-    const int4 w4 = __ldg(reinterpret_cast<const int4*>(wt + e));
-    if (e + 0 < e1) relax_edge(p, pk, maxd, u, du, c4.x, w4.x, L, next_light, next_heavy, far);
-    if (e + 1 < e1) relax_edge(p, pk, maxd, u, du, c4.y, w4.y, L, next_light, next_heavy, far);
-    if (e + 2 < e1) relax_edge(p, pk, maxd, u, du, c4.z, w4.z, L, next_light, next_heavy, far);
-    if (e + 3 < e1) relax_edge(p, pk, maxd, u, du, c4.w, w4.w, L, next_light, next_heavy, far);
+    const int4 w4 = MODE == kWalk ? make_int4(0, 0, 0, 0) : __ldg(reinterpret_cast<const int4*>(wt + e));
+    if (e + 0 < e1) visit<MODE>(p, X, owner, odu, c4.x, w4.x);
+    if (e + 1 < e1) visit<MODE>(p, X, owner, odu, c4.y, w4.y);
+    if (e + 2 < e1) visit<MODE>(p, X, owner, odu, c4.z, w4.z);
+    if (e + 3 < e1) visit<MODE>(p, X, owner, odu, c4.w, w4.w);
+  }
+}
+
+// Up to 32 rows, one per lane (len 0: none).  Rows of 32+ slots are scanned by the whole warp in
+// turn; the shorter rows are concatenated and their slots dealt round-robin to the lanes (the
+// owner of slot e is found by a binary search over the lanes' exclusive prefix sums).
+template <int MODE>
+__device__ __forceinline__ void warp_rows(const SsspParams& p, Ctx& X, int owner, u64 odu,
+                                          unsigned start, int len) {
+  const int lane = threadIdx.x & 31;
+  unsigned big = __ballot_sync(0xffffffffu, len >= 32);
+  while (big) {
+    const int leader = __ffs(big) - 1;
+    big &= big - 1;
+    warp_slots<MODE>(p, X, __shfl_sync(0xffffffffu, owner, leader),
+                     __shfl_sync(0xffffffffu, odu, leader), __shfl_sync(0xffffffffu, start, leader),
+                     0, __shfl_sync(0xffffffffu, len, leader));
+  }
+  const int mine = len < 32 ? len : 0;
+  int incl = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int excl = incl - mine;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const int32_t* col = row_col<MODE>(p);
+  const int32_t* wt = row_w<MODE>(p);
+  for (int base = 0; base < total; base += 32) {
+    const int e = base + lane;
+    int j = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int cand = j + step;
+      if (__shfl_sync(0xffffffffu, excl, cand) <= e) j = cand;
+    }
+    const int o = __shfl_sync(0xffffffffu, owner, j);
+    const u64 d = __shfl_sync(0xffffffffu, odu, j);
+    const unsigned s = __shfl_sync(0xffffffffu, start, j);
+    const int ex = __shfl_sync(0xffffffffu, excl, j);
+    if (e < total) {
+      const unsigned slot = s + static_cast<unsigned>(e - ex);
+      visit<MODE>(p, X, o, d, col[slot], MODE == kWalk ? 0 : wt[slot]);
+    }
   }
 }
 
@@ -208,6 +323,59 @@ __device__ __forceinline__ int find_heavy(const int2* list, int count, long long
   return lo;
 }
 
+// Expand a frontier: light rows in groups of 32 per warp, heavy rows in 1024-slot chunks over all
+// warps of the grid.  push / walk expand out-rows, pull expands in-rows.
+template <int MODE>
+__device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_count,
+                       const int2* heavy, u64 heavy_cnt, long long gwarp, long long nwarps) {
+  const int lane = threadIdx.x & 31;
+  const RowDesc* descs = MODE == kPull ? p.g.in_desc : p.g.out_desc;
+  for (long long base = gwarp * 32; base < light_count; base += nwarps * 32) {
+    const long long i = base + lane;
+    int owner = -1;
+    u64 du = 0;
+    RowDesc desc{0, 0};
+    if (i < light_count) {
+      owner = ld_cg(&light[i]);
+      ++X.rows;
+      if (MODE == kPush) {
+        const u64 word = ld_cg(&p.packed[owner]);
+        if (word != kPackedInf) {
+          du = X.pk.dist(word);
+          desc = descs[owner];
+        }
+      } else {
+        desc = descs[owner];
+      }
+    }
+    warp_rows<MODE>(p, X, owner, du, desc.start, desc.len);
+  }
+  const int hcount = static_cast<int>(heavy_cnt >> 40);
+  const long long chunks = static_cast<long long>(heavy_cnt & ((1ULL << 40) - 1));
+  for (long long ch = gwarp; ch < chunks; ch += nwarps) {
+    const int h = find_heavy(heavy, hcount, ch);
+    const int owner = __ldcg(&heavy[h].x);
+    const int base = __ldcg(&heavy[h].y);
+    u64 du = 0;
+    if (MODE == kPush) {
+      const u64 word = ld_cg(&p.packed[owner]);
+      if (word == kPackedInf) continue;
+      du = X.pk.dist(word);
+    }
+    if (ch == base && lane == 0) ++X.rows;
+    const RowDesc desc = descs[owner];
+    const int e0 = static_cast<int>(ch - base) * kHeavyChunk;
+    const int e1 = min(desc.len, e0 + kHeavyChunk);
+    warp_slots<MODE>(p, X, owner, du, desc.start, e0, e1);
+  }
+}
+
+__device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
+  p.packed[v] = kPackedInf;
+  touch(p, v);
+  add_candidate(p, v);
+}
+
 __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
   UpdateCtl* c = p.ctl;
   if (ld_volatile(&c->error) != 0) return;
@@ -218,13 +386,20 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
   const long long gwarp = tid >> 5;
   const long long nwarps = threads >> 5;
   const long long n = c->n_after;
-  Packing pk;
-  pk.bits = c->packing_bits;
-  pk.no_parent = pk.bits ? (1ULL << pk.bits) - 1 : 0;
-  const u64 maxd = c->max_distance;
+  Ctx X;
+  X.pk.bits = c->packing_bits;
+  X.pk.no_parent = X.pk.bits ? (1ULL << X.pk.bits) - 1 : 0;
+  X.maxd = c->max_distance;
+  X.threshold = 0;
+  X.slots = X.words = X.atomics = X.appends = X.rows = 0;
+  const Packing pk = X.pk;
   const u64 delta = static_cast<u64>(p.delta_override > 0 ? p.delta_override : c->delta);
   int gen = p.generation;
   int frontier_count = 0;
+  // work counters (see dyngb200_stats::work)
+  long long w_visits = 0, w_jumps = 0, w_inval = 0;
+  unsigned pull_slots = 0, pull_words = 0, pull_rows = 0, unpacked = 0;
+  if (tid == 0) c->phase_ns[0] = global_ns();
 
   if (p.from_scratch) {
     for (long long v = tid; v < n; v += threads)
@@ -233,6 +408,8 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     frontier_count = 1;
     if (!grid_barrier(c, bar)) return;
   } else {
+    const int gen_inv = ++gen;
+    const int gen_pull = ++gen;
     // ---- the persistent words in this update's format; growth -------------------------------
     if (p.tree_bits != pk.bits) {
       for (long long v = tid; v < n; v += threads) {
@@ -243,7 +420,7 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
         const long long d = p.dist[v];
         u64 word = kPackedInf;
         if (d < kInfinity / 2) {
-          if (d < 0 || static_cast<u64>(d) > maxd) atomicOr(&c->error, kErrOverflow);
+          if (d < 0 || static_cast<u64>(d) > X.maxd) atomicOr(&c->error, kErrOverflow);
           else word = pk.pack(static_cast<u64>(d), p.parent[v]);
         }
         p.packed[v] = word;
@@ -261,96 +438,161 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     for (long long i = tid; i < pairs; i += threads) {
       const int slot = p.pair_list[i];
       const int f = p.pair_flags[slot];
-      if (f & 3) {  // deleted or weight increased in the objective
+      if (f & (kPairDelete | kPairIncreased)) {
         changed = 1;
         const u64 key = p.pair_key[slot];
         const int32_t u = static_cast<int32_t>(key >> 32);
         const int32_t v = static_cast<int32_t>(key & 0xffffffffu);
-        if (v < p.tree_n && p.parent[v] == u) p.flag[v] = 1;
+        if (v < p.tree_n && p.parent[v] == u) {
+          if (!p.walk) {
+            p.flag[v] = 1;
+          } else if (claim(p.stamp, v, gen_inv)) {
+            // walk: roots are invalidated here and start the first level
+            p.packed[v] = kPackedInf;
+            touch(p, static_cast<int>(v));
+            add_candidate(p, v);
+            ++w_inval;
+            list_append(v, p.g.out_desc[v].len, p.heavy_degree, p.near_a, &c->walk_cnt[0],
+                        p.heavy_a, &c->walk_heavy[0]);
+          }
+        }
       }
     }
     if (__any_sync(0xffffffffu, changed) && lane == 0) c->changed = 1;
-    for (long long v = tid; v < n; v += threads) p.ancestor[v] = p.parent[v];
+    if (!p.walk) {
+      for (long long v = tid; v < n; v += threads) p.ancestor[v] = v < p.tree_n ? p.parent[v] : -1;
+      w_visits += (n - tid + threads - 1) / threads;
+    }
     if (!grid_barrier(c, bar)) return;
     if (ld_volatile(&c->error)) return;
+    if (tid == 0) c->phase_ns[1] = global_ns();
     const bool any_changed = ld_cg(&c->changed) != 0;
-    // ---- subtree invalidation by pointer jumping (fused.cuh:199-234) --------------------------
-    int max_rounds = 0;
-    while ((1LL << max_rounds) < n) ++max_rounds;
-    ++max_rounds;
-    if (any_changed) {
-      for (int round = 0; round < max_rounds; ++round) {
-        if (tid == 0) {
-          c->active[(round + 1) % 3] = 0;
-          c->rounds = round + 1;
-        }
-        int jumping = 0;
-        for (long long v = tid; v < n; v += threads) {
-          const int a = ld_cg(&p.ancestor[v]);
-          if (a < 0 || ld_cg(&p.flag[v])) continue;
-          if (ld_cg(&p.flag[a])) {
-            p.flag[v] = 1;
-            continue;
+    if (!p.walk) {
+      // ---- subtree invalidation by pointer jumping (fused.cuh:199-234) ------------------------
+      int max_rounds = 0;
+      while ((1LL << max_rounds) < n) ++max_rounds;
+      ++max_rounds;
+      if (any_changed) {
+        for (int round = 0; round < max_rounds; ++round) {
+          if (tid == 0) {
+            c->active[(round + 1) % 3] = 0;
+            c->rounds = round + 1;
           }
-          const int next = ld_cg(&p.ancestor[a]);
-          p.ancestor[v] = next;
-          jumping |= next >= 0 ? 1 : 0;
+          int jumping = 0;
+          for (long long v = tid; v < n; v += threads) {
+            ++w_visits;
+            const int a = ld_cg(&p.ancestor[v]);
+            if (a < 0 || ld_cg(&p.flag[v])) continue;
+            ++w_jumps;
+            if (ld_cg(&p.flag[a])) {
+              p.flag[v] = 1;
+              continue;
+            }
+            const int next = ld_cg(&p.ancestor[a]);
+            p.ancestor[v] = next;
+            jumping |= next >= 0 ? 1 : 0;
+          }
+          if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
+          if (!grid_barrier(c, bar)) return;
+          if (ld_cg(&c->active[round % 3]) == 0) break;
         }
-        if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
+      }
+      if (tid == 0) c->phase_ns[2] = global_ns();
+      // ---- invalidate the flagged vertices ------------------------------------------------------
+      if (any_changed) {
+        for (long long v = tid; v < n; v += threads) {
+          if (ld_cg(&p.flag[v])) {
+            p.flag[v] = 0;
+            p.stamp[v] = gen_inv;
+            invalidate(p, static_cast<int>(v));
+            ++w_inval;
+          }
+        }
+      }
+    } else {
+      // ---- subtree invalidation by a walk down the old tree's edges, level by level ---------
+      X.gen = gen_inv;
+      int level = 0;
+      while (true) {
+        const int cs = level % 3;
+        const int nc = ld_cg(&c->walk_cnt[cs]);
+        const u64 hc = ld_cg(&c->walk_heavy[cs]);
+        if (nc == 0 && (hc >> 40) == 0) break;
+        if (level > n + 1) {
+          if (tid == 0) atomicOr(&c->error, kErrNotConverged);
+          break;
+        }
+        X.next = (level & 1) ? p.near_a : p.near_b;
+        X.next_cnt = &c->walk_cnt[(level + 1) % 3];
+        X.next_heavy = (level & 1) ? p.heavy_a : p.heavy_b;
+        X.next_heavy_cnt = &c->walk_heavy[(level + 1) % 3];
+        if (tid == 0) {
+          c->walk_cnt[(level + 2) % 3] = 0;
+          c->walk_heavy[(level + 2) % 3] = 0;
+        }
+        expand<kWalk>(p, X, (level & 1) ? p.near_b : p.near_a, nc,
+                      (level & 1) ? p.heavy_b : p.heavy_a, hc, gwarp, nwarps);
         if (!grid_barrier(c, bar)) return;
-        if (ld_cg(&c->active[round % 3]) == 0) break;
+        ++level;
+      }
+      w_inval += X.appends;
+      X.appends = 0;
+      if (tid == 0) {
+        c->levels = level;
+        c->phase_ns[2] = global_ns();
       }
     }
-    // ---- invalidate; candidates = invalidated + insertion heads -------------------------------
-    ++gen;
-    long long invalidated = 0;
-    for (long long v = tid; v < n; v += threads) {
-      if (ld_cg(&p.flag[v])) {
-        p.flag[v] = 0;
-        p.packed[v] = kPackedInf;
-        p.stamp[v] = gen;
-        touch(p, static_cast<int>(v));
-        p.candidates[append_slot(&c->list_count)] = static_cast<int>(v);
-        ++invalidated;
-      }
-    }
-    warp_sum_into_ll(invalidated, &c->invalidated);
     if (!grid_barrier(c, bar)) return;
+    if (tid == 0) c->phase_ns[3] = global_ns();
+    // ---- insertion heads: pulled, or (canonical trees) offered the inserted edge ----------------
     for (long long i = tid; i < pairs; i += threads) {
       const int slot = p.pair_list[i];
-      if (!(p.pair_flags[slot] & 4)) continue;
-      const int32_t v = static_cast<int32_t>(p.pair_key[slot] & 0xffffffffu);
-      if (v != p.source && claim(p.stamp, v, gen))
-        p.candidates[append_slot(&c->list_count)] = v;
+      const int f = p.pair_flags[slot];
+      if (!(f & kPairHead)) continue;
+      const u64 key = p.pair_key[slot];
+      const int32_t v = static_cast<int32_t>(key & 0xffffffffu);
+      if (v == p.source) continue;
+      if (!p.offer_heads) {
+        if (claim(p.stamp, v, gen_inv)) add_candidate(p, v);
+        continue;
+      }
+      if (!(f & (kPairAppend | kPairUpsert))) continue;       // no new weight on (u,v)
+      if (ld_cg(&p.stamp[v]) == gen_inv) continue;              // invalidated: pulled anyway
+      const int32_t u = static_cast<int32_t>(key >> 32);
+      const u64 word = ld_cg(&p.packed[u]);
+      if (word == kPackedInf) continue;
+      const int ins = (f & kPairUseFirst) ? p.pair_first[slot] : p.pair_last[slot];
+      const u64 nd = pk.dist(word) + static_cast<u64>(p.ins_w[static_cast<long long>(ins) * p.k +
+                                                              p.objective]);
+      if (nd > X.maxd) continue;
+      const u64 cand = pk.pack(nd, u);
+      if (cand >= ld_cg(&p.packed[v])) continue;
+      const u64 old = atomicMin(&p.packed[v], cand);
+      if (cand < old) touch(p, v);
+      if (nd < pk.dist(old) && claim(p.stamp, v, gen_pull))
+        p.frontier[append_slot(&c->frontier_count)] = v;
     }
+    warp_sum_into_ll(w_inval, &c->invalidated);
     if (!grid_barrier(c, bar)) return;
-    // ---- pull pass (fused.cuh:258-285) over the in-rows ------------------------------------
-    ++gen;
-    const int candidate_count = ld_cg(&c->list_count);
-    const int32_t* in_w = p.g.in_w + static_cast<long long>(p.objective) * p.g.arena_cap;
-    for (long long i = tid; i < candidate_count; i += threads) {
-      const int v = ld_cg(&p.candidates[i]);
-      const u64 current = ld_cg(&p.packed[v]);
-      u64 best = current;
-      const RowDesc desc = p.g.in_desc[v];
-      for (int e = 0; e < desc.len; ++e) {
-        const int u = p.g.in_col[desc.start + e];
-        if (u < 0) continue;
-        const u64 word = ld_cg(&p.packed[u]);
-        if (word == kPackedInf) continue;
-        const u64 nd = pk.dist(word) + static_cast<u64>(in_w[desc.start + e]);
-        if (nd <= maxd) best = min(best, pk.pack(nd, u));
-      }
-      if (best < current) {
-        const u64 old = atomicMin(&p.packed[v], best);
-        if (best < old) touch(p, v);
-        if (pk.dist(best) < pk.dist(old) && claim(p.stamp, v, gen))
-          p.frontier[append_slot(&c->frontier_count)] = v;
-      }
+    if (tid == 0) c->phase_ns[4] = global_ns();
+    // ---- pull pass (fused.cuh:258-285): every candidate takes its best in-neighbour ----------
+    {
+      Ctx Y = X;
+      Y.gen = gen_pull;
+      Y.next = p.frontier;
+      Y.next_cnt = &c->frontier_count;
+      Y.slots = Y.words = Y.atomics = Y.appends = Y.rows = 0;
+      expand<kPull>(p, Y, p.candidates, ld_cg(&c->cand_count), p.pull_heavy,
+                    ld_cg(&c->pull_heavy), gwarp, nwarps);
+      pull_slots = Y.slots;
+      pull_words = Y.words;
+      pull_rows = Y.rows;
+      X.atomics += Y.atomics;
     }
     if (!grid_barrier(c, bar)) return;
     frontier_count = ld_cg(&c->frontier_count);
   }
+  if (tid == 0) c->phase_ns[5] = global_ns();
 
   // ---- near-far propagation (fused.cuh:288-417) ------------------------------------------------
   u64 local = kPackedInf;
@@ -361,22 +603,21 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
   warp_min_into(local, &c->minimum);
   if (!grid_barrier(c, bar)) return;
   const u64 smallest = ld_cg(reinterpret_cast<const u64*>(&c->minimum));
-  Loop L;
-  L.threshold = (smallest == kPackedInf ? 0 : smallest) + delta;
-  int* cur = p.near_a;
-  int* nxt = p.near_b;
-  int2* cur_h = p.heavy_a;
-  int2* nxt_h = p.heavy_b;
+  X.threshold = (smallest == kPackedInf ? 0 : smallest) + delta;
+  int* lists[2] = {p.near_a, p.near_b};
+  int2* hlists[2] = {p.heavy_a, p.heavy_b};
   int* far = p.far_a;
   int* far2 = p.far_b;
+  X.far_cnt = &c->far_count;
   ++gen;
-  L.gen = gen;
   for (long long i = tid; i < frontier_count; i += threads) {
     const int v = ld_cg(&p.frontier[i]);
     const u64 word = ld_cg(&p.packed[v]);
     const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
-    if (d < L.threshold) {
-      if (claim(p.stamp, v, gen)) push_near(p, v, cur, &c->near_count, cur_h, &p.heavy_counter[0]);
+    if (d < X.threshold) {
+      if (claim(p.stamp, v, gen))
+        list_append(v, p.g.out_desc[v].len, p.heavy_degree, lists[0], &c->near_cnt[0], hlists[0],
+                    &c->heavy_cnt[0]);
     } else if (atomicExch(&p.in_far[v], 1) == 0) {
       far[append_slot(&c->far_count)] = v;
     }
@@ -384,81 +625,33 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
   if (!grid_barrier(c, bar)) return;
   if (tid == 0) c->minimum = kPackedInf;
   if (!grid_barrier(c, bar)) return;
-  int iterations = 0, epochs = 0;
+  int iterations = 0, epochs = 0, it = 0;
   long long pushes = 0;
   const long long iteration_cap = 4 * n + 64;
   while (true) {
-    const int near_count = ld_cg(&c->near_count);
-    const u64 hc = ld_cg(&p.heavy_counter[0]);
-    const int heavy_count = static_cast<int>(hc >> 40);
-    const long long heavy_chunks = static_cast<long long>(hc & ((1ULL << 40) - 1));
-    if (near_count > 0 || heavy_count > 0) {
-      ++gen;
+    const int cs = it % 3;
+    const int nc = ld_cg(&c->near_cnt[cs]);
+    const u64 hc = ld_cg(&c->heavy_cnt[cs]);
+    if (nc > 0 || (hc >> 40) > 0) {
       ++iterations;
       if (iterations > iteration_cap) {
         if (tid == 0) atomicOr(&c->error, kErrNotConverged);
         break;
       }
-      L.gen = gen;
-      pushes += near_count + heavy_count;
-      // light rows: 32 frontier entries per warp
-      for (long long base = gwarp * 32; base < near_count; base += nwarps * 32) {
-        const long long i = base + lane;
-        int u = -1;
-        u64 du = 0;
-        RowDesc desc{0, 0};
-        if (i < near_count) {
-          u = ld_cg(&cur[i]);
-          const u64 word = ld_cg(&p.packed[u]);
-          if (word != kPackedInf) {
-            du = pk.dist(word);
-            desc = p.g.out_desc[u];
-          }
-        }
-        unsigned big = __ballot_sync(0xffffffffu, desc.len >= 32);
-        while (big) {
-          const int leader = __ffs(big) - 1;
-          big &= big - 1;
-          const int U = __shfl_sync(0xffffffffu, u, leader);
-          const u64 DU = __shfl_sync(0xffffffffu, du, leader);
-          const unsigned S = __shfl_sync(0xffffffffu, desc.start, leader);
-          const int LEN = __shfl_sync(0xffffffffu, desc.len, leader);
-          warp_row(p, pk, maxd, U, DU, S, 0, LEN, L, nxt, nxt_h, far);
-        }
-        if (desc.len > 0 && desc.len < 32) {
-          const int32_t* col = p.g.out_col + desc.start;
-          const int32_t* wt =
-              p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap + desc.start;
-          for (int e = 0; e < desc.len; ++e)
-            relax_edge(p, pk, maxd, u, du, col[e], wt[e], L, nxt, nxt_h, far);
-        }
-      }
-      // heavy rows: 1024-slot chunks spread over all warps
-      for (long long ch = gwarp; ch < heavy_chunks; ch += nwarps) {
-        const int h = find_heavy(cur_h, heavy_count, ch);
-        const int2 entry = make_int2(__ldcg(&cur_h[h].x), __ldcg(&cur_h[h].y));
-        const int u = entry.x;
-        const u64 word = ld_cg(&p.packed[u]);
-        if (word == kPackedInf) continue;
-        const RowDesc desc = p.g.out_desc[u];
-        const int e0 = static_cast<int>(ch - entry.y) * kHeavyChunk;
-        const int e1 = min(desc.len, e0 + kHeavyChunk);
-        warp_row(p, pk, maxd, u, pk.dist(word), desc.start, e0, e1, L, nxt, nxt_h, far);
-      }
-      if (!grid_barrier(c, bar)) return;
+      pushes += nc + static_cast<long long>(hc >> 40);
+      X.gen = ++gen;
+      X.next = lists[(it + 1) & 1];
+      X.next_cnt = &c->near_cnt[(it + 1) % 3];
+      X.next_heavy = hlists[(it + 1) & 1];
+      X.next_heavy_cnt = &c->heavy_cnt[(it + 1) % 3];
+      X.far = far;
       if (tid == 0) {
-        c->near_count = ld_cg(&c->next_count);
-        c->next_count = 0;
-        p.heavy_counter[0] = ld_cg(&p.heavy_counter[1]);
-        p.heavy_counter[1] = 0;
+        c->near_cnt[(it + 2) % 3] = 0;
+        c->heavy_cnt[(it + 2) % 3] = 0;
       }
+      expand<kPush>(p, X, lists[it & 1], nc, hlists[it & 1], hc, gwarp, nwarps);
       if (!grid_barrier(c, bar)) return;
-      int* t = cur;
-      cur = nxt;
-      nxt = t;
-      int2* th = cur_h;
-      cur_h = nxt_h;
-      nxt_h = th;
+      ++it;
       continue;
     }
     // near frontier empty: raise the threshold past the far pile
@@ -472,16 +665,17 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     }
     warp_min_into(local, &c->minimum);
     if (!grid_barrier(c, bar)) return;
-    L.threshold = max(L.threshold, ld_cg(reinterpret_cast<const u64*>(&c->minimum))) + delta;
+    X.threshold = max(X.threshold, ld_cg(reinterpret_cast<const u64*>(&c->minimum))) + delta;
     ++gen;
     for (long long i = tid; i < far_count; i += threads) {
       const int v = ld_cg(&far[i]);
       const u64 word = ld_cg(&p.packed[v]);
       const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
-      if (d < L.threshold) {
+      if (d < X.threshold) {
         p.in_far[v] = 0;
         if (claim(p.stamp, v, gen))
-          push_near(p, v, cur, &c->near_count, cur_h, &p.heavy_counter[0]);
+          list_append(v, p.g.out_desc[v].len, p.heavy_degree, lists[it & 1], &c->near_cnt[cs],
+                      hlists[it & 1], &c->heavy_cnt[cs]);
       } else {
         far2[append_slot(&c->far2_count)] = v;
       }
@@ -497,6 +691,7 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     far = far2;
     far2 = t;
   }
+  if (tid == 0) c->phase_ns[6] = global_ns();
 
   // ---- commit: unpack (fused.cuh:419-494) ------------------------------------------------------
   long long affected = 0;
@@ -511,6 +706,7 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
       const int touched = ld_cg(&c->touched_count);
       for (long long i = tid; i < touched; i += threads) {
         const int v = ld_cg(&p.touched[i]);
+        ++unpacked;
         const u64 word = ld_cg(&p.packed[v]);
         const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word));
         const int32_t par = word == kPackedInf ? -1 : pk.parent(word);
@@ -553,7 +749,20 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     }
   }
   warp_sum_into_ll(affected, &c->affected);
+  warp_sum_into_ll(w_visits, &c->work[0]);
+  warp_sum_into_ll(w_jumps, &c->work[1]);
+  warp_sum_into_ll(static_cast<long long>(pull_rows), &c->work[3]);
+  warp_sum_into_ll(static_cast<long long>(pull_slots), &c->work[4]);
+  warp_sum_into_ll(static_cast<long long>(pull_words), &c->work[5]);
+  warp_sum_into_ll(static_cast<long long>(X.rows), &c->work[6]);
+  warp_sum_into_ll(static_cast<long long>(X.slots), &c->work[7]);
+  warp_sum_into_ll(static_cast<long long>(X.words), &c->work[8]);
+  warp_sum_into_ll(static_cast<long long>(X.atomics), &c->work[9]);
+  warp_sum_into_ll(static_cast<long long>(X.appends), &c->work[10]);
+  warp_sum_into_ll(static_cast<long long>(unpacked), &c->work[11]);
   if (tid == 0) {
+    c->work[2] = 0;  // invalidated vertices: reported in c->invalidated
+    c->phase_ns[7] = global_ns();
     c->iterations = iterations;
     c->epochs = epochs;
     c->pushes = pushes;
@@ -639,9 +848,9 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
   p.far_b = ws.far_b.ptr;
   p.heavy_a = reinterpret_cast<int2*>(ws.heavy_a.ptr);
   p.heavy_b = reinterpret_cast<int2*>(ws.heavy_b.ptr);
+  p.pull_heavy = reinterpret_cast<int2*>(ws.pull_heavy.ptr);
   p.touched = ws.touched.ptr;
   p.ctl = ws.ctl.ptr;
-  p.heavy_counter = ws.ctl.ptr->heavy_counter;
   return p;
 }
 
@@ -746,6 +955,12 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     p.pair_key = ws.pair_key.ptr;
     p.pair_list = ws.pair_list.ptr;
     p.pair_flags = ws.pair_flags.ptr;
+    p.pair_first = ws.pair_first.ptr;
+    p.pair_last = ws.pair_last.ptr;
+    p.ins_w = b.ins_w;
+    p.k = g.k;
+    p.walk = (sched.invalidation == 1 && t.trusted) ? 1 : 0;
+    p.offer_heads = t.canonical ? 1 : 0;
     p.generation = ws.next_generation(1, s);
     p.touch_gen = p.generation;
     p.heavy_degree = sched.heavy_degree > 0 ? sched.heavy_degree : 2048;
@@ -831,11 +1046,16 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     st->delta = sched.delta > 0 ? sched.delta : r.delta;
     st->max_weight = r.max_w;
     st->grid_blocks = blocks;
-    st->invalidation = 0;
+    st->invalidation = (sched.invalidation == 1 && t.trusted) ? 1 : 0;
     st->apply_ms = apply_ms;
     st->sssp_ms = sssp_ms;
     st->rounds = r.rounds;
     st->touched = r.touched_count;
+    for (int i = 0; i < 12; ++i) st->work[i] = r.work[i];
+    for (int i = 0; i < 7; ++i)
+      st->phase_ms[i] = r.phase_ns[i + 1] > r.phase_ns[i]
+                            ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)
+                            : 0.0f;
   }
 }
 

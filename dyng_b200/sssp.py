@@ -73,6 +73,19 @@ class Stats:
     sssp_ms: float = 0.0
     rounds: int = 0
     touched: int = 0
+    work: tuple = ()
+    phase_ms: tuple = ()
+
+    WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
+                  "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
+                  "unpacked")
+    # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows):
+    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32)
+    PHASES = ("roots", "pointer_jumping", "invalidate", "pull", "split", "near_far", "unpack")
+
+    @property
+    def algorithmic_bytes(self) -> int:
+        return int(sum(a * b for a, b in zip(self.work, self.WORK_BYTES)))
 
     @classmethod
     def _from_native(cls, s: N.Stats) -> "Stats":
@@ -80,7 +93,8 @@ class Stats:
         return cls(ApplySummary._from_native(s.batch), s.invalidated, s.affected, s.iterations,
                    s.epochs, s.pushes, bool(s.packed_parents), engines.get(s.engine_used, "fused"),
                    s.delta, s.max_weight, s.grid_blocks, s.invalidation, float(s.apply_ms),
-                   float(s.sssp_ms), s.rounds, s.touched)
+                   float(s.sssp_ms), s.rounds, s.touched, tuple(int(x) for x in s.work),
+                   tuple(float(x) for x in s.phase_ms))
 
 
 class Result:

@@ -111,6 +111,14 @@ typedef struct dyngb200_stats {
   float sssp_ms;       /* device time of the sssp kernel */
   int64_t rounds;      /* pointer-jumping rounds */
   int64_t touched;     /* vertices whose packed word was written */
+  /* Work of the sssp kernel, for its algorithmic traffic: [0] vertex visits of the pointer-jumping
+   * rounds, [1] jumps, [2] invalidated, [3] pull candidates, [4] pulled in-slots, [5] word reads of
+   * the pull, [6] pushed vertices, [7] scanned out-slots, [8] target word reads, [9] successful
+   * atomicMin, [10] frontier appends, [11] unpacked vertices. */
+  int64_t work[12];
+  /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
+   * first split, near-far loop, unpack. */
+  float phase_ms[7];
 } dyngb200_stats;
 
 /* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */
