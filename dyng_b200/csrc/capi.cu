@@ -414,7 +414,7 @@ dyngb200_status dyngb200_graph_device_bytes(dyngb200_graph g, int64_t* bytes) {
     expects(g && bytes, "graph_device_bytes: null argument");
     const Graph& x = g->g;
     const long long k = x.k;
-    *bytes = 2 * (x.n_cap * (8 + 4 + 4) + x.arena_cap * (4 + 4 * k));
+    *bytes = 2 * (x.n_cap * (8 + 4 + 4) + x.arena_cap * (4 + 4 * k)) + 16 * x.ecap;
   });
 }
 

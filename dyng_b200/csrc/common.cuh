@@ -47,6 +47,7 @@ struct GraphCounters {
   u64 out_top, in_top;  // arena allocation tops (entries)
   u64 out_garbage, in_garbage;  // entries abandoned by relocated rows
   long long dead_out, dead_in;  // tombstones still stored
+  long long idx_live, idx_dead; // edge index: live keys and deleted markers
 };
 
 // The device view of one slack-row graph (out-rows plus the in-edge mirror).
@@ -68,7 +69,16 @@ struct GraphView {
   int allow_multi;  // multi_edges::allow
   GraphCounters* counters;
   ColumnStats* columns;  // k entries
+  // Edge index (simple graphs): open addressing on (u << 32 | v) -> absolute slot of the edge in
+  // the out arena and in the in arena.  emask + 1 entries; empty keys ~0, deleted ~0 - 1.
+  unsigned long long* ekey;
+  unsigned* eout;
+  unsigned* ein;
+  long long emask;
 };
+
+constexpr unsigned long long kKeyEmpty = ~0ULL;
+constexpr unsigned long long kKeyDeleted = ~0ULL - 1;
 
 __host__ __device__ inline int parent_bits_for(long long n) {
   int bits = 1;
@@ -126,6 +136,50 @@ __host__ __device__ inline bool distances_fit(long long n, long long max_w) {
 }
 
 #ifdef __CUDACC__
+__device__ __forceinline__ u64 mix64(u64 x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdULL;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ULL;
+  x ^= x >> 33;
+  return x;
+}
+
+__device__ __forceinline__ u64 edge_key(int32_t u, int32_t v) {
+  return (static_cast<u64>(static_cast<uint32_t>(u)) << 32) | static_cast<uint32_t>(v);
+}
+
+// Slot of a live key in the edge index, or -1.
+__device__ __forceinline__ long long index_find(const GraphView& g, u64 key) {
+  long long h = static_cast<long long>(mix64(key) & static_cast<u64>(g.emask));
+  for (long long probe = 0; probe <= g.emask; ++probe) {
+    const u64 cur = g.ekey[h];
+    if (cur == key) return h;
+    if (cur == kKeyEmpty) return -1;
+    h = (h + 1) & g.emask;
+  }
+  return -1;
+}
+
+// Claim a slot for a key that is not in the index (an empty or deleted slot); -1 if full.
+// *reused tells whether a deleted marker was replaced.
+__device__ __forceinline__ long long index_insert(const GraphView& g, u64 key, bool* reused) {
+  long long h = static_cast<long long>(mix64(key) & static_cast<u64>(g.emask));
+  for (long long probe = 0; probe <= g.emask; ++probe) {
+    u64 cur = g.ekey[h];
+    while (cur == kKeyEmpty || cur == kKeyDeleted) {
+      const u64 prev = atomicCAS(&g.ekey[h], cur, key);
+      if (prev == cur) {
+        *reused = cur == kKeyDeleted;
+        return h;
+      }
+      cur = prev;
+    }
+    h = (h + 1) & g.emask;
+  }
+  return -1;
+}
+
 __device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ u64 ld_cg(const u64* p) { return __ldcg(p); }
 __device__ __forceinline__ long long ld_cg(const long long* p) { return __ldcg(p); }

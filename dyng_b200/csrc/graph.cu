@@ -29,17 +29,7 @@ namespace dyngb200 {
 namespace {
 
 constexpr u64 kEmptyKey = ~0ULL;
-constexpr int kChunk = 2048;  // row entries scanned by one warp-sized work item
 constexpr int kBlock = 256;
-
-__device__ __forceinline__ u64 mix64(u64 x) {
-  x ^= x >> 33;
-  x *= 0xff51afd7ed558ccdULL;
-  x ^= x >> 33;
-  x *= 0xc4ceb9fe1a85ec53ULL;
-  x ^= x >> 33;
-  return x;
-}
 
 __device__ __forceinline__ u64 pair_key(int32_t u, int32_t v) {
   return (static_cast<u64>(static_cast<uint32_t>(u)) << 32) | static_cast<uint32_t>(v);
@@ -96,9 +86,6 @@ struct ApplyParams {
   int* new_cap_in;
   int* live_out;
   int* live_in;
-  int2* chunks_out;
-  int2* chunks_in;
-  long long chunk_cap;
   // column statistics deltas (k entries each)
   long long* col_sum_delta;
   long long* col_removed_at_max;
@@ -221,14 +208,6 @@ __device__ void touch_row(const ApplyParams& p, int side, int32_t r) {
   (side == 0 ? p.row_slot_out : p.row_slot_in)[r] = slot;
   (side == 0 ? p.dels_out : p.dels_in)[slot] = 0;
   (side == 0 ? p.apps_out : p.apps_in)[slot] = 0;
-  const int len = r < c->n_old ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r].len : 0;
-  if (len > 0 && !p.g.allow_multi) {
-    const int chunks = (len + kChunk - 1) / kChunk;
-    const int base = atomicAdd(side == 0 ? &c->chunks_out : &c->chunks_in, chunks);
-    int2* list = side == 0 ? p.chunks_out : p.chunks_in;
-    for (int i = 0; i < chunks && base + i < p.chunk_cap; ++i) list[base + i] = make_int2(r, i);
-    if (base + chunks > p.chunk_cap) set_error(&c->error, kErrInternal);
-  }
 }
 
 __device__ void add_op(const ApplyParams& p, int32_t u, int32_t v, int kind, int index) {
@@ -304,38 +283,22 @@ __global__ void k_pairs(ApplyParams p) {
               static_cast<unsigned long long>(missing));
 }
 
-// ---- D: match existing slots (simple graphs: at most one slot per pair) -------------------------
-// One warp per chunk of kChunk slots; each live slot probes the pair table.
-__global__ void k_scan(ApplyParams p) {
+// ---- D: match existing slots (simple graphs: at most one slot per pair, found in the edge
+// index; positions are absolute arena slots) ------------------------------------------------------
+__global__ void k_match(ApplyParams p) {
   UpdateCtl* c = p.ctl;
   if (c->error) return;
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const int n_out = min(static_cast<long long>(c->chunks_out), p.chunk_cap);
-  const int n_in = min(static_cast<long long>(c->chunks_in), p.chunk_cap);
-  for (int item = warp; item < n_out + n_in; item += warps) {
-    const int side = item < n_out ? 0 : 1;
-    const int2 ch = side == 0 ? p.chunks_out[item] : p.chunks_in[item - n_out];
-    const int32_t r = ch.x;
-    const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
-    const int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
-    const int begin = ch.y * kChunk;
-    const int end = min(desc.len, begin + kChunk);
-    for (int e = begin + lane; e < end; e += 32) {
-      const int32_t x = col[desc.start + e];
-      if (x < 0) continue;
-      const int slot = find_pair(p, side == 0 ? pair_key(r, x) : pair_key(x, r));
-      if (slot >= 0) {
-        if (side == 0) {
-          p.out_pos[slot] = e;
-          atomicAdd(&p.out_count[slot], 1);
-        } else {
-          p.in_pos[slot] = e;
-          atomicAdd(&p.in_count[slot], 1);
-        }
-      }
+  const int pairs = c->pairs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+    const int slot = p.list[i];
+    const long long e = index_find(p.g, p.key[slot]);
+    if (e >= 0) {
+      p.out_pos[slot] = static_cast<int>(p.g.eout[e]);
+      p.in_pos[slot] = static_cast<int>(p.g.ein[e]);
+      p.out_count[slot] = 1;
+      p.in_count[slot] = 1;
     }
+    p.in_pos2[slot] = static_cast<int>(e);  // index slot of the pair (or -1)
   }
 }
 
@@ -357,12 +320,12 @@ __global__ void k_scan_multi(ApplyParams p) {
       if (r >= c->n_old) continue;
       const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
       const int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
-      // first match, and match number d (the first survivor of the deletions)
+      // first match, and match number d (the first survivor of the deletions); absolute slots
       int count = 0, first = -1, target = -1;
       for (int e = 0; e < desc.len; ++e) {
         if (col[e] != want) continue;
-        if (count == 0) first = e;
-        if (count == d) target = e;
+        if (count == 0) first = static_cast<int>(desc.start) + e;
+        if (count == d) target = static_cast<int>(desc.start) + e;
         ++count;
       }
       (void)t;
@@ -445,7 +408,6 @@ __global__ void k_resolve(ApplyParams p) {
     const int final_idx = removed;  // S[removed] is the first (u,v) after the batch
     const bool final_exists = final_idx < seq;
     const bool orig_exists = cnt >= 1 && u < c->n_old;
-    const int out_base = orig_exists ? static_cast<int>(p.g.out_desc[u].start) : 0;
     // storage position of S[final_idx] when it is an original slot (final_idx is 0 or d)
     int final_pos = -1;
     if (final_exists && final_idx < cnt) {
@@ -454,12 +416,12 @@ __global__ void k_resolve(ApplyParams p) {
     for (int j = 0; j < p.k; ++j) {
       unsigned char inc = 0;
       if (orig_exists && final_exists) {
-        const long long w0 = p.g.out_w[j * p.g.arena_cap + out_base + p.out_pos[slot]];
+        const long long w0 = p.g.out_w[j * p.g.arena_cap + p.out_pos[slot]];
         long long wf;
         if (final_idx == target && writes_weights) {
           wf = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
         } else {
-          wf = p.g.out_w[j * p.g.arena_cap + out_base + final_pos];
+          wf = p.g.out_w[j * p.g.arena_cap + final_pos];
         }
         inc = wf > w0 ? 1 : 0;
       }
@@ -563,13 +525,11 @@ __global__ void k_mutate(ApplyParams p) {
     const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
     if (!tomb && !(flags & kPairUpsert)) continue;
     const int target = del_first ? d : 0;  // the original match an upsert addresses
-    for (int side = 0; side < 2; ++side) {
-      const int32_t r = side == 0 ? u : v;
-      const int32_t want = side == 0 ? v : u;
-      const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
-      int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
-      int32_t* w = (side == 0 ? p.g.out_w : p.g.in_w) + desc.start;
-      if (cnt <= 1 && !p.g.allow_multi) {
+    if (!p.g.allow_multi) {
+      // simple graphs: the single matching slot, absolute positions from the edge index
+      for (int side = 0; side < 2; ++side) {
+        int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
+        int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
         const int pos = side == 0 ? p.out_pos[slot] : p.in_pos[slot];
         if (tomb) {
           col[pos] = kDead;
@@ -586,8 +546,22 @@ __global__ void k_mutate(ApplyParams p) {
             w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
           }
         }
-        continue;
       }
+      if (tomb && !(flags & kPairAppend)) {
+        // the edge is gone: its index key becomes a deleted marker
+        p.g.ekey[p.in_pos2[slot]] = kKeyDeleted;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_live),
+                  static_cast<unsigned long long>(-1LL));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_dead), 1ULL);
+      }
+      continue;
+    }
+    for (int side = 0; side < 2; ++side) {
+      const int32_t r = side == 0 ? u : v;
+      const int32_t want = side == 0 ? v : u;
+      const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
+      int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
+      int32_t* w = (side == 0 ? p.g.out_w : p.g.in_w) + desc.start;
       // multi-edge graphs: walk the row in order
       int seen = 0;
       for (int e = 0; e < desc.len && seen < cnt; ++e) {
@@ -642,6 +616,11 @@ __global__ void k_move(ApplyParams p) {
         col[dst + pos] = x;
         for (int j = 0; j < p.k; ++j)
           w[j * p.g.arena_cap + dst + pos] = w[j * p.g.arena_cap + desc.start + e];
+        if (!p.g.allow_multi) {
+          const long long ie = index_find(p.g, side == 0 ? edge_key(r, x) : edge_key(x, r));
+          if (ie >= 0) (side == 0 ? p.g.eout : p.g.ein)[ie] = dst + pos;
+          else set_error(&c->error, kErrInternal);
+        }
       }
       written += __popc(ballot);
     }
@@ -660,6 +639,7 @@ __global__ void k_append(ApplyParams p) {
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
     const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
+    unsigned placed[2] = {0, 0};
     for (int side = 0; side < 2; ++side) {
       const int32_t r = side == 0 ? u : v;
       const int s = (side == 0 ? p.row_slot_out : p.row_slot_in)[r];
@@ -669,6 +649,7 @@ __global__ void k_append(ApplyParams p) {
                                         (side == 0 ? p.live_out : p.live_in)[s]
                                   : desc.start + desc.len;
       const unsigned pos = base + (side == 0 ? p.out_rank : p.in_rank)[slot];
+      placed[side] = pos;
       (side == 0 ? p.g.out_col : p.g.in_col)[pos] = side == 0 ? v : u;
       int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
       for (int j = 0; j < p.k; ++j) {
@@ -676,6 +657,24 @@ __global__ void k_append(ApplyParams p) {
         w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
         if (side == 0) column_in(p, j, nw);
       }
+    }
+    if (!p.g.allow_multi) {
+      // the edge index follows the new slots (an edge deleted and re-inserted keeps its key)
+      long long ie = index_find(p.g, key);
+      if (ie < 0) {
+        bool reused = false;
+        ie = index_insert(p.g, key, &reused);
+        if (ie < 0) {
+          set_error(&c->error, kErrInternal);
+          continue;
+        }
+        atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_live), 1ULL);
+        if (reused)
+          atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_dead),
+                    static_cast<unsigned long long>(-1LL));
+      }
+      p.g.eout[ie] = placed[0];
+      p.g.ein[ie] = placed[1];
     }
   }
 }
@@ -893,6 +892,53 @@ __global__ void k_insert_flags(ApplyParams p, unsigned char* out) {
   }
 }
 
+// Edge index construction: every live out-slot (u, x) inserts its key with the out position,
+// then every live in-slot (v, y) records the in position of key (y, v).
+__global__ void k_index_clear(GraphView g) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i <= g.emask;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    g.ekey[i] = kKeyEmpty;
+}
+
+__global__ void k_index_out(GraphView g, long long n, unsigned* error) {
+  long long live = 0;
+  for (long long u = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; u < n;
+       u += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const RowDesc d = g.out_desc[u];
+    for (int e = 0; e < d.len; ++e) {
+      const int32_t x = g.out_col[d.start + e];
+      if (x < 0) continue;
+      bool reused = false;
+      const long long ie = index_insert(g, edge_key(static_cast<int32_t>(u), x), &reused);
+      if (ie < 0) {
+        atomicOr(error, kErrCapacity);
+        return;
+      }
+      g.eout[ie] = d.start + e;
+      ++live;
+    }
+  }
+  if (live) atomicAdd(reinterpret_cast<unsigned long long*>(&g.counters->idx_live),
+                      static_cast<unsigned long long>(live));
+}
+
+__global__ void k_index_in(GraphView g, long long n, unsigned* error) {
+  for (long long v = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; v < n;
+       v += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const RowDesc d = g.in_desc[v];
+    for (int e = 0; e < d.len; ++e) {
+      const int32_t y = g.in_col[d.start + e];
+      if (y < 0) continue;
+      const long long ie = index_find(g, edge_key(y, static_cast<int32_t>(v)));
+      if (ie < 0) {
+        atomicOr(error, kErrInternal);
+        return;
+      }
+      g.ein[ie] = d.start + e;
+    }
+  }
+}
+
 int grid_for(long long work, int block, int sm_count) {
   long long g = (work + block - 1) / block;
   const long long cap = static_cast<long long>(sm_count) * 8;
@@ -961,9 +1007,6 @@ ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int object
   p.new_cap_in = ws.row_new_cap_in.ptr;
   p.live_out = ws.row_live_out.ptr;
   p.live_in = ws.row_live_in.ptr;
-  p.chunks_out = ws.chunks_out.ptr;
-  p.chunks_in = ws.chunks_in.ptr;
-  p.chunk_cap = static_cast<long long>(ws.chunks_out.count);
   p.col_sum_delta = ws.col_sum_delta.ptr;
   p.col_removed_at_max = ws.col_removed_at_max.ptr;
   p.col_written_max = ws.col_written_max.ptr;
@@ -1216,6 +1259,51 @@ void graph_build(Context& ctx, Graph& g, long long n, const int64_t* row_ptr, co
                                 cudaMemcpyHostToDevice, ctx.stream));
   DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
   g.host_counters = gc;
+  if (!g.props.allow_multi) graph_index_build(ctx, g, 0);
+}
+
+// (Re)build the edge index with room for `extra` more edges.
+void graph_index_build(Context& ctx, Graph& g, long long extra) {
+  cudaStream_t s = ctx.stream;
+  long long want = 1024;
+  while (want < 2 * (g.host_counters.m + extra) + 65536) want <<= 1;
+  if (want != g.ecap) {
+    g.ekey.release();
+    g.eout.release();
+    g.ein.release();
+    g.ekey.reserve(static_cast<size_t>(want));
+    g.eout.reserve(static_cast<size_t>(want));
+    g.ein.reserve(static_cast<size_t>(want));
+    g.ecap = want;
+  }
+  GraphCounters gc = g.host_counters;
+  gc.idx_live = 0;
+  gc.idx_dead = 0;
+  DYNGB200_CUDA(cudaMemcpyAsync(g.counters.ptr, &gc, sizeof(gc), cudaMemcpyHostToDevice, s));
+  Workspace& ws = ctx.ws;
+  ws.ctl.reserve(1, s);
+  DYNGB200_CUDA(cudaMemsetAsync(&ws.ctl.ptr->error, 0, sizeof(unsigned), s));
+  GraphView v = g.view();
+  const int grid = ctx.sm_count * 8;
+  k_index_clear<<<grid, kBlock, 0, s>>>(v);
+  k_index_out<<<grid, kBlock, 0, s>>>(v, gc.n, &ws.ctl.ptr->error);
+  k_index_in<<<grid, kBlock, 0, s>>>(v, gc.n, &ws.ctl.ptr->error);
+  DYNGB200_CUDA(cudaGetLastError());
+  unsigned err = 0;
+  DYNGB200_CUDA(cudaMemcpyAsync(&err, &ws.ctl.ptr->error, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(&g.host_counters, g.counters.ptr, sizeof(GraphCounters),
+                                cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+  expects(err == 0, "graph: the edge index could not be built (duplicate edges?)", DYNGB200_INTERNAL);
+}
+
+// Before a batch of `inserts` insertions: rebuild the index when deleted markers or the batch
+// would push it past 60% load.
+void graph_index_reserve(Context& ctx, Graph& g, long long inserts) {
+  if (g.props.allow_multi) return;
+  const GraphCounters& gc = g.host_counters;
+  if (static_cast<double>(gc.idx_live + gc.idx_dead + inserts) > 0.6 * static_cast<double>(g.ecap))
+    graph_index_build(ctx, g, inserts);
 }
 
 void graph_refresh_host(Context& ctx, Graph& g) {
@@ -1446,11 +1534,6 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
   const long long ops = (b.ni + b.nd) * dir;
   ws.reserve_vertices(g.n_cap, s);
   ws.reserve_batch(ops, g.k, s);
-  // chunk lists: every touched row's slots in kChunk pieces (bounded by arena / kChunk + rows)
-  const long long chunk_cap = std::min<long long>(
-      2 * ops + g.arena_cap / kChunk + 64, 2 * ws.pairs_sized + g.arena_cap / kChunk + 64);
-  ws.chunks_out.reserve(static_cast<size_t>(chunk_cap));
-  ws.chunks_in.reserve(static_cast<size_t>(chunk_cap));
   const int touch_gen = ws.next_touch_generation(s);
   const size_t cap = static_cast<size_t>(ws.pairs_sized);
   DYNGB200_CUDA(cudaMemsetAsync(ws.pair_key.ptr, 0xff, cap * sizeof(u64), s));
@@ -1474,16 +1557,14 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
                                 cudaMemcpyHostToDevice, s));
   ApplyParams p = make_params(ctx, g, b, objective, delta_opt);
   p.touch_gen = touch_gen;
-  p.chunk_cap = chunk_cap;
   const int grid_ops = grid_for(b.ni + b.nd, kBlock, ctx.sm_count);
   k_validate<<<grid_ops, kBlock, 0, s>>>(p);
   k_plan<<<1, 1, 0, s>>>(p);
   k_pairs<<<grid_ops, kBlock, 0, s>>>(p);
-  const int grid_wide = ctx.sm_count * 4;
   if (g.props.allow_multi) {
     k_scan_multi<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
   } else {
-    k_scan<<<grid_wide, kBlock, 0, s>>>(p);
+    k_match<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
   }
   k_resolve<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
   if (!g.props.sorted) {
@@ -1505,7 +1586,6 @@ void apply_commit(Context& ctx, Graph& g, const StagedBatch& b) {
   const long long dir = g.props.directed ? 1 : 2;
   const long long ops = (b.ni + b.nd) * dir;
   ApplyParams p = make_params(ctx, g, b, -1, 0);
-  p.chunk_cap = static_cast<long long>(ctx.ws.chunks_out.count);
   const int grid = grid_for(2 * ops, kBlock, ctx.sm_count);
   k_alloc<<<grid, kBlock, 0, s>>>(p);
   k_mutate<<<grid, kBlock, 0, s>>>(p);
@@ -1522,6 +1602,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
                  dyngb200_apply_summary* summary, unsigned char* weight_increased) {
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
+  graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
   const StagedBatch b = stage_batch(ctx, batch, g.k);
   UpdateCtl r{};
   DevBuf<unsigned char> flags;

@@ -149,7 +149,6 @@ struct Workspace {
   DevBuf<int> row_dels_out, row_dels_in, row_apps_out, row_apps_in, row_reloc_out, row_reloc_in;
   DevBuf<unsigned> row_new_start_out, row_new_start_in;
   DevBuf<int> row_new_cap_out, row_new_cap_in, row_live_out, row_live_in;
-  DevBuf<int2> chunks_out, chunks_in;
   DevBuf<int> row_seg_offsets, row_seg;  // append order: appended pairs per row
   DevBuf<long long> col_ins_max, col_sum_delta, col_removed_at_max, col_written_max,
       col_written_at_max;
@@ -199,6 +198,9 @@ struct Graph {
   DevBuf<int32_t> out_w, in_w;
   DevBuf<GraphCounters> counters;
   DevBuf<ColumnStats> columns;
+  DevBuf<u64> ekey;  // edge index (simple graphs)
+  DevBuf<unsigned> eout, ein;
+  long long ecap = 0;
   GraphCounters host_counters{};
   std::vector<ColumnStats> host_columns;
   int device = 0;
@@ -222,6 +224,10 @@ struct Graph {
     v.allow_multi = props.allow_multi;
     v.counters = counters.ptr;
     v.columns = columns.ptr;
+    v.ekey = ekey.ptr;
+    v.eout = eout.ptr;
+    v.ein = ein.ptr;
+    v.emask = ecap - 1;
     return v;
   }
 };
@@ -250,6 +256,8 @@ void graph_export(Context& ctx, Graph& g, int64_t* row_ptr, int32_t* col, int32_
 void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_arena_out,
                 long long need_arena_in);
 void graph_rescan_columns(Context& ctx, Graph& g);
+void graph_index_build(Context& ctx, Graph& g, long long extra);
+void graph_index_reserve(Context& ctx, Graph& g, long long inserts);
 void graph_refresh_host(Context& ctx, Graph& g);
 
 // Launches the batch applier (Step 0 checks, grouping, matching, resolution, allocation and the

@@ -935,6 +935,7 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
   cudaStream_t s = ctx.stream;
   const int objective = t.opt.objective;
   if (g.host_columns[objective].dirty) graph_rescan_columns(ctx, g);
+  graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
   const StagedBatch b = stage_batch(ctx, batch, g.k);
   const int blocks = persistent_blocks(ctx, sched);
   cudaEvent_t e0, e1, e2;

@@ -81,7 +81,7 @@ class Stats:
                   "unpacked")
     # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows):
     WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32)
-    PHASES = ("roots", "pointer_jumping", "invalidate", "pull", "split", "near_far", "unpack")
+    PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
 
     @property
     def algorithmic_bytes(self) -> int:
