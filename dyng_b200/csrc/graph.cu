@@ -35,6 +35,32 @@ __device__ __forceinline__ u64 pair_key(int32_t u, int32_t v) {
   return (static_cast<u64>(static_cast<uint32_t>(u)) << 32) | static_cast<uint32_t>(v);
 }
 
+// Warp-level sums and maxima folded into one atomic per warp (all 32 lanes must call).
+__device__ __forceinline__ void warp_add(long long v, long long* target) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0)
+    atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ void warp_add_u(unsigned long long v, unsigned long long* target) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(target, v);
+}
+__device__ __forceinline__ void warp_max(long long v, long long* target, long long floor_value) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v > floor_value) atomicMax(target, v);
+}
+
+// Per-thread column statistics deltas of the first kLocalColumns objectives (the rest go to the
+// global counters directly); flushed once per warp at the end of a kernel.
+constexpr int kLocalColumns = 4;
+struct ColumnAcc {
+  long long sum[kLocalColumns];
+  long long removed_at_max[kLocalColumns];
+  long long written_max[kLocalColumns];
+  long long written_at_max[kLocalColumns];
+  int bad[kLocalColumns];
+};
+
 struct ApplyParams {
   GraphView g;
   const int32_t* ins_src;
@@ -167,10 +193,9 @@ __global__ void k_validate(ApplyParams p) {
       }
     }
   }
-  if (top > 0) atomicMax(&c->n_after, top);
-  if (p.objective >= 0 && wmax > 1) atomicMax(&c->batch_ins_max, wmax);
-  if (dropped) atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[5]),
-                         static_cast<unsigned long long>(dropped));
+  warp_max(top, &c->n_after, 0);
+  if (p.objective >= 0) warp_max(wmax, &c->batch_ins_max, 1);
+  warp_add(dropped, &c->summary[5]);
 }
 
 // ---- B: the plan (one thread): capacity, packing bound, near-far width ------------------------
@@ -203,7 +228,7 @@ __device__ void touch_row(const ApplyParams& p, int side, int32_t r) {
   int* stamp = side == 0 ? p.touch_out_stamp : p.touch_in_stamp;
   if (atomicExch(&stamp[r], p.touch_gen) == p.touch_gen) return;
   UpdateCtl* c = p.ctl;
-  const int slot = atomicAdd(side == 0 ? &c->rows_out : &c->rows_in, 1);
+  const int slot = append_slot(side == 0 ? &c->rows_out : &c->rows_in);
   (side == 0 ? p.rows_out : p.rows_in)[slot] = r;
   (side == 0 ? p.row_slot_out : p.row_slot_in)[r] = slot;
   (side == 0 ? p.dels_out : p.dels_in)[slot] = 0;
@@ -278,9 +303,7 @@ __global__ void k_pairs(ApplyParams p) {
       if (!p.props.directed && u != v) add_op(p, v, u, 0, static_cast<int>(j));
     }
   }
-  if (missing)
-    atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[4]),
-              static_cast<unsigned long long>(missing));
+  warp_add(missing, &c->summary[4]);
 }
 
 // ---- D: match existing slots (simple graphs: at most one slot per pair, found in the edge
@@ -342,10 +365,6 @@ __global__ void k_scan_multi(ApplyParams p) {
   }
 }
 
-__device__ __forceinline__ void add_summary(UpdateCtl* c, int field, long long v) {
-  if (v) atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[field]),
-                   static_cast<unsigned long long>(v));
-}
 
 // ---- E: resolve every pair (counts, policies, classification, per-row slot demand) -------------
 __global__ void k_resolve(ApplyParams p) {
@@ -354,6 +373,7 @@ __global__ void k_resolve(ApplyParams p) {
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
   const int policy = p.props.on_existing_insert;
+  long long acc[5] = {0, 0, 0, 0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
@@ -398,11 +418,11 @@ __global__ void k_resolve(ApplyParams p) {
     if (appended && target_survives) flags |= kPairAppend;
     if (!appended && t >= 1 && policy == 0 && target_survives) flags |= kPairUpsert;
     if (use_first) flags |= kPairUseFirst;
-    add_summary(c, 0, inserted);
-    add_summary(c, 1, deleted);
-    add_summary(c, 2, updated);
-    add_summary(c, 3, ignored_ins);
-    add_summary(c, 4, ignored_del);
+    acc[0] += inserted;
+    acc[1] += deleted;
+    acc[2] += updated;
+    acc[3] += ignored_ins;
+    acc[4] += ignored_del;
     // Weight-increase classification (apply_host.cpp:348-393): first (u,v) before vs after.
     const int ins_index = use_first ? p.first[slot] : p.last[slot];
     const int final_idx = removed;  // S[removed] is the first (u,v) after the batch
@@ -445,6 +465,7 @@ __global__ void k_resolve(ApplyParams p) {
       }
     }
   }
+  for (int f = 0; f < 5; ++f) warp_add(acc[f], &c->summary[f]);
 }
 
 // ---- F: per touched row: stay in place or move to the top of the arena -------------------------
@@ -486,22 +507,56 @@ __global__ void k_alloc(ApplyParams p) {
     (side == 0 ? p.new_start_out : p.new_start_in)[s] = start;
     (side == 0 ? p.new_cap_out : p.new_cap_in)[s] = new_cap;
     (side == 0 ? p.live_out : p.live_in)[s] = live;
-    if (reloc) atomicAdd(side == 0 ? &c->relocated_out : &c->relocated_in, 1);
+    if (reloc) append_slot(side == 0 ? &c->relocated_out : &c->relocated_in);
   }
 }
 
-__device__ __forceinline__ void column_out(const ApplyParams& p, int j, long long w,
+__device__ __forceinline__ void acc_init(ColumnAcc& a) {
+  for (int j = 0; j < kLocalColumns; ++j) {
+    a.sum[j] = 0;
+    a.removed_at_max[j] = 0;
+    a.written_max[j] = 0;
+    a.written_at_max[j] = 0;
+    a.bad[j] = 0;
+  }
+}
+__device__ __forceinline__ void column_out(const ApplyParams& p, ColumnAcc& a, int j, long long w,
                                            long long old_max) {
+  if (j < kLocalColumns) {
+    a.sum[j] -= w;
+    a.removed_at_max[j] += w == old_max;
+    a.bad[j] -= w < 1;
+    return;
+  }
   atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_sum_delta[j]),
             static_cast<unsigned long long>(-w));
   if (w == old_max) atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_removed_at_max[j]), 1ULL);
   if (w < 1) atomicSub(&p.g.columns[j].bad, 1);
 }
-__device__ __forceinline__ void column_in(const ApplyParams& p, int j, long long w) {
+__device__ __forceinline__ void column_in(const ApplyParams& p, ColumnAcc& a, int j, long long w) {
+  if (j < kLocalColumns) {
+    a.sum[j] += w;
+    a.written_max[j] = max(a.written_max[j], w);
+    a.bad[j] += w < 1;
+    return;
+  }
   atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_sum_delta[j]),
             static_cast<unsigned long long>(w));
   atomicMax(&p.col_written_max[j], w);
   if (w < 1) atomicAdd(&p.g.columns[j].bad, 1);
+}
+// Flush a warp's accumulators (all lanes must call).
+__device__ __forceinline__ void acc_flush(const ApplyParams& p, ColumnAcc& a) {
+  const int k = p.k < kLocalColumns ? p.k : kLocalColumns;
+  for (int j = 0; j < k; ++j) {
+    warp_add(a.sum[j], &p.col_sum_delta[j]);
+    warp_add(a.removed_at_max[j], &p.col_removed_at_max[j]);
+    warp_max(a.written_max[j], &p.col_written_max[j], 0);
+    warp_add(a.written_at_max[j], &p.col_written_at_max[j]);
+    long long bad = a.bad[j];
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad != 0) atomicAdd(&p.g.columns[j].bad, static_cast<int>(bad));
+  }
 }
 
 // ---- G: tombstones and upserts in place -------------------------------------------------------
@@ -510,6 +565,9 @@ __global__ void k_mutate(ApplyParams p) {
   if (c->error) return;
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
+  ColumnAcc acc;
+  acc_init(acc);
+  long long idx_deleted = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
@@ -535,13 +593,13 @@ __global__ void k_mutate(ApplyParams p) {
           col[pos] = kDead;
           if (side == 0)
             for (int j = 0; j < p.k; ++j)
-              column_out(p, j, w[j * p.g.arena_cap + pos], p.g.columns[j].max_w);
+              column_out(p, acc, j, w[j * p.g.arena_cap + pos], p.g.columns[j].max_w);
         } else {
           for (int j = 0; j < p.k; ++j) {
             const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
             if (side == 0) {
-              column_out(p, j, w[j * p.g.arena_cap + pos], p.g.columns[j].max_w);
-              column_in(p, j, nw);
+              column_out(p, acc, j, w[j * p.g.arena_cap + pos], p.g.columns[j].max_w);
+              column_in(p, acc, j, nw);
             }
             w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
           }
@@ -550,9 +608,7 @@ __global__ void k_mutate(ApplyParams p) {
       if (tomb && !(flags & kPairAppend)) {
         // the edge is gone: its index key becomes a deleted marker
         p.g.ekey[p.in_pos2[slot]] = kKeyDeleted;
-        atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_live),
-                  static_cast<unsigned long long>(-1LL));
-        atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_dead), 1ULL);
+        ++idx_deleted;
       }
       continue;
     }
@@ -570,13 +626,13 @@ __global__ void k_mutate(ApplyParams p) {
           col[e] = kDead;
           if (side == 0)
             for (int j = 0; j < p.k; ++j)
-              column_out(p, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
+              column_out(p, acc, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
         } else if ((flags & kPairUpsert) && seen == target) {
           for (int j = 0; j < p.k; ++j) {
             const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
             if (side == 0) {
-              column_out(p, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
-              column_in(p, j, nw);
+              column_out(p, acc, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
+              column_in(p, acc, j, nw);
             }
             w[j * p.g.arena_cap + e] = static_cast<int32_t>(nw);
           }
@@ -585,6 +641,9 @@ __global__ void k_mutate(ApplyParams p) {
       }
     }
   }
+  acc_flush(p, acc);
+  warp_add(-idx_deleted, &p.g.counters->idx_live);
+  warp_add(idx_deleted, &p.g.counters->idx_dead);
 }
 
 // ---- H: move relocated rows (live slots, in order) ---------------------------------------------
@@ -632,6 +691,9 @@ __global__ void k_append(ApplyParams p) {
   UpdateCtl* c = p.ctl;
   if (c->error) return;
   const int pairs = c->pairs;
+  ColumnAcc acc;
+  acc_init(acc);
+  long long idx_new = 0, idx_reused = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
     const int slot = p.list[i];
     const int flags = p.flags[slot];
@@ -655,7 +717,7 @@ __global__ void k_append(ApplyParams p) {
       for (int j = 0; j < p.k; ++j) {
         const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
         w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
-        if (side == 0) column_in(p, j, nw);
+        if (side == 0) column_in(p, acc, j, nw);
       }
     }
     if (!p.g.allow_multi) {
@@ -668,15 +730,16 @@ __global__ void k_append(ApplyParams p) {
           set_error(&c->error, kErrInternal);
           continue;
         }
-        atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_live), 1ULL);
-        if (reused)
-          atomicAdd(reinterpret_cast<unsigned long long*>(&p.g.counters->idx_dead),
-                    static_cast<unsigned long long>(-1LL));
+        ++idx_new;
+        idx_reused += reused ? 1 : 0;
       }
       p.g.eout[ie] = placed[0];
       p.g.ein[ie] = placed[1];
     }
   }
+  acc_flush(p, acc);
+  warp_add(idx_new, &p.g.counters->idx_live);
+  warp_add(-idx_reused, &p.g.counters->idx_dead);
 }
 
 // ---- J: new row descriptors ----------------------------------------------------------------------
@@ -716,14 +779,10 @@ __global__ void k_rows_final(ApplyParams p) {
     descs[r] = nd;
   }
   GraphCounters* gc = p.g.counters;
-  if (garbage_out) atomicAdd(&gc->out_garbage, static_cast<u64>(garbage_out));
-  if (garbage_in) atomicAdd(&gc->in_garbage, static_cast<u64>(garbage_in));
-  if (dead_delta_out)
-    atomicAdd(reinterpret_cast<unsigned long long*>(&gc->dead_out),
-              static_cast<unsigned long long>(dead_delta_out));
-  if (dead_delta_in)
-    atomicAdd(reinterpret_cast<unsigned long long*>(&gc->dead_in),
-              static_cast<unsigned long long>(dead_delta_in));
+  warp_add_u(static_cast<u64>(garbage_out), &gc->out_garbage);
+  warp_add_u(static_cast<u64>(garbage_in), &gc->in_garbage);
+  warp_add(dead_delta_out, &gc->dead_out);
+  warp_add(dead_delta_in, &gc->dead_in);
 }
 
 // Count the weights written by the batch that equal the new maximum (for count_at_max).
@@ -731,6 +790,8 @@ __global__ void k_count_written_max(ApplyParams p) {
   UpdateCtl* c = p.ctl;
   if (c->error) return;
   const int pairs = c->pairs;
+  ColumnAcc acc;
+  acc_init(acc);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
     const int slot = p.list[i];
     const int flags = p.flags[slot];
@@ -739,10 +800,14 @@ __global__ void k_count_written_max(ApplyParams p) {
     for (int j = 0; j < p.k; ++j) {
       const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
       const long long target = max(p.col_written_max[j], p.g.columns[j].max_w);
-      if (nw == target)
-        atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_written_at_max[j]), 1ULL);
+      if (nw == target) {
+        if (j < kLocalColumns) ++acc.written_at_max[j];
+        else atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_written_at_max[j]), 1ULL);
+      }
     }
   }
+  const int k = p.k < kLocalColumns ? p.k : kLocalColumns;
+  for (int j = 0; j < k; ++j) warp_add(acc.written_at_max[j], &p.col_written_at_max[j]);
 }
 
 // One thread: graph counters and column statistics after the batch.

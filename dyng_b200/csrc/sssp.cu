@@ -22,7 +22,7 @@ namespace dyngb200 {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kHeavyChunk = 1024;
+constexpr int kHeavyChunk = 256;
 constexpr unsigned long long kBarrierTimeoutNs = 5ULL * 1000 * 1000 * 1000;
 
 struct SsspParams {
@@ -239,6 +239,33 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
   }
 }
 
+// The pull's offer of in-neighbour y over an in-slot of weight w: packed (d(y) + w, y), or INF.
+__device__ __forceinline__ u64 pull_candidate(const SsspParams& p, Ctx& X, int y, int w) {
+  ++X.slots;
+  if (y < 0) return kPackedInf;
+  const u64 word = ld_cg(&p.packed[y]);
+  ++X.words;
+  if (word == kPackedInf) return kPackedInf;
+  const u64 nd = X.pk.dist(word) + static_cast<u64>(w);
+  if (nd > X.maxd) return kPackedInf;
+  return X.pk.pack(nd, y);
+}
+
+// The best offer of a pull for `owner`: keep it if smaller; on a distance decrease the owner
+// joins the frontier of the near-far loop.
+__device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int owner, u64 cand) {
+  if (cand >= ld_cg(&p.packed[owner])) return;
+  const u64 old = atomicMin(&p.packed[owner], cand);
+  if (cand < old) {
+    ++X.atomics;
+    touch(p, owner);
+  }
+  if (X.pk.dist(cand) < X.pk.dist(old) && claim(p.stamp, owner, X.gen)) {
+    ++X.appends;
+    X.next[append_slot(X.next_cnt)] = owner;
+  }
+}
+
 template <int MODE>
 __device__ __forceinline__ const int32_t* row_col(const SsspParams& p) {
   return MODE == kPull ? p.g.in_col : p.g.out_col;
@@ -258,6 +285,23 @@ __device__ __forceinline__ void warp_slots(const SsspParams& p, Ctx& X, int owne
   const int32_t* col = row_col<MODE>(p) + start;
   const int32_t* wt = row_w<MODE>(p) + start;
   const int g1 = (e1 + 3) >> 2;
+  if (MODE == kPull) {
+    // one owner: the warp's minimum over the slots, one offer
+    u64 best = kPackedInf;
+    for (int grp = (e0 >> 2) + lane; grp < g1; grp += 32) {
+      const int e = grp << 2;
+      const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + e));
+      const int4 w4 = __ldg(reinterpret_cast<const int4*>(wt + e));
+      if (e + 0 < e1) best = min(best, pull_candidate(p, X, c4.x, w4.x));
+      if (e + 1 < e1) best = min(best, pull_candidate(p, X, c4.y, w4.y));
+      if (e + 2 < e1) best = min(best, pull_candidate(p, X, c4.z, w4.z));
+      if (e + 3 < e1) best = min(best, pull_candidate(p, X, c4.w, w4.w));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, off));
+    if (lane == 0 && best != kPackedInf) offer_owner(p, X, owner, best);
+    return;
+  }
   for (int grp = (e0 >> 2) + lane; grp < g1; grp += 32) {
     const int e = grp << 2;
     const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + e));
@@ -306,7 +350,22 @@ __device__ __forceinline__ void warp_rows(const SsspParams& p, Ctx& X, int owner
     const u64 d = __shfl_sync(0xffffffffu, odu, j);
     const unsigned s = __shfl_sync(0xffffffffu, start, j);
     const int ex = __shfl_sync(0xffffffffu, excl, j);
-    if (e < total) {
+    if (MODE == kPull) {
+      // the lanes of one owner are contiguous: a segmented minimum, then one offer per owner
+      u64 best = kPackedInf;
+      if (e < total) {
+        const unsigned slot = s + static_cast<unsigned>(e - ex);
+        best = pull_candidate(p, X, col[slot], wt[slot]);
+      }
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const u64 other = __shfl_down_sync(0xffffffffu, best, off);
+        const int oj = __shfl_down_sync(0xffffffffu, j, off);
+        if (lane + off < 32 && oj == j) best = min(best, other);
+      }
+      const int pj = __shfl_up_sync(0xffffffffu, j, 1);
+      if (e < total && (lane == 0 || pj != j) && best != kPackedInf) offer_owner(p, X, o, best);
+    } else if (e < total) {
       const unsigned slot = s + static_cast<unsigned>(e - ex);
       visit<MODE>(p, X, o, d, col[slot], MODE == kWalk ? 0 : wt[slot]);
     }
@@ -330,12 +389,16 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
                        const int2* heavy, u64 heavy_cnt, long long gwarp, long long nwarps) {
   const int lane = threadIdx.x & 31;
   const RowDesc* descs = MODE == kPull ? p.g.in_desc : p.g.out_desc;
-  for (long long base = gwarp * 32; base < light_count; base += nwarps * 32) {
+  // every warp takes `per` consecutive vertices (at most 32), so that a frontier smaller than
+  // 32 x warps still reaches every warp
+  long long per = (light_count + nwarps - 1) / nwarps;
+  per = per < 1 ? 1 : (per > 32 ? 32 : per);
+  for (long long base = gwarp * per; base < light_count; base += nwarps * per) {
     const long long i = base + lane;
     int owner = -1;
     u64 du = 0;
     RowDesc desc{0, 0};
-    if (i < light_count) {
+    if (lane < per && i < light_count) {
       owner = ld_cg(&light[i]);
       ++X.rows;
       if (MODE == kPush) {
@@ -479,18 +542,36 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
             c->rounds = round + 1;
           }
           int jumping = 0;
-          for (long long v = tid; v < n; v += threads) {
-            ++w_visits;
-            const int a = ld_cg(&p.ancestor[v]);
-            if (a < 0 || ld_cg(&p.flag[v])) continue;
-            ++w_jumps;
-            if (ld_cg(&p.flag[a])) {
-              p.flag[v] = 1;
-              continue;
+          // four vertices per thread and step, their loads issued together
+          for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
+            int a[4], f[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const long long v = v0 + q * threads;
+              a[q] = v < n ? ld_cg(&p.ancestor[v]) : -1;
+              f[q] = v < n ? ld_cg(&p.flag[v]) : 1;
             }
-            const int next = ld_cg(&p.ancestor[a]);
-            p.ancestor[v] = next;
-            jumping |= next >= 0 ? 1 : 0;
+            int fa[4], na[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const bool live = a[q] >= 0 && !f[q];
+              fa[q] = live ? ld_cg(&p.flag[a[q]]) : 0;
+              na[q] = live ? ld_cg(&p.ancestor[a[q]]) : -1;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const long long v = v0 + q * threads;
+              if (v >= n) continue;
+              ++w_visits;
+              if (a[q] < 0 || f[q]) continue;
+              ++w_jumps;
+              if (fa[q]) {
+                p.flag[v] = 1;
+                continue;
+              }
+              p.ancestor[v] = na[q];
+              jumping |= na[q] >= 0 ? 1 : 0;
+            }
           }
           if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
           if (!grid_barrier(c, bar)) return;
