@@ -345,6 +345,7 @@ def main():
                        "host_ms_p50": 1000 * float(np.percentile(host_lat[args.warmup:], 50)),
                        "sssp_phases_ms": phases, "sssp_work": work, "update_shape": shape,
                        "alg_bytes_per_update": float(np.mean(alg)),
+                       "trace_last_update": [list(t) for t in timed_stats[-1].trace],
                        "verified_vs_compute": verified,
                        "setup_s": {"generate": round(gen_s, 1), "build_and_compute": round(build_s, 1)}},
             "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,

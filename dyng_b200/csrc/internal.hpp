@@ -132,6 +132,11 @@ struct UpdateCtl {
   // work counters (algorithmic traffic) and phase timestamps of the sssp kernel
   long long work[12];
   unsigned long long phase_ns[8];
+  // trace of the first 64 push iterations / epochs: (light count, heavy chunks, ns since start)
+  int trace_n[64];
+  int trace_h[64];
+  unsigned trace_t[64];
+  int trace_len;
   // grid barrier
   unsigned bar_count;
   unsigned bar_gen;

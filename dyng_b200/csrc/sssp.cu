@@ -266,6 +266,52 @@ __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int own
   }
 }
 
+// The push split in two stages, so that a lane issues the loads of several slots before it
+// commits any of them: prepare computes the offer and loads the target's current word; commit
+// does the atomicMin and the frontier bookkeeping (the same steps as visit<kPush>).
+struct Offer {
+  int dst;
+  u64 cand;
+  u64 cur;
+};
+
+__device__ __forceinline__ void push_prepare(const SsspParams& p, Ctx& X, int u, u64 du, int y,
+                                             int w, Offer& r) {
+  ++X.slots;
+  r.dst = y;
+  r.cand = kPackedInf;
+  r.cur = 0;
+  if (y < 0 || y == p.source) return;
+  const u64 nd = du + static_cast<u64>(w);
+  if (nd > X.maxd) return;
+  r.cand = X.pk.pack(nd, u);
+  ++X.words;
+  r.cur = ld_cg(&p.packed[y]);
+}
+
+__device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const Offer& r) {
+  if (r.cand >= r.cur) return;  // also skips "no offer" (cand == INF)
+  const int dst = r.dst;
+  const u64 old = atomicMin(&p.packed[dst], r.cand);
+  if (r.cand < old) {
+    ++X.atomics;
+    touch(p, dst);
+  }
+  const u64 nd = X.pk.dist(r.cand);
+  if (nd < X.pk.dist(old)) {
+    if (nd < X.threshold) {
+      if (claim(p.stamp, dst, X.gen)) {
+        ++X.appends;
+        list_append(dst, p.g.out_desc[dst].len, p.heavy_degree, X.next, X.next_cnt, X.next_heavy,
+                    X.next_heavy_cnt);
+      }
+    } else if (atomicExch(&p.in_far[dst], 1) == 0) {
+      ++X.appends;
+      X.far[append_slot(X.far_cnt)] = dst;
+    }
+  }
+}
+
 template <int MODE>
 __device__ __forceinline__ const int32_t* row_col(const SsspParams& p) {
   return MODE == kPull ? p.g.in_col : p.g.out_col;
@@ -300,6 +346,23 @@ __device__ __forceinline__ void warp_slots(const SsspParams& p, Ctx& X, int owne
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, off));
     if (lane == 0 && best != kPackedInf) offer_owner(p, X, owner, best);
+    return;
+  }
+  if (MODE == kPush) {
+    for (int grp = (e0 >> 2) + lane; grp < g1; grp += 32) {
+      const int e = grp << 2;
+      const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + e));
+      const int4 w4 = __ldg(reinterpret_cast<const int4*>(wt + e));
+      Offer r0, r1, r2, r3;
+      push_prepare(p, X, owner, odu, e + 0 < e1 ? c4.x : -1, w4.x, r0);
+      push_prepare(p, X, owner, odu, e + 1 < e1 ? c4.y : -1, w4.y, r1);
+      push_prepare(p, X, owner, odu, e + 2 < e1 ? c4.z : -1, w4.z, r2);
+      push_prepare(p, X, owner, odu, e + 3 < e1 ? c4.w : -1, w4.w, r3);
+      push_commit(p, X, r0);
+      push_commit(p, X, r1);
+      push_commit(p, X, r2);
+      push_commit(p, X, r3);
+    }
     return;
   }
   for (int grp = (e0 >> 2) + lane; grp < g1; grp += 32) {
@@ -338,6 +401,37 @@ __device__ __forceinline__ void warp_rows(const SsspParams& p, Ctx& X, int owner
   const int total = __shfl_sync(0xffffffffu, incl, 31);
   const int32_t* col = row_col<MODE>(p);
   const int32_t* wt = row_w<MODE>(p);
+  if (MODE == kPush) {
+    // two slots per lane and step: both offers prepared before either commits
+    for (int base = 0; base < total; base += 64) {
+      Offer r[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int e = base + 32 * q + lane;
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int cand = j + step;
+          if (__shfl_sync(0xffffffffu, excl, cand) <= e) j = cand;
+        }
+        const int o = __shfl_sync(0xffffffffu, owner, j);
+        const u64 d = __shfl_sync(0xffffffffu, odu, j);
+        const unsigned s = __shfl_sync(0xffffffffu, start, j);
+        const int ex = __shfl_sync(0xffffffffu, excl, j);
+        if (e < total) {
+          const unsigned slot = s + static_cast<unsigned>(e - ex);
+          push_prepare(p, X, o, d, col[slot], wt[slot], r[q]);
+        } else {
+          r[q].cand = kPackedInf;
+          r[q].cur = 0;
+          r[q].dst = -1;
+        }
+      }
+      push_commit(p, X, r[0]);
+      push_commit(p, X, r[1]);
+    }
+    return;
+  }
   for (int base = 0; base < total; base += 32) {
     const int e = base + lane;
     int j = 0;
@@ -439,7 +533,7 @@ __device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
   add_candidate(p, v);
 }
 
-__global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
+__global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   UpdateCtl* c = p.ctl;
   if (ld_volatile(&c->error) != 0) return;
   unsigned bar = 0;
@@ -523,7 +617,19 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     }
     if (__any_sync(0xffffffffu, changed) && lane == 0) c->changed = 1;
     if (!p.walk) {
-      for (long long v = tid; v < n; v += threads) p.ancestor[v] = v < p.tree_n ? p.parent[v] : -1;
+      for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
+        int a[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * threads;
+          a[q] = v < p.tree_n ? p.parent[v] : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * threads;
+          if (v < n) p.ancestor[v] = a[q];
+        }
+      }
       w_visits += (n - tid + threads - 1) / threads;
     }
     if (!grid_barrier(c, bar)) return;
@@ -581,8 +687,17 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
       if (tid == 0) c->phase_ns[2] = global_ns();
       // ---- invalidate the flagged vertices ------------------------------------------------------
       if (any_changed) {
-        for (long long v = tid; v < n; v += threads) {
-          if (ld_cg(&p.flag[v])) {
+        for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
+          int f[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const long long v = v0 + q * threads;
+            f[q] = v < n ? ld_cg(&p.flag[v]) : 0;
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (!f[q]) continue;
+            const long long v = v0 + q * threads;
             p.flag[v] = 0;
             p.stamp[v] = gen_inv;
             invalidate(p, static_cast<int>(v));
@@ -713,6 +828,13 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     const int cs = it % 3;
     const int nc = ld_cg(&c->near_cnt[cs]);
     const u64 hc = ld_cg(&c->heavy_cnt[cs]);
+    const int step = iterations + epochs;
+    if (tid == 0 && step < 64) {
+      c->trace_n[step] = nc;
+      c->trace_h[step] = static_cast<int>(hc & 0xffffffffu);
+      c->trace_t[step] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
+      c->trace_len = step + 1;
+    }
     if (nc > 0 || (hc >> 40) > 0) {
       ++iterations;
       if (iterations > iteration_cap) {
@@ -738,6 +860,7 @@ __global__ void __launch_bounds__(kThreads) k_sssp(SsspParams p) {
     // near frontier empty: raise the threshold past the far pile
     const int far_count = ld_cg(&c->far_count);
     if (far_count == 0) break;
+    if (tid == 0 && step < 64) c->trace_n[step] = -far_count;  // an epoch: the far pile size
     ++epochs;
     local = kPackedInf;
     for (long long i = tid; i < far_count; i += threads) {
@@ -1134,6 +1257,12 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     st->rounds = r.rounds;
     st->touched = r.touched_count;
     for (int i = 0; i < 12; ++i) st->work[i] = r.work[i];
+    st->trace_len = r.trace_len;
+    for (int i = 0; i < r.trace_len && i < 64; ++i) {
+      st->trace_light[i] = r.trace_n[i];
+      st->trace_heavy[i] = r.trace_h[i];
+      st->trace_us[i] = r.trace_t[i] * 1e-3f;
+    }
     for (int i = 0; i < 7; ++i)
       st->phase_ms[i] = r.phase_ns[i + 1] > r.phase_ns[i]
                             ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)

@@ -75,6 +75,7 @@ class Stats:
     touched: int = 0
     work: tuple = ()
     phase_ms: tuple = ()
+    trace: tuple = ()  # (light, heavy chunks, start us) per near-far step; light < 0: an epoch
 
     WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
                   "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
@@ -94,7 +95,9 @@ class Stats:
                    s.epochs, s.pushes, bool(s.packed_parents), engines.get(s.engine_used, "fused"),
                    s.delta, s.max_weight, s.grid_blocks, s.invalidation, float(s.apply_ms),
                    float(s.sssp_ms), s.rounds, s.touched, tuple(int(x) for x in s.work),
-                   tuple(float(x) for x in s.phase_ms))
+                   tuple(float(x) for x in s.phase_ms),
+                   tuple((int(s.trace_light[i]), int(s.trace_heavy[i]), float(s.trace_us[i]))
+                         for i in range(min(int(s.trace_len), 64))))
 
 
 class Result:

@@ -119,6 +119,13 @@ typedef struct dyngb200_stats {
   /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
    * first split, near-far loop, unpack. */
   float phase_ms[7];
+  /* Trace of the first 64 steps of the near-far loop: light frontier size (negative: an epoch
+   * with that many far vertices), heavy chunks, and the step's start in microseconds since the
+   * kernel began. */
+  int32_t trace_len;
+  int32_t trace_light[64];
+  int32_t trace_heavy[64];
+  float trace_us[64];
 } dyngb200_stats;
 
 /* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */
