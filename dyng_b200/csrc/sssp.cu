@@ -78,9 +78,72 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
   return *reinterpret_cast<const volatile unsigned*>(p);
 }
 
-// Grid-wide barrier over co-resident blocks (cooperative launch).  Returns false once any block
-// has recorded a timeout; the caller then leaves the kernel.
+// Shared-memory staging of list appends.  A lane appends into its block's stage with a
+// warp-aggregated shared-memory atomic (ballot + popc); at the end of the phase the block copies
+// the stage to the global list with ONE global atomicAdd for its slot range, so the global list
+// counters see one atomic per block and phase instead of one per warp group.  A full stage falls
+// back to the global list directly.  Stages: the next frontier (near list, pull frontier or walk
+// level), the far pile, the touched list and the pull candidates.
+constexpr int kStages = 4;
+constexpr int kStageCap = 1024;
+enum StageId { kStNext = 0, kStFar = 1, kStTouched = 2, kStCand = 3 };
+
+struct StageSet {
+  int cnt[kStages];
+  int base[kStages];
+  int* list[kStages];
+  int* count[kStages];
+  int data[kStages][kStageCap];
+};
+
+__shared__ StageSet g_stage;
+
+__device__ __forceinline__ void staged_append(int id, int* list, int* count, int v) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  const int rank = __popc(mask & ((1u << lane) - 1));
+  int base = 0;
+  if (lane == leader) {
+    base = atomicAdd(&g_stage.cnt[id], __popc(mask));
+    g_stage.list[id] = list;
+    g_stage.count[id] = count;
+  }
+  base = __shfl_sync(mask, base, leader);
+  const int pos = base + rank;
+  if (pos < kStageCap) g_stage.data[id][pos] = v;
+  else list[append_slot(count)] = v;
+}
+
+__device__ __forceinline__ void stage_init() {
+  if (threadIdx.x < kStages) g_stage.cnt[threadIdx.x] = 0;
+  __syncthreads();
+}
+
+// Copy every non-empty stage to its global list (all threads of the block).
+__device__ __forceinline__ void stage_flush() {
+  __syncthreads();
+  if (threadIdx.x < kStages) {
+    const int id = threadIdx.x;
+    const int n = min(g_stage.cnt[id], kStageCap);
+    g_stage.base[id] = n > 0 ? atomicAdd(g_stage.count[id], n) : 0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int id = 0; id < kStages; ++id) {
+    const int n = min(g_stage.cnt[id], kStageCap);
+    int* list = g_stage.list[id];
+    const int b = g_stage.base[id];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) list[b + i] = g_stage.data[id][i];
+  }
+  __syncthreads();
+  if (threadIdx.x < kStages) g_stage.cnt[threadIdx.x] = 0;
+}
+
+// Grid-wide barrier over co-resident blocks (cooperative launch).  Flushes the block's stages
+// first.  Returns false once any block has recorded a timeout; the caller then leaves the kernel.
 __device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
+  stage_flush();
   __syncthreads();
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
@@ -127,7 +190,7 @@ __device__ __forceinline__ bool claim(int* stamp, int v, int generation) {
 
 __device__ __forceinline__ void touch(const SsspParams& p, int v) {
   if (atomicExch(&p.touch_stamp[v], p.touch_gen) != p.touch_gen) {
-    p.touched[append_slot(&p.ctl->touched_count)] = v;
+    staged_append(kStTouched, p.touched, &p.ctl->touched_count, v);
   }
 }
 
@@ -146,20 +209,21 @@ __device__ __forceinline__ void warp_sum_into_ll(long long v, long long* target)
 // its 1024-slot chunk range, reserved together with the slot by one 64-bit atomic so that chunk
 // bases grow with the slot index.
 __device__ __forceinline__ void list_append(int v, int len, int heavy_degree, int* light,
-                                            int* light_count, int2* heavy, u64* heavy_count) {
+                                            int* light_count, int2* heavy, u64* heavy_count,
+                                            int stage = kStNext) {
   if (len > heavy_degree) {
     const u64 chunks = static_cast<u64>((len + kHeavyChunk - 1) / kHeavyChunk);
     const u64 prev = atomicAdd(heavy_count, (1ULL << 40) | chunks);
     heavy[static_cast<int>(prev >> 40)] = make_int2(v, static_cast<int>(prev & ((1ULL << 40) - 1)));
   } else {
-    light[append_slot(light_count)] = v;
+    staged_append(stage, light, light_count, v);
   }
 }
 
 // A vertex to re-evaluate by the pull pass (light or heavy by in-degree).
 __device__ __forceinline__ void add_candidate(const SsspParams& p, int v) {
   list_append(v, p.g.in_desc[v].len, p.heavy_degree, p.candidates, &p.ctl->cand_count,
-              p.pull_heavy, &p.ctl->pull_heavy);
+              p.pull_heavy, &p.ctl->pull_heavy, kStCand);
 }
 
 // Per-thread state of one expansion: where improved vertices go, and work counters.
@@ -224,7 +288,7 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
     if (MODE == kPull) {
       if (claim(p.stamp, dst, X.gen)) {
         ++X.appends;
-        X.next[append_slot(X.next_cnt)] = dst;
+        staged_append(kStNext, X.next, X.next_cnt, dst);
       }
     } else if (nd < X.threshold) {
       if (claim(p.stamp, dst, X.gen)) {
@@ -234,7 +298,7 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
       }
     } else if (atomicExch(&p.in_far[dst], 1) == 0) {
       ++X.appends;
-      X.far[append_slot(X.far_cnt)] = dst;
+      staged_append(kStFar, X.far, X.far_cnt, dst);
     }
   }
 }
@@ -262,7 +326,7 @@ __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int own
   }
   if (X.pk.dist(cand) < X.pk.dist(old) && claim(p.stamp, owner, X.gen)) {
     ++X.appends;
-    X.next[append_slot(X.next_cnt)] = owner;
+    staged_append(kStNext, X.next, X.next_cnt, owner);
   }
 }
 
@@ -307,7 +371,7 @@ __device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const O
       }
     } else if (atomicExch(&p.in_far[dst], 1) == 0) {
       ++X.appends;
-      X.far[append_slot(X.far_cnt)] = dst;
+      staged_append(kStFar, X.far, X.far_cnt, dst);
     }
   }
 }
@@ -536,6 +600,7 @@ __device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
 __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   UpdateCtl* c = p.ctl;
   if (ld_volatile(&c->error) != 0) return;
+  stage_init();
   unsigned bar = 0;
   const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   const long long threads = static_cast<long long>(gridDim.x) * blockDim.x;
@@ -766,7 +831,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
       const u64 old = atomicMin(&p.packed[v], cand);
       if (cand < old) touch(p, v);
       if (nd < pk.dist(old) && claim(p.stamp, v, gen_pull))
-        p.frontier[append_slot(&c->frontier_count)] = v;
+        staged_append(kStNext, p.frontier, &c->frontier_count, v);
     }
     warp_sum_into_ll(w_inval, &c->invalidated);
     if (!grid_barrier(c, bar)) return;
@@ -815,7 +880,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
         list_append(v, p.g.out_desc[v].len, p.heavy_degree, lists[0], &c->near_cnt[0], hlists[0],
                     &c->heavy_cnt[0]);
     } else if (atomicExch(&p.in_far[v], 1) == 0) {
-      far[append_slot(&c->far_count)] = v;
+      staged_append(kStFar, far, &c->far_count, v);
     }
   }
   if (!grid_barrier(c, bar)) return;
@@ -881,7 +946,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
           list_append(v, p.g.out_desc[v].len, p.heavy_degree, lists[it & 1], &c->near_cnt[cs],
                       hlists[it & 1], &c->heavy_cnt[cs]);
       } else {
-        far2[append_slot(&c->far2_count)] = v;
+        staged_append(kStFar, far2, &c->far2_count, v);
       }
     }
     if (!grid_barrier(c, bar)) return;
