@@ -1099,7 +1099,7 @@ void Workspace::reserve_vertices(long long n_cap, cudaStream_t s) {
     DYNGB200_CUDA(cudaMemsetAsync(b->ptr, 0, n * sizeof(int), s));
   }
   for (DevBuf<int>* b : {&row_slot_out, &row_slot_in, &ancestor, &candidates, &frontier, &near_a,
-                         &near_b, &far_a, &far_b, &touched}) {
+                         &near_b, &far_a, &far_b, &touched, &cand_med, &near_med_a, &near_med_b}) {
     b->release();
     b->reserve(n, s);
   }

@@ -113,7 +113,10 @@ struct UpdateCtl {
   int cand_count;       // light pull candidates
   int frontier_count;   // vertices the pull (or the head offers) improved
   int near_cnt[3];      // light near-frontier lists, triple-buffered counters
+  int near_med_cnt[3];  // medium rows of the near frontier
   int walk_cnt[3];      // subtree-walk levels
+  int walk_med_cnt[3];
+  int cand_med_count;   // medium pull candidates
   int far_count, far2_count;
   u64 heavy_cnt[3];     // (slots << 40 | chunks) of the heavy near-frontier lists
   u64 walk_heavy[3];
@@ -162,7 +165,7 @@ struct Workspace {
   // sssp
   DevBuf<int> stamp, touch_stamp, flag, in_far, ancestor;
   DevBuf<int> candidates, frontier, near_a, near_b, far_a, far_b, heavy_a, heavy_b, pull_heavy,
-      touched;
+      touched, cand_med, near_med_a, near_med_b;
   DevBuf<UpdateCtl> ctl;
   HostBuf<UpdateCtl> host_ctl;
   int generation = 0;     // stamp generations (sssp)

@@ -60,6 +60,9 @@ struct SsspParams {
   int2* heavy_a;
   int2* heavy_b;
   int2* pull_heavy;
+  int* cand_med;
+  int* near_med_a;
+  int* near_med_b;
   int* touched;
   int generation;
   int touch_gen;
@@ -84,9 +87,9 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
 // counters see one atomic per block and phase instead of one per warp group.  A full stage falls
 // back to the global list directly.  Stages: the next frontier (near list, pull frontier or walk
 // level), the far pile, the touched list and the pull candidates.
-constexpr int kStages = 4;
-constexpr int kStageCap = 1024;
-enum StageId { kStNext = 0, kStFar = 1, kStTouched = 2, kStCand = 3 };
+constexpr int kStages = 6;
+constexpr int kStageCap = 768;
+enum StageId { kStNext = 0, kStFar = 1, kStTouched = 2, kStCand = 3, kStNextMed = 4, kStCandMed = 5 };
 
 struct StageSet {
   int cnt[kStages];
@@ -205,25 +208,41 @@ __device__ __forceinline__ void warp_sum_into_ll(long long v, long long* target)
     atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(v));
 }
 
-// Append v to a frontier: the light list, or (rows longer than heavy_degree) the heavy list with
-// its 1024-slot chunk range, reserved together with the slot by one 64-bit atomic so that chunk
-// bases grow with the slot index.
-__device__ __forceinline__ void list_append(int v, int len, int heavy_degree, int* light,
-                                            int* light_count, int2* heavy, u64* heavy_count,
-                                            int stage = kStNext) {
+// Rows are sorted into three classes when they join a frontier: light (up to 32 slots: their
+// slots are dealt over the lanes of one warp), medium (up to `heavy_degree` slots: one row per
+// warp) and heavy (split into kHeavyChunk-slot chunks spread over all warps; one 64-bit atomic
+// reserves the list slot and the chunk range together, so chunk bases grow with the slot index).
+constexpr int kLightMax = 32;
+
+struct ListSet {
+  int* light;
+  int* light_cnt;
+  int* med;
+  int* med_cnt;
+  int2* heavy;
+  u64* heavy_cnt;
+  int stage_light;
+  int stage_med;
+};
+
+__device__ __forceinline__ void list_append(const ListSet& L, int v, int len, int heavy_degree) {
   if (len > heavy_degree) {
     const u64 chunks = static_cast<u64>((len + kHeavyChunk - 1) / kHeavyChunk);
-    const u64 prev = atomicAdd(heavy_count, (1ULL << 40) | chunks);
-    heavy[static_cast<int>(prev >> 40)] = make_int2(v, static_cast<int>(prev & ((1ULL << 40) - 1)));
+    const u64 prev = atomicAdd(L.heavy_cnt, (1ULL << 40) | chunks);
+    L.heavy[static_cast<int>(prev >> 40)] =
+        make_int2(v, static_cast<int>(prev & ((1ULL << 40) - 1)));
+  } else if (len > kLightMax) {
+    staged_append(L.stage_med, L.med, L.med_cnt, v);
   } else {
-    staged_append(stage, light, light_count, v);
+    staged_append(L.stage_light, L.light, L.light_cnt, v);
   }
 }
 
-// A vertex to re-evaluate by the pull pass (light or heavy by in-degree).
+// A vertex to re-evaluate by the pull pass (classified by in-degree).
 __device__ __forceinline__ void add_candidate(const SsspParams& p, int v) {
-  list_append(v, p.g.in_desc[v].len, p.heavy_degree, p.candidates, &p.ctl->cand_count,
-              p.pull_heavy, &p.ctl->pull_heavy, kStCand);
+  const ListSet L{p.candidates, &p.ctl->cand_count, p.cand_med, &p.ctl->cand_med_count,
+                  p.pull_heavy, &p.ctl->pull_heavy, kStCand, kStCandMed};
+  list_append(L, v, p.g.in_desc[v].len, p.heavy_degree);
 }
 
 // Per-thread state of one expansion: where improved vertices go, and work counters.
@@ -232,10 +251,7 @@ struct Ctx {
   u64 maxd;
   u64 threshold;
   int gen;       // claim generation of the appends
-  int* next;     // next light list (push: near; pull: frontier; walk: next level)
-  int* next_cnt;
-  int2* next_heavy;
-  u64* next_heavy_cnt;
+  ListSet next;  // push: next near frontier; walk: next level; pull: the frontier (light only)
   int* far;
   int* far_cnt;
   unsigned slots, words, atomics, appends, rows;
@@ -254,8 +270,7 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
       touch(p, y);
       add_candidate(p, y);
       ++X.appends;
-      list_append(y, p.g.out_desc[y].len, p.heavy_degree, X.next, X.next_cnt, X.next_heavy,
-                  X.next_heavy_cnt);
+      list_append(X.next, y, p.g.out_desc[y].len, p.heavy_degree);
     }
     return;
   }
@@ -288,13 +303,12 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
     if (MODE == kPull) {
       if (claim(p.stamp, dst, X.gen)) {
         ++X.appends;
-        staged_append(kStNext, X.next, X.next_cnt, dst);
+        staged_append(kStNext, X.next.light, X.next.light_cnt, dst);
       }
     } else if (nd < X.threshold) {
       if (claim(p.stamp, dst, X.gen)) {
         ++X.appends;
-        list_append(dst, p.g.out_desc[dst].len, p.heavy_degree, X.next, X.next_cnt, X.next_heavy,
-                    X.next_heavy_cnt);
+        list_append(X.next, dst, p.g.out_desc[dst].len, p.heavy_degree);
       }
     } else if (atomicExch(&p.in_far[dst], 1) == 0) {
       ++X.appends;
@@ -326,7 +340,7 @@ __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int own
   }
   if (X.pk.dist(cand) < X.pk.dist(old) && claim(p.stamp, owner, X.gen)) {
     ++X.appends;
-    staged_append(kStNext, X.next, X.next_cnt, owner);
+    staged_append(kStNext, X.next.light, X.next.light_cnt, owner);
   }
 }
 
@@ -366,8 +380,7 @@ __device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const O
     if (nd < X.threshold) {
       if (claim(p.stamp, dst, X.gen)) {
         ++X.appends;
-        list_append(dst, p.g.out_desc[dst].len, p.heavy_degree, X.next, X.next_cnt, X.next_heavy,
-                    X.next_heavy_cnt);
+        list_append(X.next, dst, p.g.out_desc[dst].len, p.heavy_degree);
       }
     } else if (atomicExch(&p.in_far[dst], 1) == 0) {
       ++X.appends;
@@ -530,47 +543,73 @@ __device__ __forceinline__ void warp_rows(const SsspParams& p, Ctx& X, int owner
   }
 }
 
-__device__ __forceinline__ int find_heavy(const int2* list, int count, long long chunk) {
-  int lo = 0, hi = count - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (static_cast<long long>(__ldcg(&list[mid].y)) <= chunk) lo = mid;
-    else hi = mid - 1;
+// The heavy entry whose chunk range holds chunk `ch`: a 32-ary search by the whole warp (each
+// lane probes one pivot per step), so a lookup costs about log32(count) dependent loads.
+__device__ __forceinline__ int find_heavy(const int2* list, int count, long long ch) {
+  const int lane = threadIdx.x & 31;
+  int lo = 0, hi = count;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const int stride = (hi - lo + 31) >> 5;
+    const int probe = lo + lane * stride;
+    const bool ok = probe < hi && static_cast<long long>(__ldcg(&list[probe].y)) <= ch;
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    const int last = 31 - __clz(bal);  // lane 0 always holds (list[lo].y <= ch)
+    lo = lo + last * stride;
+    hi = min(hi, lo + stride);
   }
   return lo;
 }
 
-// Expand a frontier: light rows in groups of 32 per warp, heavy rows in 1024-slot chunks over all
-// warps of the grid.  push / walk expand out-rows, pull expands in-rows.
+// Expand a frontier: light rows in balanced groups of up to 32 per warp, medium rows one per warp,
+// heavy rows in kHeavyChunk-slot chunks over all warps.  push / walk expand out-rows, pull
+// expands in-rows.
 template <int MODE>
 __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_count,
-                       const int2* heavy, u64 heavy_cnt, long long gwarp, long long nwarps) {
+                       const int* med, int med_count, const int2* heavy, u64 heavy_cnt,
+                       long long gwarp, long long nwarps) {
   const int lane = threadIdx.x & 31;
   const RowDesc* descs = MODE == kPull ? p.g.in_desc : p.g.out_desc;
-  // every warp takes `per` consecutive vertices (at most 32), so that a frontier smaller than
-  // 32 x warps still reaches every warp
-  long long per = (light_count + nwarps - 1) / nwarps;
-  per = per < 1 ? 1 : (per > 32 ? 32 : per);
-  for (long long base = gwarp * per; base < light_count; base += nwarps * per) {
-    const long long i = base + lane;
-    int owner = -1;
-    u64 du = 0;
-    RowDesc desc{0, 0};
-    if (lane < per && i < light_count) {
-      owner = ld_cg(&light[i]);
-      ++X.rows;
-      if (MODE == kPush) {
-        const u64 word = ld_cg(&p.packed[owner]);
-        if (word != kPackedInf) {
-          du = X.pk.dist(word);
+  // light: `per` consecutive vertices per warp, balanced so that every warp runs the same
+  // number of rounds
+  if (light_count > 0) {
+    const long long rounds = (light_count + nwarps * 32 - 1) / (nwarps * 32);
+    long long per = (light_count + rounds * nwarps - 1) / (rounds * nwarps);
+    per = per < 1 ? 1 : (per > 32 ? 32 : per);
+    for (long long base = gwarp * per; base < light_count; base += nwarps * per) {
+      const long long i = base + lane;
+      int owner = -1;
+      u64 du = 0;
+      RowDesc desc{0, 0};
+      if (lane < per && i < light_count) {
+        owner = ld_cg(&light[i]);
+        ++X.rows;
+        if (MODE == kPush) {
+          const u64 word = ld_cg(&p.packed[owner]);
+          if (word != kPackedInf) {
+            du = X.pk.dist(word);
+            desc = descs[owner];
+          }
+        } else {
           desc = descs[owner];
         }
-      } else {
-        desc = descs[owner];
       }
+      warp_rows<MODE>(p, X, owner, du, desc.start, desc.len);
     }
-    warp_rows<MODE>(p, X, owner, du, desc.start, desc.len);
   }
+  // medium: one row per warp
+  for (long long i = gwarp; i < med_count; i += nwarps) {
+    const int owner = ld_cg(&med[i]);
+    u64 du = 0;
+    if (MODE == kPush) {
+      const u64 word = ld_cg(&p.packed[owner]);
+      if (word == kPackedInf) continue;
+      du = X.pk.dist(word);
+    }
+    if (lane == 0) ++X.rows;
+    const RowDesc desc = descs[owner];
+    warp_slots<MODE>(p, X, owner, du, desc.start, 0, desc.len);
+  }
+  // heavy: chunks
   const int hcount = static_cast<int>(heavy_cnt >> 40);
   const long long chunks = static_cast<long long>(heavy_cnt & ((1ULL << 40) - 1));
   for (long long ch = gwarp; ch < chunks; ch += nwarps) {
@@ -590,6 +629,7 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     warp_slots<MODE>(p, X, owner, du, desc.start, e0, e1);
   }
 }
+
 
 __device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
   p.packed[v] = kPackedInf;
@@ -674,8 +714,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
             touch(p, static_cast<int>(v));
             add_candidate(p, v);
             ++w_inval;
-            list_append(v, p.g.out_desc[v].len, p.heavy_degree, p.near_a, &c->walk_cnt[0],
-                        p.heavy_a, &c->walk_heavy[0]);
+            const ListSet W0{p.near_a, &c->walk_cnt[0], p.near_med_a, &c->walk_med_cnt[0],
+                             p.heavy_a, &c->walk_heavy[0], kStNext, kStNextMed};
+            list_append(W0, v, p.g.out_desc[v].len, p.heavy_degree);
           }
         }
       }
@@ -777,22 +818,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
       while (true) {
         const int cs = level % 3;
         const int nc = ld_cg(&c->walk_cnt[cs]);
+        const int mc = ld_cg(&c->walk_med_cnt[cs]);
         const u64 hc = ld_cg(&c->walk_heavy[cs]);
-        if (nc == 0 && (hc >> 40) == 0) break;
+        if (nc == 0 && mc == 0 && (hc >> 40) == 0) break;
         if (level > n + 1) {
           if (tid == 0) atomicOr(&c->error, kErrNotConverged);
           break;
         }
-        X.next = (level & 1) ? p.near_a : p.near_b;
-        X.next_cnt = &c->walk_cnt[(level + 1) % 3];
-        X.next_heavy = (level & 1) ? p.heavy_a : p.heavy_b;
-        X.next_heavy_cnt = &c->walk_heavy[(level + 1) % 3];
+        const int nb = (level + 1) & 1;
+        X.next = ListSet{nb ? p.near_b : p.near_a, &c->walk_cnt[(level + 1) % 3],
+                         nb ? p.near_med_b : p.near_med_a, &c->walk_med_cnt[(level + 1) % 3],
+                         nb ? p.heavy_b : p.heavy_a, &c->walk_heavy[(level + 1) % 3], kStNext,
+                         kStNextMed};
         if (tid == 0) {
           c->walk_cnt[(level + 2) % 3] = 0;
+          c->walk_med_cnt[(level + 2) % 3] = 0;
           c->walk_heavy[(level + 2) % 3] = 0;
         }
-        expand<kWalk>(p, X, (level & 1) ? p.near_b : p.near_a, nc,
-                      (level & 1) ? p.heavy_b : p.heavy_a, hc, gwarp, nwarps);
+        const int cb = level & 1;
+        expand<kWalk>(p, X, cb ? p.near_b : p.near_a, nc, cb ? p.near_med_b : p.near_med_a, mc,
+                      cb ? p.heavy_b : p.heavy_a, hc, gwarp, nwarps);
         if (!grid_barrier(c, bar)) return;
         ++level;
       }
@@ -840,11 +885,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
     {
       Ctx Y = X;
       Y.gen = gen_pull;
-      Y.next = p.frontier;
-      Y.next_cnt = &c->frontier_count;
+      Y.next = ListSet{p.frontier, &c->frontier_count, nullptr, nullptr, nullptr, nullptr, kStNext,
+                       kStNextMed};
       Y.slots = Y.words = Y.atomics = Y.appends = Y.rows = 0;
-      expand<kPull>(p, Y, p.candidates, ld_cg(&c->cand_count), p.pull_heavy,
-                    ld_cg(&c->pull_heavy), gwarp, nwarps);
+      expand<kPull>(p, Y, p.candidates, ld_cg(&c->cand_count), p.cand_med,
+                    ld_cg(&c->cand_med_count), p.pull_heavy, ld_cg(&c->pull_heavy), gwarp, nwarps);
       pull_slots = Y.slots;
       pull_words = Y.words;
       pull_rows = Y.rows;
@@ -866,6 +911,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   const u64 smallest = ld_cg(reinterpret_cast<const u64*>(&c->minimum));
   X.threshold = (smallest == kPackedInf ? 0 : smallest) + delta;
   int* lists[2] = {p.near_a, p.near_b};
+  int* mlists[2] = {p.near_med_a, p.near_med_b};
   int2* hlists[2] = {p.heavy_a, p.heavy_b};
   int* far = p.far_a;
   int* far2 = p.far_b;
@@ -877,8 +923,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
     const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
     if (d < X.threshold) {
       if (claim(p.stamp, v, gen))
-        list_append(v, p.g.out_desc[v].len, p.heavy_degree, lists[0], &c->near_cnt[0], hlists[0],
-                    &c->heavy_cnt[0]);
+        list_append(ListSet{lists[0], &c->near_cnt[0], mlists[0], &c->near_med_cnt[0], hlists[0],
+                            &c->heavy_cnt[0], kStNext, kStNextMed},
+                    v, p.g.out_desc[v].len, p.heavy_degree);
     } else if (atomicExch(&p.in_far[v], 1) == 0) {
       staged_append(kStFar, far, &c->far_count, v);
     }
@@ -892,32 +939,35 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   while (true) {
     const int cs = it % 3;
     const int nc = ld_cg(&c->near_cnt[cs]);
+    const int mc = ld_cg(&c->near_med_cnt[cs]);
     const u64 hc = ld_cg(&c->heavy_cnt[cs]);
     const int step = iterations + epochs;
     if (tid == 0 && step < 64) {
-      c->trace_n[step] = nc;
+      c->trace_n[step] = nc + mc;
       c->trace_h[step] = static_cast<int>(hc & 0xffffffffu);
       c->trace_t[step] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
       c->trace_len = step + 1;
     }
-    if (nc > 0 || (hc >> 40) > 0) {
+    if (nc > 0 || mc > 0 || (hc >> 40) > 0) {
       ++iterations;
       if (iterations > iteration_cap) {
         if (tid == 0) atomicOr(&c->error, kErrNotConverged);
         break;
       }
-      pushes += nc + static_cast<long long>(hc >> 40);
+      pushes += nc + mc + static_cast<long long>(hc >> 40);
       X.gen = ++gen;
-      X.next = lists[(it + 1) & 1];
-      X.next_cnt = &c->near_cnt[(it + 1) % 3];
-      X.next_heavy = hlists[(it + 1) & 1];
-      X.next_heavy_cnt = &c->heavy_cnt[(it + 1) % 3];
+      const int nb = (it + 1) & 1;
+      X.next = ListSet{lists[nb], &c->near_cnt[(it + 1) % 3], mlists[nb],
+                       &c->near_med_cnt[(it + 1) % 3], hlists[nb], &c->heavy_cnt[(it + 1) % 3],
+                       kStNext, kStNextMed};
       X.far = far;
       if (tid == 0) {
         c->near_cnt[(it + 2) % 3] = 0;
+        c->near_med_cnt[(it + 2) % 3] = 0;
         c->heavy_cnt[(it + 2) % 3] = 0;
       }
-      expand<kPush>(p, X, lists[it & 1], nc, hlists[it & 1], hc, gwarp, nwarps);
+      expand<kPush>(p, X, lists[it & 1], nc, mlists[it & 1], mc, hlists[it & 1], hc, gwarp,
+                    nwarps);
       if (!grid_barrier(c, bar)) return;
       ++it;
       continue;
@@ -943,8 +993,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
       if (d < X.threshold) {
         p.in_far[v] = 0;
         if (claim(p.stamp, v, gen))
-          list_append(v, p.g.out_desc[v].len, p.heavy_degree, lists[it & 1], &c->near_cnt[cs],
-                      hlists[it & 1], &c->heavy_cnt[cs]);
+          list_append(ListSet{lists[it & 1], &c->near_cnt[cs], mlists[it & 1],
+                              &c->near_med_cnt[cs], hlists[it & 1], &c->heavy_cnt[cs], kStNext,
+                              kStNextMed},
+                      v, p.g.out_desc[v].len, p.heavy_degree);
       } else {
         staged_append(kStFar, far2, &c->far2_count, v);
       }
@@ -1118,6 +1170,9 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
   p.heavy_a = reinterpret_cast<int2*>(ws.heavy_a.ptr);
   p.heavy_b = reinterpret_cast<int2*>(ws.heavy_b.ptr);
   p.pull_heavy = reinterpret_cast<int2*>(ws.pull_heavy.ptr);
+  p.cand_med = ws.cand_med.ptr;
+  p.near_med_a = ws.near_med_a.ptr;
+  p.near_med_b = ws.near_med_b.ptr;
   p.touched = ws.touched.ptr;
   p.ctl = ws.ctl.ptr;
   return p;
@@ -1159,7 +1214,7 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
   p.generation = ws.next_generation(1, s);
   p.touch_gen = 1;
   p.heavy_degree = ctx.schedule_set && ctx.schedule.heavy_degree > 0 ? ctx.schedule.heavy_degree
-                                                                      : 2048;
+                                                                      : 256;
   p.delta_override = 0;
   const dyngb200_schedule sched = ctx.schedule_set ? ctx.schedule : dyngb200_schedule{};
   const int blocks = persistent_blocks(ctx, sched);
@@ -1233,7 +1288,7 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     p.offer_heads = t.canonical ? 1 : 0;
     p.generation = ws.next_generation(1, s);
     p.touch_gen = p.generation;
-    p.heavy_degree = sched.heavy_degree > 0 ? sched.heavy_degree : 2048;
+    p.heavy_degree = sched.heavy_degree > 0 ? sched.heavy_degree : 256;
     p.delta_override = sched.delta;
     launch(ctx, p, blocks);
     DYNGB200_CUDA(cudaEventRecord(e2, s));
