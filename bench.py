@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--delta", type=int, default=0)
     ap.add_argument("--grid-blocks", type=int, default=0)
     ap.add_argument("--heavy-degree", type=int, default=0)
+    ap.add_argument("--small", type=int, default=0, help="small-frontier size (0 default, -1 off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
     return ap.parse_args()
@@ -230,9 +231,10 @@ def main():
                                       b.delete_src.size)
 
     sched = None
-    if args.invalidation or args.delta or args.grid_blocks or args.heavy_degree:
+    if args.invalidation or args.delta or args.grid_blocks or args.heavy_degree or args.small:
         sched = D.sssp.Schedule(delta=args.delta, grid_blocks=args.grid_blocks,
-                                invalidation=args.invalidation, heavy_degree=args.heavy_degree)
+                                invalidation=args.invalidation, heavy_degree=args.heavy_degree,
+                                small_frontier=args.small)
     host_lat = []
     timed_stats = []
     lat = []

@@ -132,6 +132,9 @@ struct UpdateCtl {
   u64 minimum;
   int changed;         // the batch holds a deleted or weight-increased edge
   int last_generation; // last stamp generation the kernel used
+  int loop_state[6];   // near-far state handed from block 0 back to the grid
+  long long loop_pushes;
+  u64 loop_threshold;
   // work counters (algorithmic traffic) and phase timestamps of the sssp kernel
   long long work[12];
   unsigned long long phase_ns[8];

@@ -36,6 +36,7 @@ struct SsspParams {
   int tree_bits;         // format of the persistent words (-1: none); another format is rebuilt
   long long tree_n;      // vertices the tree held before this call (growth fills the rest)
   int walk;              // invalidation by a subtree walk instead of pointer jumping
+  int tree_trusted;      // computed or validated: no parent cycle possible
   int offer_heads;       // canonical tree: insertion heads take the inserted edge's offer
   // pairs of the applier (update only) and the batch weights
   const u64* pair_key;
@@ -68,6 +69,7 @@ struct SsspParams {
   int touch_gen;
   int heavy_degree;
   long long delta_override;
+  int small_frontier;    // frontiers up to this size run on block 0 alone (0: never)
   UpdateCtl* ctl;
 };
 
@@ -637,6 +639,129 @@ __device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
   add_candidate(p, v);
 }
 
+// State of the near-far loop carried across a switch between the whole grid and one block.
+struct LoopState {
+  int gen;
+  int it;           // push iterations so far (selects the list buffers and counter slots)
+  int iterations;
+  int epochs;
+  int far_parity;   // which of far_a / far_b is the current far pile
+  int done;
+  long long pushes;
+  u64 threshold;
+};
+
+constexpr int kSmallFarMax = 4096;
+constexpr int kDefaultSmall = 256;  // the heuristic: frontiers up to 256 vertices run on one block
+
+__device__ __forceinline__ void block_barrier() {
+  stage_flush();
+  __threadfence();
+  __syncthreads();
+}
+
+// The near-far loop (fused.cuh:288-417) run by the whole grid (BLOCK = false) or by block 0 alone
+// (BLOCK = true, between block barriers: frontiers of up to `small` vertices do not pay for a grid
+// barrier per step).  Returns 0 when the loop is finished, 1 when the grid should hand over to
+// block 0 (small frontier) or block 0 back to the grid, -1 on a timeout.
+template <bool BLOCK>
+__device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar, u64 delta,
+                        long long iteration_cap, int small) {
+  UpdateCtl* c = p.ctl;
+  const long long tid = BLOCK ? threadIdx.x : blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long threads = BLOCK ? blockDim.x : static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long gwarp = tid >> 5;
+  const long long nwarps = threads >> 5;
+  const bool leader = BLOCK ? threadIdx.x == 0 : tid == 0;
+  int* lists[2] = {p.near_a, p.near_b};
+  int* mlists[2] = {p.near_med_a, p.near_med_b};
+  int2* hlists[2] = {p.heavy_a, p.heavy_b};
+  const Packing pk = X.pk;
+  while (true) {
+    const int cs = S.it % 3;
+    const int nc = ld_cg(&c->near_cnt[cs]);
+    const int mc = ld_cg(&c->near_med_cnt[cs]);
+    const u64 hc = ld_cg(&c->heavy_cnt[cs]);
+    const int far_count = ld_cg(&c->far_count);
+    const bool near_work = nc > 0 || mc > 0 || (hc >> 40) > 0;
+    const bool fits_block =
+        (hc >> 40) == 0 && nc + mc <= small && (near_work || far_count <= kSmallFarMax);
+    if (!near_work && far_count == 0) return 0;
+    if (small > 0 && (BLOCK ? !fits_block : fits_block)) return 1;
+    int* far = S.far_parity ? p.far_b : p.far_a;
+    int* far2 = S.far_parity ? p.far_a : p.far_b;
+    const int step = S.iterations + S.epochs;
+    if (leader && blockIdx.x == 0 && step < 64) {
+      c->trace_n[step] = near_work ? nc + mc : -far_count;
+      c->trace_h[step] = static_cast<int>(hc & 0xffffffffu) | (BLOCK ? 0x40000000 : 0);
+      c->trace_t[step] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
+      c->trace_len = step + 1;
+    }
+    if (near_work) {
+      ++S.iterations;
+      if (S.iterations > iteration_cap) {
+        if (leader) atomicOr(&c->error, kErrNotConverged);
+        return 0;
+      }
+      S.pushes += nc + mc + static_cast<long long>(hc >> 40);
+      X.gen = ++S.gen;
+      const int nb = (S.it + 1) & 1;
+      X.next = ListSet{lists[nb], &c->near_cnt[(S.it + 1) % 3], mlists[nb],
+                       &c->near_med_cnt[(S.it + 1) % 3], hlists[nb],
+                       &c->heavy_cnt[(S.it + 1) % 3], kStNext, kStNextMed};
+      X.far = far;
+      X.far_cnt = &c->far_count;
+      X.threshold = S.threshold;
+      if (leader) {
+        c->near_cnt[(S.it + 2) % 3] = 0;
+        c->near_med_cnt[(S.it + 2) % 3] = 0;
+        c->heavy_cnt[(S.it + 2) % 3] = 0;
+      }
+      expand<kPush>(p, X, lists[S.it & 1], nc, mlists[S.it & 1], mc, hlists[S.it & 1], hc, gwarp,
+                    nwarps);
+      if (BLOCK) block_barrier();
+      else if (!grid_barrier(c, bar)) return -1;
+      ++S.it;
+      continue;
+    }
+    // near frontier empty: raise the threshold past the far pile
+    ++S.epochs;
+    u64 local = kPackedInf;
+    for (long long i = tid; i < far_count; i += threads) {
+      const u64 word = ld_cg(&p.packed[ld_cg(&far[i])]);
+      if (word != kPackedInf) local = min(local, pk.dist(word));
+    }
+    warp_min_into(local, &c->minimum);
+    if (BLOCK) block_barrier();
+    else if (!grid_barrier(c, bar)) return -1;
+    S.threshold = max(S.threshold, ld_cg(reinterpret_cast<const u64*>(&c->minimum))) + delta;
+    ++S.gen;
+    const ListSet now{lists[S.it & 1], &c->near_cnt[cs], mlists[S.it & 1], &c->near_med_cnt[cs],
+                      hlists[S.it & 1], &c->heavy_cnt[cs], kStNext, kStNextMed};
+    for (long long i = tid; i < far_count; i += threads) {
+      const int v = ld_cg(&far[i]);
+      const u64 word = ld_cg(&p.packed[v]);
+      const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
+      if (d < S.threshold) {
+        p.in_far[v] = 0;
+        if (claim(p.stamp, v, S.gen)) list_append(now, v, p.g.out_desc[v].len, p.heavy_degree);
+      } else {
+        staged_append(kStFar, far2, &c->far2_count, v);
+      }
+    }
+    if (BLOCK) block_barrier();
+    else if (!grid_barrier(c, bar)) return -1;
+    if (leader) {
+      c->far_count = ld_cg(&c->far2_count);
+      c->far2_count = 0;
+      c->minimum = kPackedInf;
+    }
+    if (BLOCK) block_barrier();
+    else if (!grid_barrier(c, bar)) return -1;
+    S.far_parity ^= 1;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   UpdateCtl* c = p.ctl;
   if (ld_volatile(&c->error) != 0) return;
@@ -705,15 +830,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
         const u64 key = p.pair_key[slot];
         const int32_t u = static_cast<int32_t>(key >> 32);
         const int32_t v = static_cast<int32_t>(key & 0xffffffffu);
-        if (v < p.tree_n && p.parent[v] == u) {
-          if (!p.walk) {
-            p.flag[v] = 1;
-          } else if (claim(p.stamp, v, gen_inv)) {
-            // walk: roots are invalidated here and start the first level
-            p.packed[v] = kPackedInf;
-            touch(p, static_cast<int>(v));
-            add_candidate(p, v);
-            ++w_inval;
+        if (v < p.tree_n && p.parent[v] == u && claim(p.stamp, v, gen_inv)) {
+          // roots are invalidated here (stamp = gen_inv marks the invalidated vertices)
+          invalidate(p, static_cast<int>(v));
+          ++w_inval;
+          changed = 2;
+          if (p.walk) {
             const ListSet W0{p.near_a, &c->walk_cnt[0], p.near_med_a, &c->walk_med_cnt[0],
                              p.heavy_a, &c->walk_heavy[0], kStNext, kStNextMed};
             list_append(W0, v, p.g.out_desc[v].len, p.heavy_degree);
@@ -721,29 +843,22 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
         }
       }
     }
-    if (__any_sync(0xffffffffu, changed) && lane == 0) c->changed = 1;
-    if (!p.walk) {
-      for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
-        int a[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const long long v = v0 + q * threads;
-          a[q] = v < p.tree_n ? p.parent[v] : -1;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const long long v = v0 + q * threads;
-          if (v < n) p.ancestor[v] = a[q];
-        }
-      }
-      w_visits += (n - tid + threads - 1) / threads;
-    }
+    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(&c->changed, 1);
+    if (__any_sync(0xffffffffu, changed == 2) && lane == 0) atomicOr(&c->changed, 2);
     if (!grid_barrier(c, bar)) return;
     if (ld_volatile(&c->error)) return;
     if (tid == 0) c->phase_ns[1] = global_ns();
-    const bool any_changed = ld_cg(&c->changed) != 0;
+    // pointer jumping runs when roots exist, or (a tree imported without validation) when any
+    // edge changed, so that a parent cycle is still reported as the reference reports it
+    const int changed_bits = ld_cg(&c->changed);
+    const bool any_changed = (changed_bits & 2) || (!p.tree_trusted && (changed_bits & 1));
     if (!p.walk) {
       // ---- subtree invalidation by pointer jumping (fused.cuh:199-234) ------------------------
+      // ancestor[v]: >= 0 the current ancestor, -1 the chain ended without a root, kMarked:
+      // invalidated.  Invariant: ancestor[x] >= 0 implies no root on the tree path from x up to
+      // (excluding) ancestor[x].  Round 0 reads the parents and the roots' stamps; a vertex whose
+      // ancestor is invalidated is invalidated on the spot, so no scan follows the rounds.
+      constexpr int kMarked = -2;
       int max_rounds = 0;
       while ((1LL << max_rounds) < n) ++max_rounds;
       ++max_rounds;
@@ -756,29 +871,43 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
           int jumping = 0;
           // four vertices per thread and step, their loads issued together
           for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
-            int a[4], f[4];
+            int a[4], na[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               const long long v = v0 + q * threads;
-              a[q] = v < n ? ld_cg(&p.ancestor[v]) : -1;
-              f[q] = v < n ? ld_cg(&p.flag[v]) : 1;
+              if (v >= n) {
+                a[q] = -1;
+              } else if (round == 0) {
+                a[q] = ld_cg(&p.stamp[v]) == gen_inv ? kMarked : (v < p.tree_n ? p.parent[v] : -1);
+              } else {
+                a[q] = ld_cg(&p.ancestor[v]);
+              }
             }
-            int fa[4], na[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-              const bool live = a[q] >= 0 && !f[q];
-              fa[q] = live ? ld_cg(&p.flag[a[q]]) : 0;
-              na[q] = live ? ld_cg(&p.ancestor[a[q]]) : -1;
+              if (a[q] < 0) {
+                na[q] = a[q];
+              } else if (round == 0) {
+                na[q] = ld_cg(&p.stamp[a[q]]) == gen_inv ? kMarked : p.parent[a[q]];
+              } else {
+                na[q] = ld_cg(&p.ancestor[a[q]]);
+              }
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               const long long v = v0 + q * threads;
               if (v >= n) continue;
               ++w_visits;
-              if (a[q] < 0 || f[q]) continue;
+              if (a[q] < 0) {
+                if (round == 0) p.ancestor[v] = a[q];
+                continue;
+              }
               ++w_jumps;
-              if (fa[q]) {
-                p.flag[v] = 1;
+              if (na[q] == kMarked) {
+                p.ancestor[v] = kMarked;
+                p.stamp[v] = gen_inv;
+                invalidate(p, static_cast<int>(v));
+                ++w_inval;
                 continue;
               }
               p.ancestor[v] = na[q];
@@ -791,26 +920,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
         }
       }
       if (tid == 0) c->phase_ns[2] = global_ns();
-      // ---- invalidate the flagged vertices ------------------------------------------------------
-      if (any_changed) {
-        for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
-          int f[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const long long v = v0 + q * threads;
-            f[q] = v < n ? ld_cg(&p.flag[v]) : 0;
-          }
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            if (!f[q]) continue;
-            const long long v = v0 + q * threads;
-            p.flag[v] = 0;
-            p.stamp[v] = gen_inv;
-            invalidate(p, static_cast<int>(v));
-            ++w_inval;
-          }
-        }
-      }
     } else {
       // ---- subtree invalidation by a walk down the old tree's edges, level by level ---------
       X.gen = gen_inv;
@@ -914,7 +1023,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   int* mlists[2] = {p.near_med_a, p.near_med_b};
   int2* hlists[2] = {p.heavy_a, p.heavy_b};
   int* far = p.far_a;
-  int* far2 = p.far_b;
   X.far_cnt = &c->far_count;
   ++gen;
   for (long long i = tid; i < frontier_count; i += threads) {
@@ -933,85 +1041,42 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   if (!grid_barrier(c, bar)) return;
   if (tid == 0) c->minimum = kPackedInf;
   if (!grid_barrier(c, bar)) return;
-  int iterations = 0, epochs = 0, it = 0;
-  long long pushes = 0;
+  LoopState S{gen, 0, 0, 0, 0, 0, 0, X.threshold};
   const long long iteration_cap = 4 * n + 64;
+  const int small = p.small_frontier;
   while (true) {
-    const int cs = it % 3;
-    const int nc = ld_cg(&c->near_cnt[cs]);
-    const int mc = ld_cg(&c->near_med_cnt[cs]);
-    const u64 hc = ld_cg(&c->heavy_cnt[cs]);
-    const int step = iterations + epochs;
-    if (tid == 0 && step < 64) {
-      c->trace_n[step] = nc + mc;
-      c->trace_h[step] = static_cast<int>(hc & 0xffffffffu);
-      c->trace_t[step] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
-      c->trace_len = step + 1;
-    }
-    if (nc > 0 || mc > 0 || (hc >> 40) > 0) {
-      ++iterations;
-      if (iterations > iteration_cap) {
-        if (tid == 0) atomicOr(&c->error, kErrNotConverged);
-        break;
-      }
-      pushes += nc + mc + static_cast<long long>(hc >> 40);
-      X.gen = ++gen;
-      const int nb = (it + 1) & 1;
-      X.next = ListSet{lists[nb], &c->near_cnt[(it + 1) % 3], mlists[nb],
-                       &c->near_med_cnt[(it + 1) % 3], hlists[nb], &c->heavy_cnt[(it + 1) % 3],
-                       kStNext, kStNextMed};
-      X.far = far;
-      if (tid == 0) {
-        c->near_cnt[(it + 2) % 3] = 0;
-        c->near_med_cnt[(it + 2) % 3] = 0;
-        c->heavy_cnt[(it + 2) % 3] = 0;
-      }
-      expand<kPush>(p, X, lists[it & 1], nc, mlists[it & 1], mc, hlists[it & 1], hc, gwarp,
-                    nwarps);
-      if (!grid_barrier(c, bar)) return;
-      ++it;
-      continue;
-    }
-    // near frontier empty: raise the threshold past the far pile
-    const int far_count = ld_cg(&c->far_count);
-    if (far_count == 0) break;
-    if (tid == 0 && step < 64) c->trace_n[step] = -far_count;  // an epoch: the far pile size
-    ++epochs;
-    local = kPackedInf;
-    for (long long i = tid; i < far_count; i += threads) {
-      const u64 word = ld_cg(&p.packed[ld_cg(&far[i])]);
-      if (word != kPackedInf) local = min(local, pk.dist(word));
-    }
-    warp_min_into(local, &c->minimum);
-    if (!grid_barrier(c, bar)) return;
-    X.threshold = max(X.threshold, ld_cg(reinterpret_cast<const u64*>(&c->minimum))) + delta;
-    ++gen;
-    for (long long i = tid; i < far_count; i += threads) {
-      const int v = ld_cg(&far[i]);
-      const u64 word = ld_cg(&p.packed[v]);
-      const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
-      if (d < X.threshold) {
-        p.in_far[v] = 0;
-        if (claim(p.stamp, v, gen))
-          list_append(ListSet{lists[it & 1], &c->near_cnt[cs], mlists[it & 1],
-                              &c->near_med_cnt[cs], hlists[it & 1], &c->heavy_cnt[cs], kStNext,
-                              kStNextMed},
-                      v, p.g.out_desc[v].len, p.heavy_degree);
-      } else {
-        staged_append(kStFar, far2, &c->far2_count, v);
+    const int r = near_far<false>(p, X, S, bar, delta, iteration_cap, small);
+    if (r < 0) return;
+    if (r == 0) break;
+    // a small frontier: block 0 runs the loop alone while the other blocks wait at one barrier
+    if (blockIdx.x == 0) {
+      const int rb = near_far<true>(p, X, S, bar, delta, iteration_cap, small);
+      if (threadIdx.x == 0) {
+        S.done = rb == 0 ? 1 : 0;
+        c->loop_state[0] = S.gen;
+        c->loop_state[1] = S.it;
+        c->loop_state[2] = S.iterations;
+        c->loop_state[3] = S.epochs;
+        c->loop_state[4] = S.far_parity;
+        c->loop_state[5] = S.done;
+        c->loop_pushes = S.pushes;
+        c->loop_threshold = S.threshold;
       }
     }
     if (!grid_barrier(c, bar)) return;
-    if (tid == 0) {
-      c->far_count = ld_cg(&c->far2_count);
-      c->far2_count = 0;
-      c->minimum = kPackedInf;
-    }
-    if (!grid_barrier(c, bar)) return;
-    int* t = far;
-    far = far2;
-    far2 = t;
+    S.gen = ld_cg(&c->loop_state[0]);
+    S.it = ld_cg(&c->loop_state[1]);
+    S.iterations = ld_cg(&c->loop_state[2]);
+    S.epochs = ld_cg(&c->loop_state[3]);
+    S.far_parity = ld_cg(&c->loop_state[4]);
+    S.done = ld_cg(&c->loop_state[5]);
+    S.pushes = ld_cg(&c->loop_pushes);
+    S.threshold = ld_cg(&c->loop_threshold);
+    if (S.done) break;
   }
+  gen = S.gen;
+  const int iterations = S.iterations, epochs = S.epochs;
+  const long long pushes = S.pushes;
   if (tid == 0) c->phase_ns[6] = global_ns();
 
   // ---- commit: unpack (fused.cuh:419-494) ------------------------------------------------------
@@ -1217,6 +1282,8 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
                                                                       : 256;
   p.delta_override = 0;
   const dyngb200_schedule sched = ctx.schedule_set ? ctx.schedule : dyngb200_schedule{};
+  p.small_frontier = sched.small_frontier > 0 ? sched.small_frontier
+                                              : (sched.small_frontier < 0 ? 0 : kDefaultSmall);
   const int blocks = persistent_blocks(ctx, sched);
   cudaEvent_t e0, e1;
   DYNGB200_CUDA(cudaEventCreate(&e0));
@@ -1286,9 +1353,12 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     p.k = g.k;
     p.walk = (sched.invalidation == 1 && t.trusted) ? 1 : 0;
     p.offer_heads = t.canonical ? 1 : 0;
+    p.tree_trusted = t.trusted ? 1 : 0;
     p.generation = ws.next_generation(1, s);
     p.touch_gen = p.generation;
     p.heavy_degree = sched.heavy_degree > 0 ? sched.heavy_degree : 256;
+    p.small_frontier = sched.small_frontier > 0 ? sched.small_frontier
+                                                : (sched.small_frontier < 0 ? 0 : kDefaultSmall);
     p.delta_override = sched.delta;
     launch(ctx, p, blocks);
     DYNGB200_CUDA(cudaEventRecord(e2, s));

@@ -143,7 +143,7 @@ typedef struct dyngb200_schedule {
   int64_t delta;          /* near-far bucket width (0: heuristic) */
   int32_t grid_blocks;    /* persistent grid size (0: occupancy x SMs) */
   int32_t invalidation;   /* 0 heuristic/pointer jumping, 1 subtree walk */
-  int32_t small_frontier; /* frontiers up to this size run on one block between grid barriers (0 off) */
+  int32_t small_frontier; /* frontiers up to this many vertices run on one block (0: 256, < 0: off) */
   int32_t heavy_degree;   /* rows longer than this are split across warps (0: default) */
 } dyngb200_schedule;
 

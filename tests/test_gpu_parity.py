@@ -219,3 +219,42 @@ def test_rmat_scale16_batch():
     # every finite distance fits in 31 bits at this size
     fin = t.distances[t.distances < INF // 2]
     assert fin.max() < 2**31
+
+
+def test_schedules_never_change_results():
+    # sssp::options::delta and the schedule are tunables (sssp.hpp:78-94): every schedule gives
+    # the same bytes as the oracle
+    e = G.rmat(13, 8, w_max=1000, seed=11)
+    rp, col, w = e.csr()
+    og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
+    ot, _ = O.compute(og, 0, rule=1)
+    schedules = [None, D.sssp.Schedule(delta=1), D.sssp.Schedule(delta=100000),
+                 D.sssp.Schedule(grid_blocks=7), D.sssp.Schedule(small_frontier=-1),
+                 D.sssp.Schedule(small_frontier=100000), D.sssp.Schedule(invalidation=1),
+                 D.sssp.Schedule(heavy_degree=33), D.sssp.Schedule(heavy_degree=100000)]
+    graphs = [(D.Graph.from_csr(rp, col, w), s) for s in schedules]
+    trees = [D.sssp.compute(g, 0) for g, _ in graphs]
+    stream = G.BatchStream(e, seed=3)
+    for step in range(3):
+        b = stream.next(600, 0.75, 0.5, parents=ot.parents)
+        ost, _ = O.update(og, _obatch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                                      b.delete_dst), ot)
+        for (g, sched), t in zip(graphs, trees):
+            st = D.sssp.update(g, _batch(b.insert_src, b.insert_dst, b.insert_weights,
+                                         b.delete_src, b.delete_dst), t, schedule=sched)
+            np.testing.assert_array_equal(t.distances, ot.distances, err_msg=str(sched))
+            np.testing.assert_array_equal(t.parents, ot.parents, err_msg=str(sched))
+            assert (st.invalidated, st.affected) == (ost["invalidated"], ost["affected"])
+
+
+def test_unvalidated_cycle_is_reported_and_poisons():
+    # sssp_cuda_test.cpp:982: a parent cycle in a tree imported without validation is found by
+    # pointer jumping; the graph keeps the batch, the result is poisoned
+    g, _ = _pair(4, [(0, 1, 1), (1, 2, 1), (2, 1, 1), (2, 3, 1)], None)
+    t = D.sssp.Result.from_arrays(g, 0, [0, 1, 2, 3], [-1, 2, 1, 2], canonicalize=False,
+                                  options=D.sssp.Options(validate_inputs=False))
+    with pytest.raises(D.InvalidArgumentError):
+        D.sssp.update(g, _batch(del_src=[2], del_dst=[3]), t)
+    assert g.version() == 1
+    with pytest.raises(D.StaleResultError):
+        t.distances
