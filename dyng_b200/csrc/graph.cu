@@ -224,18 +224,46 @@ __global__ void k_plan(ApplyParams p) {
   }
 }
 
-__device__ void touch_row(const ApplyParams& p, int side, int32_t r) {
-  int* stamp = side == 0 ? p.touch_out_stamp : p.touch_in_stamp;
-  if (atomicExch(&stamp[r], p.touch_gen) == p.touch_gen) return;
-  UpdateCtl* c = p.ctl;
-  const int slot = append_slot(side == 0 ? &c->rows_out : &c->rows_in);
+// Block-staged list appends of k_pairs: new pairs and newly touched rows are collected in shared
+// memory and copied to the global lists with one atomicAdd per block and list at the end of the
+// kernel (a full stage falls back to direct global appends).
+constexpr int kPairStageCap = 1024;
+struct PairStage {
+  int cnt[3];
+  int base[3];
+  int data[3][kPairStageCap];  // 0: pair slots, 1: out rows, 2: in rows
+};
+
+__device__ __forceinline__ void place_row(const ApplyParams& p, int side, int32_t r, int slot) {
   (side == 0 ? p.rows_out : p.rows_in)[slot] = r;
   (side == 0 ? p.row_slot_out : p.row_slot_in)[r] = slot;
   (side == 0 ? p.dels_out : p.dels_in)[slot] = 0;
   (side == 0 ? p.apps_out : p.apps_in)[slot] = 0;
 }
 
-__device__ void add_op(const ApplyParams& p, int32_t u, int32_t v, int kind, int index) {
+__device__ __forceinline__ void stage_put(PairStage& st, const ApplyParams& p, int list, int v) {
+  const int pos = atomicAdd(&st.cnt[list], 1);
+  if (pos < kPairStageCap) {
+    st.data[list][pos] = v;
+    return;
+  }
+  UpdateCtl* c = p.ctl;
+  if (list == 0) {
+    p.list[append_slot(&c->pairs)] = v;
+  } else {
+    const int side = list - 1;
+    place_row(p, side, v, append_slot(side == 0 ? &c->rows_out : &c->rows_in));
+  }
+}
+
+__device__ void touch_row(PairStage& st, const ApplyParams& p, int side, int32_t r) {
+  int* stamp = side == 0 ? p.touch_out_stamp : p.touch_in_stamp;
+  if (atomicExch(&stamp[r], p.touch_gen) == p.touch_gen) return;
+  stage_put(st, p, 1 + side, r);
+}
+
+__device__ void add_op(PairStage& st, const ApplyParams& p, int32_t u, int32_t v, int kind,
+                       int index) {
   const u64 k = pair_key(u, v);
   unsigned h = static_cast<unsigned>(mix64(k)) & static_cast<unsigned>(p.mask);
   int slot = -1;
@@ -249,9 +277,9 @@ __device__ void add_op(const ApplyParams& p, int32_t u, int32_t v, int kind, int
       p.in_pos2[slot] = -1;
       p.out_count[slot] = 0;
       p.in_count[slot] = 0;
-      p.list[append_slot(&p.ctl->pairs)] = slot;
-      touch_row(p, 0, u);
-      touch_row(p, 1, v);
+      stage_put(st, p, 0, slot);
+      touch_row(st, p, 0, u);
+      touch_row(st, p, 1, v);
       break;
     }
     if (prev == k) {
@@ -275,8 +303,11 @@ __device__ void add_op(const ApplyParams& p, int32_t u, int32_t v, int kind, int
 
 // ---- C: group the effective operations by (u, v) pair ------------------------------------------
 __global__ void k_pairs(ApplyParams p) {
+  __shared__ PairStage st;
   UpdateCtl* c = p.ctl;
   if (c->error) return;
+  if (threadIdx.x < 3) st.cnt[threadIdx.x] = 0;
+  __syncthreads();
   const long long total = p.ni + p.nd;
   const long long n_after = c->n_after;
   long long missing = 0;
@@ -285,8 +316,8 @@ __global__ void k_pairs(ApplyParams p) {
     if (i < p.ni) {
       const int32_t u = p.ins_src[i], v = p.ins_dst[i];
       if (u == v && p.props.on_self_loop != 0) continue;
-      add_op(p, u, v, 1, static_cast<int>(i));
-      if (!p.props.directed && u != v) add_op(p, v, u, 1, static_cast<int>(i));
+      add_op(st, p, u, v, 1, static_cast<int>(i));
+      if (!p.props.directed && u != v) add_op(st, p, v, u, 1, static_cast<int>(i));
     } else {
       const long long j = i - p.ni;
       const int32_t u = p.del_src[j], v = p.del_dst[j];
@@ -299,11 +330,27 @@ __global__ void k_pairs(ApplyParams p) {
         }
         continue;
       }
-      add_op(p, u, v, 0, static_cast<int>(j));
-      if (!p.props.directed && u != v) add_op(p, v, u, 0, static_cast<int>(j));
+      add_op(st, p, u, v, 0, static_cast<int>(j));
+      if (!p.props.directed && u != v) add_op(st, p, v, u, 0, static_cast<int>(j));
     }
   }
   warp_add(missing, &c->summary[4]);
+  // flush the stages: one global atomic per list and block
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int n = min(st.cnt[threadIdx.x], kPairStageCap);
+    int* counter = threadIdx.x == 0 ? &c->pairs : (threadIdx.x == 1 ? &c->rows_out : &c->rows_in);
+    st.base[threadIdx.x] = n > 0 ? atomicAdd(counter, n) : 0;
+  }
+  __syncthreads();
+  for (int list = 0; list < 3; ++list) {
+    const int n = min(st.cnt[list], kPairStageCap);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int pos = st.base[list] + i;
+      if (list == 0) p.list[pos] = st.data[0][i];
+      else place_row(p, list - 1, st.data[list][i], pos);
+    }
+  }
 }
 
 // ---- D: match existing slots (simple graphs: at most one slot per pair, found in the edge
