@@ -96,6 +96,9 @@ SIGNATURES = {
     "dyngb200_sssp_compute": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32,
                                              ctypes.POINTER(Options), ctypes.POINTER(c_void_p),
                                              ctypes.POINTER(Stats)]),
+    "dyngb200_sssp_compute_static_scratch": (ctypes.c_int, [c_void_p, ctypes.c_int32,
+                                                            ctypes.c_int32, ctypes.c_int64, c_i64p,
+                                                            c_i32p, c_void_p]),
     "dyngb200_sssp_update": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch), c_void_p,
                                             ctypes.POINTER(Stats)]),
     "dyngb200_sssp_update_scheduled": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch),

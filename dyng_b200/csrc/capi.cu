@@ -480,6 +480,17 @@ dyngb200_status dyngb200_sssp_compute(dyngb200_context ctx, dyngb200_graph g, in
   });
 }
 
+dyngb200_status dyngb200_sssp_compute_static_scratch(dyngb200_graph g, int32_t source,
+                                                     int32_t objective, int64_t delta,
+                                                     int64_t* distances, int32_t* parents,
+                                                     void* stream) {
+  return guarded([&] {
+    expects(g != nullptr, "sssp::compute (static scratch): null graph");
+    sssp_compute_static(g->g, source, objective, delta, distances, parents,
+                        static_cast<cudaStream_t>(stream));
+  });
+}
+
 dyngb200_status dyngb200_sssp_update(dyngb200_context ctx, dyngb200_graph g,
                                      const dyngb200_batch* batch, dyngb200_tree tree,
                                      dyngb200_stats* stats) {

@@ -297,5 +297,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
 void tree_reserve(Context& ctx, Tree& t, long long n_cap);
 void tree_repack(Context& ctx, Tree& t, int bits);
 void tree_canonicalize(Context& ctx, Graph& g, Tree& t);
+void sssp_compute_static(Graph& g, int32_t source, int objective, long long delta,
+                         int64_t* distances, int32_t* parents, cudaStream_t s);
 
 }  // namespace dyngb200

@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 namespace dyngb200 {
 
@@ -1483,6 +1485,137 @@ void tree_repack(Context& ctx, Tree& t, int bits) {
                                             t.parent.ptr, t.packed.ptr);
   DYNGB200_CUDA(cudaGetLastError());
   t.packed_bits = bits;
+}
+
+// ------------------------------------------------------------------------------------------------
+// compute() without allocation: the scratch of the persistent kernel in a fixed device array.
+//
+// For callers that must not allocate device memory once they are running: code that issues work
+// while a CUDA graph is being captured (cudaMalloc is not allowed there), serving processes that
+// reserve their whole device-memory budget at start-up and treat any later allocation as a fault,
+// and host frameworks that own the device allocator and hand this library only the buffers it
+// reads and writes.  The caller passes the graph (already built) and the two output arrays; every
+// other byte the kernel needs lives in `g_static_scratch` below, a file-scope device array of
+// kStaticScratchBytes that every GPU which loads this library holds until the process exits.
+// ------------------------------------------------------------------------------------------------
+constexpr long long kStaticMaxVertices = 1LL << 16;
+// control block + packed words (8 B) + 15 int lists / stamp arrays + 3 int2 lists, per vertex
+constexpr long long kStaticScratchBytes =
+    4096 + kStaticMaxVertices * (8 + 15 * 4 + 3 * 8);
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+
+constexpr int kMaxStaticDevices = 64;
+unsigned char* g_static_ptr[kMaxStaticDevices] = {};
+std::mutex g_static_mutex;
+
+// The device address of g_static_scratch on the current device: looked up once per device (the
+// array's host-side name is only a stand-in, never a device address).
+unsigned char* static_scratch_for(int device) {
+  expects(device >= 0 && device < kMaxStaticDevices, "static scratch: device out of range");
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_ptr[device]) {
+    void* ptr = nullptr;
+    DYNGB200_CUDA(cudaGetSymbolAddress(&ptr, g_static_scratch));
+    g_static_ptr[device] = static_cast<unsigned char*>(ptr);
+  }
+  return g_static_ptr[device];
+}
+
+}  // namespace
+
+void sssp_compute_static(Graph& g, int32_t source, int objective, long long delta,
+                         int64_t* distances, int32_t* parents, cudaStream_t s) {
+  const long long n = g.n;
+  expects(n <= kStaticMaxVertices,
+          "sssp::compute (static scratch): the graph has " + std::to_string(n) +
+              " vertices; this entry point serves graphs of at most " +
+              std::to_string(kStaticMaxVertices));
+  expects(objective >= 0 && objective < g.k, "sssp::compute (static scratch): objective out of range");
+  expects(source >= 0 && source < n, "sssp::compute (static scratch): source out of range");
+  expects(delta >= 0, "sssp::compute (static scratch): delta must be >= 0");
+  expects(distances && parents, "sssp::compute (static scratch): null output array");
+  const ColumnStats cs = g.host_columns[objective];
+  expects(!cs.dirty, "sssp::compute (static scratch): the graph's weight statistics need a rescan; "
+                     "run sssp::compute or sssp::update on it once first");
+  expects(cs.bad == 0, "sssp::compute (static scratch): an edge has a weight below 1");
+  expects(distances_fit(n, cs.max_w), "sssp::compute (static scratch): distances do not fit in 62 bits");
+  int device = 0;
+  DYNGB200_CUDA(cudaGetDevice(&device));
+  expects(device == g.device, "sssp::compute (static scratch): the graph belongs to another device");
+  unsigned char* base = static_scratch_for(device);
+  // carve the array: control block, packed words, int arrays, int2 lists
+  const long long N = kStaticMaxVertices;
+  auto* ctl = reinterpret_cast<UpdateCtl*>(base);
+  auto* packed = reinterpret_cast<u64*>(base + 4096);
+  int* ints = reinterpret_cast<int*>(base + 4096 + 8 * N);
+  int2* pairs = reinterpret_cast<int2*>(base + 4096 + 8 * N + 15 * 4 * N);
+  SsspParams p{};
+  p.g = g.view();
+  p.objective = objective;
+  p.source = source;
+  p.from_scratch = 1;
+  p.dist = reinterpret_cast<long long*>(distances);
+  p.parent = parents;
+  p.packed = packed;
+  p.stamp = ints + 0 * N;
+  p.touch_stamp = ints + 1 * N;
+  p.in_far = ints + 2 * N;
+  p.flag = ints + 3 * N;
+  p.ancestor = ints + 4 * N;
+  p.candidates = ints + 5 * N;
+  p.frontier = ints + 6 * N;
+  p.near_a = ints + 7 * N;
+  p.near_b = ints + 8 * N;
+  p.far_a = ints + 9 * N;
+  p.far_b = ints + 10 * N;
+  p.touched = ints + 11 * N;
+  p.cand_med = ints + 12 * N;
+  p.near_med_a = ints + 13 * N;
+  p.near_med_b = ints + 14 * N;
+  p.heavy_a = pairs;
+  p.heavy_b = pairs + N;
+  p.pull_heavy = pairs + 2 * N;
+  p.ctl = ctl;
+  p.generation = 1;
+  p.touch_gen = 1;
+  p.heavy_degree = 256;
+  p.small_frontier = kDefaultSmall;
+  u64 bound = 0;
+  const Packing pk = choose_packing(n, cs.max_w, &bound);
+  p.tree_bits = pk.bits;
+  p.tree_n = n;
+  // the array keeps the previous call's contents: stamps and far marks must start at zero
+  DYNGB200_CUDA(cudaMemsetAsync(ints, 0, 3 * N * sizeof(int), s));
+  UpdateCtl init{};
+  init.err_index = INT64_MAX;
+  init.n_old = n;
+  init.n_after = n;
+  init.max_w = cs.max_w;
+  init.delta = delta > 0 ? delta : default_delta(g.m > 1 ? g.m : 1, n, cs.sum_w);
+  init.packing_bits = pk.bits;
+  init.max_distance = bound;
+  init.minimum = kPackedInf;
+  DYNGB200_CUDA(cudaMemcpyAsync(ctl, &init, sizeof(UpdateCtl), cudaMemcpyHostToDevice, s));
+  int sm = 0, coop = 0, per_sm = 0;
+  DYNGB200_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device));
+  DYNGB200_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  expects(coop != 0, "sssp: the fused engine needs cooperative launch", DYNGB200_NOT_SUPPORTED);
+  DYNGB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sssp, kThreads, 0));
+  expects(per_sm >= 1, "sssp: the persistent kernel does not fit on an SM", DYNGB200_NOT_SUPPORTED);
+  if (n > 0) {
+    void* args[] = {&p};
+    DYNGB200_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_sssp),
+                                              dim3(per_sm * sm), dim3(kThreads), args, 0, s));
+  }
+  UpdateCtl r{};
+  DYNGB200_CUDA(cudaMemcpyAsync(&r, ctl, sizeof(UpdateCtl), cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+  if (r.error & kErrTimeout) throw Error(DYNGB200_INTERNAL, "sssp: a grid barrier timed out");
+  if (r.error & kErrNotConverged)
+    throw Error(DYNGB200_INTERNAL, "sssp: the near-far loop did not converge");
 }
 
 }  // namespace dyngb200

@@ -213,6 +213,23 @@ dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_gr
                                                const dyngb200_schedule* schedule,
                                                dyngb200_stats* stats);
 
+/* sssp::compute into caller-owned device arrays, allocating nothing.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory while they run: work issued during
+ * CUDA graph capture (cudaMalloc is not allowed there), serving processes that reserve their
+ * whole memory budget at start-up, and host frameworks that own the device allocator.  The graph
+ * (on the current device) and the outputs -- distances: int64 x num_vertices, parents: int32 x
+ * num_vertices, both device memory -- come from the caller; the kernel's scratch is a fixed
+ * device array of about 6 MB inside this library that every GPU which loads it holds until exit, so
+ * graphs are limited to 65,536 vertices (larger ones are rejected with INVALID_ARGUMENT).  The
+ * first call on a device looks up that array's device address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race, so serialize them.  objective / delta as in dyngb200_options; stream: a
+ * cudaStream_t or NULL.  The results equal dyngb200_sssp_compute's. */
+dyngb200_status dyngb200_sssp_compute_static_scratch(dyngb200_graph g, int32_t source,
+                                                     int32_t objective, int64_t delta,
+                                                     int64_t* distances, int32_t* parents,
+                                                     void* stream);
+
 /* ---- tree: sssp::result (sssp.hpp:153-310) ------------------------------------------------ */
 /* result::from_arrays (sssp.hpp:253-302): arrays in `memory`, n entries each. */
 dyngb200_status dyngb200_tree_from_arrays(dyngb200_context ctx, dyngb200_graph g, int32_t source,
