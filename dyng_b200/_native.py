@@ -14,6 +14,8 @@ LIB_PATH = os.path.join(HERE, "libdyngb200.so")
 c_i32p = ctypes.POINTER(ctypes.c_int32)
 c_i64p = ctypes.POINTER(ctypes.c_int64)
 c_u8p = ctypes.POINTER(ctypes.c_uint8)
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_f64p = ctypes.POINTER(ctypes.c_double)
 c_void_p = ctypes.c_void_p
 
 
@@ -53,7 +55,8 @@ class Stats(ctypes.Structure):
                 ("rounds", ctypes.c_int64), ("touched", ctypes.c_int64),
                 ("work", ctypes.c_int64 * 12), ("phase_ms", ctypes.c_float * 7),
                 ("trace_len", ctypes.c_int32), ("trace_light", ctypes.c_int32 * 64),
-                ("trace_heavy", ctypes.c_int32 * 64), ("trace_us", ctypes.c_float * 64)]
+                ("trace_heavy", ctypes.c_int32 * 64), ("trace_us", ctypes.c_float * 64),
+                ("features", ctypes.c_float * 12), ("schedule_classes", ctypes.c_int32 * 3)]
 
 
 class Options(ctypes.Structure):
@@ -64,7 +67,7 @@ class Options(ctypes.Structure):
 class Schedule(ctypes.Structure):
     _fields_ = [("delta", ctypes.c_int64), ("grid_blocks", ctypes.c_int32),
                 ("invalidation", ctypes.c_int32), ("small_frontier", ctypes.c_int32),
-                ("heavy_degree", ctypes.c_int32)]
+                ("heavy_degree", ctypes.c_int32), ("record_features", ctypes.c_int32)]
 
 
 # Every symbol of include/dyngb200.h with (restype, argtypes).
@@ -119,6 +122,24 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(Options)]),
     "dyngb200_tree_set_options": (ctypes.c_int, [c_void_p, ctypes.POINTER(Options)]),
+    "dyngb200_tree_copy_from": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "dyngb200_graph_clone": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(c_void_p)]),
+    "dyngb200_graph_copy_from": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "dyngb200_sssp_update_learned": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch),
+                                                    c_void_p, c_void_p, ctypes.POINTER(Stats)]),
+    "dyngb200_scheduler_num_params": (ctypes.c_int64, []),
+    "dyngb200_scheduler_create": (ctypes.c_int, [c_void_p, ctypes.c_uint64,
+                                                 ctypes.POINTER(c_void_p)]),
+    "dyngb200_scheduler_destroy": (ctypes.c_int, [c_void_p]),
+    "dyngb200_scheduler_set_params": (ctypes.c_int, [c_void_p, c_void_p, c_f32p, c_f32p, c_f32p]),
+    "dyngb200_scheduler_get_params": (ctypes.c_int, [c_void_p, c_void_p, c_f32p, c_f32p, c_f32p]),
+    "dyngb200_scheduler_forward": (ctypes.c_int, [c_void_p, c_void_p, c_f32p, ctypes.c_int64,
+                                                  c_f32p]),
+    "dyngb200_scheduler_gradients": (ctypes.c_int, [c_void_p, c_void_p, c_f32p, c_i32p,
+                                                    ctypes.c_int64, c_f32p, c_f64p]),
+    "dyngb200_scheduler_train": (ctypes.c_int, [c_void_p, c_void_p, c_f32p, c_i32p,
+                                                ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.c_float, ctypes.c_uint64, c_f64p]),
 }
 
 _lib = None

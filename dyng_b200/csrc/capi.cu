@@ -20,6 +20,9 @@ struct dyngb200_graph_s {
 struct dyngb200_tree_s {
   dyngb200::Tree t;
 };
+struct dyngb200_scheduler_s {
+  dyngb200::Scheduler s;
+};
 
 namespace {
 
@@ -523,6 +526,129 @@ dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_gr
   });
 }
 
+dyngb200_status dyngb200_sssp_update_learned(dyngb200_context ctx, dyngb200_graph g,
+                                             const dyngb200_batch* batch, dyngb200_tree tree,
+                                             dyngb200_scheduler scheduler, dyngb200_stats* stats) {
+  return guarded([&] {
+    expects(ctx && g && batch && tree && scheduler, "sssp::update: null argument");
+    Context& c = ctx->ctx;
+    DeviceGuard guard(c.device);
+    expects(scheduler->s.device == c.device, "sssp::update: the scheduler belongs to another device");
+    expect_tree_current(g->g, tree->t, "sssp::update");
+    expect_batch(g->g, *batch, "sssp::update");
+    sssp_update(c, g->g, tree->t, *batch, dyngb200_schedule{}, stats, &scheduler->s);
+  });
+}
+
+int64_t dyngb200_scheduler_num_params(void) { return kMlpParams; }
+
+dyngb200_status dyngb200_scheduler_create(dyngb200_context ctx, uint64_t seed,
+                                          dyngb200_scheduler* out) {
+  return guarded([&] {
+    expects(ctx && out, "scheduler_create: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    auto h = std::make_unique<dyngb200_scheduler_s>();
+    scheduler_init(ctx->ctx, h->s, seed);
+    *out = h.release();
+  });
+}
+
+dyngb200_status dyngb200_scheduler_destroy(dyngb200_scheduler s) {
+  return guarded([&] {
+    if (!s) return;
+    DeviceGuard guard(s->s.device);
+    delete s;
+  });
+}
+
+dyngb200_status dyngb200_scheduler_set_params(dyngb200_context ctx, dyngb200_scheduler s,
+                                              const float* params, const float* feature_mean,
+                                              const float* feature_scale) {
+  return guarded([&] {
+    expects(ctx && s, "scheduler_set_params: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    expects(s->s.device == ctx->ctx.device, "scheduler: the scheduler belongs to another device");
+    scheduler_set(ctx->ctx, s->s, params, feature_mean, feature_scale);
+  });
+}
+
+dyngb200_status dyngb200_scheduler_get_params(dyngb200_context ctx, dyngb200_scheduler s,
+                                              float* params, float* feature_mean,
+                                              float* feature_scale) {
+  return guarded([&] {
+    expects(ctx && s, "scheduler_get_params: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    scheduler_get(ctx->ctx, s->s, params, feature_mean, feature_scale);
+  });
+}
+
+dyngb200_status dyngb200_scheduler_forward(dyngb200_context ctx, dyngb200_scheduler s,
+                                           const float* features, int64_t n, float* logits) {
+  return guarded([&] {
+    expects(ctx && s && (n == 0 || (features && logits)), "scheduler_forward: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    scheduler_forward(ctx->ctx, s->s, features, n, logits);
+  });
+}
+
+dyngb200_status dyngb200_scheduler_gradients(dyngb200_context ctx, dyngb200_scheduler s,
+                                             const float* features, const int32_t* labels,
+                                             int64_t n, float* grads, double* loss) {
+  return guarded([&] {
+    expects(ctx && s && features && labels, "scheduler_gradients: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    scheduler_gradients(ctx->ctx, s->s, features, labels, n, grads, loss);
+  });
+}
+
+dyngb200_status dyngb200_scheduler_train(dyngb200_context ctx, dyngb200_scheduler s,
+                                         const float* features, const int32_t* labels, int64_t n,
+                                         int32_t epochs, int32_t batch_size, float learning_rate,
+                                         uint64_t seed, double* final_loss) {
+  return guarded([&] {
+    expects(ctx && s && features && labels, "scheduler_train: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    scheduler_train(ctx->ctx, s->s, features, labels, n, epochs, batch_size, learning_rate, seed,
+                    final_loss);
+  });
+}
+
+dyngb200_status dyngb200_graph_clone(dyngb200_context ctx, dyngb200_graph g, dyngb200_graph* out) {
+  return guarded([&] {
+    expects(ctx && g && out, "graph_clone: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    expects(g->g.device == ctx->ctx.device, "graph_clone: the graph belongs to another device");
+    auto h = std::make_unique<dyngb200_graph_s>();
+    h->g.id = g_next_graph_id.fetch_add(1);
+    graph_copy(ctx->ctx, h->g, g->g);
+    *out = h.release();
+  });
+}
+
+dyngb200_status dyngb200_graph_copy_from(dyngb200_context ctx, dyngb200_graph dst,
+                                         dyngb200_graph src) {
+  return guarded([&] {
+    expects(ctx && dst && src, "graph_copy_from: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    expects(dst->g.device == ctx->ctx.device && src->g.device == ctx->ctx.device,
+            "graph_copy_from: both graphs must live on the context's device");
+    if (dst != src) graph_copy(ctx->ctx, dst->g, src->g);
+  });
+}
+
+dyngb200_status dyngb200_tree_copy_from(dyngb200_context ctx, dyngb200_tree dst,
+                                        dyngb200_tree src) {
+  return guarded([&] {
+    expects(ctx && dst && src, "tree_copy_from: null argument");
+    DeviceGuard guard(ctx->ctx.device);
+    expects(dst->t.device == ctx->ctx.device && src->t.device == ctx->ctx.device,
+            "tree_copy_from: both trees must live on the context's device");
+    expects(!src->t.poisoned, "tree_copy_from: the source was left unusable by a failed update",
+            DYNGB200_STALE_RESULT);
+    if (dst != src) tree_copy(ctx->ctx, dst->t, src->t);
+  });
+}
+
 dyngb200_status dyngb200_tree_from_arrays(dyngb200_context ctx, dyngb200_graph g, int32_t source,
                                           const int64_t* distances, const int32_t* parents,
                                           int64_t n, int32_t memory, int32_t canonicalize,
@@ -612,6 +738,9 @@ dyngb200_status dyngb200_tree_clone(dyngb200_context ctx, dyngb200_tree tree, dy
       DYNGB200_CUDA(cudaMemcpyPeerAsync(t.packed.ptr, c.device, s.packed.ptr, s.device,
                                         s.n * sizeof(u64), c.stream));
     }
+    if (s.hist.ptr)
+      DYNGB200_CUDA(cudaMemcpyPeerAsync(t.hist.ptr, c.device, s.hist.ptr, s.device,
+                                        sizeof(TreeHistory), c.stream));
     DYNGB200_CUDA(cudaStreamSynchronize(c.stream));
     *out = h.release();
   });

@@ -12,6 +12,7 @@ using u64 = unsigned long long;
 constexpr int64_t kInfinity = INT64_MAX / 4;  // sssp_infinity of the reference (problem.hpp:340)
 constexpr u64 kPackedInf = ~0ULL;
 constexpr int32_t kDead = -1;  // tombstone in a slack row's column slot
+constexpr int kDefaultSmall = 256;  // the heuristic: frontiers up to 256 vertices run on one block
 
 // Device error bits (the sticky error word; the reference's util/device_error_flags.hpp:9-43
 // has capacity / invalid_input / parent_cycle / internal).

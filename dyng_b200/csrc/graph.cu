@@ -1639,7 +1639,8 @@ StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k) {
 
 // Steps A-E (nothing in the graph changes): checks, plan, grouping, matching, resolution.
 void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
-                   long long delta_opt) {
+                   long long delta_opt, const dyngb200_schedule* sched, Tree* tree,
+                   const Scheduler* learned) {
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   const long long dir = g.props.directed ? 1 : 2;
@@ -1664,6 +1665,7 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
   init.n_after = g.n;
   init.batch_ins_max = 1;
   init.minimum = kPackedInf;
+  if (sched) schedule_into(*sched, init);
   *ws.host_ctl.ptr = init;
   DYNGB200_CUDA(cudaMemcpyAsync(ws.ctl.ptr, ws.host_ctl.ptr, sizeof(UpdateCtl),
                                 cudaMemcpyHostToDevice, s));
@@ -1672,6 +1674,10 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
   const int grid_ops = grid_for(b.ni + b.nd, kBlock, ctx.sm_count);
   k_validate<<<grid_ops, kBlock, 0, s>>>(p);
   k_plan<<<1, 1, 0, s>>>(p);
+  // the learned scheduler reads the batch, the old rows and the tree before anything changes,
+  // and writes its schedule into the control block (after the plan's default width)
+  if (tree && (learned || (sched && sched->record_features)))
+    launch_learned_schedule(ctx, g, *tree, b, learned);
   k_pairs<<<grid_ops, kBlock, 0, s>>>(p);
   if (g.props.allow_multi) {
     k_scan_multi<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
@@ -1719,7 +1725,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
   UpdateCtl r{};
   DevBuf<unsigned char> flags;
   for (int attempt = 0;; ++attempt) {
-    apply_prepare(ctx, g, b, -1, 0);
+    apply_prepare(ctx, g, b, -1, 0, nullptr);
     apply_commit(ctx, g, b);
     if (weight_increased && b.ni > 0) {
       flags.reserve(static_cast<size_t>(b.ni) * g.k);
@@ -1756,6 +1762,50 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
   g.n = g.host_counters.n;
   g.m = g.host_counters.m;
   if (summary) std::memcpy(summary, r.summary, sizeof(*summary));
+}
+
+}  // namespace dyngb200
+
+namespace dyngb200 {
+
+template <typename T>
+static void copy_buf(DevBuf<T>& dst, const DevBuf<T>& src, cudaStream_t s) {
+  if (!src.ptr) return;
+  dst.reserve(src.count);
+  DYNGB200_CUDA(cudaMemcpyAsync(dst.ptr, src.ptr, src.count * sizeof(T), cudaMemcpyDeviceToDevice, s));
+}
+
+// Device contents and host mirrors of `src` into `dst` (same device); dst keeps its identity, so
+// trees bound to dst stay bound to it.
+void graph_copy(Context& ctx, Graph& dst, const Graph& src) {
+  cudaStream_t s = ctx.stream;
+  copy_buf(dst.out_desc, src.out_desc, s);
+  copy_buf(dst.in_desc, src.in_desc, s);
+  copy_buf(dst.out_cap, src.out_cap, s);
+  copy_buf(dst.in_cap, src.in_cap, s);
+  copy_buf(dst.out_dead, src.out_dead, s);
+  copy_buf(dst.in_dead, src.in_dead, s);
+  copy_buf(dst.out_col, src.out_col, s);
+  copy_buf(dst.in_col, src.in_col, s);
+  copy_buf(dst.out_w, src.out_w, s);
+  copy_buf(dst.in_w, src.in_w, s);
+  copy_buf(dst.counters, src.counters, s);
+  copy_buf(dst.columns, src.columns, s);
+  copy_buf(dst.ekey, src.ekey, s);
+  copy_buf(dst.eout, src.eout, s);
+  copy_buf(dst.ein, src.ein, s);
+  dst.version = src.version;
+  dst.props = src.props;
+  dst.k = src.k;
+  dst.n = src.n;
+  dst.m = src.m;
+  dst.n_cap = src.n_cap;
+  dst.arena_cap = src.arena_cap;
+  dst.ecap = src.ecap;
+  dst.host_counters = src.host_counters;
+  dst.host_columns = src.host_columns;
+  dst.device = src.device;
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace dyngb200

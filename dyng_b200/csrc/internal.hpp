@@ -132,6 +132,17 @@ struct UpdateCtl {
   u64 minimum;
   int changed;         // the batch holds a deleted or weight-increased edge
   int last_generation; // last stamp generation the kernel used
+  // the schedule of this launch (0 fields: the heuristic); see dyngb200_schedule
+  long long sched_delta;
+  int sched_small;     // small-frontier size (0: off)
+  int sched_walk;      // subtree-walk invalidation
+  int sched_heavy;     // heavy-row threshold (0: 256)
+  int active_blocks;   // persistent grid size (0: all launched blocks)
+  // learned scheduler: feature accumulators (tree-edge deletions, degree sum, max degree,
+  // touched sources) and the feature vector of this update
+  long long feat_acc[4];
+  float features[12];
+  int sched_classes[3];  // the chosen class of each head (-1: no scheduler)
   int loop_state[6];   // near-far state handed from block 0 back to the grid
   long long loop_pushes;
   u64 loop_threshold;
@@ -243,7 +254,17 @@ struct Graph {
   }
 };
 
+// What the last update of a tree looked like (the learned scheduler's history features),
+// written by the sssp kernel on the device.
+struct TreeHistory {
+  long long invalidated;
+  int frontier[4];  // sizes of the first four near-far steps
+  int iterations;   // near-far iterations + epochs
+  int rounds;       // pointer-jumping rounds
+};
+
 struct Tree {
+  DevBuf<TreeHistory> hist;
   bool canonical = true;  // every parent is the lowest-id tight in-neighbour (compute, canonicalize)
   uint64_t graph_id = 0;
   uint64_t version = 0;
@@ -259,6 +280,43 @@ struct Tree {
   int device = 0;
 };
 
+// The learned scheduler: a 12 -> 64 -> 64 -> 15 MLP (bf16 weights and activations, fp32
+// accumulation), three softmax heads: near-far width class (8), invalidation / small-frontier
+// switch class (4), persistent-grid class (3).
+constexpr int kMlpIn = 12, kMlpHidden = 64, kMlpOut = 15;
+constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden +
+                           kMlpOut * kMlpHidden + kMlpOut;
+struct Scheduler {
+  int device = 0;
+  DevBuf<float> params;       // fp32 master weights
+  DevBuf<uint16_t> wbf16;     // bf16 copies of W1, W2, W3 (biases stay fp32)
+  DevBuf<float> grads, m, v;  // gradient and Adam moments
+  DevBuf<float> x;            // training features
+  DevBuf<int> y;              // training labels (3 per sample)
+  DevBuf<int> idx;            // the shuffle of one training pass
+  DevBuf<float> out;          // logits / losses
+  DevBuf<double> loss;
+  long long step = 0;
+  float feat_mean[kMlpIn] = {};
+  float feat_scale[kMlpIn] = {};  // features are standardized: (f - mean) * scale
+};
+
+// mlp.cu
+struct StagedBatch;
+void scheduler_refresh(Scheduler& s, cudaStream_t st);  // bf16 copies from the master weights
+void scheduler_init(Context& ctx, Scheduler& s, uint64_t seed);
+void scheduler_set(Context& ctx, Scheduler& s, const float* params, const float* mean,
+                   const float* scale);
+void scheduler_get(Context& ctx, const Scheduler& s, float* params, float* mean, float* scale);
+void scheduler_forward(Context& ctx, Scheduler& s, const float* x, long long n, float* logits);
+void scheduler_gradients(Context& ctx, Scheduler& s, const float* x, const int32_t* y, long long n,
+                         float* grads, double* loss);
+void scheduler_train(Context& ctx, Scheduler& s, const float* x, const int32_t* y, long long n,
+                     int epochs, int batch, float lr, uint64_t seed, double* final_loss);
+// features of the batch (and, with a scheduler, its schedule) into the control block
+void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch& b,
+                             const Scheduler* sch);
+
 // graph.cu
 void graph_build(Context& ctx, Graph& g, long long n, const int64_t* row_ptr, const int32_t* col,
                  const int32_t* w_objective_major, long long m);
@@ -270,6 +328,7 @@ void graph_rescan_columns(Context& ctx, Graph& g);
 void graph_index_build(Context& ctx, Graph& g, long long extra);
 void graph_index_reserve(Context& ctx, Graph& g, long long inserts);
 void graph_refresh_host(Context& ctx, Graph& g);
+void graph_copy(Context& ctx, Graph& dst, const Graph& src);
 
 // Launches the batch applier (Step 0 checks, grouping, matching, resolution, allocation and the
 // mutation of the slack rows).  `objective` >= 0 also records the sssp change classification for
@@ -284,19 +343,23 @@ struct StagedBatch {
   long long nd;
 };
 void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
-                   long long delta_opt);
+                   long long delta_opt, const dyngb200_schedule* sched, Tree* tree = nullptr,
+                   const Scheduler* learned = nullptr);
+void schedule_into(const dyngb200_schedule& sched, UpdateCtl& init);
 void apply_commit(Context& ctx, Graph& g, const StagedBatch& b);
 StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k);
 
 // sssp.cu
 void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st);
 void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
-                 const dyngb200_schedule& sched, dyngb200_stats* st);
+                 const dyngb200_schedule& sched, dyngb200_stats* st,
+                 const Scheduler* learned = nullptr);
 void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
                  dyngb200_apply_summary* summary, unsigned char* weight_increased);
 void tree_reserve(Context& ctx, Tree& t, long long n_cap);
 void tree_repack(Context& ctx, Tree& t, int bits);
 void tree_canonicalize(Context& ctx, Graph& g, Tree& t);
+void tree_copy(Context& ctx, Tree& dst, const Tree& src);
 void sssp_compute_static(Graph& g, int32_t source, int objective, long long delta,
                          int64_t* distances, int32_t* parents, cudaStream_t s);
 

@@ -73,6 +73,7 @@ struct SsspParams {
   long long delta_override;
   int small_frontier;    // frontiers up to this size run on block 0 alone (0: never)
   UpdateCtl* ctl;
+  TreeHistory* hist;     // the tree's record of this run (the learned scheduler's history)
 };
 
 // Pair flags of the applier (graph.cu).
@@ -104,6 +105,7 @@ struct StageSet {
 };
 
 __shared__ StageSet g_stage;
+__shared__ int g_nblk;  // blocks taking part in this launch (the schedule's grid size)
 
 __device__ __forceinline__ void staged_append(int id, int* list, int* count, int v) {
   const unsigned mask = __activemask();
@@ -158,7 +160,7 @@ __device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
     __threadfence();
     const unsigned arrived = atomicAdd(&c->bar_count, 1u) + 1u;
     int ok = 1;
-    if (arrived == gridDim.x) {
+    if (arrived == static_cast<unsigned>(g_nblk)) {
       atomicExch(&c->bar_count, 0u);
       __threadfence();
       atomicExch(&c->bar_gen, target);
@@ -654,7 +656,6 @@ struct LoopState {
 };
 
 constexpr int kSmallFarMax = 4096;
-constexpr int kDefaultSmall = 256;  // the heuristic: frontiers up to 256 vertices run on one block
 
 __device__ __forceinline__ void block_barrier() {
   stage_flush();
@@ -671,7 +672,7 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
                         long long iteration_cap, int small) {
   UpdateCtl* c = p.ctl;
   const long long tid = BLOCK ? threadIdx.x : blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  const long long threads = BLOCK ? blockDim.x : static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long threads = BLOCK ? blockDim.x : static_cast<long long>(g_nblk) * blockDim.x;
   const long long gwarp = tid >> 5;
   const long long nwarps = threads >> 5;
   const bool leader = BLOCK ? threadIdx.x == 0 : tid == 0;
@@ -767,10 +768,21 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
 __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   UpdateCtl* c = p.ctl;
   if (ld_volatile(&c->error) != 0) return;
+  // The schedule lives in the control block (written by the host, or by the scheduler's
+  // inference kernel on the device): blocks beyond its grid size leave at once.
+  const int nblk = c->active_blocks > 0 && c->active_blocks < static_cast<int>(gridDim.x)
+                       ? c->active_blocks
+                       : static_cast<int>(gridDim.x);
+  if (static_cast<int>(blockIdx.x) >= nblk) return;
+  if (threadIdx.x == 0) g_nblk = nblk;
+  if (c->sched_heavy > 0) p.heavy_degree = c->sched_heavy;
+  p.small_frontier = c->sched_small;
+  p.walk = c->sched_walk && p.tree_trusted ? 1 : 0;
+  if (c->sched_delta > 0) p.delta_override = c->sched_delta;
   stage_init();
   unsigned bar = 0;
   const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  const long long threads = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long threads = static_cast<long long>(nblk) * blockDim.x;
   const int lane = threadIdx.x & 31;
   const long long gwarp = tid >> 5;
   const long long nwarps = threads >> 5;
@@ -1155,6 +1167,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
     c->epochs = epochs;
     c->pushes = pushes;
     c->last_generation = gen;
+    if (p.hist) {
+      TreeHistory h{};
+      h.invalidated = ld_cg(&c->invalidated);
+      const int len = ld_cg(&c->trace_len);
+      for (int i = 0; i < 4; ++i) h.frontier[i] = i < len ? ld_cg(&c->trace_n[i]) : 0;
+      h.iterations = iterations + epochs;
+      h.rounds = ld_cg(&c->rounds);
+      *p.hist = h;
+    }
   }
 }
 
@@ -1191,20 +1212,26 @@ __global__ void k_pack(long long n, int bits, const long long* dist, const int32
 }  // namespace
 
 // Blocks of the persistent kernel (co-resident: cooperative launch).
+// The schedule's fields in the control block (0 / unset: the heuristic).
+void schedule_into(const dyngb200_schedule& sched, UpdateCtl& init) {
+  init.sched_delta = sched.delta > 0 ? sched.delta : 0;
+  init.sched_small = sched.small_frontier > 0 ? sched.small_frontier
+                                              : (sched.small_frontier < 0 ? 0 : kDefaultSmall);
+  init.sched_walk = sched.invalidation == 1 ? 1 : 0;
+  init.sched_heavy = sched.heavy_degree > 0 ? sched.heavy_degree : 0;
+  init.active_blocks = sched.grid_blocks > 0 ? sched.grid_blocks : 0;
+}
+
 static int persistent_blocks(Context& ctx, const dyngb200_schedule& sched) {
+  (void)sched;  // the schedule's grid size is applied on the device (active_blocks)
   if (ctx.update_blocks_per_sm == 0) {
     int per_sm = 0;
     DYNGB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sssp, kThreads, 0));
     expects(per_sm >= 1, "sssp: the persistent kernel does not fit on an SM", DYNGB200_NOT_SUPPORTED);
     ctx.update_blocks_per_sm = per_sm;
   }
-  const int max_blocks = ctx.update_blocks_per_sm * ctx.sm_count;
-  int blocks = sched.grid_blocks > 0 ? sched.grid_blocks : max_blocks;
-  if (blocks > max_blocks) blocks = max_blocks;
-  if (blocks < 1) blocks = 1;
-  return blocks;
+  return ctx.update_blocks_per_sm * ctx.sm_count;
 }
-
 
 static void launch(Context& ctx, SsspParams& p, int blocks) {
   expects(ctx.coop_supported != 0, "sssp: the fused engine needs cooperative launch",
@@ -1242,6 +1269,7 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
   p.near_med_b = ws.near_med_b.ptr;
   p.touched = ws.touched.ptr;
   p.ctl = ws.ctl.ptr;
+  p.hist = t.hist.ptr;
   return p;
 }
 
@@ -1270,6 +1298,8 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
   init.packing_bits = pk.bits;
   init.max_distance = bound;
   init.minimum = kPackedInf;
+  const dyngb200_schedule sched = ctx.schedule_set ? ctx.schedule : dyngb200_schedule{};
+  schedule_into(sched, init);
   *ws.host_ctl.ptr = init;
   DYNGB200_CUDA(cudaMemcpyAsync(ws.ctl.ptr, ws.host_ctl.ptr, sizeof(UpdateCtl),
                                 cudaMemcpyHostToDevice, s));
@@ -1280,12 +1310,7 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
   p.tree_n = n;
   p.generation = ws.next_generation(1, s);
   p.touch_gen = 1;
-  p.heavy_degree = ctx.schedule_set && ctx.schedule.heavy_degree > 0 ? ctx.schedule.heavy_degree
-                                                                      : 256;
-  p.delta_override = 0;
-  const dyngb200_schedule sched = ctx.schedule_set ? ctx.schedule : dyngb200_schedule{};
-  p.small_frontier = sched.small_frontier > 0 ? sched.small_frontier
-                                              : (sched.small_frontier < 0 ? 0 : kDefaultSmall);
+  p.heavy_degree = 256;
   const int blocks = persistent_blocks(ctx, sched);
   cudaEvent_t e0, e1;
   DYNGB200_CUDA(cudaEventCreate(&e0));
@@ -1316,14 +1341,15 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
     st->engine_used = DYNGB200_ENGINE_FUSED;
     st->delta = init.delta;
     st->max_weight = cs.max_w;
-    st->grid_blocks = blocks;
+    st->grid_blocks = init.active_blocks > 0 && init.active_blocks < blocks ? init.active_blocks
+                                                                             : blocks;
     st->sssp_ms = ms;
   }
 }
 
 // update(): the applier, then the persistent kernel, then one read-back of the control block.
 void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
-                 const dyngb200_schedule& sched, dyngb200_stats* st) {
+                 const dyngb200_schedule& sched, dyngb200_stats* st, const Scheduler* learned) {
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   const int objective = t.opt.objective;
@@ -1339,7 +1365,7 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
   for (int attempt = 0;; ++attempt) {
     tree_reserve(ctx, t, g.n_cap);
     DYNGB200_CUDA(cudaEventRecord(e0, s));
-    apply_prepare(ctx, g, b, objective, t.opt.delta);
+    apply_prepare(ctx, g, b, objective, t.opt.delta, &sched, &t, learned);
     apply_commit(ctx, g, b);
     DYNGB200_CUDA(cudaEventRecord(e1, s));
     SsspParams p = base_params(ctx, g, t);
@@ -1353,15 +1379,12 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     p.pair_last = ws.pair_last.ptr;
     p.ins_w = b.ins_w;
     p.k = g.k;
-    p.walk = (sched.invalidation == 1 && t.trusted) ? 1 : 0;
+
     p.offer_heads = t.canonical ? 1 : 0;
     p.tree_trusted = t.trusted ? 1 : 0;
     p.generation = ws.next_generation(1, s);
     p.touch_gen = p.generation;
-    p.heavy_degree = sched.heavy_degree > 0 ? sched.heavy_degree : 256;
-    p.small_frontier = sched.small_frontier > 0 ? sched.small_frontier
-                                                : (sched.small_frontier < 0 ? 0 : kDefaultSmall);
-    p.delta_override = sched.delta;
+    p.heavy_degree = 256;
     launch(ctx, p, blocks);
     DYNGB200_CUDA(cudaEventRecord(e2, s));
     DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
@@ -1440,10 +1463,10 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     st->pushes = r.pushes;
     st->packed_parents = r.packing_bits > 0;
     st->engine_used = DYNGB200_ENGINE_FUSED;
-    st->delta = sched.delta > 0 ? sched.delta : r.delta;
+    st->delta = r.sched_delta > 0 ? r.sched_delta : r.delta;
     st->max_weight = r.max_w;
-    st->grid_blocks = blocks;
-    st->invalidation = (sched.invalidation == 1 && t.trusted) ? 1 : 0;
+    st->grid_blocks = r.active_blocks > 0 && r.active_blocks < blocks ? r.active_blocks : blocks;
+    st->invalidation = (r.sched_walk && t.trusted) ? 1 : 0;
     st->apply_ms = apply_ms;
     st->sssp_ms = sssp_ms;
     st->rounds = r.rounds;
@@ -1455,6 +1478,9 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
       st->trace_heavy[i] = r.trace_h[i];
       st->trace_us[i] = r.trace_t[i] * 1e-3f;
     }
+    const bool scheduled = learned || sched.record_features;
+    for (int i = 0; i < 12; ++i) st->features[i] = scheduled ? r.features[i] : 0.0f;
+    for (int i = 0; i < 3; ++i) st->schedule_classes[i] = learned ? r.sched_classes[i] : -1;
     for (int i = 0; i < 7; ++i)
       st->phase_ms[i] = r.phase_ns[i + 1] > r.phase_ns[i]
                             ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)
@@ -1464,6 +1490,10 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
 
 // Tree arrays sized for the graph's vertex capacity (contents kept).
 void tree_reserve(Context& ctx, Tree& t, long long n_cap) {
+  if (!t.hist.ptr) {
+    t.hist.reserve(1);
+    DYNGB200_CUDA(cudaMemsetAsync(t.hist.ptr, 0, sizeof(TreeHistory), ctx.stream));
+  }
   if (t.cap >= n_cap) return;
   const size_t keep = static_cast<size_t>(t.n);
   t.dist.reserve(static_cast<size_t>(n_cap), ctx.stream, keep);
@@ -1471,6 +1501,34 @@ void tree_reserve(Context& ctx, Tree& t, long long n_cap) {
   t.packed.reserve(static_cast<size_t>(n_cap), ctx.stream, keep);
   t.cap = n_cap;
 }
+// Contents of `src` into `dst` (same device); dst stays bound to its own graph handle.
+void tree_copy(Context& ctx, Tree& dst, const Tree& src) {
+  cudaStream_t s = ctx.stream;
+  dst.version = src.version;
+  dst.source = src.source;
+  dst.opt = src.opt;
+  dst.packed_bits = src.packed_bits;
+  dst.trusted = src.trusted;
+  dst.canonical = src.canonical;
+  dst.poisoned = src.poisoned;
+  dst.device = src.device;
+  dst.n = src.n;
+  tree_reserve(ctx, dst, std::max(src.cap, src.n));
+  if (src.n > 0) {
+    const size_t n = static_cast<size_t>(src.n);
+    DYNGB200_CUDA(cudaMemcpyAsync(dst.dist.ptr, src.dist.ptr, n * sizeof(int64_t),
+                                  cudaMemcpyDeviceToDevice, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(dst.parent.ptr, src.parent.ptr, n * sizeof(int32_t),
+                                  cudaMemcpyDeviceToDevice, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(dst.packed.ptr, src.packed.ptr, n * sizeof(u64),
+                                  cudaMemcpyDeviceToDevice, s));
+  }
+  if (src.hist.ptr)
+    DYNGB200_CUDA(cudaMemcpyAsync(dst.hist.ptr, src.hist.ptr, sizeof(TreeHistory),
+                                  cudaMemcpyDeviceToDevice, s));
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+}
+
 void tree_canonicalize(Context& ctx, Graph& g, Tree& t) {
   const int grid = ctx.sm_count * 8;
   k_canonicalize<<<grid, kThreads, 0, ctx.stream>>>(g.view(), t.opt.objective, t.source, t.n,
@@ -1598,6 +1656,7 @@ void sssp_compute_static(Graph& g, int32_t source, int objective, long long delt
   init.packing_bits = pk.bits;
   init.max_distance = bound;
   init.minimum = kPackedInf;
+  init.sched_small = kDefaultSmall;
   DYNGB200_CUDA(cudaMemcpyAsync(ctl, &init, sizeof(UpdateCtl), cudaMemcpyHostToDevice, s));
   int sm = 0, coop = 0, per_sm = 0;
   DYNGB200_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device));

@@ -293,6 +293,16 @@ class Graph:
         check(N.lib().dyngb200_graph_device_bytes(self._h, ctypes.byref(b)))
         return b.value
 
+    def clone(self) -> "Graph":
+        """A new graph with this graph's contents (results of this graph are not bound to it)."""
+        h = ctypes.c_void_p()
+        check(N.lib().dyngb200_graph_clone(self._res._h, self._h, ctypes.byref(h)))
+        return Graph(h, self._res)
+
+    def copy_from(self, other: "Graph") -> None:
+        """Take other's contents; results bound to this graph stay bound to it."""
+        check(N.lib().dyngb200_graph_copy_from(self._res._h, self._h, other._h))
+
     def apply(self, batch: EdgeBatch, classify: bool = False):
         """graph::apply; with classify also the weight-increase mask (insertions x num_weights)."""
         sm = N.ApplySummary()

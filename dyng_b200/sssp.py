@@ -47,10 +47,12 @@ class Schedule:
     invalidation: int = 0
     small_frontier: int = 0
     heavy_degree: int = 0
+    record_features: bool = False  # report the learned scheduler's features in the stats
 
     def _to_native(self) -> N.Schedule:
         return N.Schedule(int(self.delta), int(self.grid_blocks), int(self.invalidation),
-                          int(self.small_frontier), int(self.heavy_degree))
+                          int(self.small_frontier), int(self.heavy_degree),
+                          int(bool(self.record_features)))
 
 
 @dataclass(frozen=True)
@@ -76,6 +78,8 @@ class Stats:
     work: tuple = ()
     phase_ms: tuple = ()
     trace: tuple = ()  # (light, heavy chunks, start us) per near-far step; light < 0: an epoch
+    features: tuple = ()  # the learned scheduler's 12 features (when a scheduler or recording ran)
+    schedule_classes: tuple = (-1, -1, -1)  # the classes the learned scheduler picked
 
     WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
                   "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
@@ -97,7 +101,9 @@ class Stats:
                    float(s.sssp_ms), s.rounds, s.touched, tuple(int(x) for x in s.work),
                    tuple(float(x) for x in s.phase_ms),
                    tuple((int(s.trace_light[i]), int(s.trace_heavy[i]), float(s.trace_us[i]))
-                         for i in range(min(int(s.trace_len), 64))))
+                         for i in range(min(int(s.trace_len), 64))),
+                   tuple(float(x) for x in s.features),
+                   tuple(int(x) for x in s.schedule_classes))
 
 
 class Result:
@@ -172,6 +178,10 @@ class Result:
         check(N.lib().dyngb200_tree_clone(self._res._h, self._h, ctypes.byref(h)))
         return Result(h, self._graph)
 
+    def copy_from(self, other: "Result") -> None:
+        """Take other's distances, parents and history; this result stays bound to its graph."""
+        check(N.lib().dyngb200_tree_copy_from(self._res._h, self._h, other._h))
+
     @classmethod
     def from_arrays(cls, graph: Graph, source: int, distances, parents, canonicalize: bool = True,
                     options: Options | None = None) -> "Result":
@@ -199,11 +209,20 @@ def compute(graph: Graph, source: int = 0, options: Options | None = None,
     return (r, Stats._from_native(st)) if stats else r
 
 
-def update(graph: Graph, batch: EdgeBatch, tree: Result, schedule: Schedule | None = None) -> Stats:
-    """sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489)."""
+def update(graph: Graph, batch: EdgeBatch, tree: Result, schedule: Schedule | None = None,
+           scheduler=None) -> Stats:
+    """sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489).
+
+    ``schedule`` fixes the schedule; ``scheduler`` (a :class:`dyng_b200.scheduler.Scheduler`)
+    picks it on the device for this batch.  Neither changes the results."""
     nb = batch._to_native()
     st = N.Stats()
-    if schedule is None:
+    if scheduler is not None:
+        if schedule is not None:
+            raise InvalidArgumentError("update: give a schedule or a scheduler, not both")
+        check(N.lib().dyngb200_sssp_update_learned(graph._res._h, graph._h, ctypes.byref(nb),
+                                                   tree._h, scheduler._h, ctypes.byref(st)))
+    elif schedule is None:
         check(N.lib().dyngb200_sssp_update(graph._res._h, graph._h, ctypes.byref(nb), tree._h,
                                            ctypes.byref(st)))
     else:

@@ -49,6 +49,7 @@ typedef enum dyngb200_engine {
 } dyngb200_engine;
 
 typedef struct dyngb200_context_s* dyngb200_context; /* resources::cuda() */
+typedef struct dyngb200_scheduler_s* dyngb200_scheduler; /* the learned scheduler (bf16 MLP) */
 typedef struct dyngb200_graph_s* dyngb200_graph;     /* graph<int32,int64,int32> on the device */
 typedef struct dyngb200_tree_s* dyngb200_tree;       /* sssp::result<int32> */
 
@@ -126,6 +127,10 @@ typedef struct dyngb200_stats {
   int32_t trace_light[64];
   int32_t trace_heavy[64];
   float trace_us[64];
+  /* The learned scheduler's view of the update (filled when a scheduler ran or the schedule asked
+   * for record_features): the 12 batch features and the class each head chose (-1: none). */
+  float features[12];
+  int32_t schedule_classes[3];
 } dyngb200_stats;
 
 /* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */
@@ -145,6 +150,7 @@ typedef struct dyngb200_schedule {
   int32_t invalidation;   /* 0 heuristic/pointer jumping, 1 subtree walk */
   int32_t small_frontier; /* frontiers up to this many vertices run on one block (0: 256, < 0: off) */
   int32_t heavy_degree;   /* rows longer than this are split across warps (0: default) */
+  int32_t record_features; /* nonzero: compute the scheduler's features into the stats */
 } dyngb200_schedule;
 
 /* ---- errors ------------------------------------------------------------------------------ */
@@ -229,6 +235,62 @@ dyngb200_status dyngb200_sssp_compute_static_scratch(dyngb200_graph g, int32_t s
                                                      int32_t objective, int64_t delta,
                                                      int64_t* distances, int32_t* parents,
                                                      void* stream);
+
+/* ---- the learned scheduler (no reference counterpart) --------------------------------------
+ * A 12 -> 64 -> 64 -> 15 MLP with bf16 weights and activations and fp32 accumulation.  Its three
+ * softmax heads pick the schedule of one update: the near-far width class (8 classes: the
+ * automatic width times 4^(c - 2)), the invalidation / small-frontier class (4: pointer jumping
+ * with the small-frontier switch at 256, pointer jumping without it, subtree walk at 256, subtree
+ * walk without it) and the persistent-grid class (3: 1/4, 1/2, all of the occupancy grid).  The
+ * features are computed on the device from the batch, the graph and the tree's record of its
+ * previous update; the schedule never changes distances or parents.
+ * Features (12, float): log2(1 + batch operations), insertion fraction, fraction of deletions
+ * that remove a tree edge, log2(1 + mean / max out-degree of the batch's sources), log2(1 + n),
+ * log2(1 + m / n), log2(1 + automatic width), and of the tree's previous update log2(1 + x) of:
+ * invalidated vertices, first near-far frontier, largest of the next three, steps.
+ * Labels: 3 int32 per sample (width, switch, grid class).  Parameters: dyngb200_scheduler_num_params
+ * floats, W1[64x12] b1[64] W2[64x64] b2[64] W3[15x64] b3[15] (row-major, out x in); the feature
+ * standardization (f - mean) * scale is applied on the device. */
+#define DYNGB200_SCHED_FEATURES 12
+#define DYNGB200_SCHED_OUTPUTS 15
+int64_t dyngb200_scheduler_num_params(void);
+dyngb200_status dyngb200_scheduler_create(dyngb200_context ctx, uint64_t seed,
+                                          dyngb200_scheduler* out);
+dyngb200_status dyngb200_scheduler_destroy(dyngb200_scheduler s);
+/* NULL pointers leave that part unchanged; new parameters reset the optimizer state. */
+dyngb200_status dyngb200_scheduler_set_params(dyngb200_context ctx, dyngb200_scheduler s,
+                                              const float* params, const float* feature_mean,
+                                              const float* feature_scale);
+dyngb200_status dyngb200_scheduler_get_params(dyngb200_context ctx, dyngb200_scheduler s,
+                                              float* params, float* feature_mean,
+                                              float* feature_scale);
+/* Logits (n x 15, host) of raw feature rows (n x 12, host), by the device kernels. */
+dyngb200_status dyngb200_scheduler_forward(dyngb200_context ctx, dyngb200_scheduler s,
+                                           const float* features, int64_t n, float* logits);
+/* Mean loss (cross-entropy summed over the heads) and its gradient over all n samples, without
+ * a step; grads: num_params floats (host) or NULL. */
+dyngb200_status dyngb200_scheduler_gradients(dyngb200_context ctx, dyngb200_scheduler s,
+                                             const float* features, const int32_t* labels,
+                                             int64_t n, float* grads, double* loss);
+/* Minibatch Adam on the device over `epochs` seeded shuffles; final_loss: the mean loss of the
+ * last pass. */
+dyngb200_status dyngb200_scheduler_train(dyngb200_context ctx, dyngb200_scheduler s,
+                                         const float* features, const int32_t* labels, int64_t n,
+                                         int32_t epochs, int32_t batch_size, float learning_rate,
+                                         uint64_t seed, double* final_loss);
+/* sssp::update with the schedule the scheduler picks on the device for this batch (stats carry
+ * the features and the chosen classes).  Results equal dyngb200_sssp_update's. */
+dyngb200_status dyngb200_sssp_update_learned(dyngb200_context ctx, dyngb200_graph g,
+                                             const dyngb200_batch* batch, dyngb200_tree tree,
+                                             dyngb200_scheduler scheduler, dyngb200_stats* stats);
+
+/* ---- snapshots (recording scheduler traces: one batch under many schedules) ---------------- */
+/* A new graph with g's contents (its own identity: trees of g are not bound to it). */
+dyngb200_status dyngb200_graph_clone(dyngb200_context ctx, dyngb200_graph g, dyngb200_graph* out);
+/* src's contents into dst, which keeps its identity (trees bound to dst stay bound). */
+dyngb200_status dyngb200_graph_copy_from(dyngb200_context ctx, dyngb200_graph dst,
+                                         dyngb200_graph src);
+dyngb200_status dyngb200_tree_copy_from(dyngb200_context ctx, dyngb200_tree dst, dyngb200_tree src);
 
 /* ---- tree: sssp::result (sssp.hpp:153-310) ------------------------------------------------ */
 /* result::from_arrays (sssp.hpp:253-302): arrays in `memory`, n entries each. */
