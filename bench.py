@@ -9,8 +9,11 @@ Seeded synthetic data (the reference publishes no number for this configuration)
 A step is one sssp::update of one batch.  `value` times the update with the batch already in
 device memory (CUDA events on the library's stream); `e2e` times the public call with the batch
 in pinned host memory (the copy to the device and the read-back of the stats inside the timed
-region).  Every run checks the final tree against a from-scratch compute (distances and
-parents bit-exact).
+region).  Two arms run on the same batches from the same starting graph and tree (a device
+snapshot restored in between): the plain schedule (the fixed heuristic) and the learned
+scheduler (dyng_b200/data/scheduler_weights.npz); `--schedule` picks the headline arm and
+config.schedules reports both.  Every run checks that both arms end in the same tree and that
+the final tree equals a from-scratch compute (distances and parents bit-exact).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch 100000] [--scale 22]
     python bench.py --impl reference ...   # the reference algorithm's CPU restatement (oracle)
@@ -42,7 +45,10 @@ def parse():
     ap.add_argument("--batch", type=int, default=100_000)
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--schedule", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--schedule", default="learned", choices=["plain", "learned"],
+                    help="the headline arm; both arms run when scheduler weights exist")
+    ap.add_argument("--scheduler-weights", default=os.path.join(ROOT, "dyng_b200", "data",
+                                                                "scheduler_weights.npz"))
     ap.add_argument("--invalidation", type=int, default=0, help="0 pointer jumping, 1 subtree walk")
     ap.add_argument("--delta", type=int, default=0)
     ap.add_argument("--grid-blocks", type=int, default=0)
@@ -195,6 +201,62 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+class Arm:
+    """One schedule's pass over the benchmark batches: W warm-up steps, then K timed steps, each
+    timed with CUDA events on the library's stream (max over ranks)."""
+
+    def __init__(self, name, schedule=None, scheduler=None):
+        self.name, self.schedule, self.scheduler = name, schedule, scheduler
+        self.lat, self.sizes, self.stats, self.host = [], [], [], []
+        self.total_ms = 0.0
+
+    def summary(self, world):
+        from dyng_b200.replicas import whole_job_rate
+        v = whole_job_rate(sum(self.sizes), self.total_ms, world)
+        return {"value": v, "ms_per_step": self.total_ms / max(len(self.lat), 1),
+                "p50_ms": float(np.percentile(self.lat, 50)),
+                "p99_ms": float(np.percentile(self.lat, 99)),
+                "apply_ms_mean": float(np.mean([s.apply_ms for s in self.stats])),
+                "sssp_ms_mean": float(np.mean([s.sssp_ms for s in self.stats]))}
+
+
+def run_arm(env, arm, next_batch, nvtx=False):
+    D, torch, g, tree, stream, args, world, local = env
+    for step in range(args.warmup + args.steps):
+        b = next_batch(step)
+        ts = [torch.from_numpy(np.ascontiguousarray(x)).to(f"cuda:{local}") for x in
+              (b.insert_src, b.insert_dst, b.insert_weights, b.delete_src, b.delete_dst)]
+        db = D.EdgeBatch.device(ts[0].data_ptr(), ts[1].data_ptr(), ts[2].data_ptr(),
+                                b.insert_src.size, ts[3].data_ptr(), ts[4].data_ptr(),
+                                b.delete_src.size)
+        torch.cuda.synchronize()
+        if step == args.warmup:
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            if nvtx:
+                torch.cuda.nvtx.range_push("timed")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        h0 = time.perf_counter()
+        e0.record(stream)
+        st = D.sssp.update(g, db, tree, schedule=arm.schedule, scheduler=arm.scheduler)
+        e1.record(stream)
+        e1.synchronize()
+        if step >= args.warmup:
+            arm.host.append(time.perf_counter() - h0)
+            arm.lat.append(e0.elapsed_time(e1))
+            arm.sizes.append(b.size)
+            arm.stats.append(st)
+        del ts
+    torch.cuda.synchronize()
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
+    from dyng_b200.replicas import max_over_ranks
+    arm.total_ms = max_over_ranks(float(sum(arm.lat)))
+    return arm
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -210,7 +272,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import dyng_b200 as D
     from dyng_b200 import generators as G
-    from dyng_b200 import _native as N
+    from dyng_b200 import scheduler as S
 
     # replicas only: every rank runs the same independent workload on its own GPU
     stream = torch.cuda.Stream()
@@ -222,56 +284,55 @@ def main():
     tree = D.sssp.compute(g, 0)
     build_s = time.time() - t0
     bs = G.BatchStream(edges, seed=7)
+    env = (D, torch, g, tree, stream, args, world, local)
 
-    def device_batch(b):
-        ts = [torch.from_numpy(np.ascontiguousarray(x)).to(f"cuda:{local}") for x in
-              (b.insert_src, b.insert_dst, b.insert_weights, b.delete_src, b.delete_dst)]
-        return ts, D.EdgeBatch.device(ts[0].data_ptr(), ts[1].data_ptr(), ts[2].data_ptr(),
-                                      b.insert_src.size, ts[3].data_ptr(), ts[4].data_ptr(),
-                                      b.delete_src.size)
-
-    sched = None
+    fixed = None
     if args.invalidation or args.delta or args.grid_blocks or args.heavy_degree or args.small:
-        sched = D.sssp.Schedule(delta=args.delta, grid_blocks=args.grid_blocks,
+        fixed = D.sssp.Schedule(delta=args.delta, grid_blocks=args.grid_blocks,
                                 invalidation=args.invalidation, heavy_degree=args.heavy_degree,
                                 small_frontier=args.small)
-    host_lat = []
-    timed_stats = []
-    lat = []
-    sizes = []
-    # warm-up + timed steps with device-resident batches
-    for step in range(args.warmup + args.steps):
-        b = bs.next(args.batch, 0.75, 0.5, parents=tree.parents)
-        keep, db = device_batch(b)
-        torch.cuda.synchronize()
-        if step == args.warmup:
-            if world > 1:
-                torch.distributed.barrier()
-            torch.cuda.synchronize()
-            sampler = ClockSampler(local)
-            sampler.start()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        h0 = time.perf_counter()
-        e0.record(stream)
-        st = D.sssp.update(g, db, tree, schedule=sched)
-        e1.record(stream)
-        e1.synchronize()
-        host_lat.append(time.perf_counter() - h0)
-        if step >= args.warmup:
-            lat.append(e0.elapsed_time(e1))
-            sizes.append(b.size)
-            timed_stats.append(st)
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    total_ms = float(sum(lat))
-    if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * sum(sizes) / (total_ms / 1000.0)
+    weights = args.scheduler_weights
+    learned = None
+    if os.path.exists(weights):
+        learned = S.Scheduler.load(weights, resources=res)
+    elif args.schedule == "learned":
+        print(f"bench: no scheduler weights at {weights}; timing the plain schedule only",
+              file=sys.stderr)
+        args.schedule = "plain"
 
-    # end to end: batches in pinned host memory through the public call
+    # the plain arm generates the batches (deletions drawn from the current tree); the learned arm
+    # replays them from the same starting graph and tree (a device snapshot restored in between)
+    recorded = []
+
+    def generate(step):
+        b = bs.next(args.batch, 0.75, 0.5, parents=tree.parents)
+        recorded.append(b)
+        return b
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    arms = {}
+    if learned is not None:
+        g_snap, t_snap = g.clone(), tree.clone()
+    arms["plain"] = run_arm(env, Arm("plain", schedule=fixed), generate,
+                            nvtx=args.schedule == "plain")
+    same = None
+    if learned is not None:
+        d_plain, p_plain = tree.distances, tree.parents
+        g.copy_from(g_snap)
+        tree.copy_from(t_snap)
+        del g_snap, t_snap
+        arms["learned"] = run_arm(env, Arm("learned", scheduler=learned), lambda i: recorded[i],
+                                  nvtx=args.schedule == "learned")
+        same = bool(np.array_equal(d_plain, tree.distances) and
+                    np.array_equal(p_plain, tree.parents))
+        del d_plain, p_plain
+    clocks = sampler.stop()
+    head = arms[args.schedule]
+    summ = {k: a.summary(world) for k, a in arms.items()}
+    value = summ[args.schedule]["value"]
+    timed_stats = head.stats
+    # end to end: batches in pinned host memory through the public call, headline schedule
     e2e_lat, e2e_sizes = [], []
     h2d = 0
     for step in range(args.steps):
@@ -282,7 +343,7 @@ def main():
         hb = D.EdgeBatch.from_arrays(*arrs)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st = D.sssp.update(g, hb, tree, schedule=sched)
+        D.sssp.update(g, hb, tree, schedule=head.schedule, scheduler=head.scheduler)
         e2e_lat.append(time.perf_counter() - t0)
         e2e_sizes.append(b.size)
         h2d = sum(a.nbytes for a in arrs)
@@ -299,7 +360,6 @@ def main():
     # roofline of the dominant kernel (the sssp persistent kernel): algorithmic bytes counted by
     # the kernel (Stats.work x Stats.WORK_BYTES) over its CUDA-event time on the launching stream
     sssp_ms = [s.sssp_ms for s in timed_stats]
-    apply_ms = [s.apply_ms for s in timed_stats]
     peak, peak_kind = peaks()
     alg = [s.algorithmic_bytes + 12 * s.affected for s in timed_stats]
     achieved = float(np.sum(alg) / (np.sum(sssp_ms) / 1000.0) / 1e9) if sssp_ms else 0.0
@@ -310,6 +370,7 @@ def main():
     shape = {k: float(np.mean([getattr(s, k) for s in timed_stats]))
              for k in ("iterations", "epochs", "pushes", "invalidated", "affected", "rounds",
                        "touched", "delta", "grid_blocks")}
+    classes = [list(s.schedule_classes) for s in timed_stats] if args.schedule == "learned" else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -330,9 +391,15 @@ def main():
                    "sample": f"failed: {exc}"}
 
     if rank == 0:
+        compare = {k: {kk: round(vv, 4) if kk != "value" else vv for kk, vv in v.items()}
+                   for k, v in summ.items()}
+        if "learned" in summ:
+            compare["learned_over_plain"] = summ["learned"]["value"] / summ["plain"]["value"]
+            compare["learned_equals_plain"] = same
         line = {
             "metric": METRIC, "value": value, "unit": "changed edges/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": summ[args.schedule]["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
             "config": {"workload": f"rmat-s{args.scale}-ef16-w1000-batch{args.batch}",
@@ -340,21 +407,22 @@ def main():
                        "batch_changes": args.batch, "insert_fraction": 0.75,
                        "schedule": args.schedule, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (graph arenas ~1 GB)",
-                       "p50_ms": float(np.percentile(lat, 50)),
-                       "p99_ms": float(np.percentile(lat, 99)),
-                       "apply_ms_mean": float(np.mean(apply_ms)),
-                       "sssp_ms_mean": float(np.mean(sssp_ms)),
-                       "host_ms_p50": 1000 * float(np.percentile(host_lat[args.warmup:], 50)),
+                       "p50_ms": summ[args.schedule]["p50_ms"],
+                       "p99_ms": summ[args.schedule]["p99_ms"],
+                       "apply_ms_mean": summ[args.schedule]["apply_ms_mean"],
+                       "sssp_ms_mean": summ[args.schedule]["sssp_ms_mean"],
+                       "host_ms_p50": 1000 * float(np.percentile(head.host, 50)),
+                       "schedules": compare, "learned_classes": classes,
                        "sssp_phases_ms": phases, "sssp_work": work, "update_shape": shape,
                        "alg_bytes_per_update": float(np.mean(alg)),
                        "trace_last_update": [list(t) for t in timed_stats[-1].trace],
                        "verified_vs_compute": verified,
                        "setup_s": {"generate": round(gen_s, 1), "build_and_compute": round(build_s, 1)}},
             "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": 512,
+                    "d2h_bytes_per_step": ctypes.sizeof(D._native.Stats),
                     "p50_ms": 1000 * float(np.percentile(e2e_lat, 50)),
                     "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
-            "gpu_launches": 14 * args.steps,
+            "gpu_launches": int(sum(s.kernel_launches for s in timed_stats)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": None,
                          "peak_kind": peak_kind, "kernel": "k_sssp"},
@@ -364,7 +432,6 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()

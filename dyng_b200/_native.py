@@ -56,7 +56,8 @@ class Stats(ctypes.Structure):
                 ("work", ctypes.c_int64 * 12), ("phase_ms", ctypes.c_float * 7),
                 ("trace_len", ctypes.c_int32), ("trace_light", ctypes.c_int32 * 64),
                 ("trace_heavy", ctypes.c_int32 * 64), ("trace_us", ctypes.c_float * 64),
-                ("features", ctypes.c_float * 12), ("schedule_classes", ctypes.c_int32 * 3)]
+                ("features", ctypes.c_float * 12), ("schedule_classes", ctypes.c_int32 * 3),
+                ("kernel_launches", ctypes.c_int64)]
 
 
 class Options(ctypes.Structure):

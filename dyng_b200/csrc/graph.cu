@@ -1397,6 +1397,7 @@ void graph_index_build(Context& ctx, Graph& g, long long extra) {
   DYNGB200_CUDA(cudaMemsetAsync(&ws.ctl.ptr->error, 0, sizeof(unsigned), s));
   GraphView v = g.view();
   const int grid = ctx.sm_count * 8;
+  ctx.launches += 3;
   k_index_clear<<<grid, kBlock, 0, s>>>(v);
   k_index_out<<<grid, kBlock, 0, s>>>(v, gc.n, &ws.ctl.ptr->error);
   k_index_in<<<grid, kBlock, 0, s>>>(v, gc.n, &ws.ctl.ptr->error);
@@ -1577,6 +1578,7 @@ void graph_rescan_columns(Context& ctx, Graph& g) {
   out.reserve(3 * k);
   DYNGB200_CUDA(cudaMemsetAsync(out.ptr, 0, 3 * k * sizeof(long long), ctx.stream));
   const int grid = grid_for(g.n, kBlock, ctx.sm_count);
+  ctx.launches += 2;
   k_rescan_columns<<<grid, kBlock, 0, ctx.stream>>>(g.view(), g.n, out.ptr);
   k_rescan_count<<<grid, kBlock, 0, ctx.stream>>>(g.view(), g.n, out.ptr);
   std::vector<long long> h(3 * k);
@@ -1674,6 +1676,7 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
   const int grid_ops = grid_for(b.ni + b.nd, kBlock, ctx.sm_count);
   k_validate<<<grid_ops, kBlock, 0, s>>>(p);
   k_plan<<<1, 1, 0, s>>>(p);
+  ctx.launches += g.props.sorted ? 5 : 8;  // validate, plan, pairs, match, resolve (+ 3 ordering)
   // the learned scheduler reads the batch, the old rows and the tree before anything changes,
   // and writes its schedule into the control block (after the plan's default width)
   if (tree && (learned || (sched && sched->record_features)))
@@ -1705,6 +1708,7 @@ void apply_commit(Context& ctx, Graph& g, const StagedBatch& b) {
   const long long ops = (b.ni + b.nd) * dir;
   ApplyParams p = make_params(ctx, g, b, -1, 0);
   const int grid = grid_for(2 * ops, kBlock, ctx.sm_count);
+  ctx.launches += 7;
   k_alloc<<<grid, kBlock, 0, s>>>(p);
   k_mutate<<<grid, kBlock, 0, s>>>(p);
   k_move<<<ctx.sm_count * 4, kBlock, 0, s>>>(p);
@@ -1731,6 +1735,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
       flags.reserve(static_cast<size_t>(b.ni) * g.k);
       ApplyParams p = make_params(ctx, g, b, -1, 0);
       k_insert_flags<<<grid_for(b.ni, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, flags.ptr);
+      ++ctx.launches;
       DYNGB200_CUDA(cudaGetLastError());
       DYNGB200_CUDA(cudaMemcpyAsync(weight_increased, flags.ptr, static_cast<size_t>(b.ni) * g.k,
                                     cudaMemcpyDeviceToHost, s));

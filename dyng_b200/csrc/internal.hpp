@@ -199,6 +199,7 @@ struct Context {
   bool own_stream = false;
   int sm_count = 0;
   int coop_supported = 0;
+  long long launches = 0;  // kernels this context has launched (reported per call in the stats)
   int update_blocks_per_sm = 0;
   int compute_blocks_per_sm = 0;
   Workspace ws;

@@ -553,6 +553,7 @@ void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch&
     k_features_acc<<<grid, 256, 0, s>>>(b.ins_src, b.ni, b.del_src, b.del_dst, b.nd,
                                         g.out_desc.ptr, g.n, t.parent.ptr, t.n,
                                         g.props.directed, c);
+    ++ctx.launches;
   }
   const int blocks = ctx.update_blocks_per_sm * ctx.sm_count;
   FeatNorm nrm{};
@@ -560,6 +561,7 @@ void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch&
   k_infer_schedule<<<1, 32, 0, s>>>(sch ? sch->params.ptr : nullptr,
                                     sch ? sch->wbf16.ptr : nullptr, nrm, c, t.hist.ptr,
                                     g.counters.ptr, b.ni, b.nd, blocks);
+  ++ctx.launches;
   DYNGB200_CUDA(cudaGetLastError());
 }
 

@@ -1237,6 +1237,7 @@ static void launch(Context& ctx, SsspParams& p, int blocks) {
   expects(ctx.coop_supported != 0, "sssp: the fused engine needs cooperative launch",
           DYNGB200_NOT_SUPPORTED);
   void* args[] = {&p};
+  ++ctx.launches;
   DYNGB200_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_sssp), dim3(blocks),
                                             dim3(kThreads), args, 0, ctx.stream));
 }
@@ -1275,6 +1276,7 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
 
 // compute(): the persistent kernel from the source (fused.cuh:167-176).
 void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
+  const long long launches0 = ctx.launches;
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   ws.reserve_vertices(g.n_cap, s);
@@ -1344,12 +1346,14 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
     st->grid_blocks = init.active_blocks > 0 && init.active_blocks < blocks ? init.active_blocks
                                                                              : blocks;
     st->sssp_ms = ms;
+    st->kernel_launches = ctx.launches - launches0;
   }
 }
 
 // update(): the applier, then the persistent kernel, then one read-back of the control block.
 void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
                  const dyngb200_schedule& sched, dyngb200_stats* st, const Scheduler* learned) {
+  const long long launches0 = ctx.launches;
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   const int objective = t.opt.objective;
@@ -1481,6 +1485,7 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
     const bool scheduled = learned || sched.record_features;
     for (int i = 0; i < 12; ++i) st->features[i] = scheduled ? r.features[i] : 0.0f;
     for (int i = 0; i < 3; ++i) st->schedule_classes[i] = learned ? r.sched_classes[i] : -1;
+    st->kernel_launches = ctx.launches - launches0;
     for (int i = 0; i < 7; ++i)
       st->phase_ms[i] = r.phase_ns[i + 1] > r.phase_ns[i]
                             ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)
@@ -1531,6 +1536,7 @@ void tree_copy(Context& ctx, Tree& dst, const Tree& src) {
 
 void tree_canonicalize(Context& ctx, Graph& g, Tree& t) {
   const int grid = ctx.sm_count * 8;
+  ++ctx.launches;
   k_canonicalize<<<grid, kThreads, 0, ctx.stream>>>(g.view(), t.opt.objective, t.source, t.n,
                                                     reinterpret_cast<const long long*>(t.dist.ptr),
                                                     t.parent.ptr);
@@ -1539,6 +1545,7 @@ void tree_canonicalize(Context& ctx, Graph& g, Tree& t) {
 
 void tree_repack(Context& ctx, Tree& t, int bits) {
   const int grid = ctx.sm_count * 8;
+  ++ctx.launches;
   k_pack<<<grid, kThreads, 0, ctx.stream>>>(t.n, bits, reinterpret_cast<const long long*>(t.dist.ptr),
                                             t.parent.ptr, t.packed.ptr);
   DYNGB200_CUDA(cudaGetLastError());

@@ -155,16 +155,53 @@ class CSR(NamedTuple):
 
 
 class EdgeBatch:
-    """An edge batch (edge_batch.hpp:88-404): insertions (upserts) and deletions.
+    """An edge batch (edge_batch.hpp:88-404; python/dyng/batch.py): insertions (upserts under the
+    default semantics) and deletions.
 
-    Arrays may be numpy (host) or device pointers wrapped by ``EdgeBatch.device``."""
+    ``EdgeBatch(insert=(src, dst[, weights]), delete=(src, dst))`` as in the reference; weights
+    of shape (n,) or (n, K) (insertion-major); insertions without weights get weight 1.  Also
+    built edge by edge (``insert_edge`` / ``delete_edge``), from flat arrays (``from_arrays``) or
+    from device pointers (``device``)."""
 
-    def __init__(self, num_weights: int = 1):
-        self.num_weights = num_weights
+    def __init__(self, insert=None, delete=None, *, num_weights: int | None = None):
+        self.num_weights = 1 if num_weights is None else int(num_weights)
         self._ins_src, self._ins_dst, self._ins_w = [], [], []
         self._del_src, self._del_dst = [], []
         self._arrays = None
         self._device = None
+        if insert is not None or delete is not None:
+            ins = tuple(insert) if insert is not None else ((), ())
+            dele = tuple(delete) if delete is not None else ((), ())
+            if len(ins) not in (2, 3) or len(dele) != 2:
+                raise InvalidArgumentError("EdgeBatch: insert is (src, dst[, weights]), delete "
+                                           "is (src, dst)")
+            s, d = _i32(ins[0]), _i32(ins[1])
+            if s.size != d.size:
+                raise InvalidArgumentError("EdgeBatch: the insert src and dst differ in length")
+            if len(ins) == 3 and ins[2] is not None:
+                w = np.asarray(ins[2])
+                if w.ndim == 2:
+                    if num_weights is None:
+                        self.num_weights = int(w.shape[1])
+                    if w.shape != (s.size, self.num_weights):
+                        raise InvalidArgumentError("EdgeBatch: weights must be (n,) or (n, K)")
+                elif w.size != s.size * self.num_weights:
+                    raise InvalidArgumentError("EdgeBatch: one weight per insertion expected")
+                w = _i32(w.reshape(-1))
+            else:
+                w = np.ones(s.size * self.num_weights, np.int32)
+            ds, dd = _i32(dele[0]), _i32(dele[1])
+            if ds.size != dd.size:
+                raise InvalidArgumentError("EdgeBatch: the delete src and dst differ in length")
+            self._arrays = (s, d, w, ds, dd)
+
+    @property
+    def num_insertions(self) -> int:
+        return self._device[3] if self._device else self.arrays()[0].size
+
+    @property
+    def num_deletions(self) -> int:
+        return self._device[6] if self._device else self.arrays()[3].size
 
     def insert_edge(self, u: int, v: int, weights=(1,)) -> "EdgeBatch":
         w = list(weights) if np.ndim(weights) else [weights]
@@ -183,12 +220,12 @@ class EdgeBatch:
         return self
 
     def clear(self) -> None:
-        self.__init__(self.num_weights)
+        self.__init__(num_weights=self.num_weights)
 
     @classmethod
     def from_arrays(cls, insert_src=None, insert_dst=None, insert_weights=None, delete_src=None,
                     delete_dst=None, num_weights: int = 1) -> "EdgeBatch":
-        b = cls(num_weights)
+        b = cls(num_weights=num_weights)
         b._arrays = (_i32(insert_src), _i32(insert_dst), _i32(insert_weights), _i32(delete_src),
                      _i32(delete_dst))
         return b
@@ -198,7 +235,7 @@ class EdgeBatch:
                delete_src: int, delete_dst: int, num_deletions: int,
                num_weights: int = 1) -> "EdgeBatch":
         """A batch whose arrays already live in device memory (raw CUDA pointers)."""
-        b = cls(num_weights)
+        b = cls(num_weights=num_weights)
         b._device = (insert_src, insert_dst, insert_weights, num_insertions, delete_src,
                      delete_dst, num_deletions)
         return b
@@ -208,12 +245,6 @@ class EdgeBatch:
             self._arrays = (_i32(self._ins_src), _i32(self._ins_dst), _i32(self._ins_w),
                             _i32(self._del_src), _i32(self._del_dst))
         return self._arrays
-
-    def num_insertions(self) -> int:
-        return self._device[3] if self._device else self.arrays()[0].size
-
-    def num_deletions(self) -> int:
-        return self._device[6] if self._device else self.arrays()[3].size
 
     def _to_native(self) -> N.Batch:
         if self._device is not None:
@@ -308,12 +339,12 @@ class Graph:
         sm = N.ApplySummary()
         nb = batch._to_native()
         if classify:
-            mask = np.zeros(max(batch.num_insertions(), 1) * batch.num_weights, np.uint8)
+            mask = np.zeros(max(batch.num_insertions, 1) * batch.num_weights, np.uint8)
             check(N.lib().dyngb200_graph_apply_classified(
                 self._res._h, self._h, ctypes.byref(nb), ctypes.byref(sm),
                 mask.ctypes.data_as(N.c_u8p)))
             k = batch.num_weights
-            return ApplySummary._from_native(sm), mask[:batch.num_insertions() * k].reshape(-1, k)
+            return ApplySummary._from_native(sm), mask[:batch.num_insertions * k].reshape(-1, k)
         check(N.lib().dyngb200_graph_apply(self._res._h, self._h, ctypes.byref(nb),
                                            ctypes.byref(sm)))
         return ApplySummary._from_native(sm)

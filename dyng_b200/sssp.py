@@ -80,6 +80,7 @@ class Stats:
     trace: tuple = ()  # (light, heavy chunks, start us) per near-far step; light < 0: an epoch
     features: tuple = ()  # the learned scheduler's 12 features (when a scheduler or recording ran)
     schedule_classes: tuple = (-1, -1, -1)  # the classes the learned scheduler picked
+    kernel_launches: int = 0  # kernels of the library the call launched
 
     WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
                   "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
@@ -103,7 +104,7 @@ class Stats:
                    tuple((int(s.trace_light[i]), int(s.trace_heavy[i]), float(s.trace_us[i]))
                          for i in range(min(int(s.trace_len), 64))),
                    tuple(float(x) for x in s.features),
-                   tuple(int(x) for x in s.schedule_classes))
+                   tuple(int(x) for x in s.schedule_classes), int(s.kernel_launches))
 
 
 class Result:

@@ -131,6 +131,7 @@ typedef struct dyngb200_stats {
    * for record_features): the 12 batch features and the class each head chose (-1: none). */
   float features[12];
   int32_t schedule_classes[3];
+  int64_t kernel_launches; /* kernels of this library the call launched */
 } dyngb200_stats;
 
 /* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */

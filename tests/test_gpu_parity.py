@@ -101,6 +101,16 @@ def test_readme_quickstart():
     assert t.distances.tolist() == [0, 4, 1, 2] and st.invalidated == 2
 
 
+def test_readme_quickstart_through_the_mirrored_python_api():
+    # the reference's README quickstart (README.md:49-59), call for call
+    g = D.Graph.from_edges([0, 0, 2, 1], [1, 2, 1, 3], [4, 1, 2, 1])
+    tree = D.sssp.compute(g, source=0)
+    assert tree.distances.tolist() == [0, 3, 1, 4]
+    batch = D.EdgeBatch(insert=([2], [3], [1]), delete=([2], [1]))
+    stats = D.sssp.update(g, batch, tree)
+    assert (tree.distances.tolist(), stats.invalidated) == ([0, 4, 1, 2], 2)
+
+
 def test_hand_cases():
     g, _ = _pair(5, [(0, 1, 5), (0, 2, 1), (2, 3, 1), (1, 4, 2), (3, 4, 2)], "mosp")
     t = D.sssp.compute(g, 0)
