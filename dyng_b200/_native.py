@@ -71,6 +71,21 @@ class Schedule(ctypes.Structure):
                 ("heavy_degree", ctypes.c_int32), ("record_features", ctypes.c_int32)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("max_group", ctypes.c_int32),
+                ("small_changes", ctypes.c_int64), ("hbm_reserve_bytes", ctypes.c_int64)]
+
+
+class RequestTimes(ctypes.Structure):
+    _fields_ = [("queued_ms", ctypes.c_double), ("service_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double), ("group_size", ctypes.c_int32)]
+
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "failed", "rounds",
+                                              "max_group", "waiting")]
+
+
 # Every symbol of include/dyngb200.h with (restype, argtypes).
 SIGNATURES = {
     "dyngb200_last_error_message": (ctypes.c_char_p, []),
@@ -129,6 +144,17 @@ SIGNATURES = {
     "dyngb200_sssp_update_learned": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch),
                                                     c_void_p, c_void_p, ctypes.POINTER(Stats)]),
     "dyngb200_scheduler_num_params": (ctypes.c_int64, []),
+    "dyngb200_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), c_void_p,
+                                              ctypes.POINTER(c_void_p)]),
+    "dyngb200_server_add_graph": (ctypes.c_int, [c_void_p, c_void_p, c_void_p,
+                                                 ctypes.POINTER(ctypes.c_int32)]),
+    "dyngb200_server_submit": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.POINTER(Batch),
+                                              ctypes.POINTER(ctypes.c_uint64)]),
+    "dyngb200_server_wait": (ctypes.c_int, [c_void_p, ctypes.c_uint64, ctypes.POINTER(Stats),
+                                            ctypes.POINTER(RequestTimes)]),
+    "dyngb200_server_drain": (ctypes.c_int, [c_void_p]),
+    "dyngb200_server_info_get": (ctypes.c_int, [c_void_p, ctypes.POINTER(ServerInfo)]),
+    "dyngb200_server_destroy": (ctypes.c_int, [c_void_p]),
     "dyngb200_scheduler_create": (ctypes.c_int, [c_void_p, ctypes.c_uint64,
                                                  ctypes.POINTER(c_void_p)]),
     "dyngb200_scheduler_destroy": (ctypes.c_int, [c_void_p]),

@@ -11,43 +11,59 @@
 #include <string>
 #include <vector>
 
-struct dyngb200_context_s {
-  dyngb200::Context ctx;
-};
-struct dyngb200_graph_s {
-  dyngb200::Graph g;
-};
-struct dyngb200_tree_s {
-  dyngb200::Tree t;
-};
-struct dyngb200_scheduler_s {
-  dyngb200::Scheduler s;
-};
+#include "handles.hpp"
+
+namespace dyngb200 {
+
+void expect_tree_current(const Graph& g, const Tree& t, const char* what) {
+  if (t.poisoned)
+    throw Error(DYNGB200_STALE_RESULT,
+                std::string(what) + ": the result was left unusable by a failed update; recompute "
+                                    "it with sssp::compute() (or import a valid tree)");
+  if (t.graph_id != g.id || t.version != g.version)
+    throw Error(DYNGB200_STALE_RESULT,
+                std::string(what) + ": the result does not match the graph's current version");
+  if (t.device != g.device)
+    throw Error(DYNGB200_INVALID_ARGUMENT, std::string(what) + ": result on another device");
+}
+
+void expect_batch(const Graph& g, const dyngb200_batch& b, const char* what) {
+  expects(b.num_insertions >= 0 && b.num_deletions >= 0, std::string(what) + ": negative sizes");
+  expects(b.num_insertions == 0 || b.num_weights == g.k,
+          std::string(what) + ": the batch has " + std::to_string(b.num_weights) +
+              " weight(s) per insertion but the graph has " + std::to_string(g.k));
+  expects(b.num_insertions == 0 || (b.insert_src && b.insert_dst && (g.k == 0 || b.insert_weights)),
+          std::string(what) + ": null insertion arrays");
+  expects(b.num_deletions == 0 || (b.delete_src && b.delete_dst),
+          std::string(what) + ": null deletion arrays");
+  expects(b.num_insertions + b.num_deletions < (1LL << 30),
+          std::string(what) + ": a batch holds at most 2^30 operations");
+}
+
+std::string& last_error() {
+  thread_local std::string message;
+  return message;
+}
+
+void context_init(Context& c, int device, void* stream) {
+  c.device = device;
+  DYNGB200_CUDA(cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device));
+  DYNGB200_CUDA(cudaDeviceGetAttribute(&c.coop_supported, cudaDevAttrCooperativeLaunch, device));
+  if (stream) {
+    c.stream = static_cast<cudaStream_t>(stream);
+  } else {
+    DYNGB200_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.own_stream = true;
+  }
+}
+
+}  // namespace dyngb200
 
 namespace {
 
 using namespace dyngb200;
 
-thread_local std::string g_last_error;
 std::atomic<uint64_t> g_next_graph_id{1};
-
-template <typename F>
-dyngb200_status guarded(F&& f) {
-  try {
-    f();
-    g_last_error.clear();
-    return DYNGB200_OK;
-  } catch (const Error& e) {
-    g_last_error = e.what();
-    return e.status;
-  } catch (const std::bad_alloc&) {
-    g_last_error = "out of host memory";
-    return DYNGB200_OUT_OF_MEMORY;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return DYNGB200_INTERNAL;
-  }
-}
 
 struct DeviceGuard {
   int prev = 0;
@@ -170,31 +186,6 @@ dyngb200_graph_s* new_graph(Context& ctx, long long n, std::vector<int32_t>& src
   return h;
 }
 
-void expect_tree_current(const Graph& g, const Tree& t, const char* what) {
-  if (t.poisoned)
-    throw Error(DYNGB200_STALE_RESULT,
-                std::string(what) + ": the result was left unusable by a failed update; recompute "
-                                    "it with sssp::compute() (or import a valid tree)");
-  if (t.graph_id != g.id || t.version != g.version)
-    throw Error(DYNGB200_STALE_RESULT,
-                std::string(what) + ": the result does not match the graph's current version");
-  if (t.device != g.device)
-    throw Error(DYNGB200_INVALID_ARGUMENT, std::string(what) + ": result on another device");
-}
-
-void expect_batch(const Graph& g, const dyngb200_batch& b, const char* what) {
-  expects(b.num_insertions >= 0 && b.num_deletions >= 0, std::string(what) + ": negative sizes");
-  expects(b.num_insertions == 0 || b.num_weights == g.k,
-          std::string(what) + ": the batch has " + std::to_string(b.num_weights) +
-              " weight(s) per insertion but the graph has " + std::to_string(g.k));
-  expects(b.num_insertions == 0 || (b.insert_src && b.insert_dst && (g.k == 0 || b.insert_weights)),
-          std::string(what) + ": null insertion arrays");
-  expects(b.num_deletions == 0 || (b.delete_src && b.delete_dst),
-          std::string(what) + ": null deletion arrays");
-  expects(b.num_insertions + b.num_deletions < (1LL << 30),
-          std::string(what) + ": a batch holds at most 2^30 operations");
-}
-
 // The O(n) checks of validate_inputs (sssp.cpp:398-460), in vertex order.
 void validate_tree(int32_t source, const std::vector<int64_t>& d, const std::vector<int32_t>& p,
                    long long bound) {
@@ -237,7 +228,7 @@ void validate_tree(int32_t source, const std::vector<int64_t>& d, const std::vec
 
 extern "C" {
 
-const char* dyngb200_last_error_message(void) { return g_last_error.c_str(); }
+const char* dyngb200_last_error_message(void) { return last_error().c_str(); }
 
 const char* dyngb200_status_name(dyngb200_status s) {
   switch (s) {
@@ -274,16 +265,7 @@ dyngb200_status dyngb200_context_create(int device, void* stream, dyngb200_conte
             DYNGB200_NOT_SUPPORTED);
     DeviceGuard guard(device);
     auto h = std::make_unique<dyngb200_context_s>();
-    Context& c = h->ctx;
-    c.device = device;
-    DYNGB200_CUDA(cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device));
-    DYNGB200_CUDA(cudaDeviceGetAttribute(&c.coop_supported, cudaDevAttrCooperativeLaunch, device));
-    if (stream) {
-      c.stream = static_cast<cudaStream_t>(stream);
-    } else {
-      DYNGB200_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-      c.own_stream = true;
-    }
+    context_init(h->ctx, device, stream);
     *out = h.release();
   });
 }

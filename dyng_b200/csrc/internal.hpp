@@ -226,6 +226,9 @@ struct Graph {
   long long ecap = 0;
   GraphCounters host_counters{};
   std::vector<ColumnStats> host_columns;
+  // pinned landing area of the per-update read-back: the counters, then the column statistics
+  // (both 8-byte aligned PODs; sized in ColumnStats units)
+  HostBuf<ColumnStats> pinned;
   int device = 0;
 
   GraphView view() {
@@ -355,6 +358,28 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st);
 void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
                  const dyngb200_schedule& sched, dyngb200_stats* st,
                  const Scheduler* learned = nullptr);
+// An update split in two for callers that queue several updates (of different graphs, each with
+// its own context) on one stream before waiting: begin() stages the batch and queues the work,
+// end() waits, retries on capacity and fills the stats.
+struct PendingUpdate {
+  Context* ctx = nullptr;
+  Graph* g = nullptr;
+  Tree* t = nullptr;
+  dyngb200_schedule sched{};
+  const Scheduler* learned = nullptr;
+  StagedBatch b{};
+  int blocks = 0;
+  long long launches0 = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+  PendingUpdate() = default;
+  PendingUpdate(const PendingUpdate&) = delete;
+  PendingUpdate& operator=(const PendingUpdate&) = delete;
+  ~PendingUpdate();
+};
+void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
+                       const dyngb200_schedule& sched, const Scheduler* learned,
+                       PendingUpdate& u);
+void sssp_update_end(PendingUpdate& u, dyngb200_stats* st);
 void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
                  dyngb200_apply_summary* summary, unsigned char* weight_increased);
 void tree_reserve(Context& ctx, Tree& t, long long n_cap);

@@ -1,0 +1,470 @@
+// The serving loop: several graphs resident on one GPU, each with its own shortest-path tree,
+// fed by batches that arrive at any time from any host thread.
+//
+// - One dispatcher thread owns the GPU work.  Requests wait in per-graph FIFO queues, so the
+//   batches of one graph apply in arrival order and every result is the one the same batches
+//   would give alone, one after the other.
+// - Continuous batching: each round takes the oldest waiting request of every graph that has
+//   one (round-robin over the graphs), as long as they are small, and queues all of their
+//   updates on one stream before waiting once (sssp_update_begin / sssp_update_end).  The host
+//   work of one update (staging, launches) overlaps the GPU work of the previous ones, and a
+//   round needs one host-device synchronisation instead of one per update.  A large batch runs
+//   in a round of its own.
+// - Admission by free HBM: a graph is registered only if its workspace fits beside the reserve,
+//   and a batch is dispatched only if its estimated scratch fits in the free device memory beyond
+//   the reserve; otherwise it fails with OUT_OF_MEMORY instead of taking the device down.
+// - Every graph has its own context (workspace, control block) on the server's one stream.
+#include "handles.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+struct dyngb200_server_s;
+
+namespace dyngb200 {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServerRequest {
+  uint64_t ticket = 0;
+  int slot = 0;
+  std::unique_ptr<HostBuf<int32_t>> data;  // pinned copy of the batch's five arrays
+  dyngb200_batch batch{};
+  long long ops = 0;
+  Clock::time_point arrival, start, finish;
+  int group_size = 0;
+  bool done = false;
+  dyngb200_status status = DYNGB200_OK;
+  std::string message;
+  dyngb200_stats stats{};
+};
+
+struct ServerGraph {
+  std::unique_ptr<Context> ctx;
+  Graph* g = nullptr;
+  Tree* t = nullptr;
+  std::deque<ServerRequest*> queue;
+};
+
+class Server {
+ public:
+  Server(const dyngb200_server_config& cfg, const Scheduler* learned);
+  ~Server();
+  int add_graph(Graph& g, Tree& t);
+  uint64_t submit(int slot, const dyngb200_batch& b);
+  ServerRequest wait(uint64_t ticket);
+  void drain();
+  dyngb200_server_info info();
+
+ private:
+  void run();
+  void dispatch(std::vector<ServerRequest*>& group);
+  long long estimate_bytes(const ServerGraph& sg, const ServerRequest& r) const;
+  std::unique_ptr<HostBuf<int32_t>> take_buffer(size_t n);
+  void give_buffer(std::unique_ptr<HostBuf<int32_t>> b);
+
+  dyngb200_server_config cfg_{};
+  const Scheduler* learned_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  std::vector<std::unique_ptr<ServerGraph>> graphs_;
+  std::unordered_map<uint64_t, std::unique_ptr<ServerRequest>> requests_;
+  std::vector<std::unique_ptr<HostBuf<int32_t>>> pool_;
+  std::mutex mu_;
+  std::condition_variable work_cv_, done_cv_;
+  std::thread worker_;
+  bool stop_ = false;
+  uint64_t next_ticket_ = 1;
+  size_t next_graph_ = 0;  // round-robin start
+  long long waiting_ = 0, running_ = 0;
+  long long held_bytes_ = 0;  // pinned copies of queued batches (submit waits above the cap)
+  static constexpr long long kHeldCap = 1LL << 30;
+  dyngb200_server_info info_{};
+};
+
+}  // namespace dyngb200
+
+namespace dyngb200 {
+
+// Bytes of the pinned copy a queued request holds.
+long long held_of(const ServerRequest& r) {
+  const long long ni = r.batch.num_insertions, nd = r.batch.num_deletions;
+  const long long k = r.batch.num_weights > 0 ? r.batch.num_weights : 0;
+  return (2 * ni + ni * k + 2 * nd) * static_cast<long long>(sizeof(int32_t));
+}
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+Server::Server(const dyngb200_server_config& cfg, const Scheduler* learned)
+    : cfg_(cfg), learned_(learned) {
+  if (cfg_.max_group <= 0) cfg_.max_group = 8;
+  if (cfg_.small_changes <= 0) cfg_.small_changes = 65536;
+  if (cfg_.hbm_reserve_bytes <= 0) cfg_.hbm_reserve_bytes = 1LL << 30;
+  expects(!learned_ || learned_->device == cfg_.device,
+          "server: the scheduler belongs to another device");
+  DYNGB200_CUDA(cudaSetDevice(cfg_.device));
+  DYNGB200_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  worker_ = std::thread([this] { run(); });
+}
+
+Server::~Server() {
+  {
+    std::unique_lock<std::mutex> lk(mu_);
+    stop_ = true;
+  }
+  work_cv_.notify_all();
+  if (worker_.joinable()) worker_.join();
+  graphs_.clear();
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Server::add_graph(Graph& g, Tree& t) {
+  expects(g.device == cfg_.device, "server::add_graph: the graph belongs to another device");
+  expect_tree_current(g, t, "server::add_graph");
+  auto sg = std::make_unique<ServerGraph>();
+  sg->ctx = std::make_unique<Context>();
+  context_init(*sg->ctx, cfg_.device, stream_);
+  // admission: the context's per-vertex workspace (~100 B per vertex of capacity) must fit
+  size_t free_b = 0, total_b = 0;
+  DYNGB200_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const long long need = 100LL * g.n_cap + (16LL << 20);
+  if (static_cast<long long>(free_b) - need < cfg_.hbm_reserve_bytes)
+    throw Error(DYNGB200_OUT_OF_MEMORY,
+                "server::add_graph: the graph's workspace (" + std::to_string(need) +
+                    " bytes) does not fit beside the reserve of " +
+                    std::to_string(cfg_.hbm_reserve_bytes) + " bytes (" +
+                    std::to_string(free_b) + " free)");
+  sg->ctx->ws.reserve_vertices(g.n_cap, stream_);
+  DYNGB200_CUDA(cudaStreamSynchronize(stream_));
+  sg->g = &g;
+  sg->t = &t;
+  std::unique_lock<std::mutex> lk(mu_);
+  graphs_.push_back(std::move(sg));
+  return static_cast<int>(graphs_.size()) - 1;
+}
+
+std::unique_ptr<HostBuf<int32_t>> Server::take_buffer(size_t n) {
+  std::unique_lock<std::mutex> lk(mu_);
+  size_t best = pool_.size();
+  for (size_t i = 0; i < pool_.size(); ++i)
+    if (pool_[i]->count >= n && (best == pool_.size() || pool_[i]->count < pool_[best]->count))
+      best = i;
+  if (best < pool_.size()) {
+    auto b = std::move(pool_[best]);
+    pool_.erase(pool_.begin() + static_cast<long>(best));
+    return b;
+  }
+  lk.unlock();
+  auto b = std::make_unique<HostBuf<int32_t>>();
+  size_t cap = 1024;
+  while (cap < n) cap *= 2;
+  b->reserve(cap);
+  return b;
+}
+
+void Server::give_buffer(std::unique_ptr<HostBuf<int32_t>> b) {
+  std::unique_lock<std::mutex> lk(mu_);
+  if (pool_.size() < 64) pool_.push_back(std::move(b));
+}
+
+uint64_t Server::submit(int slot, const dyngb200_batch& b) {
+  {
+    std::unique_lock<std::mutex> lk(mu_);
+    expects(slot >= 0 && slot < static_cast<int>(graphs_.size()),
+            "server::submit: no graph in slot " + std::to_string(slot));
+    expect_batch(*graphs_[slot]->g, b, "server::submit");
+  }
+  auto r = std::make_unique<ServerRequest>();
+  r->slot = slot;
+  r->arrival = Clock::now();
+  const long long ni = b.num_insertions, nd = b.num_deletions;
+  const int k = b.num_weights > 0 ? b.num_weights : 0;
+  const size_t total = static_cast<size_t>(2 * ni + ni * k + 2 * nd);
+  {
+    // backpressure: queued batches hold at most kHeldCap bytes of pinned copies
+    std::unique_lock<std::mutex> lk(mu_);
+    const long long want = static_cast<long long>(total * sizeof(int32_t));
+    done_cv_.wait(lk, [&] { return held_bytes_ == 0 || held_bytes_ + want <= kHeldCap; });
+    held_bytes_ += want;
+  }
+  const long long bytes = static_cast<long long>(total * sizeof(int32_t));
+  uint64_t ticket = 0;
+  try {
+    r->data = take_buffer(total);
+    int32_t* p = r->data->ptr;
+    auto put = [&](const int32_t* src, long long count) {
+      if (count > 0) {
+        if (b.memory == DYNGB200_DEVICE)
+          DYNGB200_CUDA(cudaMemcpy(p, src, count * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        else
+          std::memcpy(p, src, count * sizeof(int32_t));
+      }
+      int32_t* at = p;
+      p += count;
+      return at;
+    };
+    r->batch = b;
+    r->batch.insert_src = put(b.insert_src, ni);
+    r->batch.insert_dst = put(b.insert_dst, ni);
+    r->batch.insert_weights = put(b.insert_weights, ni * k);
+    r->batch.delete_src = put(b.delete_src, nd);
+    r->batch.delete_dst = put(b.delete_dst, nd);
+    r->batch.memory = DYNGB200_HOST;
+    r->ops = ni + nd;
+    std::unique_lock<std::mutex> lk(mu_);
+    expects(!stop_, "server::submit: the server is shutting down");
+    r->ticket = next_ticket_++;
+    ticket = r->ticket;
+    graphs_[slot]->queue.push_back(r.get());
+    requests_.emplace(ticket, std::move(r));
+    ++waiting_;
+    ++info_.submitted;
+  } catch (...) {
+    std::unique_lock<std::mutex> lk(mu_);
+    held_bytes_ -= bytes;
+    if (r && r->data && pool_.size() < 64) pool_.push_back(std::move(r->data));
+    throw;
+  }
+  work_cv_.notify_one();
+  return ticket;
+}
+
+ServerRequest Server::wait(uint64_t ticket) {
+  std::unique_lock<std::mutex> lk(mu_);
+  auto it = requests_.find(ticket);
+  expects(it != requests_.end(), "server::wait: unknown ticket " + std::to_string(ticket));
+  ServerRequest* r = it->second.get();
+  done_cv_.wait(lk, [&] { return r->done; });
+  ServerRequest out;
+  out.ticket = r->ticket;
+  out.slot = r->slot;
+  out.ops = r->ops;
+  out.arrival = r->arrival;
+  out.start = r->start;
+  out.finish = r->finish;
+  out.group_size = r->group_size;
+  out.done = true;
+  out.status = r->status;
+  out.message = r->message;
+  out.stats = r->stats;
+  requests_.erase(it);
+  return out;
+}
+
+void Server::drain() {
+  std::unique_lock<std::mutex> lk(mu_);
+  done_cv_.wait(lk, [&] { return waiting_ == 0 && running_ == 0; });
+}
+
+dyngb200_server_info Server::info() {
+  std::unique_lock<std::mutex> lk(mu_);
+  dyngb200_server_info i = info_;
+  i.waiting = waiting_;
+  return i;
+}
+
+// Scratch a batch may need beyond what its graph holds: staging, the applier's pair tables and
+// row lists, and the slack arenas growing by a batch's worth of appends in both directions.
+long long Server::estimate_bytes(const ServerGraph& sg, const ServerRequest& r) const {
+  const long long dir = sg.g->props.directed ? 1 : 2;
+  const long long k = sg.g->k;
+  return r.ops * (20 + dir * (96 + 2 * (4 + 4 * k) * 3 / 2)) + (1LL << 20);
+}
+
+void Server::run() {
+  cudaSetDevice(cfg_.device);
+  std::vector<ServerRequest*> group;
+  for (;;) {
+    group.clear();
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      work_cv_.wait(lk, [&] { return stop_ || waiting_ > 0; });
+      if (waiting_ == 0 && stop_) return;
+      size_t free_b = 0, total_b = 0;
+      long long free_left = -1;
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+        free_left = static_cast<long long>(free_b) - cfg_.hbm_reserve_bytes;
+      const size_t ng = graphs_.size();
+      for (size_t step = 0; step < ng && static_cast<int>(group.size()) < cfg_.max_group; ++step) {
+        const size_t gi = (next_graph_ + step) % ng;
+        ServerGraph& sg = *graphs_[gi];
+        if (sg.queue.empty()) continue;
+        ServerRequest* r = sg.queue.front();
+        const bool large = r->ops > cfg_.small_changes;
+        if (large && !group.empty()) continue;  // a large batch runs in a round of its own
+        sg.queue.pop_front();
+        --waiting_;
+        r->start = Clock::now();
+        const long long need = estimate_bytes(sg, *r);
+        if (free_left >= 0 && need > free_left) {
+          // admission: the batch's scratch does not fit beside the reserve; fail it, keep the rest
+          r->status = DYNGB200_OUT_OF_MEMORY;
+          r->message = "server: admission refused: the batch needs about " + std::to_string(need) +
+                       " bytes of device memory beyond the reserve, " +
+                       std::to_string(std::max(free_left, 0LL)) + " are free";
+          r->finish = Clock::now();
+          r->done = true;
+          ++info_.failed;
+          held_bytes_ -= held_of(*r);
+          if (pool_.size() < 64) pool_.push_back(std::move(r->data));
+          r->data.reset();
+          continue;
+        }
+        if (free_left >= 0) free_left -= need;
+        group.push_back(r);
+        if (large) break;
+      }
+      next_graph_ = ng ? (next_graph_ + 1) % ng : 0;
+      running_ += static_cast<long long>(group.size());
+    }
+    done_cv_.notify_all();  // admission failures are done
+    if (!group.empty()) dispatch(group);
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      running_ -= static_cast<long long>(group.size());
+      ++info_.rounds;
+      info_.max_group = std::max<long long>(info_.max_group, static_cast<long long>(group.size()));
+    }
+    done_cv_.notify_all();
+  }
+}
+
+// One round: every update of the group queued on the shared stream, then one wait, then each
+// update's results.  Distinct graphs, distinct contexts: no scratch is shared inside a round.
+void Server::dispatch(std::vector<ServerRequest*>& group) {
+  const size_t n = group.size();
+  std::vector<std::unique_ptr<PendingUpdate>> pending(n);
+  std::vector<char> begun(n, 0);
+  for (size_t i = 0; i < n; ++i) {
+    ServerRequest* r = group[i];
+    ServerGraph& sg = *graphs_[r->slot];
+    r->group_size = static_cast<int>(n);
+    try {
+      expect_tree_current(*sg.g, *sg.t, "sssp::update");
+      pending[i] = std::make_unique<PendingUpdate>();
+      sssp_update_begin(*sg.ctx, *sg.g, *sg.t, r->batch, dyngb200_schedule{}, learned_,
+                        *pending[i]);
+      begun[i] = 1;
+    } catch (const Error& e) {
+      r->status = e.status;
+      r->message = e.what();
+    } catch (const std::exception& e) {
+      r->status = DYNGB200_INTERNAL;
+      r->message = e.what();
+    }
+  }
+  cudaStreamSynchronize(stream_);  // errors surface in sssp_update_end
+  for (size_t i = 0; i < n; ++i) {
+    ServerRequest* r = group[i];
+    if (begun[i]) {
+      try {
+        sssp_update_end(*pending[i], &r->stats);
+      } catch (const Error& e) {
+        r->status = e.status;
+        r->message = e.what();
+      } catch (const std::exception& e) {
+        r->status = DYNGB200_INTERNAL;
+        r->message = e.what();
+      }
+    }
+    pending[i].reset();
+    const long long bytes = held_of(*r);
+    give_buffer(std::move(r->data));
+    r->finish = Clock::now();
+    std::unique_lock<std::mutex> lk(mu_);
+    held_bytes_ -= bytes;
+    r->done = true;
+    if (r->status == DYNGB200_OK) ++info_.completed;
+    else ++info_.failed;
+  }
+}
+
+}  // namespace dyngb200
+
+struct dyngb200_server_s {
+  std::unique_ptr<dyngb200::Server> s;
+};
+
+using dyngb200::guarded;
+
+extern "C" {
+
+dyngb200_status dyngb200_server_create(const dyngb200_server_config* config,
+                                       dyngb200_scheduler learned, dyngb200_server* out) {
+  return guarded([&] {
+    dyngb200::expects(config && out, "server_create: null argument");
+    int count = 0;
+    DYNGB200_CUDA(cudaGetDeviceCount(&count));
+    dyngb200::expects(config->device >= 0 && config->device < count,
+                      "server_create: no CUDA device " + std::to_string(config->device),
+                      DYNGB200_NOT_SUPPORTED);
+    auto h = std::make_unique<dyngb200_server_s>();
+    h->s = std::make_unique<dyngb200::Server>(*config, learned ? &learned->s : nullptr);
+    *out = h.release();
+  });
+}
+
+dyngb200_status dyngb200_server_add_graph(dyngb200_server s, dyngb200_graph g, dyngb200_tree t,
+                                          int32_t* slot) {
+  return guarded([&] {
+    dyngb200::expects(s && g && t && slot, "server_add_graph: null argument");
+    *slot = s->s->add_graph(g->g, t->t);
+  });
+}
+
+dyngb200_status dyngb200_server_submit(dyngb200_server s, int32_t slot,
+                                       const dyngb200_batch* batch, uint64_t* ticket) {
+  return guarded([&] {
+    dyngb200::expects(s && batch && ticket, "server_submit: null argument");
+    *ticket = s->s->submit(slot, *batch);
+  });
+}
+
+dyngb200_status dyngb200_server_wait(dyngb200_server s, uint64_t ticket, dyngb200_stats* stats,
+                                     dyngb200_request_times* times) {
+  dyngb200::ServerRequest r;
+  const dyngb200_status st = guarded([&] {
+    dyngb200::expects(s != nullptr, "server_wait: null server");
+    r = s->s->wait(ticket);
+  });
+  if (st != DYNGB200_OK) return st;
+  if (stats) *stats = r.stats;
+  if (times) {
+    times->queued_ms = dyngb200::ms_between(r.arrival, r.start);
+    times->service_ms = dyngb200::ms_between(r.start, r.finish);
+    times->total_ms = dyngb200::ms_between(r.arrival, r.finish);
+    times->group_size = r.group_size;
+  }
+  dyngb200::last_error() = r.message;
+  return r.status;
+}
+
+dyngb200_status dyngb200_server_drain(dyngb200_server s) {
+  return guarded([&] {
+    dyngb200::expects(s != nullptr, "server_drain: null server");
+    s->s->drain();
+  });
+}
+
+dyngb200_status dyngb200_server_info_get(dyngb200_server s, dyngb200_server_info* info) {
+  return guarded([&] {
+    dyngb200::expects(s && info, "server_info: null argument");
+    *info = s->s->info();
+  });
+}
+
+dyngb200_status dyngb200_server_destroy(dyngb200_server s) {
+  return guarded([&] { delete s; });
+}
+
+}  // extern "C"

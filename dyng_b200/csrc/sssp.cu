@@ -1351,72 +1351,109 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
 }
 
 // update(): the applier, then the persistent kernel, then one read-back of the control block.
-void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
-                 const dyngb200_schedule& sched, dyngb200_stats* st, const Scheduler* learned) {
-  const long long launches0 = ctx.launches;
+// The pinned read-back area of a graph: the counters first, then the column statistics.
+constexpr size_t kCounterSlots = (sizeof(GraphCounters) + sizeof(ColumnStats) - 1) / sizeof(ColumnStats);
+
+// One attempt of an update, queued on the context's stream: the applier, the persistent kernel,
+// and the read-back of the control block, counters and column statistics into pinned memory.
+static void enqueue_attempt(PendingUpdate& u) {
+  Context& ctx = *u.ctx;
+  Graph& g = *u.g;
+  Tree& t = *u.t;
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
-  const int objective = t.opt.objective;
-  if (g.host_columns[objective].dirty) graph_rescan_columns(ctx, g);
+  tree_reserve(ctx, t, g.n_cap);
+  DYNGB200_CUDA(cudaEventRecord(u.e0, s));
+  apply_prepare(ctx, g, u.b, t.opt.objective, t.opt.delta, &u.sched, &t, u.learned);
+  apply_commit(ctx, g, u.b);
+  DYNGB200_CUDA(cudaEventRecord(u.e1, s));
+  SsspParams p = base_params(ctx, g, t);
+  p.from_scratch = 0;
+  p.tree_n = t.n;
+  p.tree_bits = t.packed_bits;
+  p.pair_key = ws.pair_key.ptr;
+  p.pair_list = ws.pair_list.ptr;
+  p.pair_flags = ws.pair_flags.ptr;
+  p.pair_first = ws.pair_first.ptr;
+  p.pair_last = ws.pair_last.ptr;
+  p.ins_w = u.b.ins_w;
+  p.k = g.k;
+  p.offer_heads = t.canonical ? 1 : 0;
+  p.tree_trusted = t.trusted ? 1 : 0;
+  p.generation = ws.next_generation(1, s);
+  p.touch_gen = p.generation;
+  p.heavy_degree = 256;
+  launch(ctx, p, u.blocks);
+  DYNGB200_CUDA(cudaEventRecord(u.e2, s));
+  g.pinned.reserve(kCounterSlots + g.host_columns.size());
+  DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
+                                cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(g.pinned.ptr, g.counters.ptr, sizeof(GraphCounters),
+                                cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(g.pinned.ptr + kCounterSlots, g.columns.ptr,
+                                g.host_columns.size() * sizeof(ColumnStats),
+                                cudaMemcpyDeviceToHost, s));
+}
+
+PendingUpdate::~PendingUpdate() {
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (e2) cudaEventDestroy(e2);
+}
+
+// update(), first half: host checks that need no device result, the batch staged on the device
+// and the first attempt queued.  Nothing waits for the GPU here (batches in pinned host memory
+// or device memory), so several updates of different graphs on one stream queue back to back.
+void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
+                       const dyngb200_schedule& sched, const Scheduler* learned,
+                       PendingUpdate& u) {
+  u.ctx = &ctx;
+  u.g = &g;
+  u.t = &t;
+  u.sched = sched;
+  u.learned = learned;
+  u.launches0 = ctx.launches;
+  if (g.host_columns[t.opt.objective].dirty) graph_rescan_columns(ctx, g);
   graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
-  const StagedBatch b = stage_batch(ctx, batch, g.k);
-  const int blocks = persistent_blocks(ctx, sched);
-  cudaEvent_t e0, e1, e2;
-  DYNGB200_CUDA(cudaEventCreate(&e0));
-  DYNGB200_CUDA(cudaEventCreate(&e1));
-  DYNGB200_CUDA(cudaEventCreate(&e2));
+  u.b = stage_batch(ctx, batch, g.k);
+  u.blocks = persistent_blocks(ctx, sched);
+  DYNGB200_CUDA(cudaEventCreate(&u.e0));
+  DYNGB200_CUDA(cudaEventCreate(&u.e1));
+  DYNGB200_CUDA(cudaEventCreate(&u.e2));
+  enqueue_attempt(u);
+}
+
+// update(), second half: waits for the queued attempt, grows and retries on a capacity error
+// (nothing was changed), then the error translation, the commit bookkeeping and the stats.
+void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
+  Context& ctx = *u.ctx;
+  Graph& g = *u.g;
+  Tree& t = *u.t;
+  Workspace& ws = ctx.ws;
+  const Scheduler* learned = u.learned;
+  const dyngb200_schedule& sched = u.sched;
+  const int blocks = u.blocks;
+  const long long launches0 = u.launches0;
   UpdateCtl r{};
   for (int attempt = 0;; ++attempt) {
-    tree_reserve(ctx, t, g.n_cap);
-    DYNGB200_CUDA(cudaEventRecord(e0, s));
-    apply_prepare(ctx, g, b, objective, t.opt.delta, &sched, &t, learned);
-    apply_commit(ctx, g, b);
-    DYNGB200_CUDA(cudaEventRecord(e1, s));
-    SsspParams p = base_params(ctx, g, t);
-    p.from_scratch = 0;
-    p.tree_n = t.n;
-    p.tree_bits = t.packed_bits;
-    p.pair_key = ws.pair_key.ptr;
-    p.pair_list = ws.pair_list.ptr;
-    p.pair_flags = ws.pair_flags.ptr;
-    p.pair_first = ws.pair_first.ptr;
-    p.pair_last = ws.pair_last.ptr;
-    p.ins_w = b.ins_w;
-    p.k = g.k;
-
-    p.offer_heads = t.canonical ? 1 : 0;
-    p.tree_trusted = t.trusted ? 1 : 0;
-    p.generation = ws.next_generation(1, s);
-    p.touch_gen = p.generation;
-    p.heavy_degree = 256;
-    launch(ctx, p, blocks);
-    DYNGB200_CUDA(cudaEventRecord(e2, s));
-    DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
-                                  cudaMemcpyDeviceToHost, s));
-    DYNGB200_CUDA(cudaMemcpyAsync(&g.host_counters, g.counters.ptr, sizeof(GraphCounters),
-                                  cudaMemcpyDeviceToHost, s));
-    DYNGB200_CUDA(cudaMemcpyAsync(g.host_columns.data(), g.columns.ptr,
-                                  g.host_columns.size() * sizeof(ColumnStats),
-                                  cudaMemcpyDeviceToHost, s));
-    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
     r = *ws.host_ctl.ptr;
+    g.host_counters = *reinterpret_cast<const GraphCounters*>(g.pinned.ptr);
+    std::memcpy(g.host_columns.data(), g.pinned.ptr + kCounterSlots,
+                g.host_columns.size() * sizeof(ColumnStats));
     ws.generation = std::max(ws.generation, r.last_generation);
     if ((r.error & kErrCapacity) && attempt < 4) {
       // nothing was changed: grow the vertex capacity or the arenas and run again
-      const long long need_n = std::max<long long>(r.n_after, g.n_cap);
       graph_grow(ctx, g, r.n_after > g.n_cap ? r.n_after : 0,
                  static_cast<long long>(r.top_out), static_cast<long long>(r.top_in));
-      (void)need_n;
+      enqueue_attempt(u);
       continue;
     }
     break;
   }
   float apply_ms = 0, sssp_ms = 0;
-  cudaEventElapsedTime(&apply_ms, e0, e1);
-  cudaEventElapsedTime(&sssp_ms, e1, e2);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(e2);
+  cudaEventElapsedTime(&apply_ms, u.e0, u.e1);
+  cudaEventElapsedTime(&sssp_ms, u.e1, u.e2);
   if (r.error & (kErrInvalidBatch | kErrCapacity)) {
     // found before the commit: the graph and the tree are unchanged
     std::string msg = "sssp::update: invalid batch";
@@ -1491,6 +1528,14 @@ void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
                             ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)
                             : 0.0f;
   }
+}
+
+// update(): sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489).
+void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
+                 const dyngb200_schedule& sched, dyngb200_stats* st, const Scheduler* learned) {
+  PendingUpdate u;
+  sssp_update_begin(ctx, g, t, batch, sched, learned, u);
+  sssp_update_end(u, st);
 }
 
 // Tree arrays sized for the graph's vertex capacity (contents kept).

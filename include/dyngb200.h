@@ -285,6 +285,54 @@ dyngb200_status dyngb200_sssp_update_learned(dyngb200_context ctx, dyngb200_grap
                                              const dyngb200_batch* batch, dyngb200_tree tree,
                                              dyngb200_scheduler scheduler, dyngb200_stats* stats);
 
+/* ---- the serving loop (no reference counterpart) ----------------------------------------------
+ * Several graphs resident on one GPU, each with its shortest-path tree, updated by batches that
+ * arrive at any time from any host thread.  One dispatcher thread runs the updates: the batches
+ * of one graph apply in arrival order (each result equals running the same batches alone, in
+ * order); each round queues the oldest small batch of every waiting graph on one stream and waits
+ * once (continuous batching); a batch larger than small_changes runs in a round of its own.
+ * Admission: a graph is registered only if its workspace fits beside hbm_reserve_bytes of free
+ * device memory, a batch is dispatched only if its scratch estimate fits beyond that reserve
+ * (else its wait returns OUT_OF_MEMORY).  Registered graphs and trees belong to the server until
+ * it is destroyed: do not use them elsewhere meanwhile. */
+typedef struct dyngb200_server_s* dyngb200_server;
+typedef struct dyngb200_server_config {
+  int32_t device;
+  int32_t max_group;         /* updates queued before one wait (0: 8) */
+  int64_t small_changes;     /* batches up to this many changes share a round (0: 65536) */
+  int64_t hbm_reserve_bytes; /* device memory admission keeps free (0: 1 GiB) */
+} dyngb200_server_config;
+typedef struct dyngb200_request_times {
+  double queued_ms;   /* submit -> dispatch */
+  double service_ms;  /* dispatch -> result */
+  double total_ms;    /* submit -> result */
+  int32_t group_size; /* updates in the request's round */
+} dyngb200_request_times;
+typedef struct dyngb200_server_info {
+  int64_t submitted;
+  int64_t completed;
+  int64_t failed;
+  int64_t rounds;
+  int64_t max_group;
+  int64_t waiting;
+} dyngb200_server_info;
+/* learned: a scheduler used for every update (NULL: the fixed heuristic). */
+dyngb200_status dyngb200_server_create(const dyngb200_server_config* config,
+                                       dyngb200_scheduler learned, dyngb200_server* out);
+dyngb200_status dyngb200_server_add_graph(dyngb200_server s, dyngb200_graph g, dyngb200_tree t,
+                                          int32_t* slot);
+/* The batch is copied (its arrays may be reused when the call returns); memory: any space. */
+dyngb200_status dyngb200_server_submit(dyngb200_server s, int32_t slot,
+                                       const dyngb200_batch* batch, uint64_t* ticket);
+/* Blocks until the request is done; returns the update's own status (its message in
+ * dyngb200_last_error_message).  Each ticket is waited for once; stats / times may be NULL. */
+dyngb200_status dyngb200_server_wait(dyngb200_server s, uint64_t ticket, dyngb200_stats* stats,
+                                     dyngb200_request_times* times);
+dyngb200_status dyngb200_server_drain(dyngb200_server s);
+dyngb200_status dyngb200_server_info_get(dyngb200_server s, dyngb200_server_info* info);
+/* Finishes every submitted request, then stops the dispatcher. */
+dyngb200_status dyngb200_server_destroy(dyngb200_server s);
+
 /* ---- snapshots (recording scheduler traces: one batch under many schedules) ---------------- */
 /* A new graph with g's contents (its own identity: trees of g are not bound to it). */
 dyngb200_status dyngb200_graph_clone(dyngb200_context ctx, dyngb200_graph g, dyngb200_graph* out);
