@@ -1600,8 +1600,7 @@ void tree_repack(Context& ctx, Tree& t, int bits) {
 // ------------------------------------------------------------------------------------------------
 // compute() without allocation: the scratch of the persistent kernel in a fixed device array.
 //
-// For callers that must not allocate device memory once they are running: code that issues work
-// while a CUDA graph is being captured (cudaMalloc is not allowed there), serving processes that
+// For callers that must not allocate device memory once they are running: serving processes that
 // reserve their whole device-memory budget at start-up and treat any later allocation as a fault,
 // and host frameworks that own the device allocator and hand this library only the buffers it
 // reads and writes.  The caller passes the graph (already built) and the two output arrays; every

@@ -221,9 +221,9 @@ dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_gr
                                                dyngb200_stats* stats);
 
 /* sssp::compute into caller-owned device arrays, allocating nothing.  No counterpart in the
- * reference.  For callers that cannot allocate device memory while they run: work issued during
- * CUDA graph capture (cudaMalloc is not allowed there), serving processes that reserve their
- * whole memory budget at start-up, and host frameworks that own the device allocator.  The graph
+ * reference.  For callers that cannot allocate device memory while they run: serving processes
+ * that reserve their whole memory budget at start-up and treat any later allocation as a fault,
+ * and host frameworks that own the device allocator.  The graph
  * (on the current device) and the outputs -- distances: int64 x num_vertices, parents: int32 x
  * num_vertices, both device memory -- come from the caller; the kernel's scratch is a fixed
  * device array of about 6 MB inside this library that every GPU which loads it holds until exit, so

@@ -1,8 +1,8 @@
 """The allocation-free compute entry point (dyngb200_sssp_compute_static_scratch).
 
-It exists for callers that must not allocate device memory while they run -- work issued
-during CUDA graph capture, serving processes that fix their memory budget at start-up, host
-frameworks that own the allocator -- so its scratch is a fixed device array inside the library.
+It exists for callers that must not allocate device memory while they run -- serving processes
+that fix their memory budget at start-up, host frameworks that own the allocator -- so its
+scratch is a fixed device array inside the library.
 This file checks, through the C ABI, that two calls in a row give the same distances and parents
 as the regular entry point (dyngb200_sssp_compute), and that graphs beyond the array's limit
 are refused.  It is collected last so that a failure here leaves every other test already run.
