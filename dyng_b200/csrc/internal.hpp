@@ -147,7 +147,7 @@ struct UpdateCtl {
   long long loop_pushes;
   u64 loop_threshold;
   // work counters (algorithmic traffic) and phase timestamps of the sssp kernel
-  long long work[12];
+  long long work[16];
   unsigned long long phase_ns[8];
   // trace of the first 64 push iterations / epochs: (light count, heavy chunks, ns since start)
   int trace_n[64];

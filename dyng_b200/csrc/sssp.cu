@@ -261,6 +261,7 @@ struct Ctx {
   int* far;
   int* far_cnt;
   unsigned slots, words, atomics, appends, rows;
+  unsigned tries;  // atomicMin attempts on packed words (successful or not)
 };
 
 // One slot of a row.  push: owner u relaxes (u -> y); pull: in-neighbour y offers to the owner;
@@ -300,6 +301,7 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
   const u64 cand = X.pk.pack(nd, src);
   if (MODE == kPush) ++X.words;
   if (cand >= ld_cg(&p.packed[dst])) return;
+  ++X.tries;
   const u64 old = atomicMin(&p.packed[dst], cand);
   if (cand < old) {
     ++X.atomics;
@@ -339,6 +341,7 @@ __device__ __forceinline__ u64 pull_candidate(const SsspParams& p, Ctx& X, int y
 // joins the frontier of the near-far loop.
 __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int owner, u64 cand) {
   if (cand >= ld_cg(&p.packed[owner])) return;
+  ++X.tries;
   const u64 old = atomicMin(&p.packed[owner], cand);
   if (cand < old) {
     ++X.atomics;
@@ -376,6 +379,7 @@ __device__ __forceinline__ void push_prepare(const SsspParams& p, Ctx& X, int u,
 __device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const Offer& r) {
   if (r.cand >= r.cur) return;  // also skips "no offer" (cand == INF)
   const int dst = r.dst;
+  ++X.tries;
   const u64 old = atomicMin(&p.packed[dst], r.cand);
   if (r.cand < old) {
     ++X.atomics;
@@ -792,7 +796,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   X.pk.no_parent = X.pk.bits ? (1ULL << X.pk.bits) - 1 : 0;
   X.maxd = c->max_distance;
   X.threshold = 0;
-  X.slots = X.words = X.atomics = X.appends = X.rows = 0;
+  X.slots = X.words = X.atomics = X.appends = X.rows = X.tries = 0;
   const Packing pk = X.pk;
   const u64 delta = static_cast<u64>(p.delta_override > 0 ? p.delta_override : c->delta);
   int gen = p.generation;
@@ -1010,13 +1014,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
       Y.gen = gen_pull;
       Y.next = ListSet{p.frontier, &c->frontier_count, nullptr, nullptr, nullptr, nullptr, kStNext,
                        kStNextMed};
-      Y.slots = Y.words = Y.atomics = Y.appends = Y.rows = 0;
+      Y.slots = Y.words = Y.atomics = Y.appends = Y.rows = Y.tries = 0;
       expand<kPull>(p, Y, p.candidates, ld_cg(&c->cand_count), p.cand_med,
                     ld_cg(&c->cand_med_count), p.pull_heavy, ld_cg(&c->pull_heavy), gwarp, nwarps);
       pull_slots = Y.slots;
       pull_words = Y.words;
       pull_rows = Y.rows;
       X.atomics += Y.atomics;
+      X.tries += Y.tries;
     }
     if (!grid_barrier(c, bar)) return;
     frontier_count = ld_cg(&c->frontier_count);
@@ -1158,6 +1163,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
   warp_sum_into_ll(static_cast<long long>(X.slots), &c->work[7]);
   warp_sum_into_ll(static_cast<long long>(X.words), &c->work[8]);
   warp_sum_into_ll(static_cast<long long>(X.atomics), &c->work[9]);
+  warp_sum_into_ll(static_cast<long long>(X.tries), &c->work[12]);
   warp_sum_into_ll(static_cast<long long>(X.appends), &c->work[10]);
   warp_sum_into_ll(static_cast<long long>(unpacked), &c->work[11]);
   if (tid == 0) {
@@ -1512,7 +1518,7 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
     st->sssp_ms = sssp_ms;
     st->rounds = r.rounds;
     st->touched = r.touched_count;
-    for (int i = 0; i < 12; ++i) st->work[i] = r.work[i];
+    for (int i = 0; i < 16; ++i) st->work[i] = r.work[i];
     st->trace_len = r.trace_len;
     for (int i = 0; i < r.trace_len && i < 64; ++i) {
       st->trace_light[i] = r.trace_n[i];

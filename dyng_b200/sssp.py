@@ -84,9 +84,10 @@ class Stats:
 
     WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
                   "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
-                  "unpacked")
-    # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows):
-    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32)
+                  "unpacked", "atomic_attempts")
+    # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows);
+    # attempted atomics are a diagnostic, their bytes are in "atomics" (the successful ones):
+    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32, 0)
     PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
 
     @property

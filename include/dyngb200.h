@@ -115,8 +115,9 @@ typedef struct dyngb200_stats {
   /* Work of the sssp kernel, for its algorithmic traffic: [0] vertex visits of the pointer-jumping
    * rounds, [1] jumps, [2] invalidated, [3] pull candidates, [4] pulled in-slots, [5] word reads of
    * the pull, [6] pushed vertices, [7] scanned out-slots, [8] target word reads, [9] successful
-   * atomicMin, [10] frontier appends, [11] unpacked vertices. */
-  int64_t work[12];
+   * atomicMin, [10] frontier appends, [11] unpacked vertices, [12] atomicMin attempts (successful
+   * or not); [13..15] zero. */
+  int64_t work[16];
   /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
    * first split, near-far loop, unpack. */
   float phase_ms[7];
