@@ -121,6 +121,16 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def traffic(args):
+    """DRAM bytes per k_sssp launch from the committed ncu capture of this workload (None when
+    the workload differs from the captured one)."""
+    path = os.path.join(ROOT, "profiles", "k_sssp_dram_rmat-s22_batch100k.json")
+    if not os.path.exists(path) or (args.scale, args.batch) != (22, 100_000):
+        return None
+    with open(path) as f:
+        return int(json.load(f)["dram_bytes_per_launch"])
+
+
 def make_workload(args, device):
     from dyng_b200 import generators as G
     t0 = time.time()
@@ -424,7 +434,7 @@ def main():
                     "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
             "gpu_launches": int(sum(s.kernel_launches for s in timed_stats)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "frac": achieved / peak if peak else None, "traffic": traffic(args),
                          "peak_kind": peak_kind, "kernel": "k_sssp"},
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -78,7 +78,8 @@ class ServerConfig(ctypes.Structure):
 
 class RequestTimes(ctypes.Structure):
     _fields_ = [("queued_ms", ctypes.c_double), ("service_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double), ("group_size", ctypes.c_int32)]
+                ("total_ms", ctypes.c_double), ("group_size", ctypes.c_int32),
+                ("begin_ms", ctypes.c_double), ("round_ms", ctypes.c_double)]
 
 
 class ServerInfo(ctypes.Structure):

@@ -40,7 +40,7 @@ struct ServerRequest {
   std::unique_ptr<HostBuf<int32_t>> data;  // pinned copy of the batch's five arrays
   dyngb200_batch batch{};
   long long ops = 0;
-  Clock::time_point arrival, start, finish;
+  Clock::time_point arrival, start, begun, synced, finish;
   int group_size = 0;
   bool done = false;
   dyngb200_status status = DYNGB200_OK;
@@ -251,6 +251,8 @@ ServerRequest Server::wait(uint64_t ticket) {
   out.ops = r->ops;
   out.arrival = r->arrival;
   out.start = r->start;
+  out.begun = r->begun;
+  out.synced = r->synced;
   out.finish = r->finish;
   out.group_size = r->group_size;
   out.done = true;
@@ -355,6 +357,7 @@ void Server::dispatch(std::vector<ServerRequest*>& group) {
       sssp_update_begin(*sg.ctx, *sg.g, *sg.t, r->batch, dyngb200_schedule{}, learned_,
                         *pending[i]);
       begun[i] = 1;
+      r->begun = Clock::now();
     } catch (const Error& e) {
       r->status = e.status;
       r->message = e.what();
@@ -364,8 +367,11 @@ void Server::dispatch(std::vector<ServerRequest*>& group) {
     }
   }
   cudaStreamSynchronize(stream_);  // errors surface in sssp_update_end
+  const Clock::time_point synced = Clock::now();
   for (size_t i = 0; i < n; ++i) {
     ServerRequest* r = group[i];
+    r->synced = synced;
+    if (!begun[i]) r->begun = r->start;
     if (begun[i]) {
       try {
         sssp_update_end(*pending[i], &r->stats);
@@ -444,6 +450,9 @@ dyngb200_status dyngb200_server_wait(dyngb200_server s, uint64_t ticket, dyngb20
     times->service_ms = dyngb200::ms_between(r.start, r.finish);
     times->total_ms = dyngb200::ms_between(r.arrival, r.finish);
     times->group_size = r.group_size;
+    const bool ran = r.synced.time_since_epoch().count() != 0;
+    times->begin_ms = ran ? dyngb200::ms_between(r.start, r.begun) : 0.0;
+    times->round_ms = ran ? dyngb200::ms_between(r.start, r.synced) : 0.0;
   }
   dyngb200::last_error() = r.message;
   return r.status;

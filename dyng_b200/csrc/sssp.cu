@@ -769,7 +769,7 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 2) k_sssp(SsspParams p) {
+__global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
   UpdateCtl* c = p.ctl;
   if (ld_volatile(&c->error) != 0) return;
   // The schedule lives in the control block (written by the host, or by the scheduler's

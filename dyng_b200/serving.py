@@ -60,7 +60,8 @@ class Server:
         check(N.lib().dyngb200_server_wait(self._h, int(ticket), ctypes.byref(st),
                                            ctypes.byref(tm)))
         return Stats._from_native(st), {"queued_ms": tm.queued_ms, "service_ms": tm.service_ms,
-                                        "total_ms": tm.total_ms, "group_size": tm.group_size}
+                                        "total_ms": tm.total_ms, "group_size": tm.group_size,
+                                        "begin_ms": tm.begin_ms, "round_ms": tm.round_ms}
 
     def drain(self) -> None:
         check(N.lib().dyngb200_server_drain(self._h))
@@ -129,7 +130,8 @@ def run_load(server, slots, pools, rate, seconds, rng, size_range=(100, 1_000_00
     def collect():
         for i, tk in enumerate(iter(tickets_q.get, None)):
             st, tm = server.wait(tk[0])
-            done.append((tk[1], tk[2], tm["total_ms"], tm["queued_ms"], tm["group_size"]))
+            done.append((tk[1], tk[2], tm["total_ms"], tm["queued_ms"], tm["group_size"],
+                         tm["service_ms"], tm["begin_ms"], tm["round_ms"]))
 
     import queue
     tickets_q = queue.Queue()
@@ -158,7 +160,13 @@ def summarize(done, wall, rate):
             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
             "p99_over_p50": float(np.percentile(lat, 99) / max(np.percentile(lat, 50), 1e-9)),
             "changed_edges_per_s": changes / wall,
-            "mean_group": float(np.mean([d[4] for d in done]))}
+            "mean_group": float(np.mean([d[4] for d in done])),
+            "parts_p50_ms": {k: float(np.percentile([d[i] for d in done], 50))
+                             for k, i in (("queued", 3), ("service", 5), ("begin", 6),
+                                          ("round", 7))},
+            "parts_p99_ms": {k: float(np.percentile([d[i] for d in done], 99))
+                             for k, i in (("queued", 3), ("service", 5), ("begin", 6),
+                                          ("round", 7))}}
 
 
 def main(argv=None):
@@ -190,6 +198,12 @@ def main(argv=None):
         pools.append(_Pool(edges, rng))
         keep.append((g, t))
         print(f"graph {i}: scale {sc}, {edges.src.size} edges", flush=True)
+    # warm-up (not measured): every graph sees the largest batch size twice, so workspaces,
+    # pair tables, pinned copies and the edge indexes have grown before the timed loads
+    for _ in range(2):
+        tickets = [server.submit(sl, pools[i].batch(rng, a.max_batch)) for i, sl in enumerate(slots)]
+        for tk in tickets:
+            server.wait(tk)
     for rate in (float(r) for r in a.rates.split(",")):
         done, wall = run_load(server, slots, pools, rate, a.seconds, rng, (100, a.max_batch))
         out = summarize(done, wall, rate)

@@ -308,6 +308,8 @@ typedef struct dyngb200_request_times {
   double service_ms;  /* dispatch -> result */
   double total_ms;    /* submit -> result */
   int32_t group_size; /* updates in the request's round */
+  double begin_ms;    /* host time queuing this update's work (staging, launches) */
+  double round_ms;    /* dispatch -> the round's work complete on the GPU */
 } dyngb200_request_times;
 typedef struct dyngb200_server_info {
   int64_t submitted;
