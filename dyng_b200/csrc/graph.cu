@@ -198,6 +198,26 @@ __global__ void k_validate(ApplyParams p) {
   warp_add(dropped, &c->summary[5]);
 }
 
+// ---- the per-batch reset: an empty pair table and zero column deltas ---------------------------
+__global__ void k_clear_tables(u64* key, int* d, int* t, int* first, int* last, long long cap,
+                               long long* sum_delta, long long* removed_at_max,
+                               long long* written_max, long long* written_at_max, int k) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < cap;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    key[i] = ~0ULL;
+    d[i] = 0;
+    t[i] = 0;
+    first[i] = 0x7f7f7f7f;
+    last[i] = -1;
+    if (i < k) {
+      sum_delta[i] = 0;
+      removed_at_max[i] = 0;
+      written_max[i] = 0;
+      written_at_max[i] = 0;
+    }
+  }
+}
+
 // ---- B: the plan (one thread): capacity, packing bound, near-far width ------------------------
 __global__ void k_plan(ApplyParams p) {
   UpdateCtl* c = p.ctl;
@@ -515,36 +535,73 @@ __global__ void k_resolve(ApplyParams p) {
   for (int f = 0; f < 5; ++f) warp_add(acc[f], &c->summary[f]);
 }
 
+// Warp-wide reservation on a shared counter: every lane asks for `amount` (0: none), one atomic
+// for the warp, each lane gets the start of its own range.  All 32 lanes must call.
+__device__ __forceinline__ u64 warp_reserve(u64 amount, u64* counter) {
+  const int lane = threadIdx.x & 31;
+  u64 incl = amount;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u64 t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const u64 total = __shfl_sync(0xffffffffu, incl, 31);
+  u64 base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(counter, total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + incl - amount;
+}
+
 // ---- F: per touched row: stay in place or move to the top of the arena -------------------------
+// A row that overflows its slack (or is mostly tombstones) gets a new place at the arena top.  The warps iterate together so that the arena
+// space of a warp's relocated rows is reserved with one atomic per side.
 __global__ void k_alloc(ApplyParams p) {
   UpdateCtl* c = p.ctl;
   if (c->error) return;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
+  const int total = rows_out + rows_in;
   const double headroom = p.props.headroom;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows_out + rows_in;
-       i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < total; i0 += stride) {
+    const int i = i0 + lane;
+    const bool active = i < total;
     const int side = i < rows_out ? 0 : 1;
     const int s = side == 0 ? i : i - rows_out;
-    const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
-    const bool existing = r < c->n_old;
-    const RowDesc desc = existing ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r] : RowDesc{0, 0};
-    const int cap = existing ? (side == 0 ? p.g.out_cap : p.g.in_cap)[r] : 0;
-    const int dead = existing ? (side == 0 ? p.g.out_dead : p.g.in_dead)[r] : 0;
-    const int dels = (side == 0 ? p.dels_out : p.dels_in)[s];
-    const int apps = (side == 0 ? p.apps_out : p.apps_in)[s];
-    const int live = desc.len - dead - dels;
-    const int tomb = dead + dels;
-    const bool compact = tomb > 8 && tomb * 4 > desc.len;
-    int reloc = 0;
-    unsigned start = desc.start;
-    int new_cap = cap;
-    if (desc.len + apps > cap || compact) {
-      reloc = 1;
-      const long long want = static_cast<long long>(live) + apps;
-      long long extra = static_cast<long long>(ceil(static_cast<double>(want) * headroom));
-      if (extra < 4) extra = 4;
-      new_cap = static_cast<int>((want + extra + 3) & ~3LL);
-      const u64 at = atomicAdd(side == 0 ? &c->top_out : &c->top_in, static_cast<u64>(new_cap));
+    int reloc = 0, new_cap = 0, live = 0;
+    unsigned start = 0;
+    if (active) {
+      const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
+      const bool existing = r < c->n_old;
+      const RowDesc desc = existing ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r] : RowDesc{0, 0};
+      const int cap = existing ? (side == 0 ? p.g.out_cap : p.g.in_cap)[r] : 0;
+      const int dead = existing ? (side == 0 ? p.g.out_dead : p.g.in_dead)[r] : 0;
+      const int dels = (side == 0 ? p.dels_out : p.dels_in)[s];
+      const int apps = (side == 0 ? p.apps_out : p.apps_in)[s];
+      live = desc.len - dead - dels;
+      const int tomb = dead + dels;
+      const bool compact = tomb > 8 && tomb * 4 > desc.len;
+      start = desc.start;
+      new_cap = cap;
+      if (desc.len + apps > cap || compact) {
+        reloc = 1;
+        const long long want = static_cast<long long>(live) + apps;
+        long long extra = static_cast<long long>(ceil(static_cast<double>(want) * headroom));
+        if (extra < 4) extra = 4;
+        new_cap = static_cast<int>((want + extra + 3) & ~3LL);
+      }
+    }
+    const u64 at_out = warp_reserve(reloc && side == 0 ? static_cast<u64>(new_cap) : 0, &c->top_out);
+    const u64 at_in = warp_reserve(reloc && side == 1 ? static_cast<u64>(new_cap) : 0, &c->top_in);
+    const unsigned n_out = __popc(__ballot_sync(0xffffffffu, reloc && side == 0));
+    const unsigned n_in = __popc(__ballot_sync(0xffffffffu, reloc && side == 1));
+    if (lane == 0) {
+      if (n_out) atomicAdd(&c->relocated_out, static_cast<int>(n_out));
+      if (n_in) atomicAdd(&c->relocated_in, static_cast<int>(n_in));
+    }
+    if (!active) continue;
+    if (reloc) {
+      const u64 at = side == 0 ? at_out : at_in;
       if (at + new_cap > static_cast<u64>(p.g.arena_cap) || at + new_cap > 0xffffffffULL) {
         set_error(&c->error, kErrCapacity);
       }
@@ -554,7 +611,6 @@ __global__ void k_alloc(ApplyParams p) {
     (side == 0 ? p.new_start_out : p.new_start_in)[s] = start;
     (side == 0 ? p.new_cap_out : p.new_cap_in)[s] = new_cap;
     (side == 0 ? p.live_out : p.live_in)[s] = live;
-    if (reloc) append_slot(side == 0 ? &c->relocated_out : &c->relocated_in);
   }
 }
 
@@ -1085,7 +1141,7 @@ ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int object
   p.props = g.props;
   p.delta_opt = delta_opt;
   p.key = ws.pair_key.ptr;
-  p.mask = static_cast<int>(ws.pairs_sized - 1);
+  p.mask = static_cast<int>(ws.pairs_active - 1);
   p.d = ws.pair_d.ptr;
   p.t = ws.pair_t.ptr;
   p.first = ws.pair_first.ptr;
@@ -1185,6 +1241,7 @@ void Workspace::reserve_batch(long long ops, int k, cudaStream_t s) {
     row_new_start_in.reserve(c, s);
     pairs_sized = cap;
   }
+  pairs_active = cap;
   const size_t inc = static_cast<size_t>(pairs_sized) * static_cast<size_t>(k > 0 ? k : 1);
   pair_inc.reserve(inc, s);
   for (DevBuf<long long>* b : {&col_ins_max, &col_sum_delta, &col_removed_at_max,
@@ -1651,16 +1708,12 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
   ws.reserve_batch(ops, g.k, s);
   const int touch_gen = ws.next_touch_generation(s);
   const size_t cap = static_cast<size_t>(ws.pairs_sized);
-  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_key.ptr, 0xff, cap * sizeof(u64), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_d.ptr, 0, cap * sizeof(int), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_t.ptr, 0, cap * sizeof(int), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_first.ptr, 0x7f, cap * sizeof(int), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.pair_last.ptr, 0xff, cap * sizeof(int), s));
-  const size_t kk = static_cast<size_t>(g.k > 0 ? g.k : 1);
-  DYNGB200_CUDA(cudaMemsetAsync(ws.col_sum_delta.ptr, 0, kk * sizeof(long long), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.col_removed_at_max.ptr, 0, kk * sizeof(long long), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.col_written_max.ptr, 0, kk * sizeof(long long), s));
-  DYNGB200_CUDA(cudaMemsetAsync(ws.col_written_at_max.ptr, 0, kk * sizeof(long long), s));
+  // the pair table of this batch (pairs_active entries) and the column deltas, in one launch
+  k_clear_tables<<<grid_for(ws.pairs_active, kBlock, ctx.sm_count), kBlock, 0, s>>>(
+      ws.pair_key.ptr, ws.pair_d.ptr, ws.pair_t.ptr, ws.pair_first.ptr, ws.pair_last.ptr,
+      ws.pairs_active, ws.col_sum_delta.ptr, ws.col_removed_at_max.ptr, ws.col_written_max.ptr,
+      ws.col_written_at_max.ptr, g.k > 0 ? g.k : 1);
+  ++ctx.launches;
   UpdateCtl init{};
   init.err_index = INT64_MAX;
   init.n_old = g.n;

@@ -154,9 +154,11 @@ struct UpdateCtl {
   int trace_h[64];
   unsigned trace_t[64];
   int trace_len;
-  // grid barrier
+  // grid barrier: blocks arrive on one of kBarGroups group counters, the last of each group on
+  // bar_count, the last group flips bar_gen
   unsigned bar_count;
   unsigned bar_gen;
+  unsigned bar_group[32];
 };
 
 // Scratch memory of a context, sized on demand and reused (the reference's workspace pool).
@@ -186,6 +188,7 @@ struct Workspace {
   int touch_generation = 0;  // row-touch generations (applier)
   long long n_sized = 0;
   long long pairs_sized = 0;
+  long long pairs_active = 0;  // pair-table size of the current batch (<= pairs_sized)
 
   void reserve_vertices(long long n_cap, cudaStream_t s);
   void reserve_batch(long long ops, int k, cudaStream_t s);

@@ -26,6 +26,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kHeavyChunk = 256;
 constexpr unsigned long long kBarrierTimeoutNs = 5ULL * 1000 * 1000 * 1000;
+constexpr unsigned kBarGroups = 32;  // arrival groups of the grid barrier (UpdateCtl::bar_group)
 
 struct SsspParams {
   GraphView g;
@@ -158,9 +159,20 @@ __device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
   if (threadIdx.x == 0) {
     const unsigned target = gen + 1;
     __threadfence();
-    const unsigned arrived = atomicAdd(&c->bar_count, 1u) + 1u;
+    // two-level arrival: about nblk / 32 atomics on each group counter and one per group on the
+    // root, instead of nblk atomics in a row on one address
+    const unsigned nblk = static_cast<unsigned>(g_nblk);
+    const unsigned groups = nblk < kBarGroups ? nblk : kBarGroups;
+    const unsigned grp = blockIdx.x % groups;
+    const unsigned members = nblk / groups + (grp < nblk % groups ? 1u : 0u);
+    bool last = false;
+    if (atomicAdd(&c->bar_group[grp], 1u) + 1u == members) {
+      atomicExch(&c->bar_group[grp], 0u);
+      __threadfence();
+      last = atomicAdd(&c->bar_count, 1u) + 1u == groups;
+    }
     int ok = 1;
-    if (arrived == static_cast<unsigned>(g_nblk)) {
+    if (last) {
       atomicExch(&c->bar_count, 0u);
       __threadfence();
       atomicExch(&c->bar_gen, target);
@@ -724,8 +736,19 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
         c->near_med_cnt[(S.it + 2) % 3] = 0;
         c->heavy_cnt[(S.it + 2) % 3] = 0;
       }
+      const unsigned long long t_busy = (!BLOCK && step == 0) ? global_ns() : 0;
       expand<kPush>(p, X, lists[S.it & 1], nc, mlists[S.it & 1], mc, hlists[S.it & 1], hc, gwarp,
                     nwarps);
+      if (!BLOCK && step == 0) {
+        // balance of the first step: the slowest warp's and the summed busy time, and warps
+        const long long busy = static_cast<long long>(global_ns() - t_busy);
+        if ((threadIdx.x & 31) == 0) {
+          atomicMax(&c->work[13], busy);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&c->work[14]),
+                    static_cast<unsigned long long>(busy));
+          atomicAdd(reinterpret_cast<unsigned long long*>(&c->work[15]), 1ULL);
+        }
+      }
       if (BLOCK) block_barrier();
       else if (!grid_barrier(c, bar)) return -1;
       ++S.it;
@@ -881,19 +904,39 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
       while ((1LL << max_rounds) < n) ++max_rounds;
       ++max_rounds;
       if (any_changed) {
+        // Round 0 visits every vertex of the block's own range; a vertex whose new ancestor is
+        // still a vertex (it jumps again) goes to the block's survivor list, and later rounds
+        // visit only those lists (near_a / near_b, one region of `span` entries per block: a
+        // block's survivors never exceed the vertices it visited).  No global atomics.
+        __shared__ int s_pj_cnt;
+        const long long span = (n + nblk - 1) / nblk;
+        const long long lo = static_cast<long long>(blockIdx.x) * span;
+        const long long hi = min(n, lo + span);
+        int cur_cnt = 0;
         for (int round = 0; round < max_rounds; ++round) {
           if (tid == 0) {
             c->active[(round + 1) % 3] = 0;
             c->rounds = round + 1;
           }
+          if (threadIdx.x == 0) s_pj_cnt = 0;
+          __syncthreads();
+          const int* cur = (round & 1) ? p.near_a + lo : p.near_b + lo;
+          int* next = (round & 1) ? p.near_b + lo : p.near_a + lo;
+          const long long count = round == 0 ? hi - lo : cur_cnt;
           int jumping = 0;
-          // four vertices per thread and step, their loads issued together
-          for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
-            int a[4], na[4];
+          // four entries per thread and step, their loads issued together; the warps iterate
+          // together (the bound is tested on the warp's first entry) for the ballots below
+          for (long long i0 = threadIdx.x & ~31; i0 < count; i0 += 4LL * blockDim.x) {
+            int vv[4], a[4], na[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-              const long long v = v0 + q * threads;
-              if (v >= n) {
+              const long long i = i0 + lane + q * blockDim.x;
+              vv[q] = i < count ? (round == 0 ? static_cast<int>(lo + i) : cur[i]) : -1;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int v = vv[q];
+              if (v < 0) {
                 a[q] = -1;
               } else if (round == 0) {
                 a[q] = ld_cg(&p.stamp[v]) == gen_inv ? kMarked : (v < p.tree_n ? p.parent[v] : -1);
@@ -913,25 +956,38 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-              const long long v = v0 + q * threads;
-              if (v >= n) continue;
-              ++w_visits;
-              if (a[q] < 0) {
-                if (round == 0) p.ancestor[v] = a[q];
-                continue;
+              const int v = vv[q];
+              bool survives = false;
+              if (v >= 0) {
+                ++w_visits;
+                if (a[q] < 0) {
+                  if (round == 0) p.ancestor[v] = a[q];
+                } else {
+                  ++w_jumps;
+                  if (na[q] == kMarked) {
+                    p.ancestor[v] = kMarked;
+                    p.stamp[v] = gen_inv;
+                    invalidate(p, v);
+                    ++w_inval;
+                  } else {
+                    p.ancestor[v] = na[q];
+                    survives = na[q] >= 0;
+                  }
+                }
               }
-              ++w_jumps;
-              if (na[q] == kMarked) {
-                p.ancestor[v] = kMarked;
-                p.stamp[v] = gen_inv;
-                invalidate(p, static_cast<int>(v));
-                ++w_inval;
-                continue;
+              // warp-aggregated append to the block's survivor list
+              const unsigned m = __ballot_sync(0xffffffffu, survives);
+              if (m) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&s_pj_cnt, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (survives) next[base + __popc(m & ((1u << lane) - 1))] = v;
+                jumping = 1;
               }
-              p.ancestor[v] = na[q];
-              jumping |= na[q] >= 0 ? 1 : 0;
             }
           }
+          __syncthreads();
+          cur_cnt = s_pj_cnt;
           if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
           if (!grid_barrier(c, bar)) return;
           if (ld_cg(&c->active[round % 3]) == 0) break;
@@ -1353,6 +1409,8 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
                                                                              : blocks;
     st->sssp_ms = ms;
     st->kernel_launches = ctx.launches - launches0;
+    st->affected = r.affected;
+    for (int i = 0; i < 16; ++i) st->work[i] = r.work[i];
   }
 }
 

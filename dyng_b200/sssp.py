@@ -55,57 +55,90 @@ class Schedule:
                           int(bool(self.record_features)))
 
 
-@dataclass(frozen=True)
 class Stats:
-    """sssp::stats (sssp.hpp:100-117) plus the schedule that ran and the device times."""
+    """sssp::stats (sssp.hpp:100-117) plus the schedule that ran and the device times.
 
-    batch: ApplySummary = field(default_factory=ApplySummary)
-    invalidated: int = 0
-    affected: int = 0
-    iterations: int = 0
-    epochs: int = 0
-    pushes: int = 0
-    packed_parents: bool = True
-    engine_used: str = "fused"
-    delta: int = 0
-    max_weight: int = 0
-    grid_blocks: int = 0
-    invalidation: int = 0
-    apply_ms: float = 0.0
-    sssp_ms: float = 0.0
-    rounds: int = 0
-    touched: int = 0
-    work: tuple = ()
-    phase_ms: tuple = ()
-    trace: tuple = ()  # (light, heavy chunks, start us) per near-far step; light < 0: an epoch
-    features: tuple = ()  # the learned scheduler's 12 features (when a scheduler or recording ran)
-    schedule_classes: tuple = (-1, -1, -1)  # the classes the learned scheduler picked
-    kernel_launches: int = 0  # kernels of the library the call launched
+    A view of the native stats record: fields are converted when first read, so an update pays
+    no Python conversion for the fields its caller never looks at."""
 
     WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
                   "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
-                  "unpacked", "atomic_attempts")
+                  "unpacked", "atomic_attempts", "step0_max_warp_ns", "step0_sum_warp_ns",
+                  "step0_warps")
     # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows);
     # attempted atomics are a diagnostic, their bytes are in "atomics" (the successful ones):
-    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32, 0)
+    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32, 0, 0, 0, 0)
     PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
+    _SCALARS = ("invalidated", "affected", "iterations", "epochs", "pushes", "delta",
+                "max_weight", "grid_blocks", "invalidation", "rounds", "touched",
+                "kernel_launches")
+
+    __slots__ = ("_s",)
+
+    def __init__(self, native: N.Stats | None = None):
+        self._s = native if native is not None else N.Stats()
+
+    @classmethod
+    def _from_native(cls, s: N.Stats) -> "Stats":
+        return cls(s)
+
+    def __getattr__(self, name):
+        if name in Stats._SCALARS:
+            return int(getattr(self._s, name))
+        raise AttributeError(name)
+
+    @property
+    def batch(self) -> ApplySummary:
+        return ApplySummary._from_native(self._s.batch)
+
+    @property
+    def packed_parents(self) -> bool:
+        return bool(self._s.packed_parents)
+
+    @property
+    def engine_used(self) -> str:
+        engines = {v: k for k, v in _ENGINES.items()}
+        return engines.get(self._s.engine_used, "fused")
+
+    @property
+    def apply_ms(self) -> float:
+        return float(self._s.apply_ms)
+
+    @property
+    def sssp_ms(self) -> float:
+        return float(self._s.sssp_ms)
+
+    @property
+    def work(self) -> tuple:
+        return tuple(int(x) for x in self._s.work)
+
+    @property
+    def phase_ms(self) -> tuple:
+        return tuple(float(x) for x in self._s.phase_ms)
+
+    @property
+    def trace(self) -> tuple:
+        """(light, heavy chunks, start us) per near-far step; light < 0: an epoch."""
+        s = self._s
+        return tuple((int(s.trace_light[i]), int(s.trace_heavy[i]), float(s.trace_us[i]))
+                     for i in range(min(int(s.trace_len), 64)))
+
+    @property
+    def features(self) -> tuple:
+        return tuple(float(x) for x in self._s.features)
+
+    @property
+    def schedule_classes(self) -> tuple:
+        return tuple(int(x) for x in self._s.schedule_classes)
 
     @property
     def algorithmic_bytes(self) -> int:
         return int(sum(a * b for a, b in zip(self.work, self.WORK_BYTES)))
 
-    @classmethod
-    def _from_native(cls, s: N.Stats) -> "Stats":
-        engines = {v: k for k, v in _ENGINES.items()}
-        return cls(ApplySummary._from_native(s.batch), s.invalidated, s.affected, s.iterations,
-                   s.epochs, s.pushes, bool(s.packed_parents), engines.get(s.engine_used, "fused"),
-                   s.delta, s.max_weight, s.grid_blocks, s.invalidation, float(s.apply_ms),
-                   float(s.sssp_ms), s.rounds, s.touched, tuple(int(x) for x in s.work),
-                   tuple(float(x) for x in s.phase_ms),
-                   tuple((int(s.trace_light[i]), int(s.trace_heavy[i]), float(s.trace_us[i]))
-                         for i in range(min(int(s.trace_len), 64))),
-                   tuple(float(x) for x in s.features),
-                   tuple(int(x) for x in s.schedule_classes), int(s.kernel_launches))
+    def __repr__(self):
+        return (f"Stats(invalidated={self.invalidated}, affected={self.affected}, "
+                f"iterations={self.iterations}, epochs={self.epochs}, delta={self.delta}, "
+                f"apply_ms={self.apply_ms:.3f}, sssp_ms={self.sssp_ms:.3f})")
 
 
 class Result:

@@ -116,7 +116,8 @@ typedef struct dyngb200_stats {
    * rounds, [1] jumps, [2] invalidated, [3] pull candidates, [4] pulled in-slots, [5] word reads of
    * the pull, [6] pushed vertices, [7] scanned out-slots, [8] target word reads, [9] successful
    * atomicMin, [10] frontier appends, [11] unpacked vertices, [12] atomicMin attempts (successful
-   * or not); [13..15] zero. */
+   * or not); the first near-far step's balance: [13] the slowest warp's busy ns, [14] the warps'
+   * summed busy ns, [15] warps. */
   int64_t work[16];
   /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
    * first split, near-far loop, unpack. */
