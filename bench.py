@@ -433,6 +433,8 @@ def main():
                        "sssp_phases_ms": phases, "sssp_work": work, "update_shape": shape,
                        "alg_bytes_per_update": float(np.mean(alg)),
                        "trace_last_update": [list(t) for t in timed_stats[-1].trace],
+                       "pj_rounds_us_last_update": list(timed_stats[-1].pj_rounds_us),
+                       "pj_done_us_last_update": list(timed_stats[-1].pj_done_us),
                        "verified_vs_compute": verified, "compute_from_scratch": compute_info,
                        "setup_s": {"generate": round(gen_s, 1), "build_and_compute": round(build_s, 1)}},
             "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,

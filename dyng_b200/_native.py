@@ -53,11 +53,12 @@ class Stats(ctypes.Structure):
                 ("grid_blocks", ctypes.c_int32), ("invalidation", ctypes.c_int32),
                 ("apply_ms", ctypes.c_float), ("sssp_ms", ctypes.c_float),
                 ("rounds", ctypes.c_int64), ("touched", ctypes.c_int64),
-                ("work", ctypes.c_int64 * 16), ("phase_ms", ctypes.c_float * 7),
+                ("work", ctypes.c_int64 * 24), ("phase_ms", ctypes.c_float * 7),
                 ("trace_len", ctypes.c_int32), ("trace_light", ctypes.c_int32 * 64),
                 ("trace_heavy", ctypes.c_int32 * 64), ("trace_us", ctypes.c_float * 64),
                 ("features", ctypes.c_float * 12), ("schedule_classes", ctypes.c_int32 * 3),
-                ("kernel_launches", ctypes.c_int64)]
+                ("kernel_launches", ctypes.c_int64), ("pj_round_us", ctypes.c_float * 24),
+                ("pj_done_us", ctypes.c_float * 24)]
 
 
 class Options(ctypes.Structure):

@@ -147,13 +147,15 @@ struct UpdateCtl {
   long long loop_pushes;
   u64 loop_threshold;
   // work counters (algorithmic traffic) and phase timestamps of the sssp kernel
-  long long work[16];
+  long long work[24];
   unsigned long long phase_ns[8];
   // trace of the first 64 push iterations / epochs: (light count, heavy chunks, ns since start)
   int trace_n[64];
   int trace_h[64];
   unsigned trace_t[64];
   int trace_len;
+  unsigned pj_t[24];  // start of each pointer-jumping round (ns since the kernel began)
+  unsigned pj_done[24];  // the last block's arrival at the barrier ending each round
   // grid barrier: blocks arrive on one of kBarGroups group counters, the last of each group on
   // bar_count, the last group flips bar_gen
   unsigned bar_count;
@@ -180,6 +182,7 @@ struct Workspace {
   DevBuf<int32_t> b_ins_src, b_ins_dst, b_ins_w, b_del_src, b_del_dst;
   // sssp
   DevBuf<int> stamp, touch_stamp, flag, in_far, ancestor;
+  DevBuf<int> pj_blk;  // per-block survivor counts of pointer jumping
   DevBuf<int> candidates, frontier, near_a, near_b, far_a, far_b, heavy_a, heavy_b, pull_heavy,
       touched, cand_med, near_med_a, near_med_b;
   DevBuf<UpdateCtl> ctl;

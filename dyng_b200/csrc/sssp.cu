@@ -26,7 +26,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kHeavyChunk = 256;
 constexpr unsigned long long kBarrierTimeoutNs = 5ULL * 1000 * 1000 * 1000;
-constexpr unsigned kBarGroups = 32;  // arrival groups of the grid barrier (UpdateCtl::bar_group)
+constexpr unsigned kBarGroups = 32;
+constexpr int kPjMaxBlocks = 1024;   // persistent blocks the pointer-jumping lists support  // arrival groups of the grid barrier (UpdateCtl::bar_group)
 
 struct SsspParams {
   GraphView g;
@@ -74,7 +75,8 @@ struct SsspParams {
   long long delta_override;
   int small_frontier;    // frontiers up to this size run on block 0 alone (0: never)
   UpdateCtl* ctl;
-  TreeHistory* hist;     // the tree's record of this run (the learned scheduler's history)
+  TreeHistory* hist;
+  int* pj_blk;           // survivor counts of the pointer-jumping rounds: 2 x kPjMaxBlocks     // the tree's record of this run (the learned scheduler's history)
 };
 
 // Pair flags of the applier (graph.cu).
@@ -301,12 +303,13 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
     dst = y;
     du = odu;
   } else {
-    const u64 word = ld_cg(&p.packed[y]);
+    // the source's word is distance 0 for good: no load (it is the hottest address of a pull)
+    const u64 word = y == p.source ? 0 : ld_cg(&p.packed[y]);
     ++X.words;
     if (word == kPackedInf) return;
     src = y;
     dst = owner;
-    du = X.pk.dist(word);
+    du = y == p.source ? 0 : X.pk.dist(word);
   }
   const u64 nd = du + static_cast<u64>(w);
   if (nd > X.maxd) return;
@@ -341,10 +344,11 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
 __device__ __forceinline__ u64 pull_candidate(const SsspParams& p, Ctx& X, int y, int w) {
   ++X.slots;
   if (y < 0) return kPackedInf;
-  const u64 word = ld_cg(&p.packed[y]);
+  // the source's word is distance 0 for good: no load (it is the hottest address of a pull)
+  const u64 word = y == p.source ? 0 : ld_cg(&p.packed[y]);
   ++X.words;
   if (word == kPackedInf) return kPackedInf;
-  const u64 nd = X.pk.dist(word) + static_cast<u64>(w);
+  const u64 nd = (y == p.source ? 0 : X.pk.dist(word)) + static_cast<u64>(w);
   if (nd > X.maxd) return kPackedInf;
   return X.pk.pack(nd, y);
 }
@@ -482,7 +486,7 @@ template <int MODE>
 __device__ __forceinline__ void warp_rows(const SsspParams& p, Ctx& X, int owner, u64 odu,
                                           unsigned start, int len) {
   const int lane = threadIdx.x & 31;
-  unsigned big = __ballot_sync(0xffffffffu, len >= 32);
+  unsigned big = __ballot_sync(0xffffffffu, len > kLightMax);
   while (big) {
     const int leader = __ffs(big) - 1;
     big &= big - 1;
@@ -490,7 +494,7 @@ __device__ __forceinline__ void warp_rows(const SsspParams& p, Ctx& X, int owner
                      __shfl_sync(0xffffffffu, odu, leader), __shfl_sync(0xffffffffu, start, leader),
                      0, __shfl_sync(0xffffffffu, len, leader));
   }
-  const int mine = len < 32 ? len : 0;
+  const int mine = len <= kLightMax ? len : 0;
   int incl = mine;
   for (int o = 1; o < 32; o <<= 1) {
     const int t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -588,8 +592,20 @@ __device__ __forceinline__ int find_heavy(const int2* list, int count, long long
 template <int MODE>
 __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_count,
                        const int* med, int med_count, const int2* heavy, u64 heavy_cnt,
-                       long long gwarp, long long nwarps) {
+                       long long gwarp, long long nwarps, long long* probe = nullptr) {
   const int lane = threadIdx.x & 31;
+  unsigned long long t_part = probe ? global_ns() : 0;
+  // probe: the warp's time in each part, summed into probe[0..2], maxed into probe[3..5]
+  auto part_done = [&](int part) {
+    if (!probe) return;
+    const unsigned long long now = global_ns();
+    if (lane == 0) {
+      const long long d = static_cast<long long>(now - t_part);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&probe[part]), static_cast<unsigned long long>(d));
+      atomicMax(&probe[3 + part], d);
+    }
+    t_part = now;
+  };
   const RowDesc* descs = MODE == kPull ? p.g.in_desc : p.g.out_desc;
   // light: `per` consecutive vertices per warp, balanced so that every warp runs the same
   // number of rounds
@@ -618,6 +634,7 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
       warp_rows<MODE>(p, X, owner, du, desc.start, desc.len);
     }
   }
+  part_done(0);
   // medium: one row per warp
   for (long long i = gwarp; i < med_count; i += nwarps) {
     const int owner = ld_cg(&med[i]);
@@ -631,6 +648,7 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     const RowDesc desc = descs[owner];
     warp_slots<MODE>(p, X, owner, du, desc.start, 0, desc.len);
   }
+  part_done(1);
   // heavy: chunks
   const int hcount = static_cast<int>(heavy_cnt >> 40);
   const long long chunks = static_cast<long long>(heavy_cnt & ((1ULL << 40) - 1));
@@ -650,6 +668,7 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     const int e1 = min(desc.len, e0 + kHeavyChunk);
     warp_slots<MODE>(p, X, owner, du, desc.start, e0, e1);
   }
+  part_done(2);
 }
 
 
@@ -738,7 +757,7 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
       }
       const unsigned long long t_busy = (!BLOCK && step == 0) ? global_ns() : 0;
       expand<kPush>(p, X, lists[S.it & 1], nc, mlists[S.it & 1], mc, hlists[S.it & 1], hc, gwarp,
-                    nwarps);
+                    nwarps, (!BLOCK && step == 0) ? &c->work[16] : nullptr);
       if (!BLOCK && step == 0) {
         // balance of the first step: the slowest warp's and the summed busy time, and warps
         const long long busy = static_cast<long long>(global_ns() - t_busy);
@@ -897,62 +916,110 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
       // ---- subtree invalidation by pointer jumping (fused.cuh:199-234) ------------------------
       // ancestor[v]: >= 0 the current ancestor, -1 the chain ended without a root, kMarked:
       // invalidated.  Invariant: ancestor[x] >= 0 implies no root on the tree path from x up to
-      // (excluding) ancestor[x].  Round 0 reads the parents and the roots' stamps; a vertex whose
-      // ancestor is invalidated is invalidated on the spot, so no scan follows the rounds.
+      // (excluding) ancestor[x].  A vertex whose ancestor is invalidated is invalidated on the
+      // spot, so no scan follows the rounds.
       constexpr int kMarked = -2;
       int max_rounds = 0;
       while ((1LL << max_rounds) < n) ++max_rounds;
       ++max_rounds;
       if (any_changed) {
-        // Round 0 visits every vertex of the block's own range; a vertex whose new ancestor is
-        // still a vertex (it jumps again) goes to the block's survivor list, and later rounds
-        // visit only those lists (near_a / near_b, one region of `span` entries per block: a
-        // block's survivors never exceed the vertices it visited).  No global atomics.
+        // Round 0 visits every vertex; a vertex whose new ancestor is still a vertex (it jumps
+        // again) is written to its block's survivor region (heavy_a / heavy_b, `span` (vertex,
+        // ancestor) entries per block) with no global atomic.  Later rounds see the regions, concatenated in block
+        // order, as one list (each block scans the per-block counts) and split it evenly over
+        // the blocks: a block visits at most `span` entries, so its survivors fit its region.
         __shared__ int s_pj_cnt;
+        __shared__ int s_prefix[kPjMaxBlocks + 1];
         const long long span = (n + nblk - 1) / nblk;
         const long long lo = static_cast<long long>(blockIdx.x) * span;
         const long long hi = min(n, lo + span);
-        int cur_cnt = 0;
+        // ancestor[] starts as the parents with the roots marked, written by a sequential pass
+        // over the block's range, so that every round gathers one random word per vertex
+        // (ancestor[a]) instead of two (parent[a] and stamp[a])
+        for (long long v = lo + threadIdx.x; v < hi; v += blockDim.x) {
+          const int st = ld_cg(&p.stamp[v]);
+          const int pa = v < p.tree_n ? p.parent[v] : -1;
+          // a child of the source has no ancestor that can be a root: its chain ends at once
+          // (and nothing ever gathers ancestor[source], which every chain would reach)
+          p.ancestor[v] = st == gen_inv ? kMarked : (pa == p.source ? -1 : pa);
+        }
+        if (tid == 0) c->work[22] = n;
+        if (!grid_barrier(c, bar)) return;
         for (int round = 0; round < max_rounds; ++round) {
           if (tid == 0) {
             c->active[(round + 1) % 3] = 0;
             c->rounds = round + 1;
+            if (round < 24) c->pj_t[round] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
           }
           if (threadIdx.x == 0) s_pj_cnt = 0;
-          __syncthreads();
-          const int* cur = (round & 1) ? p.near_a + lo : p.near_b + lo;
-          int* next = (round & 1) ? p.near_b + lo : p.near_a + lo;
-          const long long count = round == 0 ? hi - lo : cur_cnt;
+          long long total = n;
+          if (round > 0) {
+            const int* cnt = p.pj_blk + ((round - 1) & 1) * kPjMaxBlocks;
+            for (int q = threadIdx.x; q < nblk; q += blockDim.x) s_prefix[q + 1] = ld_cg(&cnt[q]);
+            if (threadIdx.x == 0) s_prefix[0] = 0;
+            __syncthreads();
+            if (threadIdx.x < 32) {
+              // inclusive scan of s_prefix[1..nblk] by warp 0: chunks of `per`, then the chunk sums
+              const int per = (nblk + 31) / 32;
+              const int b0 = 1 + lane * per, b1 = min(nblk + 1, b0 + per);
+              int run = 0;
+              for (int q = b0; q < b1; ++q) {
+                run += s_prefix[q];
+                s_prefix[q] = run;
+              }
+              int incl = run;
+              for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+              }
+              const int before = incl - run;
+              for (int q = b0; q < b1; ++q) s_prefix[q] += before;
+            }
+            __syncthreads();
+            total = s_prefix[nblk];
+          } else {
+            __syncthreads();
+          }
+          const long long vspan = (total + nblk - 1) / nblk;
+          const long long vlo = static_cast<long long>(blockIdx.x) * vspan;
+          const long long vhi = min(total, vlo + vspan);
+          // survivor entries are (vertex, its ancestor): a round gathers only ancestor[a]
+          const int2* cur = (round & 1) ? p.heavy_a : p.heavy_b;  // the previous round's regions
+          int2* next = ((round & 1) ? p.heavy_b : p.heavy_a) + lo;  // this block's region
           int jumping = 0;
           // four entries per thread and step, their loads issued together; the warps iterate
           // together (the bound is tested on the warp's first entry) for the ballots below
-          for (long long i0 = threadIdx.x & ~31; i0 < count; i0 += 4LL * blockDim.x) {
+          for (long long i0 = vlo + (threadIdx.x & ~31); i0 < vhi; i0 += 4LL * blockDim.x) {
             int vv[4], a[4], na[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               const long long i = i0 + lane + q * blockDim.x;
-              vv[q] = i < count ? (round == 0 ? static_cast<int>(lo + i) : cur[i]) : -1;
+              a[q] = -1;
+              if (i >= vhi) {
+                vv[q] = -1;
+              } else if (round == 0) {
+                vv[q] = static_cast<int>(i);
+              } else {
+                // the region holding entry i: the last block whose prefix is <= i
+                int lo_b = 0, hi_b = nblk;
+                while (hi_b - lo_b > 1) {
+                  const int mid = (lo_b + hi_b) >> 1;
+                  if (s_prefix[mid] <= i) lo_b = mid;
+                  else hi_b = mid;
+                }
+                const int2 e = __ldcg(&cur[static_cast<long long>(lo_b) * span + (i - s_prefix[lo_b])]);
+                vv[q] = e.x;
+                a[q] = e.y;
+              }
+            }
+            if (round == 0) {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) a[q] = vv[q] < 0 ? -1 : ld_cg(&p.ancestor[vv[q]]);
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-              const int v = vv[q];
-              if (v < 0) {
-                a[q] = -1;
-              } else if (round == 0) {
-                a[q] = ld_cg(&p.stamp[v]) == gen_inv ? kMarked : (v < p.tree_n ? p.parent[v] : -1);
-              } else {
-                a[q] = ld_cg(&p.ancestor[v]);
-              }
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              if (a[q] < 0) {
-                na[q] = a[q];
-              } else if (round == 0) {
-                na[q] = ld_cg(&p.stamp[a[q]]) == gen_inv ? kMarked : p.parent[a[q]];
-              } else {
-                na[q] = ld_cg(&p.ancestor[a[q]]);
-              }
+              na[q] = a[q] < 0 ? a[q] : ld_cg(&p.ancestor[a[q]]);
+              if (na[q] == p.source) na[q] = -1;  // reaching the source ends a chain
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -960,9 +1027,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
               bool survives = false;
               if (v >= 0) {
                 ++w_visits;
-                if (a[q] < 0) {
-                  if (round == 0) p.ancestor[v] = a[q];
-                } else {
+                if (a[q] >= 0) {
                   ++w_jumps;
                   if (na[q] == kMarked) {
                     p.ancestor[v] = kMarked;
@@ -975,19 +1040,23 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
                   }
                 }
               }
-              // warp-aggregated append to the block's survivor list
+              // warp-aggregated append to the block's survivor region
               const unsigned m = __ballot_sync(0xffffffffu, survives);
               if (m) {
                 int base = 0;
                 if (lane == 0) base = atomicAdd(&s_pj_cnt, __popc(m));
                 base = __shfl_sync(0xffffffffu, base, 0);
-                if (survives) next[base + __popc(m & ((1u << lane) - 1))] = v;
+                if (survives) next[base + __popc(m & ((1u << lane) - 1))] = make_int2(v, na[q]);
                 jumping = 1;
               }
             }
           }
           __syncthreads();
-          cur_cnt = s_pj_cnt;
+          if (threadIdx.x == 0) {
+            p.pj_blk[(round & 1) * kPjMaxBlocks + blockIdx.x] = s_pj_cnt;
+            if (round < 24)
+              atomicMax(&c->pj_done[round], static_cast<unsigned>(global_ns() - c->phase_ns[0]));
+          }
           if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
           if (!grid_barrier(c, bar)) return;
           if (ld_cg(&c->active[round % 3]) == 0) break;
@@ -1292,6 +1361,8 @@ static int persistent_blocks(Context& ctx, const dyngb200_schedule& sched) {
     expects(per_sm >= 1, "sssp: the persistent kernel does not fit on an SM", DYNGB200_NOT_SUPPORTED);
     ctx.update_blocks_per_sm = per_sm;
   }
+  expects(ctx.update_blocks_per_sm * ctx.sm_count <= kPjMaxBlocks,
+          "sssp: more persistent blocks than the pointer-jumping lists support", DYNGB200_NOT_SUPPORTED);
   return ctx.update_blocks_per_sm * ctx.sm_count;
 }
 
@@ -1333,6 +1404,8 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
   p.touched = ws.touched.ptr;
   p.ctl = ws.ctl.ptr;
   p.hist = t.hist.ptr;
+  ws.pj_blk.reserve(2 * kPjMaxBlocks);
+  p.pj_blk = ws.pj_blk.ptr;
   return p;
 }
 
@@ -1410,7 +1483,7 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
     st->sssp_ms = ms;
     st->kernel_launches = ctx.launches - launches0;
     st->affected = r.affected;
-    for (int i = 0; i < 16; ++i) st->work[i] = r.work[i];
+    for (int i = 0; i < 24; ++i) st->work[i] = r.work[i];
   }
 }
 
@@ -1576,7 +1649,7 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
     st->sssp_ms = sssp_ms;
     st->rounds = r.rounds;
     st->touched = r.touched_count;
-    for (int i = 0; i < 16; ++i) st->work[i] = r.work[i];
+    for (int i = 0; i < 24; ++i) st->work[i] = r.work[i];
     st->trace_len = r.trace_len;
     for (int i = 0; i < r.trace_len && i < 64; ++i) {
       st->trace_light[i] = r.trace_n[i];
@@ -1587,6 +1660,8 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
     for (int i = 0; i < 12; ++i) st->features[i] = scheduled ? r.features[i] : 0.0f;
     for (int i = 0; i < 3; ++i) st->schedule_classes[i] = learned ? r.sched_classes[i] : -1;
     st->kernel_launches = ctx.launches - launches0;
+    for (int i = 0; i < 24 && i < r.rounds; ++i) st->pj_round_us[i] = r.pj_t[i] * 1e-3f;
+    for (int i = 0; i < 24 && i < r.rounds; ++i) st->pj_done_us[i] = r.pj_done[i] * 1e-3f;
     for (int i = 0; i < 7; ++i)
       st->phase_ms[i] = r.phase_ns[i + 1] > r.phase_ns[i]
                             ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)

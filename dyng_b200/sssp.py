@@ -64,10 +64,12 @@ class Stats:
     WORK_NAMES = ("round_visits", "jumps", "invalidated", "pull_candidates", "pull_slots",
                   "pull_words", "pushes", "push_slots", "push_words", "atomics", "appends",
                   "unpacked", "atomic_attempts", "step0_max_warp_ns", "step0_sum_warp_ns",
-                  "step0_warps")
+                  "step0_warps", "step0_light_ns", "step0_medium_ns", "step0_heavy_ns",
+                  "step0_max_light_ns", "step0_max_medium_ns", "step0_max_heavy_ns",
+                  "pj_seeded")
     # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows);
     # attempted atomics are a diagnostic, their bytes are in "atomics" (the successful ones):
-    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32, 0, 0, 0, 0)
+    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32) + (0,) * 10 + (12,)
     PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
     _SCALARS = ("invalidated", "affected", "iterations", "epochs", "pushes", "delta",
                 "max_weight", "grid_blocks", "invalidation", "rounds", "touched",
@@ -122,6 +124,16 @@ class Stats:
         s = self._s
         return tuple((int(s.trace_light[i]), int(s.trace_heavy[i]), float(s.trace_us[i]))
                      for i in range(min(int(s.trace_len), 64)))
+
+    @property
+    def pj_rounds_us(self) -> tuple:
+        """Start of each pointer-jumping round (us since the kernel began)."""
+        return tuple(float(self._s.pj_round_us[i]) for i in range(min(int(self._s.rounds), 24)))
+
+    @property
+    def pj_done_us(self) -> tuple:
+        """The last block's arrival at the barrier ending each pointer-jumping round (us)."""
+        return tuple(float(self._s.pj_done_us[i]) for i in range(min(int(self._s.rounds), 24)))
 
     @property
     def features(self) -> tuple:

@@ -117,8 +117,9 @@ typedef struct dyngb200_stats {
    * the pull, [6] pushed vertices, [7] scanned out-slots, [8] target word reads, [9] successful
    * atomicMin, [10] frontier appends, [11] unpacked vertices, [12] atomicMin attempts (successful
    * or not); the first near-far step's balance: [13] the slowest warp's busy ns, [14] the warps'
-   * summed busy ns, [15] warps. */
-  int64_t work[16];
+   * summed busy ns, [15] warps, [16..18] the warps' summed ns in light / medium / heavy rows,
+   * [19..21] the slowest warp's ns in each; [22] vertices seeded for pointer jumping; [23] zero. */
+  int64_t work[24];
   /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
    * first split, near-far loop, unpack. */
   float phase_ms[7];
@@ -134,6 +135,8 @@ typedef struct dyngb200_stats {
   float features[12];
   int32_t schedule_classes[3];
   int64_t kernel_launches; /* kernels of this library the call launched */
+  float pj_round_us[24];    /* start of each pointer-jumping round, us since the kernel began */
+  float pj_done_us[24];     /* the last block's arrival at the barrier ending each round */
 } dyngb200_stats;
 
 /* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */
