@@ -146,6 +146,9 @@ SIGNATURES = {
     "dyngb200_sssp_update_learned": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch),
                                                     c_void_p, c_void_p, ctypes.POINTER(Stats)]),
     "dyngb200_scheduler_num_params": (ctypes.c_int64, []),
+    "dyngb200_sssp_update_each": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch),
+                                                 ctypes.POINTER(c_void_p), ctypes.c_int32,
+                                                 ctypes.POINTER(Stats)]),
     "dyngb200_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), c_void_p,
                                               ctypes.POINTER(c_void_p)]),
     "dyngb200_server_add_graph": (ctypes.c_int, [c_void_p, c_void_p, c_void_p,

@@ -508,6 +508,30 @@ dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_gr
   });
 }
 
+dyngb200_status dyngb200_sssp_update_each(dyngb200_context ctx, dyngb200_graph g,
+                                          const dyngb200_batch* batch, dyngb200_tree* trees,
+                                          int32_t count, dyngb200_stats* stats) {
+  return guarded([&] {
+    expects(ctx && g && batch && trees, "dyng::update_each: null argument");
+    expects(count >= 1, "dyng::update_each: the list of results is empty (applying a batch "
+                        "without updating any result would leave every result stale; use "
+                        "graph_apply)");
+    Context& c = ctx->ctx;
+    DeviceGuard guard(c.device);
+    std::vector<Tree*> ts(static_cast<size_t>(count));
+    for (int i = 0; i < count; ++i) {
+      expects(trees[i] != nullptr, "dyng::update_each: result " + std::to_string(i) + " is null");
+      for (int j = 0; j < i; ++j)
+        expects(trees[j] != trees[i], "dyng::update_each: result " + std::to_string(i) +
+                                          " is listed twice");
+      expect_tree_current(g->g, trees[i]->t, "dyng::update_each");
+      ts[i] = &trees[i]->t;
+    }
+    expect_batch(g->g, *batch, "dyng::update_each");
+    sssp_update_each(c, g->g, *batch, ts.data(), count, stats);
+  });
+}
+
 dyngb200_status dyngb200_sssp_update_learned(dyngb200_context ctx, dyngb200_graph g,
                                              const dyngb200_batch* batch, dyngb200_tree tree,
                                              dyngb200_scheduler scheduler, dyngb200_stats* stats) {

@@ -386,6 +386,8 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
                        const dyngb200_schedule& sched, const Scheduler* learned,
                        PendingUpdate& u);
 void sssp_update_end(PendingUpdate& u, dyngb200_stats* st);
+void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree* const* trees,
+                      int count, dyngb200_stats* stats);
 void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
                  dyngb200_apply_summary* summary, unsigned char* weight_increased);
 void tree_reserve(Context& ctx, Tree& t, long long n_cap);

@@ -76,7 +76,10 @@ struct SsspParams {
   int small_frontier;    // frontiers up to this size run on block 0 alone (0: never)
   UpdateCtl* ctl;
   TreeHistory* hist;
-  int* pj_blk;           // survivor counts of the pointer-jumping rounds: 2 x kPjMaxBlocks     // the tree's record of this run (the learned scheduler's history)
+  int* pj_blk;           // survivor counts of the pointer-jumping rounds: 2 x kPjMaxBlocks
+  const unsigned char* inc;  // the applier's weight-increase flags (pairs x k)
+  int use_inc;           // 1: changed edges of `objective` from inc[] (a batch applied for another
+                         // objective), 0: from the pair flags     // the tree's record of this run (the learned scheduler's history)
 };
 
 // Pair flags of the applier (graph.cu).
@@ -885,7 +888,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
     for (long long i = tid; i < pairs; i += threads) {
       const int slot = p.pair_list[i];
       const int f = p.pair_flags[slot];
-      if (f & (kPairDelete | kPairIncreased)) {
+      const bool increased = p.use_inc ? p.inc[static_cast<long long>(slot) * p.k + p.objective] != 0
+                                       : (f & kPairIncreased) != 0;
+      if ((f & kPairDelete) || increased) {
         changed = 1;
         const u64 key = p.pair_key[slot];
         const int32_t u = static_cast<int32_t>(key >> 32);
@@ -1562,48 +1567,11 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
 
 // update(), second half: waits for the queued attempt, grows and retries on a capacity error
 // (nothing was changed), then the error translation, the commit bookkeeping and the stats.
-void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
-  Context& ctx = *u.ctx;
-  Graph& g = *u.g;
-  Tree& t = *u.t;
-  Workspace& ws = ctx.ws;
-  const Scheduler* learned = u.learned;
-  const dyngb200_schedule& sched = u.sched;
-  const int blocks = u.blocks;
-  const long long launches0 = u.launches0;
-  UpdateCtl r{};
-  for (int attempt = 0;; ++attempt) {
-    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-    r = *ws.host_ctl.ptr;
-    g.host_counters = *reinterpret_cast<const GraphCounters*>(g.pinned.ptr);
-    std::memcpy(g.host_columns.data(), g.pinned.ptr + kCounterSlots,
-                g.host_columns.size() * sizeof(ColumnStats));
-    ws.generation = std::max(ws.generation, r.last_generation);
-    if ((r.error & kErrCapacity) && attempt < 4) {
-      // nothing was changed: grow the vertex capacity or the arenas and run again
-      graph_grow(ctx, g, r.n_after > g.n_cap ? r.n_after : 0,
-                 static_cast<long long>(r.top_out), static_cast<long long>(r.top_in));
-      enqueue_attempt(u);
-      continue;
-    }
-    break;
-  }
-  float apply_ms = 0, sssp_ms = 0;
-  cudaEventElapsedTime(&apply_ms, u.e0, u.e1);
-  cudaEventElapsedTime(&sssp_ms, u.e1, u.e2);
-  if (r.error & (kErrInvalidBatch | kErrCapacity)) {
-    // found before the commit: the graph and the tree are unchanged
-    std::string msg = "sssp::update: invalid batch";
-    if (r.err_index == -2) msg = "sssp::update: distances do not fit in 62 bits";
-    else if (r.err_index != INT64_MAX) msg += " (operation " + std::to_string(r.err_index) + ")";
-    if (r.error & kErrCapacity) throw Error(DYNGB200_CAPACITY, "sssp::update: capacity exceeded");
-    throw Error(DYNGB200_INVALID_ARGUMENT, msg);
-  }
-  // the batch is committed from here on
-  g.version += 1;
-  g.n = g.host_counters.n;
-  g.m = g.host_counters.m;
-  t.version = g.version;
+// After the commit: the tree's errors (poisoning it), its new state and the stats.
+static void finish_tree(Context& ctx, Graph& g, Tree& t, const UpdateCtl& r, int blocks,
+                        float apply_ms, float sssp_ms, const Scheduler* learned,
+                        const dyngb200_schedule& sched, long long launches0,
+                        dyngb200_stats* st) {
   if (r.error & kErrInternal) {
     t.poisoned = true;
     throw Error(DYNGB200_INTERNAL, "sssp::update: the in-edge mirror disagrees with the rows");
@@ -1669,12 +1637,221 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
   }
 }
 
+void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
+  Context& ctx = *u.ctx;
+  Graph& g = *u.g;
+  Tree& t = *u.t;
+  Workspace& ws = ctx.ws;
+  const Scheduler* learned = u.learned;
+  const dyngb200_schedule& sched = u.sched;
+  const int blocks = u.blocks;
+  const long long launches0 = u.launches0;
+  UpdateCtl r{};
+  for (int attempt = 0;; ++attempt) {
+    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+    r = *ws.host_ctl.ptr;
+    g.host_counters = *reinterpret_cast<const GraphCounters*>(g.pinned.ptr);
+    std::memcpy(g.host_columns.data(), g.pinned.ptr + kCounterSlots,
+                g.host_columns.size() * sizeof(ColumnStats));
+    ws.generation = std::max(ws.generation, r.last_generation);
+    if ((r.error & kErrCapacity) && attempt < 4) {
+      // nothing was changed: grow the vertex capacity or the arenas and run again
+      graph_grow(ctx, g, r.n_after > g.n_cap ? r.n_after : 0,
+                 static_cast<long long>(r.top_out), static_cast<long long>(r.top_in));
+      enqueue_attempt(u);
+      continue;
+    }
+    break;
+  }
+  float apply_ms = 0, sssp_ms = 0;
+  cudaEventElapsedTime(&apply_ms, u.e0, u.e1);
+  cudaEventElapsedTime(&sssp_ms, u.e1, u.e2);
+  if (r.error & (kErrInvalidBatch | kErrCapacity)) {
+    // found before the commit: the graph and the tree are unchanged
+    std::string msg = "sssp::update: invalid batch";
+    if (r.err_index == -2) msg = "sssp::update: distances do not fit in 62 bits";
+    else if (r.err_index != INT64_MAX) msg += " (operation " + std::to_string(r.err_index) + ")";
+    if (r.error & kErrCapacity) throw Error(DYNGB200_CAPACITY, "sssp::update: capacity exceeded");
+    throw Error(DYNGB200_INVALID_ARGUMENT, msg);
+  }
+  // the batch is committed from here on
+  g.version += 1;
+  g.n = g.host_counters.n;
+  g.m = g.host_counters.m;
+  t.version = g.version;
+  finish_tree(ctx, g, t, r, blocks, apply_ms, sssp_ms, learned, sched, launches0, st);
+}
+
 // update(): sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489).
 void sssp_update(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
                  const dyngb200_schedule& sched, dyngb200_stats* st, const Scheduler* learned) {
   PendingUpdate u;
   sssp_update_begin(ctx, g, t, batch, sched, learned, u);
   sssp_update_end(u, st);
+}
+
+// ---- update_each: one batch, the trees of several objectives -------------------------------
+
+namespace {
+// Per objective j of a batch: out[2j] = the largest insertion weight, out[2j + 1] = the smallest;
+// out[2k] = the largest vertex id + 1 the batch names.
+__global__ void k_batch_extrema(const int32_t* ins_src, const int32_t* ins_dst,
+                                const int32_t* ins_w, long long ni, const int32_t* del_src,
+                                const int32_t* del_dst, long long nd, int k, long long* out) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < ni + nd;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const bool ins = i < ni;
+    const long long j = ins ? i : i - ni;
+    const long long u = ins ? ins_src[j] : del_src[j];
+    const long long v = ins ? ins_dst[j] : del_dst[j];
+    atomicMax(&out[2 * k], max(u, v) + 1);
+    if (ins) {
+      for (int c = 0; c < k; ++c) {
+        const long long w = ins_w[j * k + c];
+        atomicMax(&out[2 * c], w);
+        atomicMin(&out[2 * c + 1], w);
+      }
+    }
+  }
+}
+}  // namespace
+
+// The sssp part of an update for a tree of another objective than the one the batch was applied
+// with: the applier's state (pairs, flags, summary) is still in the workspace; the plan of this
+// objective comes from the graph as it was before the batch (`pre_*`).
+static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied,
+                       const std::vector<ColumnStats>& pre_cols, const GraphCounters& pre_counters,
+                       long long batch_max_w, const int32_t* ins_w, dyngb200_stats* st) {
+  const long long launches0 = ctx.launches;
+  Workspace& ws = ctx.ws;
+  cudaStream_t s = ctx.stream;
+  const int obj = t.opt.objective;
+  UpdateCtl init{};
+  init.err_index = INT64_MAX;
+  init.n_old = applied.n_old;
+  init.n_after = applied.n_after;
+  init.pairs = applied.pairs;
+  std::memcpy(init.summary, applied.summary, sizeof(init.summary));
+  init.batch_ins_max = std::max<long long>(1, batch_max_w);
+  init.max_w = std::max<long long>(pre_cols[obj].max_w, init.batch_ins_max);
+  init.delta = t.opt.delta > 0 ? t.opt.delta
+                               : default_delta(std::max<long long>(pre_counters.m, 1),
+                                               pre_counters.n, pre_cols[obj].sum_w);
+  u64 bound = 0;
+  const Packing pk = choose_packing(init.n_after, init.max_w, &bound);
+  init.packing_bits = pk.bits;
+  init.max_distance = bound;
+  init.minimum = kPackedInf;
+  const dyngb200_schedule sched{};
+  schedule_into(sched, init);
+  *ws.host_ctl.ptr = init;
+  tree_reserve(ctx, t, g.n_cap);
+  cudaEvent_t e1, e2;
+  DYNGB200_CUDA(cudaEventCreate(&e1));
+  DYNGB200_CUDA(cudaEventCreate(&e2));
+  DYNGB200_CUDA(cudaMemcpyAsync(ws.ctl.ptr, ws.host_ctl.ptr, sizeof(UpdateCtl),
+                                cudaMemcpyHostToDevice, s));
+  const int blocks = persistent_blocks(ctx, sched);
+  SsspParams p = base_params(ctx, g, t);
+  p.from_scratch = 0;
+  p.tree_n = t.n;
+  p.tree_bits = t.packed_bits;
+  p.pair_key = ws.pair_key.ptr;
+  p.pair_list = ws.pair_list.ptr;
+  p.pair_flags = ws.pair_flags.ptr;
+  p.pair_first = ws.pair_first.ptr;
+  p.pair_last = ws.pair_last.ptr;
+  p.ins_w = ins_w;
+  p.k = g.k;
+  p.inc = ws.pair_inc.ptr;
+  p.use_inc = 1;
+  p.offer_heads = t.canonical ? 1 : 0;
+  p.tree_trusted = t.trusted ? 1 : 0;
+  p.generation = ws.next_generation(1, s);
+  p.touch_gen = p.generation;
+  p.heavy_degree = 256;
+  DYNGB200_CUDA(cudaEventRecord(e1, s));
+  launch(ctx, p, blocks);
+  DYNGB200_CUDA(cudaEventRecord(e2, s));
+  DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
+                                cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+  const UpdateCtl r = *ws.host_ctl.ptr;
+  ws.generation = std::max(ws.generation, r.last_generation);
+  float sssp_ms = 0;
+  cudaEventElapsedTime(&sssp_ms, e1, e2);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  t.version = g.version;
+  finish_tree(ctx, g, t, r, blocks, 0.0f, sssp_ms, nullptr, sched, launches0, st);
+}
+
+// update_each (update.hpp:331): the batch is applied once; every tree is brought up to date.
+// Errors found before the batch is applied (for any of the objectives) leave the graph and every
+// tree unchanged; an error after it poisons that tree only, the others are still updated, and the
+// first error is rethrown.
+void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree* const* trees,
+                      int count, dyngb200_stats* stats) {
+  cudaStream_t s = ctx.stream;
+  for (int i = 0; i < count; ++i)
+    if (g.host_columns[trees[i]->opt.objective].dirty) graph_rescan_columns(ctx, g);
+  const StagedBatch b = stage_batch(ctx, batch, g.k);
+  // before the batch is applied: every objective's weights and 62-bit bound
+  const int k = g.k;
+  std::vector<long long> ext(2 * k + 1, 0);
+  for (int c = 0; c < k; ++c) ext[2 * c + 1] = INT64_MAX;
+  DevBuf<long long> d_ext;
+  d_ext.reserve(ext.size());
+  DYNGB200_CUDA(cudaMemcpyAsync(d_ext.ptr, ext.data(), ext.size() * sizeof(long long),
+                                cudaMemcpyHostToDevice, s));
+  if (b.ni + b.nd > 0) {
+    k_batch_extrema<<<std::max(1, ctx.sm_count * 4), kThreads, 0, s>>>(
+        b.ins_src, b.ins_dst, b.ins_w, b.ni, b.del_src, b.del_dst, b.nd, k, d_ext.ptr);
+    ++ctx.launches;
+    DYNGB200_CUDA(cudaGetLastError());
+  }
+  DYNGB200_CUDA(cudaMemcpyAsync(ext.data(), d_ext.ptr, ext.size() * sizeof(long long),
+                                cudaMemcpyDeviceToHost, s));
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+  const long long n_bound = std::max<long long>(g.n, ext[2 * k]);
+  for (int i = 0; i < count; ++i) {
+    const int obj = trees[i]->opt.objective;
+    if (b.ni > 0)
+      expects(ext[2 * obj + 1] >= 1, "dyng::update_each: an insertion weight of objective " +
+                                         std::to_string(obj) + " is below 1");
+    const long long mw = std::max<long long>(g.host_columns[obj].max_w, b.ni > 0 ? ext[2 * obj] : 1);
+    expects(distances_fit(n_bound, mw),
+            "dyng::update_each: distances of objective " + std::to_string(obj) +
+                " do not fit in 62 bits");
+  }
+  const std::vector<ColumnStats> pre_cols = g.host_columns;
+  const GraphCounters pre_counters = g.host_counters;
+  const uint64_t version0 = g.version;
+  // the first tree applies the batch (an error before the commit leaves everything unchanged)
+  std::string first_msg;
+  dyngb200_status first_status = DYNGB200_OK;
+  try {
+    sssp_update(ctx, g, *trees[0], batch, dyngb200_schedule{}, stats ? &stats[0] : nullptr);
+  } catch (const Error& e) {
+    if (g.version == version0) throw;  // nothing was applied
+    first_status = e.status;
+    first_msg = e.what();
+  }
+  const UpdateCtl applied = *ctx.ws.host_ctl.ptr;
+  for (int i = 1; i < count; ++i) {
+    try {
+      const int obj = trees[i]->opt.objective;
+      sssp_rerun(ctx, g, *trees[i], applied, pre_cols, pre_counters,
+                 b.ni > 0 ? ext[2 * obj] : 1, b.ins_w, stats ? &stats[i] : nullptr);
+    } catch (const Error& e) {
+      trees[i]->poisoned = true;
+      if (first_status == DYNGB200_OK) {
+        first_status = e.status;
+        first_msg = e.what();
+      }
+    }
+  }
+  if (first_status != DYNGB200_OK) throw Error(first_status, first_msg);
 }
 
 // Tree arrays sized for the graph's vertex capacity (contents kept).

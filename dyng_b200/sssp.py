@@ -256,6 +256,18 @@ def compute(graph: Graph, source: int = 0, options: Options | None = None,
     return (r, Stats._from_native(st)) if stats else r
 
 
+def update_each(graph: Graph, batch: EdgeBatch, results) -> list:
+    """dyng::update_each (update.hpp:331) for sssp results: the batch is applied once and every
+    result (e.g. one per objective) is updated; one Stats per result, in order."""
+    results = list(results)
+    nb = batch._to_native()
+    handles = (ctypes.c_void_p * max(len(results), 1))(*[r._h.value for r in results])
+    out = (N.Stats * max(len(results), 1))()
+    check(N.lib().dyngb200_sssp_update_each(graph._res._h, graph._h, ctypes.byref(nb), handles,
+                                            len(results), out))
+    return [Stats(out[i]) for i in range(len(results))]
+
+
 def update(graph: Graph, batch: EdgeBatch, tree: Result, schedule: Schedule | None = None,
            scheduler=None) -> Stats:
     """sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489).

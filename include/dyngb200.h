@@ -218,6 +218,14 @@ dyngb200_status dyngb200_sssp_compute(dyngb200_context ctx, dyngb200_graph g, in
 dyngb200_status dyngb200_sssp_update(dyngb200_context ctx, dyngb200_graph g,
                                      const dyngb200_batch* batch, dyngb200_tree tree,
                                      dyngb200_stats* stats);
+/* dyng::update_each(resources::cuda(), g, batch, results) (update.hpp:331) for sssp results,
+ * e.g. the K objectives of a multi-weight graph: the batch is applied once and every tree is
+ * updated (one stats per tree, in order).  Errors found before the batch is applied, for any
+ * tree, leave the graph and all trees unchanged; an error after it poisons that tree only, the
+ * others are still updated, and the first error is returned. */
+dyngb200_status dyngb200_sssp_update_each(dyngb200_context ctx, dyngb200_graph g,
+                                          const dyngb200_batch* batch, dyngb200_tree* trees,
+                                          int32_t count, dyngb200_stats* stats);
 /* sssp::update with an explicit schedule (the learned scheduler's entry point; no reference
  * counterpart beyond options::delta / options::cuda_engine, which are tunables the same way). */
 dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_graph g,

@@ -57,6 +57,48 @@ def test_fixtures_compute_and_update(fixtures):
     assert done > 34
 
 
+def test_fixtures_update_each_objective_on_one_graph(fixtures):
+    # dyng::update_each (update.hpp:331): the K trees of a fixture on one graph, the batch applied
+    # once; every tree equals the golden of its objective (the MOSP compat driver's use)
+    done = 0
+    for name in _cases(fixtures):
+        c = fixture_case(fixtures, name)
+        k = c["k"]
+        if k < 2:
+            continue
+        g = D.Graph.from_csr(c["row_ptr"], c["col"], c["w"], D.GraphProperties.mosp_compatible(),
+                             num_weights=k)
+        trees = [D.sssp.Result.from_arrays(g, 0, c["init_d"][j], c["init_p"][j],
+                                           canonicalize=False, options=D.sssp.Options(objective=j))
+                 for j in range(k)]
+        stats = D.sssp.update_each(g, _batch(c["ins_src"], c["ins_dst"], c["ins_w"], c["del_src"],
+                                             c["del_dst"], k), trees)
+        assert g.version() == 1 and len(stats) == k
+        for j, (t, st) in enumerate(zip(trees, stats)):
+            np.testing.assert_array_equal(t.distances, c["upd_d"][j], err_msg=f"{name} obj{j}")
+            np.testing.assert_array_equal(t.parents, c["upd_p"][j], err_msg=f"{name} obj{j}")
+            assert st.invalidated == c["invalidated"][j], (name, j)
+            assert t.graph_version == 1
+        done += 1
+    assert done >= 10
+
+
+def test_update_each_errors_keep_every_tree():
+    # an error before the batch is applied (a weight below 1 in the second objective) changes
+    # nothing; a tree listed twice is refused
+    g = D.Graph.from_edges([0, 1], [1, 2], [[3, 4], [5, 6]], num_weights=2)
+    t0 = D.sssp.compute(g, 0, D.sssp.Options(objective=0))
+    t1 = D.sssp.compute(g, 0, D.sssp.Options(objective=1))
+    with pytest.raises(D.InvalidArgumentError):
+        D.sssp.update_each(g, _batch([0], [2], [1, 0], k=2), [t0, t1])
+    assert g.version() == 0 and t0.distances.tolist() == [0, 3, 8]
+    with pytest.raises(D.InvalidArgumentError):
+        D.sssp.update_each(g, _batch([0], [2], [1, 1], k=2), [t0, t0])
+    st = D.sssp.update_each(g, _batch([0], [2], [1, 1], k=2), [t0, t1])
+    assert t0.distances.tolist() == [0, 3, 1] and t1.distances.tolist() == [0, 4, 1]
+    assert [s.batch.inserted_edges for s in st] == [1, 1]
+
+
 def test_fixtures_applied_csr(fixtures):
     checked = 0
     for name in _cases(fixtures):

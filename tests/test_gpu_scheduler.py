@@ -64,7 +64,7 @@ def _torch_loss_and_grad(params, mean, scale, x, y):
     for head, (b, n) in enumerate(S.HEADS):
         loss = loss + torch.nn.functional.cross_entropy(lo[:, b:b + n], yt[:, head])
     loss.backward()
-    return float(loss), P.grad.numpy()
+    return float(loss.detach()), P.grad.numpy()
 
 
 def test_gradients_match_torch_fp32(D):
