@@ -1489,6 +1489,12 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
     st->kernel_launches = ctx.launches - launches0;
     st->affected = r.affected;
     for (int i = 0; i < 24; ++i) st->work[i] = r.work[i];
+    st->trace_len = r.trace_len;
+    for (int i = 0; i < r.trace_len && i < 64; ++i) {
+      st->trace_light[i] = r.trace_n[i];
+      st->trace_heavy[i] = r.trace_h[i];
+      st->trace_us[i] = r.trace_t[i] * 1e-3f;
+    }
   }
 }
 

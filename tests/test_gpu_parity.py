@@ -273,6 +273,29 @@ def test_rmat_scale16_batch():
     assert fin.max() < 2**31
 
 
+def test_large_frontiers_match_the_oracle():
+    # frontiers of tens of thousands of rows (the edge-parallel expansion): a Bellman-Ford-like
+    # width on R-MAT scale 17 for compute, and a 60k-change batch, against the oracle
+    e = G.rmat(17, 16, w_max=1000, seed=4)
+    rp, col, w = e.csr()
+    g = D.Graph.from_csr(rp, col, w)
+    og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
+    t, cst = D.sssp.compute(g, 0, D.sssp.Options(delta=1 << 40), stats=True)
+    ot, _ = O.compute(og, 0, rule=1)
+    np.testing.assert_array_equal(t.distances, ot.distances)
+    np.testing.assert_array_equal(t.parents, ot.parents)
+    assert max(light for light, _, _ in cst.trace) >= 8192
+    b = G.BatchStream(e, seed=3).next(60000, 0.6, 0.5, parents=ot.parents)
+    st = D.sssp.update(g, _batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                                 b.delete_dst), t, schedule=D.sssp.Schedule(delta=1 << 40))
+    ost, _ = O.update(og, _obatch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                                  b.delete_dst), ot)
+    np.testing.assert_array_equal(t.distances, ot.distances)
+    np.testing.assert_array_equal(t.parents, ot.parents)
+    assert (st.invalidated, st.affected) == (ost["invalidated"], ost["affected"])
+    assert max(light for light, _, _ in st.trace) >= 8192
+
+
 def test_schedules_never_change_results():
     # sssp::options::delta and the schedule are tunables (sssp.hpp:78-94): every schedule gives
     # the same bytes as the oracle
