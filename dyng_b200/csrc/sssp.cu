@@ -5,8 +5,8 @@
 //
 // What differs from the reference's kernel (the results do not):
 //   - the packed (distance << b | parent) words persist between updates in the tree, so an update
-//     does not pack and unpack all n vertices: only the vertices whose word changed (the
-//     `touched` list) are unpacked and compared for `affected`;
+//     does not pack all n vertices; the unpack compares every word with its (distance, parent)
+//     and writes the changed ones (`affected`), so the relaxations keep no list of written words;
 //   - frontier rows longer than `heavy_degree` are split into 1024-slot chunks spread over all
 //     warps (one 64-bit atomic reserves a list slot and its chunk range together), shorter rows
 //     of 32+ slots are scanned by a whole warp, the rest by one lane each;
@@ -214,12 +214,6 @@ __device__ __forceinline__ bool claim(int* stamp, int v, int generation) {
   return atomicExch(&stamp[v], generation) != generation;
 }
 
-__device__ __forceinline__ void touch(const SsspParams& p, int v) {
-  if (atomicExch(&p.touch_stamp[v], p.touch_gen) != p.touch_gen) {
-    staged_append(kStTouched, p.touched, &p.ctl->touched_count, v);
-  }
-}
-
 __device__ __forceinline__ void warp_min_into(u64 v, u64* target) {
   for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0 && v != kPackedInf) atomicMin(target, v);
@@ -291,7 +285,6 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
   if (MODE == kWalk) {
     if (y < p.tree_n && p.parent[y] == owner && claim(p.stamp, y, X.gen)) {
       p.packed[y] = kPackedInf;
-      touch(p, y);
       add_candidate(p, y);
       ++X.appends;
       list_append(X.next, y, p.g.out_desc[y].len, p.heavy_degree);
@@ -321,10 +314,7 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
   if (cand >= ld_cg(&p.packed[dst])) return;
   ++X.tries;
   const u64 old = atomicMin(&p.packed[dst], cand);
-  if (cand < old) {
-    ++X.atomics;
-    touch(p, dst);
-  }
+  if (cand < old) ++X.atomics;
   if (nd < X.pk.dist(old)) {
     if (MODE == kPull) {
       if (claim(p.stamp, dst, X.gen)) {
@@ -362,10 +352,7 @@ __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int own
   if (cand >= ld_cg(&p.packed[owner])) return;
   ++X.tries;
   const u64 old = atomicMin(&p.packed[owner], cand);
-  if (cand < old) {
-    ++X.atomics;
-    touch(p, owner);
-  }
+  if (cand < old) ++X.atomics;
   if (X.pk.dist(cand) < X.pk.dist(old) && claim(p.stamp, owner, X.gen)) {
     ++X.appends;
     staged_append(kStNext, X.next.light, X.next.light_cnt, owner);
@@ -400,10 +387,7 @@ __device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const O
   const int dst = r.dst;
   ++X.tries;
   const u64 old = atomicMin(&p.packed[dst], r.cand);
-  if (r.cand < old) {
-    ++X.atomics;
-    touch(p, dst);
-  }
+  if (r.cand < old) ++X.atomics;
   const u64 nd = X.pk.dist(r.cand);
   if (nd < X.pk.dist(old)) {
     if (nd < X.threshold) {
@@ -677,7 +661,6 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
 
 __device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
   p.packed[v] = kPackedInf;
-  touch(p, v);
   add_candidate(p, v);
 }
 
@@ -1131,7 +1114,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
       const u64 cand = pk.pack(nd, u);
       if (cand >= ld_cg(&p.packed[v])) continue;
       const u64 old = atomicMin(&p.packed[v], cand);
-      if (cand < old) touch(p, v);
       if (nd < pk.dist(old) && claim(p.stamp, v, gen_pull))
         staged_append(kStNext, p.frontier, &c->frontier_count, v);
     }
@@ -1238,17 +1220,33 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         p.parent[v] = word == kPackedInf ? -1 : pk.parent(word);
       }
     } else {
-      const int touched = ld_cg(&c->touched_count);
-      for (long long i = tid; i < touched; i += threads) {
-        const int v = ld_cg(&p.touched[i]);
-        ++unpacked;
-        const u64 word = ld_cg(&p.packed[v]);
-        const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word));
-        const int32_t par = word == kPackedInf ? -1 : pk.parent(word);
-        if (p.dist[v] != d || p.parent[v] != par) {
-          p.dist[v] = d;
-          p.parent[v] = par;
-          ++affected;
+      // every vertex's word against its (distance, parent): the changed ones are written and
+      // counted (no list of written words is kept during the update)
+      // four vertices per thread and step, all loads issued before any compare
+      for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
+        u64 word[4];
+        long long od[4];
+        int32_t op[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * threads;
+          word[q] = v < n ? ld_cg(&p.packed[v]) : kPackedInf;
+          od[q] = v < n ? p.dist[v] : kInfinity;
+          op[q] = v < n ? p.parent[v] : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * threads;
+          if (v >= n) continue;
+          ++unpacked;
+          const long long d =
+              word[q] == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word[q]));
+          const int32_t par = word[q] == kPackedInf ? -1 : pk.parent(word[q]);
+          if (od[q] != d || op[q] != par) {
+            p.dist[v] = d;
+            p.parent[v] = par;
+            ++affected;
+          }
         }
       }
     }
@@ -1622,7 +1620,7 @@ static void finish_tree(Context& ctx, Graph& g, Tree& t, const UpdateCtl& r, int
     st->apply_ms = apply_ms;
     st->sssp_ms = sssp_ms;
     st->rounds = r.rounds;
-    st->touched = r.touched_count;
+    st->touched = r.affected;
     for (int i = 0; i < 24; ++i) st->work[i] = r.work[i];
     st->trace_len = r.trace_len;
     for (int i = 0; i < r.trace_len && i < 64; ++i) {

@@ -69,7 +69,7 @@ class Stats:
                   "pj_seeded")
     # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows);
     # attempted atomics are a diagnostic, their bytes are in "atomics" (the successful ones):
-    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 32) + (0,) * 10 + (12,)
+    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 20) + (0,) * 10 + (12,)
     PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
     _SCALARS = ("invalidated", "affected", "iterations", "epochs", "pushes", "delta",
                 "max_weight", "grid_blocks", "invalidation", "rounds", "touched",

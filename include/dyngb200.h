@@ -111,11 +111,11 @@ typedef struct dyngb200_stats {
   float apply_ms;      /* device time of the batch applier */
   float sssp_ms;       /* device time of the sssp kernel */
   int64_t rounds;      /* pointer-jumping rounds */
-  int64_t touched;     /* vertices whose packed word was written */
+  int64_t touched;     /* vertices the commit rewrote (their distance or parent changed) */
   /* Work of the sssp kernel, for its algorithmic traffic: [0] vertex visits of the pointer-jumping
    * rounds, [1] jumps, [2] invalidated, [3] pull candidates, [4] pulled in-slots, [5] word reads of
    * the pull, [6] pushed vertices, [7] scanned out-slots, [8] target word reads, [9] successful
-   * atomicMin, [10] frontier appends, [11] unpacked vertices, [12] atomicMin attempts (successful
+   * atomicMin, [10] frontier appends, [11] vertices the commit compared, [12] atomicMin attempts (successful
    * or not); the first near-far step's balance: [13] the slowest warp's busy ns, [14] the warps'
    * summed busy ns, [15] warps, [16..18] the warps' summed ns in light / medium / heavy rows,
    * [19..21] the slowest warp's ns in each; [22] vertices seeded for pointer jumping; [23] zero. */
