@@ -351,9 +351,11 @@ __device__ __forceinline__ u64 pull_candidate(const SsspParams& p, Ctx& X, int y
 __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int owner, u64 cand) {
   if (cand >= ld_cg(&p.packed[owner])) return;
   ++X.tries;
+  // atomicMin and claim together (see push_commit): a lost race appends the owner anyway
   const u64 old = atomicMin(&p.packed[owner], cand);
+  const bool claimed = claim(p.stamp, owner, X.gen);
   if (cand < old) ++X.atomics;
-  if (X.pk.dist(cand) < X.pk.dist(old) && claim(p.stamp, owner, X.gen)) {
+  if (claimed) {
     ++X.appends;
     staged_append(kStNext, X.next.light, X.next.light_cnt, owner);
   }
@@ -385,21 +387,22 @@ __device__ __forceinline__ void push_prepare(const SsspParams& p, Ctx& X, int u,
 __device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const Offer& r) {
   if (r.cand >= r.cur) return;  // also skips "no offer" (cand == INF)
   const int dst = r.dst;
-  ++X.tries;
-  const u64 old = atomicMin(&p.packed[dst], r.cand);
-  if (r.cand < old) ++X.atomics;
   const u64 nd = X.pk.dist(r.cand);
-  if (nd < X.pk.dist(old)) {
-    if (nd < X.threshold) {
-      if (claim(p.stamp, dst, X.gen)) {
-        ++X.appends;
-        list_append(X.next, dst, p.g.out_desc[dst].len, p.heavy_degree);
-      }
-    } else if (atomicExch(&p.in_far[dst], 1) == 0) {
-      ++X.appends;
-      staged_append(kStFar, X.far, X.far_cnt, dst);
-    }
-  }
+  const bool near = nd < X.threshold;
+  ++X.tries;
+  // The atomicMin, the claim (of the next near frontier, or of the far pile) and the row length
+  // are independent: issued together, they cost one round trip instead of three.  The claim is
+  // taken on the offer alone (the target's word read before was larger): when another lane's
+  // smaller word wins the atomicMin meanwhile, the vertex is still appended and is pushed once
+  // more with its current word -- redundant, never wrong.
+  const int len = near ? p.g.out_desc[dst].len : 0;
+  const u64 old = atomicMin(&p.packed[dst], r.cand);
+  const bool claimed = near ? claim(p.stamp, dst, X.gen) : atomicExch(&p.in_far[dst], 1) == 0;
+  if (r.cand < old) ++X.atomics;
+  if (!claimed) return;
+  ++X.appends;
+  if (near) list_append(X.next, dst, len, p.heavy_degree);
+  else staged_append(kStFar, X.far, X.far_cnt, dst);
 }
 
 template <int MODE>
