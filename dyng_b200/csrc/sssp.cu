@@ -349,7 +349,8 @@ __device__ __forceinline__ u64 pull_candidate(const SsspParams& p, Ctx& X, int y
 // The best offer of a pull for `owner`: keep it if smaller; on a distance decrease the owner
 // joins the frontier of the near-far loop.
 __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int owner, u64 cand) {
-  if (cand >= ld_cg(&p.packed[owner])) return;
+  // no read of the owner's word first: pull owners are mostly invalidated (their word is INF),
+  // so the atomicMin nearly always wins and the read would only add a round trip
   ++X.tries;
   // atomicMin and claim together (see push_commit): a lost race appends the owner anyway
   const u64 old = atomicMin(&p.packed[owner], cand);
