@@ -181,6 +181,33 @@ __device__ __forceinline__ long long index_insert(const GraphView& g, u64 key, b
   return -1;
 }
 
+// The slot of `key`: found along its probe chain, or else claimed (the first deleted slot of the
+// chain, else the empty slot that ends it).  One walk of the chain instead of a find and an
+// insert.  Concurrent calls must not insert the same key (the applier inserts each pair once).
+__device__ __forceinline__ long long index_find_or_insert(const GraphView& g, u64 key,
+                                                          bool* inserted, bool* reused) {
+  long long h = static_cast<long long>(mix64(key) & static_cast<u64>(g.emask));
+  long long first_deleted = -1;
+  for (long long probe = 0; probe <= g.emask; ++probe) {
+    const u64 cur = g.ekey[h];
+    if (cur == key) {
+      *inserted = false;
+      return h;
+    }
+    if (cur == kKeyDeleted && first_deleted < 0) first_deleted = h;
+    if (cur == kKeyEmpty) break;
+    h = (h + 1) & g.emask;
+  }
+  // not in the index: claim the first deleted slot seen, else insert from scratch
+  if (first_deleted >= 0 && atomicCAS(&g.ekey[first_deleted], kKeyDeleted, key) == kKeyDeleted) {
+    *inserted = true;
+    *reused = true;
+    return first_deleted;
+  }
+  *inserted = true;
+  return index_insert(g, key, reused);
+}
+
 __device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ u64 ld_cg(const u64* p) { return __ldcg(p); }
 __device__ __forceinline__ long long ld_cg(const long long* p) { return __ldcg(p); }

@@ -804,35 +804,33 @@ __global__ void k_append(ApplyParams p) {
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
     const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
-    unsigned placed[2] = {0, 0};
-    for (int side = 0; side < 2; ++side) {
-      const int32_t r = side == 0 ? u : v;
-      const int s = (side == 0 ? p.row_slot_out : p.row_slot_in)[r];
-      const int reloc = (side == 0 ? p.reloc_out : p.reloc_in)[s];
-      const RowDesc desc = r < c->n_old ? (side == 0 ? p.g.out_desc : p.g.in_desc)[r] : RowDesc{0, 0};
-      const unsigned base = reloc ? (side == 0 ? p.new_start_out : p.new_start_in)[s] +
-                                        (side == 0 ? p.live_out : p.live_in)[s]
-                                  : desc.start + desc.len;
-      const unsigned pos = base + (side == 0 ? p.out_rank : p.in_rank)[slot];
-      placed[side] = pos;
-      (side == 0 ? p.g.out_col : p.g.in_col)[pos] = side == 0 ? v : u;
-      int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
-      for (int j = 0; j < p.k; ++j) {
-        const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
-        w[j * p.g.arena_cap + pos] = static_cast<int32_t>(nw);
-        if (side == 0) column_in(p, acc, j, nw);
-      }
+    // both sides' loads first (they are independent), then the stores
+    const int s0 = p.row_slot_out[u], s1 = p.row_slot_in[v];
+    const int rk0 = p.out_rank[slot], rk1 = p.in_rank[slot];
+    const int reloc0 = p.reloc_out[s0], reloc1 = p.reloc_in[s1];
+    const RowDesc d0 = u < c->n_old ? p.g.out_desc[u] : RowDesc{0, 0};
+    const RowDesc d1 = v < c->n_old ? p.g.in_desc[v] : RowDesc{0, 0};
+    const unsigned ns0 = p.new_start_out[s0], ns1 = p.new_start_in[s1];
+    const int lv0 = p.live_out[s0], lv1 = p.live_in[s1];
+    const unsigned placed[2] = {(reloc0 ? ns0 + lv0 : d0.start + d0.len) + rk0,
+                                (reloc1 ? ns1 + lv1 : d1.start + d1.len) + rk1};
+    p.g.out_col[placed[0]] = v;
+    p.g.in_col[placed[1]] = u;
+    for (int j = 0; j < p.k; ++j) {
+      const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+      p.g.out_w[j * p.g.arena_cap + placed[0]] = static_cast<int32_t>(nw);
+      p.g.in_w[j * p.g.arena_cap + placed[1]] = static_cast<int32_t>(nw);
+      column_in(p, acc, j, nw);
     }
     if (!p.g.allow_multi) {
       // the edge index follows the new slots (an edge deleted and re-inserted keeps its key)
-      long long ie = index_find(p.g, key);
+      bool inserted = false, reused = false;
+      const long long ie = index_find_or_insert(p.g, key, &inserted, &reused);
       if (ie < 0) {
-        bool reused = false;
-        ie = index_insert(p.g, key, &reused);
-        if (ie < 0) {
-          set_error(&c->error, kErrInternal);
-          continue;
-        }
+        set_error(&c->error, kErrInternal);
+        continue;
+      }
+      if (inserted) {
         ++idx_new;
         idx_reused += reused ? 1 : 0;
       }

@@ -294,7 +294,11 @@ __global__ void k_infer_schedule(const float* params, const uint16_t* w, FeatNor
   __shared__ float f[kMlpIn];
   __shared__ float xs[kMlpIn];
   __shared__ float h1[kMlpHidden], h2[kMlpHidden], lo[kMlpOut];
-  const int lane = threadIdx.x & 31;
+  __shared__ uint16_t sw[kBfCount];  // the bf16 weights, staged with coalesced loads
+  const int lane = threadIdx.x;
+  if (params) {
+    for (int i = threadIdx.x; i < kBfCount; i += blockDim.x) sw[i] = w[i];
+  }
   if (lane == 0) {
     const long long ops = ni + nd;
     const long long n = gc->n, m = gc->m;
@@ -316,14 +320,33 @@ __global__ void k_infer_schedule(const float* params, const uint16_t* w, FeatNor
     f[10] = lg(static_cast<double>(abs(fmax)));
     f[11] = lg(static_cast<double>(h.iterations));
   }
-  __syncwarp();
+  __syncthreads();
   if (lane < kMlpIn) c->features[lane] = f[lane];
   if (!params) {
     if (lane < 3) c->sched_classes[lane] = -1;
     return;
   }
-  load_features(f, nrm, xs);
-  warp_forward(params, w, xs, h1, h2, lo);
+  // the MLP with one thread per output, in the arithmetic (and order) of warp_forward
+  if (lane < kMlpIn) xs[lane] = round_bf((f[lane] - nrm.mean[lane]) * nrm.scale[lane]);
+  __syncthreads();
+  if (lane < kMlpHidden) {
+    float acc = params[kOffB1 + lane];
+    for (int i = 0; i < kMlpIn; ++i) acc = fmaf(bf(sw[kBfW1 + lane * kMlpIn + i]), xs[i], acc);
+    h1[lane] = round_bf(fmaxf(acc, 0.0f));
+  }
+  __syncthreads();
+  if (lane < kMlpHidden) {
+    float acc = params[kOffB2 + lane];
+    for (int i = 0; i < kMlpHidden; ++i) acc = fmaf(bf(sw[kBfW2 + lane * kMlpHidden + i]), h1[i], acc);
+    h2[lane] = round_bf(fmaxf(acc, 0.0f));
+  }
+  __syncthreads();
+  if (lane < kMlpOut) {
+    float acc = params[kOffB3 + lane];
+    for (int i = 0; i < kMlpHidden; ++i) acc = fmaf(bf(sw[kBfW3 + lane * kMlpHidden + i]), h2[i], acc);
+    lo[lane] = acc;
+  }
+  __syncthreads();
   if (lane == 0) {
     int cls[3];
     for (int head = 0; head < 3; ++head) {
@@ -558,7 +581,7 @@ void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch&
   const int blocks = ctx.update_blocks_per_sm * ctx.sm_count;
   FeatNorm nrm{};
   if (sch) nrm = norm_of(*sch);
-  k_infer_schedule<<<1, 32, 0, s>>>(sch ? sch->params.ptr : nullptr,
+  k_infer_schedule<<<1, 128, 0, s>>>(sch ? sch->params.ptr : nullptr,
                                     sch ? sch->wbf16.ptr : nullptr, nrm, c, t.hist.ptr,
                                     g.counters.ptr, b.ni, b.nd, blocks);
   ++ctx.launches;
