@@ -1574,7 +1574,39 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
   const long long m = g.m;
   const long long garbage = static_cast<long long>(
       std::max(g.host_counters.out_garbage, g.host_counters.in_garbage));
-  const bool compact = garbage > m / 2 + 1024 || need_out > g.arena_cap || need_in > g.arena_cap;
+  const bool compact = garbage > m / 2 + 1024;
+  if (!compact && (need_out > g.arena_cap || need_in > g.arena_cap)) {
+    // more arena on the device: the used part of each column copied to a 1.5x larger arena at
+    // the same slot offsets (row descriptors and the edge index stay valid)
+    const long long top = static_cast<long long>(std::max(g.host_counters.out_top,
+                                                          g.host_counters.in_top));
+    const long long new_cap = std::max(std::max(need_out, need_in) + (need_out + need_in) / 4,
+                                       g.arena_cap + g.arena_cap / 2);
+    expects(new_cap < (1LL << 32), "graph: the slack arena would pass 2^32 slots",
+            DYNGB200_CAPACITY);
+    const size_t k = static_cast<size_t>(g.k > 0 ? g.k : 1);
+    for (DevBuf<int32_t>* d : {&g.out_col, &g.in_col}) {
+      DevBuf<int32_t> fresh;
+      fresh.reserve(static_cast<size_t>(new_cap));
+      DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, static_cast<size_t>(top) * sizeof(int32_t),
+                                    cudaMemcpyDeviceToDevice, ctx.stream));
+      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+      std::swap(d->ptr, fresh.ptr);
+      std::swap(d->count, fresh.count);
+    }
+    for (DevBuf<int32_t>* d : {&g.out_w, &g.in_w}) {
+      DevBuf<int32_t> fresh;
+      fresh.reserve(static_cast<size_t>(new_cap) * k);
+      for (size_t j = 0; j < k; ++j)
+        DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr + j * new_cap, d->ptr + j * g.arena_cap,
+                                      static_cast<size_t>(top) * sizeof(int32_t),
+                                      cudaMemcpyDeviceToDevice, ctx.stream));
+      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+      std::swap(d->ptr, fresh.ptr);
+      std::swap(d->count, fresh.count);
+    }
+    g.arena_cap = new_cap;
+  }
   if (compact) {
     // rebuild from the exported CSR (append order is storage order, so it is kept)
     std::vector<int64_t> rp(static_cast<size_t>(n) + 1);

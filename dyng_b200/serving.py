@@ -159,6 +159,8 @@ def summarize(done, wall, rate):
     return {"rate": rate, "requests": len(done), "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
             "p99_over_p50": float(np.percentile(lat, 99) / max(np.percentile(lat, 50), 1e-9)),
+            "max_ms": float(lat.max()),
+            "service_max_ms": float(max(d[5] for d in done)),
             "changed_edges_per_s": changes / wall,
             "mean_group": float(np.mean([d[4] for d in done])),
             "parts_p50_ms": {k: float(np.percentile([d[i] for d in done], 50))

@@ -296,6 +296,30 @@ def test_large_frontiers_match_the_oracle():
     assert max(light for light, _, _ in st.trace) >= 8192
 
 
+def test_arena_growth_and_compaction_keep_results():
+    # batches far larger than the slack rows: the arenas grow on the device (and, after heavy
+    # churn, the graph is compacted); every step equals the oracle, and the exported CSR too
+    rng = np.random.default_rng(21)
+    n, s, d, w = random_graph(rng, "sparse", 2000)
+    g = D.Graph.from_edges(s, d, w, num_vertices=n)
+    og = O.Graph.from_edges(n, s, d, w, 1)
+    t = D.sssp.compute(g, 0)
+    ot, _ = O.compute(og, 0, rule=1)
+    for step in range(6):
+        b = random_batch(rng, n, s, d, 40000 if step % 2 == 0 else 30000, tree_parents=ot.parents)
+        D.sssp.update(g, _batch(b["ins_src"], b["ins_dst"], b["ins_w"], b["del_src"],
+                                b["del_dst"]), t)
+        O.update(og, _obatch(b["ins_src"], b["ins_dst"], b["ins_w"], b["del_src"],
+                             b["del_dst"]), ot)
+        np.testing.assert_array_equal(t.distances, ot.distances, err_msg=f"step {step}")
+        np.testing.assert_array_equal(t.parents, ot.parents, err_msg=f"step {step}")
+    csr = g.to_csr()
+    want = og.to_csr()
+    np.testing.assert_array_equal(csr.row_ptr, want["row_ptr"])
+    np.testing.assert_array_equal(csr.col_ind, want["col"])
+    np.testing.assert_array_equal(csr.weights.reshape(-1), want["w"].reshape(-1))
+
+
 def test_schedules_never_change_results():
     # sssp::options::delta and the schedule are tunables (sssp.hpp:78-94): every schedule gives
     # the same bytes as the oracle
