@@ -80,12 +80,20 @@ class ServerConfig(ctypes.Structure):
 class RequestTimes(ctypes.Structure):
     _fields_ = [("queued_ms", ctypes.c_double), ("service_ms", ctypes.c_double),
                 ("total_ms", ctypes.c_double), ("group_size", ctypes.c_int32),
-                ("begin_ms", ctypes.c_double), ("round_ms", ctypes.c_double)]
+                ("begin_ms", ctypes.c_double), ("round_ms", ctypes.c_double),
+                ("copy_ms", ctypes.c_double)]
+
+
+class GraphStorage(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "vertex_capacity", "arena_slots", "out_top", "in_top", "out_garbage", "in_garbage",
+        "index_slots", "arena_growths", "compactions", "index_builds")] + [
+        (n, ctypes.c_double) for n in ("grow_ms", "compact_ms", "index_ms", "maintenance_ms_max")]
 
 
 class ServerInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "failed", "rounds",
-                                              "max_group", "waiting")]
+                                              "max_group", "waiting", "admission_us_max")]
 
 
 # Every symbol of include/dyngb200.h with (restype, argtypes).
@@ -114,6 +122,7 @@ SIGNATURES = {
     "dyngb200_graph_to_csr": (ctypes.c_int, [c_void_p, c_void_p, c_i64p, c_i32p, c_i32p, c_i64p,
                                              c_i32p, c_i32p]),
     "dyngb200_graph_device_bytes": (ctypes.c_int, [c_void_p, c_i64p]),
+    "dyngb200_graph_storage_get": (ctypes.c_int, [c_void_p, ctypes.POINTER(GraphStorage)]),
     "dyngb200_sssp_compute": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32,
                                              ctypes.POINTER(Options), ctypes.POINTER(c_void_p),
                                              ctypes.POINTER(Stats)]),

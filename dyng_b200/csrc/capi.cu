@@ -65,19 +65,6 @@ using namespace dyngb200;
 
 std::atomic<uint64_t> g_next_graph_id{1};
 
-struct DeviceGuard {
-  int prev = 0;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = 0;
-    cudaGetDevice(&cur);
-    if (cur != prev) cudaSetDevice(prev);
-  }
-};
-
 // Copy n elements of an array in `memory` to a host vector.
 template <typename T>
 std::vector<T> to_host(Context& ctx, const T* p, size_t n, int memory) {
@@ -400,6 +387,27 @@ dyngb200_status dyngb200_graph_device_bytes(dyngb200_graph g, int64_t* bytes) {
     const Graph& x = g->g;
     const long long k = x.k;
     *bytes = 2 * (x.n_cap * (8 + 4 + 4) + x.arena_cap * (4 + 4 * k)) + 16 * x.ecap;
+  });
+}
+
+dyngb200_status dyngb200_graph_storage_get(dyngb200_graph g, dyngb200_graph_storage* out) {
+  return guarded([&] {
+    expects(g && out, "graph_storage_get: null argument");
+    const Graph& x = g->g;
+    out->vertex_capacity = x.n_cap;
+    out->arena_slots = x.arena_cap;
+    out->out_top = static_cast<int64_t>(x.host_counters.out_top);
+    out->in_top = static_cast<int64_t>(x.host_counters.in_top);
+    out->out_garbage = static_cast<int64_t>(x.host_counters.out_garbage);
+    out->in_garbage = static_cast<int64_t>(x.host_counters.in_garbage);
+    out->index_slots = x.props.allow_multi ? 0 : x.ecap;
+    out->arena_growths = x.arena_growths;
+    out->compactions = x.compactions;
+    out->index_builds = x.index_builds;
+    out->grow_ms = x.grow_ms;
+    out->compact_ms = x.compact_ms;
+    out->index_ms = x.index_ms;
+    out->maintenance_ms_max = x.maintenance_ms_max;
   });
 }
 

@@ -19,7 +19,10 @@
 // insertion, so the pairs are grouped by a hash table instead of rebuilding rows in batch order.
 #include "internal.hpp"
 
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -1066,18 +1069,22 @@ __global__ void k_index_clear(GraphView g) {
     g.ekey[i] = kKeyEmpty;
 }
 
+// One warp per row, the lanes over its slots: hub rows (tens of thousands of slots in R-MAT
+// graphs) do not serialise one thread.
 __global__ void k_index_out(GraphView g, long long n, unsigned* error) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
   long long live = 0;
-  for (long long u = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; u < n;
-       u += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long u = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < n;
+       u += warps) {
     const RowDesc d = g.out_desc[u];
-    for (int e = 0; e < d.len; ++e) {
+    for (int e = lane; e < d.len; e += 32) {
       const int32_t x = g.out_col[d.start + e];
       if (x < 0) continue;
       bool reused = false;
       const long long ie = index_insert(g, edge_key(static_cast<int32_t>(u), x), &reused);
       if (ie < 0) {
-        atomicOr(error, kErrCapacity);
+        atomicOr(error, kErrCapacity);  // a full table: the build fails, no other walk needed
         return;
       }
       g.eout[ie] = d.start + e;
@@ -1089,10 +1096,12 @@ __global__ void k_index_out(GraphView g, long long n, unsigned* error) {
 }
 
 __global__ void k_index_in(GraphView g, long long n, unsigned* error) {
-  for (long long v = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; v < n;
-       v += static_cast<long long>(gridDim.x) * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+  for (long long v = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
+       v += warps) {
     const RowDesc d = g.in_desc[v];
-    for (int e = 0; e < d.len; ++e) {
+    for (int e = lane; e < d.len; e += 32) {
       const int32_t y = g.in_col[d.start + e];
       if (y < 0) continue;
       const long long ie = index_find(g, edge_key(y, static_cast<int32_t>(v)));
@@ -1101,6 +1110,63 @@ __global__ void k_index_in(GraphView g, long long n, unsigned* error) {
         return;
       }
       g.ein[ie] = d.start + e;
+    }
+  }
+}
+
+// Compaction of one side, on the device: the live slots of every row (col >= 0), in storage
+// order, packed into a fresh arena with new slack (slack_cap of the live length).  One warp per
+// row; the row descriptors are rewritten in place by the warp that read them.
+__device__ __forceinline__ long long row_slack(long long len, double headroom) {
+  if (len <= 0) return 0;
+  long long extra = static_cast<long long>(ceil(static_cast<double>(len) * headroom));
+  if (extra < 4) extra = 4;
+  return (len + extra + 3) & ~3LL;
+}
+
+__global__ void k_compact_count(const RowDesc* desc, const int32_t* col, long long n,
+                                double headroom, long long* cap) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+  for (long long v = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
+       v += warps) {
+    const RowDesc d = desc[v];
+    int live = 0;
+    for (int e = lane; e < d.len; e += 32) live += col[d.start + e] >= 0;
+    for (int o = 16; o > 0; o >>= 1) live += __shfl_down_sync(0xffffffffu, live, o);
+    if (lane == 0) cap[v] = row_slack(live, headroom);
+  }
+}
+
+__global__ void k_compact_copy(RowDesc* desc, int32_t* cap_out, int32_t* dead,
+                               const int32_t* col, const int32_t* w, long long old_arena,
+                               const long long* start, int32_t* ncol, int32_t* nw,
+                               long long new_arena, int k, long long n) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+  for (long long v = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n;
+       v += warps) {
+    const RowDesc d = desc[v];
+    const long long to = start[v];
+    int at = 0;
+    for (int e0 = 0; e0 < d.len; e0 += 32) {
+      const int e = e0 + lane;
+      const int32_t x = e < d.len ? col[d.start + e] : kDead;
+      const unsigned live = __ballot_sync(0xffffffffu, x >= 0);
+      if (x >= 0) {
+        const long long dst = to + at + __popc(live & below);
+        ncol[dst] = x;
+        for (int j = 0; j < k; ++j)
+          nw[j * new_arena + dst] = w[j * old_arena + d.start + e];
+      }
+      at += __popc(live);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      desc[v] = RowDesc{static_cast<uint32_t>(to), at};
+      cap_out[v] = static_cast<int32_t>(start[v + 1] - to);
+      dead[v] = 0;
     }
   }
 }
@@ -1429,11 +1495,30 @@ void graph_build(Context& ctx, Graph& g, long long n, const int64_t* row_ptr, co
   if (!g.props.allow_multi) graph_index_build(ctx, g, 0);
 }
 
-// (Re)build the edge index with room for `extra` more edges.
-void graph_index_build(Context& ctx, Graph& g, long long extra) {
+namespace {
+// Host time of one storage maintenance step (growth, compaction, index build), added to the
+// graph's totals when it ends.
+struct MaintenanceTimer {
+  Graph& g;
+  double& total;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  MaintenanceTimer(Graph& graph, double& sum) : g(graph), total(sum) {}
+  ~MaintenanceTimer() {
+    const double ms = std::chrono::duration<double, std::milli>(
+                          std::chrono::steady_clock::now() - t0).count();
+    total += ms;
+    g.maintenance_ms_max = std::max(g.maintenance_ms_max, ms);
+  }
+};
+}  // namespace
+
+// (Re)build the edge index with room for `extra` more edges and at least `min_cap` slots.
+void graph_index_build(Context& ctx, Graph& g, long long extra, long long min_cap) {
+  MaintenanceTimer timer(g, g.index_ms);
+  ++g.index_builds;
   cudaStream_t s = ctx.stream;
   long long want = 1024;
-  while (want < 2 * (g.host_counters.m + extra) + 65536) want <<= 1;
+  while (want < 2 * (g.host_counters.m + extra) + 65536 || want < min_cap) want <<= 1;
   if (want != g.ecap) {
     g.ekey.release();
     g.eout.release();
@@ -1566,8 +1651,80 @@ void graph_export(Context& ctx, Graph& g, int64_t* row_ptr, int32_t* col, int32_
   }
 }
 
-// Grow the vertex capacity and/or the arenas.  Heavily fragmented arenas are compacted instead
-// (a rebuild through the host layout).
+// Compaction on the device: both sides packed into fresh arenas sized for the live slots plus
+// the demand of the batch that ran out of room (need_* = the tops that batch reached), then the
+// edge index rebuilt over the new slot positions.  Storage order inside every row is kept.
+void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in) {
+  MaintenanceTimer timer(g, g.compact_ms);
+  cudaStream_t s = ctx.stream;
+  const long long n = g.n;
+  const int k = g.k > 0 ? g.k : 1;
+  const int grid = ctx.sm_count * 8;
+  DevBuf<long long> cap, start;
+  cap.reserve(static_cast<size_t>(n) + 1);
+  start.reserve(static_cast<size_t>(n) + 1);
+  long long top[2] = {0, 0};
+  size_t temp_bytes = 0;
+  DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
+  DevBuf<unsigned char> temp;
+  temp.reserve(temp_bytes);
+  const long long demand[2] = {
+      std::max(0LL, need_out - static_cast<long long>(g.host_counters.out_top)),
+      std::max(0LL, need_in - static_cast<long long>(g.host_counters.in_top))};
+  // pass 1: the new tops of both sides decide the one arena size the sides share
+  for (int side = 0; side < 2; ++side) {
+    DYNGB200_CUDA(cudaMemsetAsync(cap.ptr + n, 0, sizeof(long long), s));
+    ctx.launches += 1;
+    k_compact_count<<<grid, kBlock, 0, s>>>((side == 0 ? g.out_desc : g.in_desc).ptr,
+                                            (side == 0 ? g.out_col : g.in_col).ptr, n,
+                                            g.props.headroom, cap.ptr);
+    DYNGB200_CUDA(cudaGetLastError());
+    DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(temp.ptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
+    DYNGB200_CUDA(cudaMemcpyAsync(&top[side], start.ptr + n, sizeof(long long),
+                                  cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+  }
+  long long base = std::max(top[0] + demand[0], top[1] + demand[1]);
+  const long long arena = round4(base + std::max(base / 2, 1LL << 16));
+  expects(arena < 0xffffffffLL, "graph: the slack arena exceeds 2^32 slots", DYNGB200_CAPACITY);
+  // pass 2: side by side, so that one old and one new arena are held at a time
+  for (int side = 0; side < 2; ++side) {
+    DevBuf<int32_t>& col = side == 0 ? g.out_col : g.in_col;
+    DevBuf<int32_t>& w = side == 0 ? g.out_w : g.in_w;
+    RowDesc* desc = (side == 0 ? g.out_desc : g.in_desc).ptr;
+    DYNGB200_CUDA(cudaMemsetAsync(cap.ptr + n, 0, sizeof(long long), s));
+    ctx.launches += 2;
+    k_compact_count<<<grid, kBlock, 0, s>>>(desc, col.ptr, n, g.props.headroom, cap.ptr);
+    DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(temp.ptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
+    DevBuf<int32_t> ncol, nw;
+    ncol.reserve(static_cast<size_t>(arena));
+    nw.reserve(static_cast<size_t>(arena) * static_cast<size_t>(k));
+    DYNGB200_CUDA(cudaMemsetAsync(ncol.ptr, 0xff, static_cast<size_t>(arena) * sizeof(int32_t), s));
+    k_compact_copy<<<grid, kBlock, 0, s>>>(desc, (side == 0 ? g.out_cap : g.in_cap).ptr,
+                                           (side == 0 ? g.out_dead : g.in_dead).ptr, col.ptr,
+                                           w.ptr, g.arena_cap, start.ptr, ncol.ptr, nw.ptr, arena,
+                                           g.k, n);
+    DYNGB200_CUDA(cudaGetLastError());
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    col.swap(ncol);
+    w.swap(nw);
+  }
+  g.arena_cap = arena;
+  ++g.compactions;
+  GraphCounters& gc = g.host_counters;
+  gc.out_top = static_cast<u64>(top[0]);
+  gc.in_top = static_cast<u64>(top[1]);
+  gc.out_garbage = gc.in_garbage = 0;
+  gc.dead_out = gc.dead_in = 0;
+  if (!g.props.allow_multi) {
+    graph_index_build(ctx, g, 0, g.ecap);  // same room as before; uploads the counters too
+  } else {
+    DYNGB200_CUDA(cudaMemcpyAsync(g.counters.ptr, &gc, sizeof(gc), cudaMemcpyHostToDevice, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
+// Grow the vertex capacity and/or the arenas.  Heavily fragmented arenas are compacted instead.
 void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, long long need_in) {
   graph_refresh_host(ctx, g);
   const long long n = g.n;
@@ -1576,12 +1733,15 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
       std::max(g.host_counters.out_garbage, g.host_counters.in_garbage));
   const bool compact = garbage > m / 2 + 1024;
   if (!compact && (need_out > g.arena_cap || need_in > g.arena_cap)) {
+    MaintenanceTimer timer(g, g.grow_ms);
     // more arena on the device: the used part of each column copied to a 1.5x larger arena at
     // the same slot offsets (row descriptors and the edge index stay valid)
     const long long top = static_cast<long long>(std::max(g.host_counters.out_top,
                                                           g.host_counters.in_top));
-    const long long new_cap = std::max(std::max(need_out, need_in) + (need_out + need_in) / 4,
-                                       g.arena_cap + g.arena_cap / 2);
+    // a multiple of 4 slots: weight column j starts at j * arena_cap, and rows are read with
+    // 16-byte loads
+    const long long new_cap = round4(std::max(
+        std::max(need_out, need_in) + (need_out + need_in) / 4, g.arena_cap + g.arena_cap / 2));
     expects(new_cap < (1LL << 32), "graph: the slack arena would pass 2^32 slots",
             DYNGB200_CAPACITY);
     const size_t k = static_cast<size_t>(g.k > 0 ? g.k : 1);
@@ -1591,8 +1751,7 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
       DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, static_cast<size_t>(top) * sizeof(int32_t),
                                     cudaMemcpyDeviceToDevice, ctx.stream));
       DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      std::swap(d->ptr, fresh.ptr);
-      std::swap(d->count, fresh.count);
+      d->swap(fresh);
     }
     for (DevBuf<int32_t>* d : {&g.out_w, &g.in_w}) {
       DevBuf<int32_t> fresh;
@@ -1602,37 +1761,12 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
                                       static_cast<size_t>(top) * sizeof(int32_t),
                                       cudaMemcpyDeviceToDevice, ctx.stream));
       DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      std::swap(d->ptr, fresh.ptr);
-      std::swap(d->count, fresh.count);
+      d->swap(fresh);
     }
     g.arena_cap = new_cap;
+    ++g.arena_growths;
   }
-  if (compact) {
-    // rebuild from the exported CSR (append order is storage order, so it is kept)
-    std::vector<int64_t> rp(static_cast<size_t>(n) + 1);
-    std::vector<int32_t> col(static_cast<size_t>(m)), w(static_cast<size_t>(m) * g.k);
-    // export in storage order: temporarily pretend append order
-    const int sorted = g.props.sorted;
-    g.props.sorted = 0;
-    graph_export(ctx, g, rp.data(), col.data(), w.data(), nullptr, nullptr, nullptr);
-    g.props.sorted = sorted;
-    // keep the in-mirror's relative order: rebuild it by transposition (stable per source)
-    const long long keep_n = std::max(n, need_n);
-    std::vector<int64_t> rp2(static_cast<size_t>(keep_n) + 1, rp[n]);
-    std::copy(rp.begin(), rp.end(), rp2.begin());
-    graph_build(ctx, g, keep_n, rp2.data(), col.data(), w.data(), m);
-    g.n = n;
-    GraphCounters gc = g.host_counters;
-    gc.n = n;
-    DYNGB200_CUDA(cudaMemcpyAsync(g.counters.ptr, &gc, sizeof(gc), cudaMemcpyHostToDevice,
-                                  ctx.stream));
-    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-    g.host_counters = gc;
-    if (need_n > g.n_cap) {
-      // graph_build sized n_cap from keep_n already
-    }
-    return;
-  }
+  if (compact) graph_compact(ctx, g, need_out, need_in);
   if (need_n > g.n_cap) {
     const long long new_cap = std::max(need_n + 1024, g.n_cap * 2);
     for (DevBuf<RowDesc>* d : {&g.out_desc, &g.in_desc}) {
@@ -1642,8 +1776,7 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
       DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, g.n_cap * sizeof(RowDesc),
                                     cudaMemcpyDeviceToDevice, ctx.stream));
       DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      std::swap(d->ptr, fresh.ptr);
-      std::swap(d->count, fresh.count);
+      d->swap(fresh);
     }
     for (DevBuf<int32_t>* d : {&g.out_cap, &g.in_cap, &g.out_dead, &g.in_dead}) {
       DevBuf<int32_t> fresh;
@@ -1652,8 +1785,7 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
       DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, g.n_cap * sizeof(int32_t),
                                     cudaMemcpyDeviceToDevice, ctx.stream));
       DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      std::swap(d->ptr, fresh.ptr);
-      std::swap(d->count, fresh.count);
+      d->swap(fresh);
     }
     g.n_cap = new_cap;
   }

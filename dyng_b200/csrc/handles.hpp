@@ -26,6 +26,20 @@ namespace dyngb200 {
 void expect_tree_current(const Graph& g, const Tree& t, const char* what);
 // Sizes, weight count and array pointers of a batch.
 void expect_batch(const Graph& g, const dyngb200_batch& b, const char* what);
+// Makes `dev` the calling thread's current device for a scope.
+struct DeviceGuard {
+  int prev = 0;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != prev) cudaSetDevice(prev);
+  }
+};
+
 // Context set-up: device attributes and the stream (a caller's stream, or one of its own).
 void context_init(Context& c, int device, void* stream);
 

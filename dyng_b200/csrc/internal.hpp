@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dyngb200.h"
@@ -40,32 +41,51 @@ inline void expects(bool ok, const std::string& msg,
   if (!ok) throw Error(s, msg);
 }
 
+// memory.cu: device memory from a per-device pool that keeps freed memory (cudaMalloc /
+// cudaFree semantics otherwise: a free waits for the device first).
+void* device_alloc(size_t bytes, int* device);
+void device_free(void* p, int device) noexcept;
+void device_pool_reserve(size_t bytes);        // pre-fill the current device's pool
+long long device_pool_idle_bytes(int device);  // pooled bytes not in use
+
 // A device buffer that grows on demand (contents are not preserved unless asked).
 template <typename T>
 struct DevBuf {
   T* ptr = nullptr;
   size_t count = 0;
+  int dev = 0;  // the device of ptr
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
+  void swap(DevBuf& o) noexcept {
+    std::swap(ptr, o.ptr);
+    std::swap(count, o.count);
+    std::swap(dev, o.dev);
+  }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) device_free(ptr, dev);
     ptr = nullptr;
     count = 0;
   }
   // Ensure room for n elements; keeps the first `keep` elements when it reallocates.
   void reserve(size_t n, cudaStream_t stream = 0, size_t keep = 0) {
     if (n <= count) return;
-    T* fresh = nullptr;
-    DYNGB200_CUDA(cudaMalloc(&fresh, (n ? n : 1) * sizeof(T)));
+    int d = 0;
+    T* fresh = static_cast<T*>(device_alloc((n ? n : 1) * sizeof(T), &d));
     if (ptr && keep) {
-      DYNGB200_CUDA(cudaMemcpyAsync(fresh, ptr, keep * sizeof(T), cudaMemcpyDeviceToDevice, stream));
-      DYNGB200_CUDA(cudaStreamSynchronize(stream));
+      const cudaError_t e = cudaMemcpyAsync(fresh, ptr, keep * sizeof(T), cudaMemcpyDeviceToDevice,
+                                            stream);
+      const cudaError_t e2 = e == cudaSuccess ? cudaStreamSynchronize(stream) : e;
+      if (e2 != cudaSuccess) {
+        device_free(fresh, d);
+        DYNGB200_CUDA(e2);
+      }
     }
-    if (ptr) cudaFree(ptr);
+    if (ptr) device_free(ptr, dev);
     ptr = fresh;
     count = n;
+    dev = d;
   }
 };
 
@@ -221,6 +241,8 @@ struct Graph {
   int k = 1;
   long long n = 0, m = 0;  // host mirrors after the last completed call
   long long n_cap = 0, arena_cap = 0;
+  long long arena_growths = 0, compactions = 0, index_builds = 0;
+  double grow_ms = 0, compact_ms = 0, index_ms = 0, maintenance_ms_max = 0;
   DevBuf<RowDesc> out_desc, in_desc;
   DevBuf<int32_t> out_cap, in_cap, out_dead, in_dead;
   DevBuf<int32_t> out_col, in_col;
@@ -238,6 +260,9 @@ struct Graph {
   int device = 0;
 
   GraphView view() {
+    // the kernels read rows with 16-byte loads: every weight column must start aligned
+    expects(arena_cap % 4 == 0, "graph: the arena size is not a multiple of 4 slots",
+            DYNGB200_INTERNAL);
     GraphView v{};
     v.out_desc = out_desc.ptr;
     v.out_cap = out_cap.ptr;
@@ -335,7 +360,7 @@ void graph_export(Context& ctx, Graph& g, int64_t* row_ptr, int32_t* col, int32_
 void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_arena_out,
                 long long need_arena_in);
 void graph_rescan_columns(Context& ctx, Graph& g);
-void graph_index_build(Context& ctx, Graph& g, long long extra);
+void graph_index_build(Context& ctx, Graph& g, long long extra, long long min_cap = 0);
 void graph_index_reserve(Context& ctx, Graph& g, long long inserts);
 void graph_refresh_host(Context& ctx, Graph& g);
 void graph_copy(Context& ctx, Graph& dst, const Graph& src);

@@ -40,7 +40,7 @@ struct ServerRequest {
   std::unique_ptr<HostBuf<int32_t>> data;  // pinned copy of the batch's five arrays
   dyngb200_batch batch{};
   long long ops = 0;
-  Clock::time_point arrival, start, begun, synced, finish;
+  Clock::time_point arrival, ready, start, begun, synced, finish;
   int group_size = 0;
   bool done = false;
   dyngb200_status status = DYNGB200_OK;
@@ -67,6 +67,7 @@ class Server {
 
  private:
   void run();
+  void monitor();
   void dispatch(std::vector<ServerRequest*>& group);
   long long estimate_bytes(const ServerGraph& sg, const ServerRequest& r) const;
   std::unique_ptr<HostBuf<int32_t>> take_buffer(size_t n);
@@ -81,6 +82,10 @@ class Server {
   std::mutex mu_;
   std::condition_variable work_cv_, done_cv_;
   std::thread worker_;
+  std::thread monitor_;  // samples the free device memory for admission (off the dispatcher)
+  std::condition_variable monitor_cv_;
+  long long free_sample_ = -1;   // bytes free at the last sample (-1: none)
+  long long admitted_since_ = 0; // scratch estimates admitted after that sample
   bool stop_ = false;
   uint64_t next_ticket_ = 1;
   size_t next_graph_ = 0;  // round-robin start
@@ -114,7 +119,36 @@ Server::Server(const dyngb200_server_config& cfg, const Scheduler* learned)
           "server: the scheduler belongs to another device");
   DYNGB200_CUDA(cudaSetDevice(cfg_.device));
   DYNGB200_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  size_t free_b = 0, total_b = 0;
+  DYNGB200_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  free_sample_ = static_cast<long long>(free_b);
   worker_ = std::thread([this] { run(); });
+  monitor_ = std::thread([this] { monitor(); });
+}
+
+// The free-memory query can take tens of milliseconds on a busy machine: it runs here, every
+// kMonitorMs, and the dispatcher reads the last sample minus what it admitted since.
+void Server::monitor() {
+  cudaSetDevice(cfg_.device);
+  constexpr int kMonitorMs = 20;
+  std::unique_lock<std::mutex> lk(mu_);
+  while (!stop_) {
+    monitor_cv_.wait_for(lk, std::chrono::milliseconds(kMonitorMs), [&] { return stop_; });
+    if (stop_) break;
+    lk.unlock();
+    size_t free_b = 0, total_b = 0;
+    const Clock::time_point q0 = Clock::now();
+    const bool ok = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
+    const long long pooled = device_pool_idle_bytes(cfg_.device);  // free to the library too
+    const long long us =
+        std::chrono::duration_cast<std::chrono::microseconds>(Clock::now() - q0).count();
+    lk.lock();
+    info_.admission_us_max = std::max<long long>(info_.admission_us_max, us);
+    if (ok) {
+      free_sample_ = static_cast<long long>(free_b) + pooled;
+      admitted_since_ = 0;
+    }
+  }
 }
 
 Server::~Server() {
@@ -123,13 +157,16 @@ Server::~Server() {
     stop_ = true;
   }
   work_cv_.notify_all();
+  monitor_cv_.notify_all();
   if (worker_.joinable()) worker_.join();
+  if (monitor_.joinable()) monitor_.join();
   graphs_.clear();
   if (stream_) cudaStreamDestroy(stream_);
 }
 
 int Server::add_graph(Graph& g, Tree& t) {
   expects(g.device == cfg_.device, "server::add_graph: the graph belongs to another device");
+  DeviceGuard guard(cfg_.device);
   expect_tree_current(g, t, "server::add_graph");
   auto sg = std::make_unique<ServerGraph>();
   sg->ctx = std::make_unique<Context>();
@@ -146,6 +183,12 @@ int Server::add_graph(Graph& g, Tree& t) {
                     std::to_string(free_b) + " free)");
   sg->ctx->ws.reserve_vertices(g.n_cap, stream_);
   DYNGB200_CUDA(cudaStreamSynchronize(stream_));
+  // room for the graph to grow (an index doubling, an arena growth) kept in the device pool, so
+  // that growth while serving does not wait for the driver
+  const long long graph_bytes =
+      2 * (g.n_cap * 16 + g.arena_cap * (4 + 4LL * g.k)) + 16 * g.ecap;
+  if (static_cast<long long>(free_b) - need - graph_bytes / 2 > 2 * cfg_.hbm_reserve_bytes)
+    device_pool_reserve(static_cast<size_t>(graph_bytes / 2));
   sg->g = &g;
   sg->t = &t;
   std::unique_lock<std::mutex> lk(mu_);
@@ -221,6 +264,7 @@ uint64_t Server::submit(int slot, const dyngb200_batch& b) {
     r->batch.delete_dst = put(b.delete_dst, nd);
     r->batch.memory = DYNGB200_HOST;
     r->ops = ni + nd;
+    r->ready = Clock::now();
     std::unique_lock<std::mutex> lk(mu_);
     expects(!stop_, "server::submit: the server is shutting down");
     r->ticket = next_ticket_++;
@@ -250,6 +294,7 @@ ServerRequest Server::wait(uint64_t ticket) {
   out.slot = r->slot;
   out.ops = r->ops;
   out.arrival = r->arrival;
+  out.ready = r->ready;
   out.start = r->start;
   out.begun = r->begun;
   out.synced = r->synced;
@@ -292,10 +337,8 @@ void Server::run() {
       std::unique_lock<std::mutex> lk(mu_);
       work_cv_.wait(lk, [&] { return stop_ || waiting_ > 0; });
       if (waiting_ == 0 && stop_) return;
-      size_t free_b = 0, total_b = 0;
-      long long free_left = -1;
-      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
-        free_left = static_cast<long long>(free_b) - cfg_.hbm_reserve_bytes;
+      const bool known = free_sample_ >= 0;
+      long long free_left = known ? free_sample_ - admitted_since_ - cfg_.hbm_reserve_bytes : 0;
       const size_t ng = graphs_.size();
       for (size_t step = 0; step < ng && static_cast<int>(group.size()) < cfg_.max_group; ++step) {
         const size_t gi = (next_graph_ + step) % ng;
@@ -308,7 +351,7 @@ void Server::run() {
         --waiting_;
         r->start = Clock::now();
         const long long need = estimate_bytes(sg, *r);
-        if (free_left >= 0 && need > free_left) {
+        if (known && need > free_left) {
           // admission: the batch's scratch does not fit beside the reserve; fail it, keep the rest
           r->status = DYNGB200_OUT_OF_MEMORY;
           r->message = "server: admission refused: the batch needs about " + std::to_string(need) +
@@ -322,7 +365,8 @@ void Server::run() {
           r->data.reset();
           continue;
         }
-        if (free_left >= 0) free_left -= need;
+        free_left -= need;
+        admitted_since_ += need;
         group.push_back(r);
         if (large) break;
       }
@@ -453,6 +497,7 @@ dyngb200_status dyngb200_server_wait(dyngb200_server s, uint64_t ticket, dyngb20
     const bool ran = r.synced.time_since_epoch().count() != 0;
     times->begin_ms = ran ? dyngb200::ms_between(r.start, r.begun) : 0.0;
     times->round_ms = ran ? dyngb200::ms_between(r.start, r.synced) : 0.0;
+    times->copy_ms = dyngb200::ms_between(r.arrival, r.ready);
   }
   dyngb200::last_error() = r.message;
   return r.status;

@@ -324,6 +324,12 @@ class Graph:
         check(N.lib().dyngb200_graph_device_bytes(self._h, ctypes.byref(b)))
         return b.value
 
+    def storage(self) -> dict:
+        """The slack-row storage: arena slots, tops, abandoned slots, growths, compactions."""
+        st = N.GraphStorage()
+        check(N.lib().dyngb200_graph_storage_get(self._h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in N.GraphStorage._fields_}
+
     def clone(self) -> "Graph":
         """A new graph with this graph's contents (results of this graph are not bound to it)."""
         h = ctypes.c_void_p()

@@ -61,7 +61,8 @@ class Server:
                                            ctypes.byref(tm)))
         return Stats._from_native(st), {"queued_ms": tm.queued_ms, "service_ms": tm.service_ms,
                                         "total_ms": tm.total_ms, "group_size": tm.group_size,
-                                        "begin_ms": tm.begin_ms, "round_ms": tm.round_ms}
+                                        "begin_ms": tm.begin_ms, "round_ms": tm.round_ms,
+                                        "copy_ms": tm.copy_ms}
 
     def drain(self) -> None:
         check(N.lib().dyngb200_server_drain(self._h))
@@ -131,7 +132,7 @@ def run_load(server, slots, pools, rate, seconds, rng, size_range=(100, 1_000_00
         for i, tk in enumerate(iter(tickets_q.get, None)):
             st, tm = server.wait(tk[0])
             done.append((tk[1], tk[2], tm["total_ms"], tm["queued_ms"], tm["group_size"],
-                         tm["service_ms"], tm["begin_ms"], tm["round_ms"]))
+                         tm["service_ms"], tm["begin_ms"], tm["round_ms"], tm["copy_ms"], tk[3]))
 
     import queue
     tickets_q = queue.Queue()
@@ -144,9 +145,10 @@ def run_load(server, slots, pools, rate, seconds, rng, size_range=(100, 1_000_00
         now = time.perf_counter()
         if due > now:
             time.sleep(due - now)
+        t_sub = time.perf_counter() - t0
         tk = server.submit(slots[targets[i]], batches[i])
         tickets.append(tk)
-        tickets_q.put((tk, int(targets[i]), int(sizes[i])))
+        tickets_q.put((tk, int(targets[i]), int(sizes[i]), t_sub))
     tickets_q.put(None)
     th.join()
     wall = time.perf_counter() - t0
@@ -164,11 +166,29 @@ def summarize(done, wall, rate):
             "changed_edges_per_s": changes / wall,
             "mean_group": float(np.mean([d[4] for d in done])),
             "parts_p50_ms": {k: float(np.percentile([d[i] for d in done], 50))
-                             for k, i in (("queued", 3), ("service", 5), ("begin", 6),
-                                          ("round", 7))},
+                             for k, i in PARTS},
             "parts_p99_ms": {k: float(np.percentile([d[i] for d in done], 99))
-                             for k, i in (("queued", 3), ("service", 5), ("begin", 6),
-                                          ("round", 7))}}
+                             for k, i in PARTS},
+            "by_size": by_size(done)}
+
+
+def by_size(done):
+    """p50 / p99 latency per decade of batch size (the load mixes 100 .. 1M changes, whose own
+    service times differ by 10x, so the overall p99 / p50 mostly measures the mix)."""
+    out = {}
+    for lo in (100, 1_000, 10_000, 100_000):
+        lat = [d[2] for d in done if lo <= d[1] < lo * 10 or (lo == 100_000 and d[1] >= lo)]
+        if lat:
+            out[f"{lo}+"] = {"n": len(lat), "p50_ms": float(np.percentile(lat, 50)),
+                             "p99_ms": float(np.percentile(lat, 99))}
+    return out
+
+
+STORAGE_KEYS = ("arena_growths", "compactions", "index_builds", "grow_ms", "compact_ms",
+                "index_ms", "maintenance_ms_max")
+PARTS = (("queued", 3), ("service", 5), ("begin", 6), ("round", 7), ("copy", 8))
+RECORD = ("graph", "changes", "total_ms", "queued_ms", "group_size", "service_ms", "begin_ms",
+          "round_ms", "copy_ms", "submitted_s")
 
 
 def main(argv=None):
@@ -183,6 +203,7 @@ def main(argv=None):
     ap.add_argument("--max-batch", type=int, default=1_000_000)
     ap.add_argument("--learned", default="", help="scheduler weights (.npz); empty: heuristic")
     ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--dump", default="", help="write every request's record to this .npz")
     a = ap.parse_args(argv)
     rng = np.random.default_rng(a.seed)
     res = Resources(0)
@@ -206,11 +227,17 @@ def main(argv=None):
         tickets = [server.submit(sl, pools[i].batch(rng, a.max_batch)) for i, sl in enumerate(slots)]
         for tk in tickets:
             server.wait(tk)
+    records = {}
     for rate in (float(r) for r in a.rates.split(",")):
         done, wall = run_load(server, slots, pools, rate, a.seconds, rng, (100, a.max_batch))
         out = summarize(done, wall, rate)
         out["info"] = server.info()
+        out["storage"] = [{k: round(v, 3) for k, v in g.storage().items()
+                           if k in STORAGE_KEYS} for g, _ in keep]
         print(json.dumps(out), flush=True)
+        records[f"rate{rate:g}"] = np.array(done, dtype=np.float64)
+    if a.dump:
+        np.savez(a.dump, fields=np.array(RECORD), **records)
     server.close()
 
 

@@ -208,6 +208,21 @@ dyngb200_status dyngb200_graph_to_csr(dyngb200_context ctx, dyngb200_graph g, in
                                       int32_t* in_col, int32_t* in_weights);
 /* Device memory held by the graph, in bytes. */
 dyngb200_status dyngb200_graph_device_bytes(dyngb200_graph g, int64_t* bytes);
+/* The slack-row storage behind a graph (no reference counterpart: the reference's CSR has no
+ * slack).  Figures as of the last completed call on the graph. */
+typedef struct dyngb200_graph_storage {
+  int64_t vertex_capacity;         /* rows allocated per side */
+  int64_t arena_slots;             /* slots of each side's arena */
+  int64_t out_top, in_top;         /* slots handed out (rows, their slack, abandoned space) */
+  int64_t out_garbage, in_garbage; /* slots abandoned by rows that moved */
+  int64_t index_slots;             /* edge index capacity (0 for multigraphs) */
+  int64_t arena_growths;           /* arena enlargements, done on the device */
+  int64_t compactions;             /* compactions, done on the device */
+  int64_t index_builds;            /* edge index (re)builds */
+  double grow_ms, compact_ms, index_ms; /* host time of the above, summed (includes the wait) */
+  double maintenance_ms_max;       /* the longest single growth, compaction or index build */
+} dyngb200_graph_storage;
+dyngb200_status dyngb200_graph_storage_get(dyngb200_graph g, dyngb200_graph_storage* out);
 
 /* ---- sssp (cpp/include/dyng/sssp.hpp:415-489) -------------------------------------------- */
 /* sssp::compute(resources::cuda(), g, source, opt) (sssp.hpp:415-421). opt may be NULL. */
@@ -322,6 +337,7 @@ typedef struct dyngb200_request_times {
   int32_t group_size; /* updates in the request's round */
   double begin_ms;    /* host time queuing this update's work (staging, launches) */
   double round_ms;    /* dispatch -> the round's work complete on the GPU */
+  double copy_ms;     /* inside submit: the batch copied into the server's pinned buffer */
 } dyngb200_request_times;
 typedef struct dyngb200_server_info {
   int64_t submitted;
@@ -330,6 +346,7 @@ typedef struct dyngb200_server_info {
   int64_t rounds;
   int64_t max_group;
   int64_t waiting;
+  int64_t admission_us_max; /* longest free-memory query (a helper thread's), microseconds */
 } dyngb200_server_info;
 /* learned: a scheduler used for every update (NULL: the fixed heuristic). */
 dyngb200_status dyngb200_server_create(const dyngb200_server_config* config,

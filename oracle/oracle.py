@@ -6,7 +6,8 @@ restatement of the reference, never as part of the product path.
 
 The oracle restates dynG's host path (cpp/src/graph/apply_host.cpp:57-518,
 cpp/src/algorithms/sssp/sequential.cpp:57-381, cpp/src/algorithms/sssp/sssp.cpp:136-165,
-377-460, 563-576, 643-689) in plain C.  Its parity with the reference is pinned by
+377-460, 563-576, 643-689) and mosp's finalize step (cpp/src/algorithms/mosp/sequential.cpp:33-232,
+mosp.cpp:108-131, 259-301) in plain C.  Its parity with the reference is pinned by
 tests/test_oracle.py against the reference's golden fixtures (tests/golden/).
 """
 from __future__ import annotations
@@ -138,6 +139,12 @@ def lib():
         L.orc_packs_parents.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
         L.orc_distances_fit.restype = ctypes.c_int
         L.orc_distances_fit.argtypes = [ctypes.c_int64, ctypes.c_int64]
+        L.orc_mosp_combine.restype = ctypes.c_int64
+        L.orc_mosp_combine.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int, _i32p, _i32p,
+                                       ctypes.c_int32, _i32p, _i32p, _i32p, _i64p]
+        L.orc_mosp_path_costs.restype = ctypes.c_int32
+        L.orc_mosp_path_costs.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int32, ctypes.c_int,
+                                          _i64p]
         _lib = L
     return _lib
 
@@ -330,3 +337,56 @@ def default_delta(m, n, weight_sum) -> int:
 
 def packs_parents(n, max_weight, rule=0) -> bool:
     return bool(lib().orc_packs_parents(n, max_weight, rule))
+
+
+def preference_scale(preferences, num_objectives: int) -> int:
+    """L = lcm(preferences), 1 for none (mosp.cpp:108-131); each >= 1, L <= 2^20."""
+    if not preferences:
+        return 1
+    if len(preferences) != num_objectives:
+        raise OracleError("one preference per objective")
+    scale = 1
+    for p in preferences:
+        if int(p) < 1:
+            raise OracleError("a preference must be >= 1")
+        scale = scale // np.gcd(scale, int(p)) * int(p)
+        if scale > 1 << 20:
+            raise OracleError("lcm(preferences) exceeds 2^20")
+    return int(scale)
+
+
+@dataclass
+class MospTree:
+    distances: np.ndarray   # combined distances, in units of 1/L
+    parents: np.ndarray     # the MOSP tree
+    costs: np.ndarray       # n x columns path costs (INF where unreachable)
+    combined_edges: int
+    scale: int
+
+
+def mosp_finalize(g: Graph, source: int, parents, preferences=None, cost_columns=None) -> MospTree:
+    """Steps 2-3 of MOSP_Update on K trees of g (mosp.cpp:259-301): the combined graph, its tree
+    (sssp::compute with lowest-id ties) and the path costs over the first `cost_columns` weight
+    columns (K by default)."""
+    K = len(parents)
+    n = g.n
+    L = preference_scale(preferences, K)
+    terms = np.asarray([L if not preferences else L // int(p) for p in (preferences or [1] * K)],
+                       np.int32)
+    base = int(L * (K + 1))
+    par = np.ascontiguousarray(np.stack([np.asarray(p, np.int32) for p in parents]))
+    cap = max(1, K * n)
+    src, dst, w = (np.zeros(cap, np.int32) for _ in range(3))
+    wsum = ctypes.c_int64(0)
+    m = int(lib().orc_mosp_combine(n, int(source), K, _p32(par), _p32(terms), base, _p32(src),
+                                   _p32(dst), _p32(w), ctypes.byref(wsum)))
+    cg = Graph.from_edges(n, src[:m], dst[:m], w[:m], 1)
+    tree, _ = compute(cg, int(source), rule=1)
+    C = K if cost_columns is None else int(cost_columns)
+    costs = np.zeros(max(1, n * C), np.int64)
+    missing = int(lib().orc_mosp_path_costs(g._h, _p32(tree.parents), int(source), C,
+                                            _p64(costs)))
+    if missing >= 0:
+        raise OracleError(f"the MOSP tree edge ({int(tree.parents[missing])}, {missing}) is not "
+                          "an edge of the graph")
+    return MospTree(tree.distances, tree.parents, costs[:n * C].reshape(n, C), m, L)

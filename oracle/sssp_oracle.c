@@ -23,10 +23,15 @@
  *                              (make_packing / choose_packing; selected with rule = 1)
  *   - canonicalize / validate  cpp/src/algorithms/sssp/sssp.cpp:377-460 (canonicalize_tree,
  *                              validate_tree_sequential), :571-599 (normalize_imported_tree)
+ *   - mosp's finalize step     cpp/src/algorithms/mosp/sequential.cpp:33-170 (combined_edge and
+ *                              the combined graph), :172-232 (mospPathCosts), mosp.cpp:259-301
+ *                              (preference terms and base weight); the combined graph is solved
+ *                              with the compute above
  *
  * Parity of this restatement is pinned by tests/test_oracle.py against the reference's own golden
- * fixtures (cpp/tests/data/mosp_sssp: 34 cases, and cpp/tests/data/mosp_graph_io: applied and
- * transposed CSR plus weight-increase masks), converted by tests/golden/make_golden.py.
+ * fixtures (cpp/tests/data/mosp_sssp: 34 cases, cpp/tests/data/mosp_graph_io: applied and
+ * transposed CSR plus weight-increase masks, cpp/tests/data/mosp_combined: 9 combined-graph
+ * cases), converted by tests/golden/make_golden.py.
  *
  * Errors are returned as negative status codes with a message in the caller's buffer; nothing
  * aborts.  All memory is owned by the orc_graph handle or by the caller.
@@ -1131,4 +1136,100 @@ int orc_validate_tree(const orc_graph* g, int32_t source, int k, const int64_t* 
     return ORC_INVALID_ARGUMENT;
   }
   return ORC_OK;
+}
+
+/* ---------------------------------------------------------------------------------------------
+ * mosp's finalize step (cpp/src/algorithms/mosp/sequential.cpp:33-170, mosp.cpp:259-301)
+ *
+ * The combined graph of K trees: edge (p, v) for every distinct parent p among
+ * parents[0][v] .. parents[K-1][v] (v != source), weighted
+ * base - sum over the trees i with parents[i][v] == p of terms[i]; base = L * (K + 1) and
+ * terms[i] = L / Pref_i.  The caller solves it with orc_sssp_compute (lowest-id ties).
+ * ------------------------------------------------------------------------------------------- */
+static int combined_edge(const int32_t* parents, int64_t n, int K, int64_t v, int k,
+                         const int32_t* terms, int32_t base, int32_t* p_out, int32_t* w_out) {
+  const int32_t p = parents[(size_t)k * (size_t)n + (size_t)v];
+  if (p < 0) return 0;
+  for (int j = 0; j < k; ++j)
+    if (parents[(size_t)j * (size_t)n + (size_t)v] == p) return 0; /* counted once, first */
+  int32_t w = base - terms[k];
+  for (int j = k + 1; j < K; ++j)
+    if (parents[(size_t)j * (size_t)n + (size_t)v] == p) w -= terms[j];
+  *p_out = p;
+  *w_out = w;
+  return 1;
+}
+
+/* Writes the combined edges (src, dst, w; room for K * n) in vertex-then-objective order and
+ * returns their number; *weight_sum receives the sum of their weights. */
+int64_t orc_mosp_combine(int64_t n, int32_t source, int K, const int32_t* parents,
+                         const int32_t* terms, int32_t base, int32_t* src, int32_t* dst,
+                         int32_t* w, int64_t* weight_sum) {
+  int64_t m = 0, sum = 0;
+  for (int64_t v = 0; v < n; ++v) {
+    if (v == source) continue;
+    for (int k = 0; k < K; ++k) {
+      int32_t p, wt;
+      if (!combined_edge(parents, n, K, v, k, terms, base, &p, &wt)) continue;
+      src[m] = p;
+      dst[m] = (int32_t)v;
+      w[m] = wt;
+      sum += wt;
+      ++m;
+    }
+  }
+  if (weight_sum) *weight_sum = sum;
+  return m;
+}
+
+/* mospPathCosts (sequential.cpp:172-232): the first `columns` objective values of the tree path
+ * to every vertex; the weights of tree edge (p, v) are those of the first edge p -> v in row
+ * order.  Traversal from the source over the tree's children lists; vertices it does not reach
+ * keep ORC_INF.  Returns -1, or the first vertex (in traversal order) whose tree edge is not an
+ * edge of the graph. */
+int32_t orc_mosp_path_costs(const orc_graph* g, const int32_t* tree, int32_t source, int columns,
+                            int64_t* costs) {
+  const int64_t n = g->n;
+  const size_t C = (size_t)columns;
+  for (size_t i = 0; i < (size_t)n * C; ++i) costs[i] = ORC_INF;
+  if (n == 0) return -1;
+  int64_t* start = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+  int64_t* cursor = (int64_t*)xmalloc(((size_t)n + 1) * sizeof(int64_t));
+  int32_t* children = (int32_t*)xmalloc((size_t)n * sizeof(int32_t));
+  int32_t* queue = (int32_t*)xmalloc((size_t)n * sizeof(int32_t));
+  for (int64_t v = 0; v < n; ++v)
+    if (v != source && tree[v] >= 0) start[tree[v] + 1]++;
+  for (int64_t v = 0; v < n; ++v) start[v + 1] += start[v];
+  memcpy(cursor, start, ((size_t)n + 1) * sizeof(int64_t));
+  for (int64_t v = 0; v < n; ++v)
+    if (v != source && tree[v] >= 0) children[cursor[tree[v]]++] = (int32_t)v;
+  for (size_t j = 0; j < C; ++j) costs[(size_t)source * C + j] = 0;
+  int64_t head = 0, tail = 0;
+  int32_t missing = -1;
+  queue[tail++] = source;
+  while (head < tail && missing < 0) {
+    const int32_t p = queue[head++];
+    for (int64_t c = start[p]; c < start[p + 1] && missing < 0; ++c) {
+      const int32_t v = children[c];
+      int64_t edge = -1;
+      for (int64_t e = g->row_ptr[p]; e < g->row_ptr[p + 1]; ++e)
+        if (g->col[e] == v) {
+          edge = e;
+          break;
+        }
+      if (edge < 0) {
+        missing = v;
+        break;
+      }
+      for (size_t j = 0; j < C; ++j)
+        costs[(size_t)v * C + j] =
+            costs[(size_t)p * C + j] + (int64_t)g->w[j * (size_t)g->m + (size_t)edge];
+      queue[tail++] = v;
+    }
+  }
+  free(start);
+  free(cursor);
+  free(children);
+  free(queue);
+  return missing;
 }

@@ -16,3 +16,9 @@ def pytest_configure(config):
 def fixtures():
     import numpy as np
     return np.load(os.path.join(ROOT, "tests", "golden", "mosp_fixtures.npz"))
+
+
+@pytest.fixture(scope="session")
+def combined_fixtures():
+    import numpy as np
+    return np.load(os.path.join(ROOT, "tests", "golden", "mosp_combined.npz"))

@@ -1,15 +1,20 @@
-"""Convert the reference's golden sssp fixtures into tests/golden/mosp_fixtures.npz.
+"""Convert the reference's golden fixtures into tests/golden/mosp_fixtures.npz and
+tests/golden/mosp_combined.npz.
 
 Run once, in a checkout where the dynG reference tree is present:
 
     python tests/golden/make_golden.py /path/to/dyng
 
-It reads (never modifies) two fixture directories of the reference:
+It reads (never modifies) three fixture directories of the reference:
   - cpp/tests/data/mosp_sssp/   34 cases (cases.txt): for every objective k the initial tree
     (init/obj<k>/{distancesOriginal,SSSPTreeOriginal}.txt, "v d" / "v INF", "v p"), the tree
     after one update (updated/obj<k>/...) and stats.txt ("obj<k> invalidated <n>");
   - cpp/tests/data/mosp_graph_io/<case>/applied/  the CSR after the batch, its transpose and the
-    weight-increase mask (one line per insertion, K flags).
+    weight-increase mask (one line per insertion, K flags);
+  - cpp/tests/data/mosp_combined/  8 cases (cases.txt: name, input dir, init dir, K, preferences):
+    the combined graph after the batch (combined/distancesCsr.txt "v d", SSSPTreeCsr.txt "v p",
+    mospCosts.txt "v c_1 .. c_KG" over every weight column of the graph), from the K initial
+    trees under init/.
 Inputs: graphCsr{RowPtr,ColInd,Values}.txt (one row offset / neighbour per line, K weights per
 line), insert.txt ("u v w1 .. wK") and delete.txt ("u v").  Blank lines are skipped.
 
@@ -113,6 +118,58 @@ def main(root):
                 [[int(x) for x in r[:k]] for r in mask], np.uint8).reshape(-1, k)
     out["cases"] = np.asarray(names)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "mosp_fixtures.npz")
+    np.savez_compressed(dst, **out)
+    print(f"wrote {dst}: {len(names)} cases")
+    combined(data)
+
+
+def _columns(prefix):
+    rows = _rows(prefix + "Values.txt")
+    return len(rows[0]) if rows else 1
+
+
+def combined(data):
+    out = {}
+    names = []
+    for line in open(os.path.join(data, "mosp_combined", "cases.txt")):
+        toks = line.split()
+        if not toks:
+            continue
+        name, inp, init, k, pref = toks[0], toks[1], toks[2], int(toks[3]), toks[4]
+        names.append(name)
+        ind = os.path.join(data, inp)
+        kg = _columns(os.path.join(ind, "graphCsr"))
+        rp, col, w = _csr(os.path.join(ind, "graphCsr"), kg)
+        n = rp.size - 1
+        ins = _rows(os.path.join(ind, "insert.txt"))
+        dele = _rows(os.path.join(ind, "delete.txt"))
+        out[f"{name}/k"] = np.int64(k)
+        out[f"{name}/kg"] = np.int64(kg)
+        out[f"{name}/pref"] = np.asarray([int(x) for x in pref.split(",")], np.int32)
+        out[f"{name}/row_ptr"] = rp
+        out[f"{name}/col"] = col
+        out[f"{name}/w"] = w
+        out[f"{name}/ins"] = np.asarray([[int(x) for x in r[:2 + kg]] for r in ins],
+                                        np.int32).reshape(-1, 2 + kg)
+        out[f"{name}/del"] = np.asarray([[int(x) for x in r[:2]] for r in dele],
+                                        np.int32).reshape(-1, 2)
+        for j in range(k):
+            ob = os.path.join(data, init, f"obj{j}")
+            out[f"{name}/init_d{j}"] = _vertex_values(
+                os.path.join(ob, "distancesOriginal.txt"), n, True)
+            out[f"{name}/init_p{j}"] = _vertex_values(
+                os.path.join(ob, "SSSPTreeOriginal.txt"), n, False).astype(np.int32)
+        cd = os.path.join(data, "mosp_combined", name, "combined")
+        nu = len(_rows(os.path.join(cd, "distancesCsr.txt")))
+        out[f"{name}/combined_d"] = _vertex_values(os.path.join(cd, "distancesCsr.txt"), nu, True)
+        out[f"{name}/combined_p"] = _vertex_values(
+            os.path.join(cd, "SSSPTreeCsr.txt"), nu, False).astype(np.int32)
+        costs = np.zeros((nu, kg), np.int64)
+        for toks in _rows(os.path.join(cd, "mospCosts.txt")):
+            costs[int(toks[0])] = [INF if t == "INF" else int(t) for t in toks[1:1 + kg]]
+        out[f"{name}/costs"] = costs
+    out["cases"] = np.asarray(names)
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "mosp_combined.npz")
     np.savez_compressed(dst, **out)
     print(f"wrote {dst}: {len(names)} cases")
 

@@ -35,6 +35,26 @@ def fixture_case(z, name):
     return case
 
 
+def combined_case(z, name):
+    """Decode one case of tests/golden/mosp_combined.npz (K objectives of a graph with KG weight
+    columns, preferences, the combined tree and the path costs over all KG columns)."""
+    k, kg = int(z[f"{name}/k"]), int(z[f"{name}/kg"])
+    ins = z[f"{name}/ins"].reshape(-1, 2 + kg)
+    dele = z[f"{name}/del"].reshape(-1, 2)
+    return {
+        "k": k, "kg": kg, "pref": [int(x) for x in z[f"{name}/pref"]],
+        "row_ptr": z[f"{name}/row_ptr"], "col": z[f"{name}/col"],
+        "w": z[f"{name}/w"].reshape(kg, -1),
+        "ins_src": ins[:, 0].copy(), "ins_dst": ins[:, 1].copy(),
+        "ins_w": ins[:, 2:].copy().ravel(),  # insertion-major, KG per insertion
+        "del_src": dele[:, 0].copy(), "del_dst": dele[:, 1].copy(),
+        "init_d": [z[f"{name}/init_d{j}"] for j in range(k)],
+        "init_p": [z[f"{name}/init_p{j}"] for j in range(k)],
+        "combined_d": z[f"{name}/combined_d"], "combined_p": z[f"{name}/combined_p"],
+        "costs": z[f"{name}/costs"].reshape(-1, kg),
+    }
+
+
 # The random shapes of the reference's randomized differential test
 # (cpp/tests/algorithms/sssp/sssp_random_test.cpp:467-580): sparse, dense, grid, hub, chain graphs
 # with tiny, [1,100] and large weights; chains of batches.

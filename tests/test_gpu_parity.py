@@ -320,6 +320,51 @@ def test_arena_growth_and_compaction_keep_results():
     np.testing.assert_array_equal(csr.weights.reshape(-1), want["w"].reshape(-1))
 
 
+@pytest.mark.parametrize("k", [1, 2])
+def test_device_growth_and_compaction_keep_rows_and_results(k):
+    # one batch far larger than the arena (it grows, on the device), then churn until the
+    # abandoned slots pass half the edges and the next overflow compacts both sides on the
+    # device; every step equals the oracle, and the exported CSR keeps the storage order
+    rng = np.random.default_rng(40 + k)
+    n, s, d, _ = random_graph(rng, "sparse", 2000)
+    w = rng.integers(1, 60, (k, s.size)).reshape(-1)
+    g = D.Graph.from_edges(s, d, w, num_vertices=n, num_weights=k)
+    og = O.Graph.from_edges(n, s, d, w, k)
+    obj = k - 1
+    t = D.sssp.compute(g, 0, D.sssp.Options(objective=obj))
+    ot, _ = O.compute(og, 0, objective=obj, rule=1)
+    for step in range(24):
+        size = 240000 if step == 0 else 20000
+        b = random_batch(rng, n, s, d, size, tree_parents=ot.parents)
+        ni = len(b["ins_src"])
+        iw = rng.integers(1, 60, ni * k)
+        D.sssp.update(g, _batch(b["ins_src"], b["ins_dst"], iw, b["del_src"], b["del_dst"], k), t)
+        O.update(og, _obatch(b["ins_src"], b["ins_dst"], iw, b["del_src"], b["del_dst"], k), ot)
+        np.testing.assert_array_equal(t.distances, ot.distances, err_msg=f"step {step}")
+        np.testing.assert_array_equal(t.parents, ot.parents, err_msg=f"step {step}")
+        st = g.storage()
+        if step == 0:
+            assert st["arena_growths"] >= 1 and st["compactions"] == 0, st
+        if st["compactions"] >= 1:
+            break
+    assert st["compactions"] >= 1, st
+    csr = g.to_csr()
+    want = og.to_csr()
+    np.testing.assert_array_equal(csr.row_ptr, want["row_ptr"])
+    np.testing.assert_array_equal(csr.col_ind, want["col"])
+    np.testing.assert_array_equal(csr.weights.reshape(-1), want["w"].reshape(-1))
+    # the edge index was rebuilt over the moved slots: deleting and upserting through it works
+    ed = og.to_csr()
+    u = np.repeat(np.arange(n), np.diff(ed["row_ptr"]))[:50]
+    v = ed["col"][:50]
+    iw = rng.integers(1, 60, 50 * k)
+    D.sssp.update(g, _batch(u, v, iw, u[::2], v[::2], k), t)
+    O.update(og, _obatch(u, v, iw, u[::2], v[::2], k), ot)
+    np.testing.assert_array_equal(t.distances, ot.distances)
+    np.testing.assert_array_equal(t.parents, ot.parents)
+    np.testing.assert_array_equal(g.to_csr().col_ind, og.to_csr()["col"])
+
+
 def test_schedules_never_change_results():
     # sssp::options::delta and the schedule are tunables (sssp.hpp:78-94): every schedule gives
     # the same bytes as the oracle

@@ -7,13 +7,17 @@ reproduces the reference's bytes before anything is compared against it:
     `invalidated` == the recorded counter, for all 34 cases and every objective;
   - cpp/tests/data/mosp_graph_io/*/applied: the applied CSR, its transpose and the
     weight-increase mask of apply_batch_host;
-  - the README quickstart and hand cases of cpp/tests/algorithms/sssp/sssp_test.cpp:74-330.
+  - the README quickstart and hand cases of cpp/tests/algorithms/sssp/sssp_test.cpp:74-330;
+  - cpp/tests/data/mosp_combined: mosp's finalize step (the combined graph of the K updated
+    trees under the case's preferences, its tree and the path costs over every weight column)
+    equals the combined files of all 8 cases (python/tests/test_cli.py:686-723 replays them);
+  - hand cases of cpp/tests/algorithms/mosp/mosp_test.cpp:249-280.
 """
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.helpers import INF, fixture_case
+from tests.helpers import INF, combined_case, fixture_case
 
 
 def _cases(z):
@@ -226,3 +230,76 @@ def test_packing_rules():
     assert O.packs_parents(n, w, 1)
     assert not O.packs_parents(n, w, 0)
     assert O.default_delta(100, 10, 1000) == 32
+
+
+def oracle_mosp_update(c):
+    """The K trees of a combined case updated by its batch (each on its own copy of the graph:
+    the batch is applied once per copy), the updated graph, and mosp's finalize step."""
+    k, kg = c["k"], c["kg"]
+    trees, g = [], None
+    for j in range(k):
+        g = O.Graph.from_csr(c["row_ptr"], c["col"], c["w"], kg, O.mosp_props())
+        t = O.from_arrays(g, 0, c["init_d"][j], c["init_p"][j], canonicalize=False, objective=j,
+                          rule=1)
+        O.update(g, O.Batch(c["ins_src"], c["ins_dst"], c["ins_w"], c["del_src"], c["del_dst"],
+                            kg), t)
+        trees.append(t)
+    return trees, g, O.mosp_finalize(g, 0, [t.parents for t in trees], c["pref"], kg)
+
+
+def test_combined_fixtures(combined_fixtures):
+    names = [str(x) for x in combined_fixtures["cases"]]
+    assert len(names) == 8
+    for name in names:
+        c = combined_case(combined_fixtures, name)
+        _, _, m = oracle_mosp_update(c)
+        np.testing.assert_array_equal(m.distances, c["combined_d"], err_msg=name)
+        np.testing.assert_array_equal(m.parents, c["combined_p"], err_msg=name)
+        np.testing.assert_array_equal(m.costs, c["costs"], err_msg=name)
+
+
+def test_mosp_default_preferences_weigh_an_edge_by_its_trees():
+    # mosp_test.cpp:249-269: 0->1->3 is best for objective 0, 0->2->3 for objective 1
+    g = O.Graph.from_edges(4, [0, 0, 1, 2], [1, 2, 3, 3], [1, 5, 5, 1, 1, 5, 5, 1], 2)
+    parents = [O.compute(g, 0, objective=j, rule=1)[0].parents for j in range(2)]
+    m = O.mosp_finalize(g, 0, parents)
+    assert m.scale == 1 and m.distances.tolist() == [0, 1, 1, 3]
+    assert m.parents.tolist() == [-1, 0, 0, 1] and m.costs[3].tolist() == [2, 10]
+    m = O.mosp_finalize(g, 0, parents, [2, 1])
+    assert m.scale == 2 and m.distances.tolist() == [0, 3, 3, 7]
+    assert m.parents.tolist() == [-1, 0, 0, 2] and m.costs[3].tolist() == [10, 2]
+
+
+def test_mosp_unreachable_vertices_have_no_parent_and_infinite_costs():
+    # mosp_test.cpp:271-279
+    g = O.Graph.from_edges(4, [0, 2], [1, 3], [1, 1, 1, 1], 2)
+    parents = [O.compute(g, 0, objective=j, rule=1)[0].parents for j in range(2)]
+    m = O.mosp_finalize(g, 0, parents)
+    assert m.distances.tolist() == [0, 1, INF, INF] and m.parents.tolist() == [-1, 0, -1, -1]
+    assert m.costs[2].tolist() == [INF, INF] and m.costs[0].tolist() == [0, 0]
+
+
+THESIS_EDGES = [(0, 1, 2, 1, 5), (0, 2, 4, 1, 1), (1, 3, 2, 4, 2), (2, 1, 10, 15, 2),
+                (2, 3, 5, 16, 3), (3, 4, 1, 1, 1), (4, 1, 4, 3, 2), (4, 5, 1, 2, 2),
+                (4, 6, 5, 6, 2), (5, 6, 1, 1, 1)]
+
+
+def test_mosp_thesis_worked_example():
+    # mosp_test.cpp:155-211: compute, the thesis' batch, then the MOSP path to u7 and its costs
+    # under two preference vectors
+    for pref, path, cost in (([4, 1, 4], [6, 5, 1, 0], [15, 3, 20]),
+                             ([4, 4, 1], [6, 4, 3, 2, 0], [15, 24, 7])):
+        trees = []
+        for j in range(3):
+            g = O.Graph.from_edges(7, [e[0] for e in THESIS_EDGES], [e[1] for e in THESIS_EDGES],
+                                   [x for e in THESIS_EDGES for x in e[2:]], 3, O.mosp_props())
+            t, _ = O.compute(g, 0, objective=j, rule=1)
+            O.update(g, O.Batch([3, 1], [5, 5], [10, 2, 12, 12, 1, 14], [1, 4], [3, 1], 3), t)
+            trees.append(t)
+        assert [t.parents.tolist() for t in trees] == [
+            [-1, 0, 0, 2, 3, 4, 5], [-1, 0, 0, 2, 3, 1, 5], [-1, 2, 0, 2, 3, 4, 4]]
+        m = O.mosp_finalize(g, 0, [t.parents for t in trees], pref)
+        walk = [6]
+        while m.parents[walk[-1]] >= 0:
+            walk.append(int(m.parents[walk[-1]]))
+        assert m.scale == 4 and walk == path and m.costs[6].tolist() == cost
