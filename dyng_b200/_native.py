@@ -91,6 +91,20 @@ class GraphStorage(ctypes.Structure):
         (n, ctypes.c_double) for n in ("grow_ms", "compact_ms", "index_ms", "maintenance_ms_max")]
 
 
+class MospOptions(ctypes.Structure):
+    _fields_ = [("num_objectives", ctypes.c_int32), ("num_preferences", ctypes.c_int32),
+                ("preferences", ctypes.POINTER(ctypes.c_int32)), ("delta", ctypes.c_int64),
+                ("compute_path_costs", ctypes.c_int32), ("validate_inputs", ctypes.c_int32)]
+
+
+class MospStats(ctypes.Structure):
+    _fields_ = [("batch", ApplySummary), ("affected", ctypes.c_int64),
+                ("combined_edges", ctypes.c_int64), ("preference_scale", ctypes.c_int64),
+                ("iterations", ctypes.c_int64), ("converged", ctypes.c_int32),
+                ("combine_ms", ctypes.c_float), ("solve_ms", ctypes.c_float),
+                ("costs_ms", ctypes.c_float)]
+
+
 class ServerInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "failed", "rounds",
                                               "max_group", "waiting", "admission_us_max")]
@@ -122,6 +136,25 @@ SIGNATURES = {
     "dyngb200_graph_to_csr": (ctypes.c_int, [c_void_p, c_void_p, c_i64p, c_i32p, c_i32p, c_i64p,
                                              c_i32p, c_i32p]),
     "dyngb200_graph_device_bytes": (ctypes.c_int, [c_void_p, c_i64p]),
+    "dyngb200_mosp_compute": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32,
+                                             ctypes.POINTER(MospOptions), ctypes.POINTER(c_void_p)]),
+    "dyngb200_mosp_from_arrays": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.POINTER(c_i64p), ctypes.POINTER(c_i32p),
+                                                 ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.POINTER(MospOptions),
+                                                 ctypes.POINTER(c_void_p)]),
+    "dyngb200_mosp_update": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(Batch), c_void_p,
+                                            ctypes.POINTER(MospStats), ctypes.POINTER(Stats)]),
+    "dyngb200_mosp_destroy": (ctypes.c_int, [c_void_p]),
+    "dyngb200_mosp_info": (ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_int32), c_i64p, c_i64p,
+                                          ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "dyngb200_mosp_tree": (ctypes.c_int, [c_void_p, ctypes.c_int32, ctypes.POINTER(c_void_p)]),
+    "dyngb200_mosp_combined": (ctypes.c_int, [c_void_p, c_i64p, c_i32p, ctypes.c_int32]),
+    "dyngb200_mosp_path_costs": (ctypes.c_int, [c_void_p, c_i64p]),
+    "dyngb200_mosp_path_costs_columns": (ctypes.c_int, [c_void_p, c_void_p, c_void_p,
+                                                        ctypes.c_int32, c_i64p]),
+    "dyngb200_mosp_set_options": (ctypes.c_int, [c_void_p, ctypes.POINTER(MospOptions)]),
     "dyngb200_graph_storage_get": (ctypes.c_int, [c_void_p, ctypes.POINTER(GraphStorage)]),
     "dyngb200_sssp_compute": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32,
                                              ctypes.POINTER(Options), ctypes.POINTER(c_void_p),

@@ -7,6 +7,7 @@ io/result_io.hpp), read and written byte for byte:
   delete.txt                               "u v" per line
   distances*.txt                           "v d" per line, "v INF" for an unreachable vertex
   SSSPTree*.txt                            "v p" per line, p = -1 for none
+  mospCosts.txt                            "v c_1 .. c_K" per line, "INF" for an unreachable cost
 
 Every file ends with a newline after its last line; an empty file is empty.
 """
@@ -97,8 +98,25 @@ def read_tree(path: str) -> np.ndarray:
 
 
 def write_distances(path: str, d) -> None:
-    _write_lines(path, (f"{v} INF" if int(x) >= INF_DISTANCE else f"{v} {int(x)}"
+    """Values >= INF / 2 print as INF (io/result_io.cpp:165-181)."""
+    _write_lines(path, (f"{v} INF" if int(x) >= INF_DISTANCE // 2 else f"{v} {int(x)}"
                         for v, x in enumerate(d)))
+
+
+def write_path_costs(path: str, costs) -> None:
+    """n x K costs, one vertex per line (io/result_io.cpp:185-209)."""
+    c = np.asarray(costs)
+    _write_lines(path, (" ".join([str(v)] + ["INF" if int(x) >= INF_DISTANCE // 2 else str(int(x))
+                                             for x in row]) for v, row in enumerate(c)))
+
+
+def read_path_costs(path: str) -> np.ndarray:
+    rows = _read_rows(path)
+    k = len(rows[0]) - 1 if rows else 0
+    out = np.zeros((len(rows), k), np.int64)
+    for r in rows:
+        out[int(r[0])] = [INF_DISTANCE if t == "INF" else int(t) for t in r[1:]]
+    return out
 
 
 def write_tree(path: str, p) -> None:

@@ -241,6 +241,69 @@ dyngb200_status dyngb200_sssp_update(dyngb200_context ctx, dyngb200_graph g,
 dyngb200_status dyngb200_sssp_update_each(dyngb200_context ctx, dyngb200_graph g,
                                           const dyngb200_batch* batch, dyngb200_tree* trees,
                                           int32_t count, dyngb200_stats* stats);
+/* ---- mosp (cpp/include/dyng/mosp.hpp): K objectives, the combined graph, the MOSP tree ------ */
+/* mosp::options (mosp.hpp:79-101).  preferences: NULL / num_preferences 0 for all ones, else one
+ * per objective, each >= 1 (a lower value is a higher priority), lcm <= 2^20. */
+typedef struct dyngb200_mosp_options {
+  int32_t num_objectives;       /* the first K weight columns; 0 = every column (K <= 64) */
+  int32_t num_preferences;
+  const int32_t* preferences;
+  int64_t delta;                /* near-far width of the K sssp updates; 0 = automatic */
+  int32_t compute_path_costs;   /* path costs at compute() / update() (1 by default) */
+  int32_t validate_inputs;      /* from_arrays: sssp's checks of every imported tree */
+} dyngb200_mosp_options;
+/* mosp::stats (mosp.hpp:115-125). */
+typedef struct dyngb200_mosp_stats {
+  dyngb200_apply_summary batch;
+  int64_t affected;          /* vertices whose combined distance or MOSP parent changed */
+  int64_t combined_edges;
+  int64_t preference_scale;  /* L = lcm(preferences): combined distances are in units of 1/L */
+  int64_t iterations;        /* summed over the K sssp updates and the combined solve */
+  int32_t converged;
+  float combine_ms, solve_ms, costs_ms; /* host time of the finalize stages (with their waits) */
+} dyngb200_mosp_stats;
+typedef struct dyngb200_mosp_s* dyngb200_mosp;
+/* mosp::compute(resources::cuda(), g, source, opt) (mosp.hpp:444-449); opt may be NULL. */
+dyngb200_status dyngb200_mosp_compute(dyngb200_context ctx, dyngb200_graph g, int32_t source,
+                                      const dyngb200_mosp_options* opt, dyngb200_mosp* out);
+/* mosp::result::from_arrays (mosp.hpp:300-347): K trees of g (distances[k], parents[k]: n
+ * values each, in `memory`), imported as sssp::result::from_arrays imports one tree, then the
+ * combined graph, the MOSP tree and the path costs.  K must equal the objectives opt selects. */
+dyngb200_status dyngb200_mosp_from_arrays(dyngb200_context ctx, dyngb200_graph g, int32_t source,
+                                          int32_t num_trees, const int64_t* const* distances,
+                                          const int32_t* const* parents, int64_t n,
+                                          int32_t memory, int32_t canonicalize,
+                                          const dyngb200_mosp_options* opt, dyngb200_mosp* out);
+/* mosp::update(resources::cuda(), g, batch, r) (mosp.hpp:502-506): the batch applied once, the
+ * K trees updated (dyng::update_each), then the combined graph solved again.  objective_stats:
+ * NULL or K entries.  An error before the batch is applied changes nothing; an error after it
+ * leaves the result unusable (stale_result_error on every access). */
+dyngb200_status dyngb200_mosp_update(dyngb200_context ctx, dyngb200_graph g,
+                                     const dyngb200_batch* batch, dyngb200_mosp r,
+                                     dyngb200_mosp_stats* stats, dyngb200_stats* objective_stats);
+dyngb200_status dyngb200_mosp_destroy(dyngb200_mosp r);
+/* K, n, L, the source and the graph version the result matches. */
+dyngb200_status dyngb200_mosp_info(dyngb200_mosp r, int32_t* num_objectives, int64_t* num_vertices,
+                                   int64_t* preference_scale, int32_t* source,
+                                   uint64_t* graph_version);
+/* The sssp tree of one objective (mosp::result::distances(k) / parents(k)): a borrowed handle,
+ * owned by r and valid until r is destroyed; do not destroy it. */
+dyngb200_status dyngb200_mosp_tree(dyngb200_mosp r, int32_t objective, dyngb200_tree* out);
+/* combined_distances() / combined_parents(): n values each into buffers in `memory` (either may
+ * be NULL). */
+dyngb200_status dyngb200_mosp_combined(dyngb200_mosp r, int64_t* distances, int32_t* parents,
+                                       int32_t memory);
+/* path_costs(): n x K values, vertex-major, into a host buffer; INVALID_ARGUMENT if they were
+ * not computed at the last compute() / update(). */
+dyngb200_status dyngb200_mosp_path_costs(dyngb200_mosp r, int64_t* costs);
+/* The path costs along the current MOSP tree over the first `columns` weight columns of g
+ * (MOSP's mospCosts.txt covers every column of the graph), n x columns into a host buffer. */
+dyngb200_status dyngb200_mosp_path_costs_columns(dyngb200_context ctx, dyngb200_graph g,
+                                                 dyngb200_mosp r, int32_t columns, int64_t* costs);
+/* result::set_options: delta, compute_path_costs and validate_inputs change (from the next
+ * update); num_objectives and preferences must stay the same. */
+dyngb200_status dyngb200_mosp_set_options(dyngb200_mosp r, const dyngb200_mosp_options* opt);
+
 /* sssp::update with an explicit schedule (the learned scheduler's entry point; no reference
  * counterpart beyond options::delta / options::cuda_engine, which are tunables the same way). */
 dyngb200_status dyngb200_sssp_update_scheduled(dyngb200_context ctx, dyngb200_graph g,

@@ -3,17 +3,20 @@
 CPU: the writers reproduce the reference's fixture files byte for byte (where the reference tree
 is present), and every reader/writer pair round-trips.  GPU: the driver, run on each golden case
 written out in MOSP's format, writes the golden updated trees byte for byte and reports the
-golden `invalidated` per objective (the reference's mosp_compat replay of the 34 cases)."""
+golden `invalidated` per objective (the reference's mosp_compat replay of the 34 cases); with
+--mosp it writes the golden combinedGraph/ files of the 8 preference cases byte for byte
+(python/tests/test_cli.py:686-723)."""
 import os
 
 import numpy as np
 import pytest
 
 from dyng_b200 import mosp_io as io
-from tests.helpers import fixture_case
+from tests.helpers import combined_case, fixture_case
 
-REFERENCE_FIXTURES = os.path.join(os.environ.get("DYNG_REFERENCE", "/root/reference"),
-                                  "cpp", "tests", "data", "mosp_sssp")
+REFERENCE_DATA = os.path.join(os.environ.get("DYNG_REFERENCE", "/root/reference"),
+                              "cpp", "tests", "data")
+REFERENCE_FIXTURES = os.path.join(REFERENCE_DATA, "mosp_sssp")
 
 
 def _cases(z):
@@ -83,6 +86,33 @@ def _write_case(root, c):
                       c["init_p"][j])
 
 
+def test_cost_files_round_trip(tmp_path):
+    costs = np.array([[0, 0, 0], [7, 17, io.INF_DISTANCE], [3, 4, 5]], np.int64)
+    io.write_path_costs(str(tmp_path / "c.txt"), costs)
+    assert (tmp_path / "c.txt").read_bytes() == b"0 0 0 0\n1 7 17 INF\n2 3 4 5\n"
+    assert np.array_equal(io.read_path_costs(str(tmp_path / "c.txt")), costs)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE_DATA, "mosp_combined")),
+                    reason="reference tree absent")
+def test_combined_writers_reproduce_the_reference_files(tmp_path):
+    root = os.path.join(REFERENCE_DATA, "mosp_combined")
+    done = 0
+    for case in sorted(os.listdir(root)):
+        cd = os.path.join(root, case, "combined")
+        if not os.path.isdir(cd):
+            continue
+        d, p, c = (os.path.join(cd, x) for x in ("distancesCsr.txt", "SSSPTreeCsr.txt",
+                                                  "mospCosts.txt"))
+        io.write_distances(str(tmp_path / "d.txt"), io.read_distances(d))
+        io.write_tree(str(tmp_path / "p.txt"), io.read_tree(p))
+        io.write_path_costs(str(tmp_path / "c.txt"), io.read_path_costs(c))
+        for mine, theirs in (("d.txt", d), ("p.txt", p), ("c.txt", c)):
+            assert (tmp_path / mine).read_bytes() == open(theirs, "rb").read(), theirs
+        done += 1
+    assert done == 8
+
+
 @pytest.mark.gpu
 def test_compat_driver_replays_every_golden_case(fixtures, tmp_path):
     from dyng_b200 import compat
@@ -103,3 +133,33 @@ def test_compat_driver_replays_every_golden_case(fixtures, tmp_path):
             assert (got / "SSSPTreeUpdated.txt").read_bytes() == (root / "want_p.txt").read_bytes()
         done += 1
     assert done == len(_cases(fixtures)) >= 34
+
+
+@pytest.mark.gpu
+def test_compat_driver_mosp_mode_replays_the_combined_cases(combined_fixtures, tmp_path):
+    from dyng_b200 import compat
+    names = [str(x) for x in combined_fixtures["cases"]]
+    for name in names:
+        c = combined_case(combined_fixtures, name)
+        root = tmp_path / name
+        io.write_csr(str(root / "input" / "graphCsr"), c["row_ptr"], c["col"], c["w"])
+        io.write_changes(str(root / "input"), c["ins_src"], c["ins_dst"],
+                         c["ins_w"].reshape(-1, c["kg"]), c["del_src"], c["del_dst"])
+        for j in range(c["k"]):
+            io.write_distances(str(root / "init" / f"obj{j}" / "distancesOriginal.txt"),
+                               c["init_d"][j])
+            io.write_tree(str(root / "init" / f"obj{j}" / "SSSPTreeOriginal.txt"), c["init_p"][j])
+        lines = []
+        compat.main(["--graph", str(root / "input" / "graphCsr"), "--changes", str(root / "input"),
+                     "--init", str(root / "init"), "--out", str(root / "out"), "-k", str(c["k"]),
+                     "--mosp", "--pref", ",".join(str(p) for p in c["pref"])])
+        io.write_distances(str(root / "want_d.txt"), c["combined_d"])
+        io.write_tree(str(root / "want_p.txt"), c["combined_p"])
+        io.write_path_costs(str(root / "want_c.txt"), c["costs"])
+        got = root / "out" / "combinedGraph"
+        assert (got / "distancesCsr.txt").read_bytes() == (root / "want_d.txt").read_bytes(), name
+        assert (got / "SSSPTreeCsr.txt").read_bytes() == (root / "want_p.txt").read_bytes(), name
+        assert (got / "mospCosts.txt").read_bytes() == (root / "want_c.txt").read_bytes(), name
+        assert sorted(p.name for p in (root / "out").iterdir()) == ["combinedGraph"] + [
+            f"obj{j}" for j in range(c["k"])]
+    assert len(names) == 8
