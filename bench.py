@@ -44,6 +44,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=100_000)
     ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--graph", default="rmat", choices=["rmat", "grid"],
+                    help="rmat: R-MAT ef16 (headline); grid: side x side 4-neighbour grid with "
+                         "0.1%% shortcuts, lognormal weights, source at the centre, 50/50 batches "
+                         "whose deletions are tree edges within 64 hops of the source")
+    ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--schedule", default="learned", choices=["plain", "learned"],
                     help="the headline arm; both arms run when scheduler weights exist")
@@ -125,7 +130,7 @@ def traffic(args):
     """DRAM bytes per k_sssp launch from the committed ncu capture of this workload (None when
     the workload differs from the captured one)."""
     path = os.path.join(ROOT, "profiles", "k_sssp_dram_rmat-s22_batch100k.json")
-    if not os.path.exists(path) or (args.scale, args.batch) != (22, 100_000):
+    if not os.path.exists(path) or (args.graph, args.scale, args.batch) != ("rmat", 22, 100_000):
         return None
     with open(path) as f:
         return int(json.load(f)["dram_bytes_per_launch"])
@@ -134,17 +139,49 @@ def traffic(args):
 def make_workload(args, device):
     from dyng_b200 import generators as G
     t0 = time.time()
-    edges = G.rmat(args.scale, 16, w_max=1000, seed=1, device=device)
+    if args.graph == "grid":
+        edges = G.grid(args.side, seed=1)
+    else:
+        edges = G.rmat(args.scale, 16, w_max=1000, seed=1, device=device)
     return edges, time.time() - t0
 
 
-def cpu_baseline_sample(edges, tree_d, tree_p, batches, budget_s=20.0):
+def workload_name(args):
+    if args.graph == "grid":
+        return f"grid-{args.side}x{args.side}-lognormal-batch{args.batch}"
+    return f"rmat-s{args.scale}-ef16-w1000-batch{args.batch}"
+
+
+def source_of(args):
+    """R-MAT: vertex 0; grid: the centre vertex."""
+    return (args.side // 2) * args.side + args.side // 2 if args.graph == "grid" else 0
+
+
+def insert_fraction(args):
+    return 0.5 if args.graph == "grid" else 0.75
+
+
+def batch_maker(args, stream):
+    """next(parents) -> one batch of the workload: R-MAT 75% insertions, half of the deletions
+    tree edges; grid 50/50, the deletions tree edges within 64 lattice hops of the source (the
+    rest uniform)."""
+    if args.graph != "grid":
+        return lambda parents: stream.next(args.batch, 0.75, 0.5, parents=parents)
+    side = args.side
+    v = np.arange(side * side, dtype=np.int64)
+    c = side // 2
+    hops = np.abs(v % side - c) + np.abs(v // side - c)
+    return lambda parents: stream.next(args.batch, 0.5, 1.0, parents=parents,
+                                       near_source_hops=64, dist_hops=hops)
+
+
+def cpu_baseline_sample(edges, tree_d, tree_p, batches, budget_s=20.0, source=0):
     """The oracle (the reference's algorithm restated in C, one thread) on the same graph and
     batches: time sssp::update per batch until the budget is spent."""
     from oracle import oracle as O
     rp, col, w = edges.csr()
     og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
-    ot = O.from_arrays(og, 0, tree_d, tree_p, canonicalize=False, validate=False, rule=1)
+    ot = O.from_arrays(og, source, tree_d, tree_p, canonicalize=False, validate=False, rule=1)
     done, changes, spent = 0, 0, 0.0
     for b in batches:
         t0 = time.perf_counter()
@@ -175,17 +212,18 @@ def run_reference(args):
     if device:
         import dyng_b200 as D
         g = D.Graph.from_csr(rp, col, w)
-        t = D.sssp.compute(g, 0)
+        t = D.sssp.compute(g, source_of(args))
         d0, p0 = t.distances, t.parents
         del t, g
     else:
-        ot0, _ = O.compute(og, 0, rule=1)
+        ot0, _ = O.compute(og, source_of(args), rule=1)
         d0, p0 = ot0.distances, ot0.parents
-    ot = O.from_arrays(og, 0, d0, p0, canonicalize=False, validate=False, rule=1)
+    ot = O.from_arrays(og, source_of(args), d0, p0, canonicalize=False, validate=False, rule=1)
     stream = G.BatchStream(edges, seed=7)
+    make_batch = batch_maker(args, stream)
     times, sizes = [], []
     for step in range(args.warmup + args.steps):
-        b = stream.next(args.batch, 0.75, 0.5, parents=ot.parents)
+        b = make_batch(ot.parents)
         t0 = time.perf_counter()
         O.update(og, O.Batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
                              b.delete_dst), ot)
@@ -199,8 +237,8 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"rmat-s{args.scale}-ef16-w1000-batch{args.batch}",
-                       "batch_changes": args.batch, "insert_fraction": 0.75,
+            "config": {"workload": workload_name(args),
+                       "batch_changes": args.batch, "insert_fraction": insert_fraction(args),
                        "p50_ms": 1000 * float(np.percentile(times, 50)),
                        "p99_ms": 1000 * float(np.percentile(times, 99))},
             "cpu_baseline": {"value": value, "unit": "changed edges/s", "cores": 1,
@@ -291,9 +329,11 @@ def main():
     rp, col, w = edges.csr()
     t0 = time.time()
     g = D.Graph.from_csr(rp, col, w, resources=res)
-    tree = D.sssp.compute(g, 0)
+    source = source_of(args)
+    tree = D.sssp.compute(g, source)
     build_s = time.time() - t0
     bs = G.BatchStream(edges, seed=7)
+    make_batch = batch_maker(args, bs)
     env = (D, torch, g, tree, stream, args, world, local)
 
     fixed = None
@@ -315,7 +355,7 @@ def main():
     recorded = []
 
     def generate(step):
-        b = bs.next(args.batch, 0.75, 0.5, parents=tree.parents)
+        b = make_batch(tree.parents)
         recorded.append(b)
         return b
 
@@ -346,7 +386,7 @@ def main():
     e2e_lat, e2e_sizes = [], []
     h2d = 0
     for step in range(args.steps):
-        b = bs.next(args.batch, 0.75, 0.5, parents=tree.parents)
+        b = make_batch(tree.parents)
         pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in
                   (b.insert_src, b.insert_dst, b.insert_weights, b.delete_src, b.delete_dst)]
         arrs = [p.numpy() for p in pinned]
@@ -363,7 +403,7 @@ def main():
     verified = None
     compute_info = None
     if not args.no_verify:
-        fresh, cst = D.sssp.compute(g, 0, stats=True)
+        fresh, cst = D.sssp.compute(g, source, stats=True)
         verified = bool(np.array_equal(fresh.distances, tree.distances) and
                         np.array_equal(fresh.parents, tree.parents))
         # the same kernel on bulk work: a from-scratch solve of the final graph
@@ -393,13 +433,14 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cbs = G.BatchStream(edges, seed=7)
-            batches = [cbs.next(args.batch, 0.75, 0.5, parents=None) for _ in range(4)]
+            cmake = batch_maker(args, cbs)
+            batches = [cmake(None) for _ in range(4)]
             # the sample starts from the initial tree of the same graph
             g0 = D.Graph.from_csr(rp, col, w, resources=res)
-            t_init = D.sssp.compute(g0, 0)
+            t_init = D.sssp.compute(g0, source)
             d0, p0 = t_init.distances, t_init.parents
             del t_init, g0
-            v, done, spent = cpu_baseline_sample(edges, d0, p0, batches)
+            v, done, spent = cpu_baseline_sample(edges, d0, p0, batches, source=source)
             cpu = {"value": v, "unit": "changed edges/s", "cores": 1, "kind": "port",
                    "sample": f"oracle sssp::update on {done} of the workload's {args.batch}-change "
                              f"batches ({spent:.1f} s), same graph"}
@@ -419,9 +460,10 @@ def main():
             "ms_per_step": summ[args.schedule]["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
-            "config": {"workload": f"rmat-s{args.scale}-ef16-w1000-batch{args.batch}",
+            "config": {"workload": workload_name(args),
                        "vertices": int(edges.num_vertices), "edges": int(edges.src.size),
-                       "batch_changes": args.batch, "insert_fraction": 0.75,
+                       "batch_changes": args.batch, "insert_fraction": insert_fraction(args),
+                       "source": source,
                        "schedule": args.schedule, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (graph arenas ~1 GB)",
                        "p50_ms": summ[args.schedule]["p50_ms"],

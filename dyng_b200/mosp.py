@@ -219,3 +219,72 @@ def update(graph: Graph, batch: EdgeBatch, result: Result) -> Stats:
                  tuple(_SsspStats(per[i]) for i in range(k)), int(st.combined_edges),
                  int(st.preference_scale), float(st.combine_ms), float(st.solve_ms),
                  float(st.costs_ms))
+
+
+def main(argv=None):
+    """python -m dyng_b200.mosp: time mosp.update on a synthetic multi-objective graph.
+
+    A side x side grid (4-neighbour, bidirectional, 0.1% shortcuts; a road-network stand-in) or
+    an R-MAT graph with K weight columns U[1,100], source 0, batches of `--batch` changes (half
+    insertions, half deletions of live edges), `--steps` timed updates after `--warmup`.  Prints
+    one JSON line: per-update ms (p50), the K sssp updates and the finalize stages, and checks the
+    result against mosp.compute on the final graph."""
+    import argparse
+    import json
+    import time
+    from .generators import BatchStream, grid, rmat
+    ap = argparse.ArgumentParser(prog="python -m dyng_b200.mosp")
+    ap.add_argument("--graph", default="grid", choices=["grid", "rmat"])
+    ap.add_argument("--side", type=int, default=1024)
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("-k", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=50_000)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=2)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(12345)
+    e = grid(a.side, seed=3) if a.graph == "grid" else rmat(a.scale, 16, w_max=100, seed=3)
+    w = rng.integers(1, 101, (a.k, e.src.size)).astype(np.int32)
+    rp = np.zeros(e.num_vertices + 1, np.int64)
+    order = np.lexsort((e.dst, e.src))
+    src, dst = e.src[order], e.dst[order]
+    np.add.at(rp, src.astype(np.int64) + 1, 1)
+    rp = np.cumsum(rp)
+    g = Graph.from_csr(rp, dst, w[:, order], num_weights=a.k)
+    t0 = time.perf_counter()
+    r = compute(g, 0)
+    compute_ms = 1000 * (time.perf_counter() - t0)
+    stream = BatchStream(e, seed=777)
+    lat, parts = [], []
+    for step in range(a.warmup + a.steps):
+        b = stream.next(a.batch, 0.5, 0.0, parents=None)
+        iw = rng.integers(1, 101, b.insert_src.size * a.k).astype(np.int32)
+        eb = EdgeBatch.from_arrays(b.insert_src, b.insert_dst, iw, b.delete_src, b.delete_dst,
+                                   num_weights=a.k)
+        t0 = time.perf_counter()
+        st = update(g, eb, r)
+        dt = 1000 * (time.perf_counter() - t0)
+        if step >= a.warmup:
+            lat.append(dt)
+            parts.append([sum(o.apply_ms + o.sssp_ms for o in st.objectives),
+                          sum(o.sssp_ms for o in st.objectives), st.combine_ms, st.solve_ms,
+                          st.costs_ms])
+    fresh = compute(g, 0)
+    same = bool(np.array_equal(fresh.combined_distances, r.combined_distances) and
+                np.array_equal(fresh.combined_parents, r.combined_parents) and
+                np.array_equal(fresh.path_costs, r.path_costs))
+    p = np.mean(np.array(parts), axis=0)
+    print(json.dumps({
+        "workload": (f"grid-{a.side}x{a.side}" if a.graph == "grid" else f"rmat-s{a.scale}-ef16")
+                    + f"-K{a.k}-w100-batch{a.batch}",
+        "vertices": int(e.num_vertices), "edges": int(e.src.size), "K": a.k,
+        "update_ms_p50": float(np.percentile(lat, 50)), "update_ms_mean": float(np.mean(lat)),
+        "objectives_ms": round(float(p[0]), 3), "objectives_sssp_ms": round(float(p[1]), 3),
+        "sssp_ms_per_objective": round(float(p[1]) / a.k, 3),
+        "combine_ms": round(float(p[2]), 3), "combined_solve_ms": round(float(p[3]), 3),
+        "path_costs_ms": round(float(p[4]), 3), "compute_ms": round(compute_ms, 1),
+        "combined_edges": st.combined_edges, "equals_compute": same}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
