@@ -16,6 +16,7 @@ config.schedules reports both.  Every run checks that both arms end in the same 
 the final tree equals a from-scratch compute (distances and parents bit-exact).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch 100000] [--scale 22]
+    python bench.py --graph grid [--side 4096] [--batch 10000]   # the high-diameter workload
     python bench.py --impl reference ...   # the reference algorithm's CPU restatement (oracle)
 """
 from __future__ import annotations
@@ -47,7 +48,7 @@ def parse():
     ap.add_argument("--graph", default="rmat", choices=["rmat", "grid"],
                     help="rmat: R-MAT ef16 (headline); grid: side x side 4-neighbour grid with "
                          "0.1%% shortcuts, lognormal weights, source at the centre, 50/50 batches "
-                         "whose deletions are tree edges within 64 hops of the source")
+                         "whose deletions concentrate within 64 hops of the source")
     ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--schedule", default="learned", choices=["plain", "learned"],
@@ -162,17 +163,16 @@ def insert_fraction(args):
 
 
 def batch_maker(args, stream):
-    """next(parents) -> one batch of the workload: R-MAT 75% insertions, half of the deletions
-    tree edges; grid 50/50, the deletions tree edges within 64 lattice hops of the source (the
-    rest uniform)."""
+    """next(parents) -> one batch of the workload.  R-MAT: 75% insertions, half of the deletions
+    tree edges.  Grid: 50/50; the deletions concentrate within 64 lattice hops of the source (a
+    quarter of the live edges there per batch, the rest uniform over the live edges) and the
+    near edges deleted by the previous batch come back as insertions (the rest uniform pairs),
+    so the region around the source churns without being cut off."""
     if args.graph != "grid":
         return lambda parents: stream.next(args.batch, 0.75, 0.5, parents=parents)
-    side = args.side
-    v = np.arange(side * side, dtype=np.int64)
-    c = side // 2
-    hops = np.abs(v % side - c) + np.abs(v // side - c)
-    return lambda parents: stream.next(args.batch, 0.5, 1.0, parents=parents,
-                                       near_source_hops=64, dist_hops=hops)
+    from dyng_b200 import generators as G
+    churn = G.NearSourceChurn(stream, args.side, source_of(args))
+    return lambda parents: churn.next(args.batch)
 
 
 def cpu_baseline_sample(edges, tree_d, tree_p, batches, budget_s=20.0, source=0):

@@ -136,6 +136,9 @@ SIGNATURES = {
     "dyngb200_graph_to_csr": (ctypes.c_int, [c_void_p, c_void_p, c_i64p, c_i32p, c_i32p, c_i64p,
                                              c_i32p, c_i32p]),
     "dyngb200_graph_device_bytes": (ctypes.c_int, [c_void_p, c_i64p]),
+    "dyngb200_scheduler_set_feature_range": (ctypes.c_int, [c_void_p, c_f32p, c_f32p]),
+    "dyngb200_scheduler_get_feature_range": (ctypes.c_int, [c_void_p, c_f32p, c_f32p,
+                                                            ctypes.POINTER(ctypes.c_int32)]),
     "dyngb200_mosp_compute": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32,
                                              ctypes.POINTER(MospOptions), ctypes.POINTER(c_void_p)]),
     "dyngb200_mosp_from_arrays": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int32, ctypes.c_int32,

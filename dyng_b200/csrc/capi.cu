@@ -596,6 +596,35 @@ dyngb200_status dyngb200_scheduler_get_params(dyngb200_context ctx, dyngb200_sch
   });
 }
 
+dyngb200_status dyngb200_scheduler_set_feature_range(dyngb200_scheduler s, const float* lo,
+                                                     const float* hi) {
+  return guarded([&] {
+    expects(s != nullptr, "scheduler_set_feature_range: null scheduler");
+    expects((lo == nullptr) == (hi == nullptr),
+            "scheduler_set_feature_range: give both bounds or neither");
+    Scheduler& x = s->s;
+    x.has_range = lo != nullptr;
+    for (int i = 0; i < kMlpIn; ++i) {
+      if (lo) expects(lo[i] <= hi[i], "scheduler_set_feature_range: lower bound above upper");
+      x.feat_lo[i] = lo ? lo[i] : 0.0f;
+      x.feat_hi[i] = hi ? hi[i] : 0.0f;
+    }
+  });
+}
+
+dyngb200_status dyngb200_scheduler_get_feature_range(dyngb200_scheduler s, float* lo, float* hi,
+                                                     int32_t* has_range) {
+  return guarded([&] {
+    expects(s != nullptr, "scheduler_get_feature_range: null scheduler");
+    const Scheduler& x = s->s;
+    if (has_range) *has_range = x.has_range ? 1 : 0;
+    for (int i = 0; i < kMlpIn; ++i) {
+      if (lo) lo[i] = x.feat_lo[i];
+      if (hi) hi[i] = x.feat_hi[i];
+    }
+  });
+}
+
 dyngb200_status dyngb200_scheduler_forward(dyngb200_context ctx, dyngb200_scheduler s,
                                            const float* features, int64_t n, float* logits) {
   return guarded([&] {

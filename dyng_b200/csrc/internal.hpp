@@ -334,6 +334,11 @@ struct Scheduler {
   long long step = 0;
   float feat_mean[kMlpIn] = {};
   float feat_scale[kMlpIn] = {};  // features are standardized: (f - mean) * scale
+  // the raw feature range it was trained on: an update whose features leave it keeps the plain
+  // schedule (no extrapolation)
+  float feat_lo[kMlpIn] = {};
+  float feat_hi[kMlpIn] = {};
+  bool has_range = false;
 };
 
 // mlp.cu

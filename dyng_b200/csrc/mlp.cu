@@ -84,6 +84,8 @@ __device__ __forceinline__ void warp_forward(const float* params, const uint16_t
 struct FeatNorm {
   float mean[kMlpIn];
   float scale[kMlpIn];
+  float lo[kMlpIn], hi[kMlpIn];  // the trained range (used by inference when `ranged`)
+  int ranged;
 };
 
 __device__ __forceinline__ void load_features(const float* x, const FeatNorm& nrm, float* xs) {
@@ -326,6 +328,14 @@ __global__ void k_infer_schedule(const float* params, const uint16_t* w, FeatNor
     if (lane < 3) c->sched_classes[lane] = -1;
     return;
   }
+  // outside the trained range the network would extrapolate: keep the plain schedule
+  bool outside = false;
+  if (nrm.ranged)
+    for (int i = 0; i < kMlpIn; ++i) outside |= f[i] < nrm.lo[i] || f[i] > nrm.hi[i];
+  if (outside) {
+    if (lane < 3) c->sched_classes[lane] = -2;
+    return;
+  }
   // the MLP with one thread per output, in the arithmetic (and order) of warp_forward
   if (lane < kMlpIn) xs[lane] = round_bf((f[lane] - nrm.mean[lane]) * nrm.scale[lane]);
   __syncthreads();
@@ -378,7 +388,10 @@ FeatNorm norm_of(const Scheduler& s) {
   for (int i = 0; i < kMlpIn; ++i) {
     nrm.mean[i] = s.feat_mean[i];
     nrm.scale[i] = s.feat_scale[i];
+    nrm.lo[i] = s.feat_lo[i];
+    nrm.hi[i] = s.feat_hi[i];
   }
+  nrm.ranged = s.has_range ? 1 : 0;
   return nrm;
 }
 

@@ -17,8 +17,9 @@
 //   3. `affected` compares the new MOSP tree with the previous one (two trees, swapped);
 //   4. path costs: the first edge p -> v of each tree edge in the graph's row order (the edge
 //      index of a simple graph, else a warp-per-row scan keeping the lowest slot), then pointer
-//      jumping that sums the weights along the tree in log(depth) rounds; copied to the host
-//      (the reference keeps path costs in host memory on every backend).
+//      jumping that sums the weights along the tree in log(depth) rounds; kept on the device and
+//      copied into the caller's host buffer when read (path_costs() is host memory, as in the
+//      reference).
 #include "handles.hpp"
 
 #include <cub/device/device_scan.cuh>
@@ -257,7 +258,7 @@ struct Mosp {
   Graph combined;      // the combined graph of the last finalize step
   Tree mosp[2];        // the MOSP tree: current and spare
   int cur = 0;
-  std::vector<int64_t> costs;  // n x K, host memory (the reference's path_costs())
+  DevBuf<int64_t> costs;  // n x K of the last compute() / update(), copied out when read
   bool has_costs = false;
   bool poisoned = false;
   uint64_t graph_id = 0, version = 0;
@@ -335,8 +336,8 @@ struct FinalizeCounts {
 };
 
 // Path costs over the first `columns` weight columns of g along the current MOSP tree (n x
-// columns, vertex-major, into `out`).
-void mosp_path_costs(Context& ctx, Graph& g, Mosp& m, int columns, std::vector<int64_t>& out) {
+// columns, vertex-major): returns the scratch buffer that holds them (m.acc[0] or m.acc[1]).
+int mosp_path_costs(Context& ctx, Graph& g, Mosp& m, int columns) {
   cudaStream_t s = ctx.stream;
   const long long n = g.n;
   const Tree& t = m.tree();
@@ -376,10 +377,6 @@ void mosp_path_costs(Context& ctx, Graph& g, Mosp& m, int columns, std::vector<i
   }
   int missing = big;
   DYNGB200_CUDA(cudaMemcpyAsync(&missing, m.missing.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
-  out.resize(static_cast<size_t>(n) * columns);
-  if (n > 0)
-    DYNGB200_CUDA(cudaMemcpyAsync(out.data(), m.acc[b].ptr, out.size() * sizeof(int64_t),
-                                  cudaMemcpyDeviceToHost, s));
   DYNGB200_CUDA(cudaStreamSynchronize(s));
   if (missing != big) {
     int32_t p = -1;
@@ -388,6 +385,7 @@ void mosp_path_costs(Context& ctx, Graph& g, Mosp& m, int columns, std::vector<i
                 "mosp: the MOSP tree edge (" + std::to_string(p) + ", " + std::to_string(missing) +
                     ") is not an edge of the graph (do the trees belong to this graph?)");
   }
+  return b;
 }
 
 // Steps 2-3 of MOSP_Update on the current K trees (mosp.cpp:259-301): the combined graph, its
@@ -507,7 +505,8 @@ FinalizeCounts mosp_finalize(Context& ctx, Graph& g, Mosp& m, bool count_affecte
   t0 = std::chrono::steady_clock::now();
   m.has_costs = false;
   if (m.opt.compute_path_costs) {
-    mosp_path_costs(ctx, g, m, K, m.costs);
+    const int b = mosp_path_costs(ctx, g, m, K);
+    m.costs.swap(m.acc[b]);  // kept on the device; dyngb200_mosp_path_costs copies them out
     m.has_costs = true;
   }
   out.costs_ms = ms_since(t0);
@@ -704,8 +703,11 @@ dyngb200_status dyngb200_mosp_path_costs(dyngb200_mosp r, int64_t* costs) {
     Mosp& m = usable(r, "mosp::result::path_costs");
     expects(m.has_costs, "mosp::result::path_costs: the path costs were not computed "
                          "(options.compute_path_costs was false at the last compute() or update())");
-    expects(costs != nullptr || m.costs.empty(), "mosp::result::path_costs: null output");
-    if (!m.costs.empty()) std::memcpy(costs, m.costs.data(), m.costs.size() * sizeof(int64_t));
+    const size_t count = static_cast<size_t>(m.mosp[m.cur].n) * static_cast<size_t>(m.num_k);
+    expects(costs != nullptr || count == 0, "mosp::result::path_costs: null output");
+    DeviceGuard guard(m.device);
+    if (count) DYNGB200_CUDA(cudaMemcpy(costs, m.costs.ptr, count * sizeof(int64_t),
+                                        cudaMemcpyDeviceToHost));
   });
 }
 
@@ -722,10 +724,11 @@ dyngb200_status dyngb200_mosp_path_costs_columns(dyngb200_context ctx, dyngb200_
     expects(columns >= 1 && columns <= gr.k, "mosp path costs: columns " +
                                                  std::to_string(columns) + " is out of range [1, " +
                                                  std::to_string(gr.k) + "]");
-    std::vector<int64_t> out;
-    mosp_path_costs(ctx->ctx, gr, m, columns, out);
-    expects(costs != nullptr || out.empty(), "mosp path costs: null output");
-    if (!out.empty()) std::memcpy(costs, out.data(), out.size() * sizeof(int64_t));
+    const int b = mosp_path_costs(ctx->ctx, gr, m, columns);
+    const size_t count = static_cast<size_t>(gr.n) * static_cast<size_t>(columns);
+    expects(costs != nullptr || count == 0, "mosp path costs: null output");
+    if (count) DYNGB200_CUDA(cudaMemcpy(costs, m.acc[b].ptr, count * sizeof(int64_t),
+                                        cudaMemcpyDeviceToHost));
   });
 }
 

@@ -228,6 +228,44 @@ class BatchStream:
         return Batch(is_, id_, w, ds.astype(np.int32), dd.astype(np.int32))
 
 
+class NearSourceChurn:
+    """Batches for a grid around a centre source: half deletions, concentrated within `hops`
+    lattice hops of the source (at most a quarter of the live edges there per batch, the rest
+    uniform over the live edges), half insertions, which bring back the near edges the previous
+    batch deleted (the rest uniform pairs, lognormal weights).  The region around the source
+    churns without being cut off from it."""
+
+    def __init__(self, stream: BatchStream, side: int, source: int, hops: int = 64,
+                 insert_fraction: float = 0.5):
+        self.stream = stream
+        self.insert_fraction = insert_fraction
+        src = stream.src.astype(np.int64)
+        cx, cy = source % side, source // side
+        self.near = np.nonzero(np.abs(src % side - cx) + np.abs(src // side - cy) <= hops)[0]
+        self.back = np.zeros(0, np.int64)
+
+    def next(self, size: int) -> Batch:
+        st = self.stream
+        rng = st.rng
+        ni = int(round(size * self.insert_fraction))
+        nd = size - ni
+        live_near = self.near[st.alive[self.near]]
+        k = min(nd, live_near.size // 4)
+        pick_near = rng.choice(live_near, k, replace=False) if k else np.zeros(0, np.int64)
+        live = np.nonzero(st.alive)[0]
+        pick = np.concatenate([pick_near, live[rng.integers(0, live.size, nd - k)]])
+        st.alive[pick] = False
+        reins = self.back[:ni]
+        st.alive[reins] = True
+        m = ni - reins.size
+        is_ = np.concatenate([st.src[reins], rng.integers(0, st.n, m).astype(np.int32)])
+        id_ = np.concatenate([st.dst[reins], rng.integers(0, st.n, m).astype(np.int32)])
+        iw = np.clip(np.rint(rng.lognormal(3.0, 1.0, ni)), 1, 10000).astype(np.int32)
+        self.back = pick_near
+        return Batch(is_.astype(np.int32), id_.astype(np.int32), iw,
+                     st.src[pick].astype(np.int32), st.dst[pick].astype(np.int32))
+
+
 def uniform_batch(edges: EdgeList, num_deletions: int, num_insertions: int, seed=7, w_min=1,
                   w_max=100) -> Batch:
     """Deletions sampled uniformly from the edges, insertions of uniform random pairs."""

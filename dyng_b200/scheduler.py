@@ -120,6 +120,18 @@ def reference_forward(params: np.ndarray, mean: np.ndarray, scale: np.ndarray,
     return h
 
 
+def within_range(classes: np.ndarray, features: np.ndarray, lo, hi) -> np.ndarray:
+    """The classes the update runs with: the plain schedule's where a feature row leaves the
+    trained range [lo, hi] (as the inference kernel decides; no range: unchanged)."""
+    c = np.array(classes, np.int32, copy=True).reshape(-1, 3)
+    if lo is None:
+        return c
+    x = np.atleast_2d(np.asarray(features, np.float32))
+    out = ((x < np.asarray(lo, np.float32)) | (x > np.asarray(hi, np.float32))).any(axis=1)
+    c[out] = DEFAULT_CLASSES
+    return c
+
+
 def classes_of(logits: np.ndarray) -> np.ndarray:
     """Per-head argmax (first maximum wins, as in the kernel)."""
     lo = np.atleast_2d(logits)
@@ -175,6 +187,27 @@ class Scheduler:
             args.append(ptr)
         check(N.lib().dyngb200_scheduler_set_params(self._res._h, self._h, *args))
 
+    def set_feature_range(self, lo=None, hi=None) -> None:
+        """The raw feature range of the training set: outside it an update keeps the plain
+        schedule (stats.schedule_classes == (-2, -2, -2)).  None, None: no range."""
+        if lo is None and hi is None:
+            check(N.lib().dyngb200_scheduler_set_feature_range(self._h, None, None))
+            return
+        a, pa = _f32(lo)
+        b, pb = _f32(hi)
+        if a.size != NUM_FEATURES or b.size != NUM_FEATURES:
+            raise InvalidArgumentError("scheduler.set_feature_range: 12 values per bound")
+        check(N.lib().dyngb200_scheduler_set_feature_range(self._h, pa, pb))
+
+    def get_feature_range(self):
+        lo = np.zeros(NUM_FEATURES, np.float32)
+        hi = np.zeros(NUM_FEATURES, np.float32)
+        has = ctypes.c_int32()
+        check(N.lib().dyngb200_scheduler_get_feature_range(self._h, lo.ctypes.data_as(N.c_f32p),
+                                                           hi.ctypes.data_as(N.c_f32p),
+                                                           ctypes.byref(has)))
+        return (lo, hi) if has.value else (None, None)
+
     def forward(self, features) -> np.ndarray:
         """Logits (n x 15) of raw feature rows, computed by the device kernels."""
         x, px = _f32(np.atleast_2d(features))
@@ -186,7 +219,9 @@ class Scheduler:
         return out
 
     def predict(self, features) -> np.ndarray:
-        return classes_of(self.forward(features))
+        """The classes updates with these features run with (the trained range applied)."""
+        return within_range(classes_of(self.forward(features)), features,
+                            *self.get_feature_range())
 
     def gradients(self, features, labels):
         """(mean loss, gradient of the flat parameters) over all samples, without a step."""
@@ -213,14 +248,27 @@ class Scheduler:
 
     def save(self, path: str, **extra) -> None:
         p, m, s = self.get_params()
-        np.savez(path, params=p, feature_mean=m, feature_scale=s, **extra)
+        lo, hi = self.get_feature_range()
+        rng = {} if lo is None else {"feature_lo": lo, "feature_hi": hi}
+        np.savez(path, params=p, feature_mean=m, feature_scale=s, **rng, **extra)
 
     @classmethod
     def load(cls, path: str = PRETRAINED, resources: Resources | None = None) -> "Scheduler":
         with np.load(path) as z:
             sch = cls(resources)
             sch.set_params(z["params"], z["feature_mean"], z["feature_scale"])
+            if "feature_lo" in z.files:
+                sch.set_feature_range(z["feature_lo"], z["feature_hi"])
         return sch
+
+
+def feature_range(features: np.ndarray, margin: float = 0.5):
+    """The range of a training set, widened by `margin` (features are log2-scaled counts and
+    fractions: 0.5 is a factor 1.4 on a count) or a tenth of the span, whichever is larger."""
+    x = np.asarray(features, np.float64)
+    lo, hi = x.min(axis=0), x.max(axis=0)
+    pad = np.maximum(margin, 0.1 * (hi - lo))
+    return (lo - pad).astype(np.float32), (hi + pad).astype(np.float32)
 
 
 def standardization(features: np.ndarray):
@@ -241,6 +289,8 @@ class Workload:
     build: object
     batches: int
     max_batch: int = 1_000_000
+    source: int = 0
+    churn_side: int = 0  # > 0: a grid of this side, batches churn around the source
 
 
 def default_workloads():
@@ -251,6 +301,8 @@ def default_workloads():
         Workload("rmat-s22-ef16", lambda: rmat(22, 16, w_max=1000, seed=1, device="cuda"), 84,
                  1_000_000),
         Workload("grid-2048", lambda: grid(2048, seed=2), 40, 1_000_000),
+        Workload("grid-4096-centre", lambda: grid(4096, seed=1), 30, 1_000_000,
+                 source=2048 * 4096 + 2048, churn_side=4096),
     ]
 
 
@@ -263,7 +315,7 @@ def record_traces(workloads=None, seed: int = 11, resources: Resources | None = 
     before each), and once more with the default schedule, which also advances the stream.
     Times are the library's device times of the update (applier + sssp kernel)."""
     from .graph import EdgeBatch, Graph
-    from .generators import BatchStream
+    from .generators import BatchStream, NearSourceChurn
     from .sssp import Schedule, compute, update
     res = resources or default_resources()
     workloads = workloads or default_workloads()
@@ -275,16 +327,21 @@ def record_traces(workloads=None, seed: int = 11, resources: Resources | None = 
     for wi, wl in enumerate(workloads):
         edges = wl.build()
         g = Graph.from_csr(*edges.csr(), resources=res)
-        tree = compute(g, 0)
+        tree = compute(g, wl.source)
         g_snap, t_snap = g.clone(), tree.clone()
         stream = BatchStream(edges, seed=seed + 101 * wi)
+        churn = NearSourceChurn(stream, wl.churn_side, wl.source) if wl.churn_side else None
         log(f"{wl.name}: n={edges.num_vertices} m={edges.src.size}")
         for bi in range(wl.batches):
             size = int(round(np.exp(rng.uniform(np.log(100), np.log(wl.max_batch)))))
             ins_frac = float(rng.choice([0.0, 0.25, 0.5, 0.75, 1.0, rng.uniform()]))
             tree_frac = float(rng.uniform(0.0, 0.6))
-            b = stream.next(size, insert_fraction=ins_frac, tree_fraction=tree_frac,
-                            parents=tree.parents)
+            if churn is not None:
+                ins_frac, tree_frac = churn.insert_fraction, 0.0
+                b = churn.next(size)
+            else:
+                b = stream.next(size, insert_fraction=ins_frac, tree_fraction=tree_frac,
+                                parents=tree.parents)
             eb = EdgeBatch.from_arrays(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
                                        b.delete_dst)
             g_snap.copy_from(g)
@@ -320,6 +377,30 @@ def record_traces(workloads=None, seed: int = 11, resources: Resources | None = 
     out["settings"] = np.asarray(settings, np.int32)
     out["workload_names"] = np.asarray([w.name for w in workloads])
     return out
+
+
+def merge_traces(parts) -> dict:
+    """One trace set from several (same 96 settings); workload indices renumbered."""
+    settings = np.asarray(parts[0]["settings"])
+    out = {}
+    names = []
+    offset = 0
+    for t in parts:
+        if not np.array_equal(np.asarray(t["settings"]), settings):
+            raise InvalidArgumentError("merge_traces: the trace sets swept different settings")
+        for k, v in t.items():
+            if k in ("settings", "workload_names"):
+                continue
+            v = np.asarray(v)
+            if k == "workload":
+                v = v + offset
+            out.setdefault(k, []).append(v)
+        names += [str(x) for x in t["workload_names"]]
+        offset += len(t["workload_names"])
+    merged = {k: np.concatenate(v) for k, v in out.items()}
+    merged["settings"] = settings
+    merged["workload_names"] = np.asarray(names)
+    return merged
 
 
 def labels_of(traces: dict) -> np.ndarray:
@@ -365,6 +446,7 @@ def train_on_traces(traces: dict, epochs: int = 400, batch_size: int = 32,
     mean, scale = standardization(x[~hold])
     sch = Scheduler(resources, seed=seed)
     sch.set_params(feature_mean=mean, feature_scale=scale)
+    sch.set_feature_range(*feature_range(x[~hold]))
     loss = sch.train(x[~hold], y[~hold], epochs=epochs, batch_size=batch_size,
                      learning_rate=learning_rate, seed=seed)
     pred = sch.predict(x)
@@ -383,6 +465,10 @@ def main(argv=None):
     r.add_argument("--seed", type=int, default=11)
     r.add_argument("--scale-batches", type=float, default=1.0,
                    help="multiply every workload's batch count (0.1: a quick run)")
+    r.add_argument("--workloads", default="", help="comma-separated names (default: all)")
+    mg = sub.add_parser("merge", help="concatenate trace files recorded with the same settings")
+    mg.add_argument("inputs", nargs="+")
+    mg.add_argument("--out", required=True)
     t = sub.add_parser("train", help="train on recorded traces (on the GPU)")
     t.add_argument("traces")
     t.add_argument("--out", required=True)
@@ -391,8 +477,18 @@ def main(argv=None):
     t.add_argument("--lr", type=float, default=2e-3)
     t.add_argument("--seed", type=int, default=0)
     a = ap.parse_args(argv)
+    if a.cmd == "merge":
+        parts = []
+        for path in a.inputs:
+            with np.load(path) as z:
+                parts.append({k: z[k] for k in z.files})
+        np.savez_compressed(a.out, **merge_traces(parts))
+        return
     if a.cmd == "record":
         wls = default_workloads()
+        if a.workloads:
+            keep = set(a.workloads.split(","))
+            wls = [w for w in wls if w.name in keep]
         for w in wls:
             w.batches = max(1, int(round(w.batches * a.scale_batches)))
         traces = record_traces(wls, seed=a.seed, log=lambda s: print(s, flush=True))

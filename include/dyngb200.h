@@ -131,7 +131,8 @@ typedef struct dyngb200_stats {
   int32_t trace_heavy[64];
   float trace_us[64];
   /* The learned scheduler's view of the update (filled when a scheduler ran or the schedule asked
-   * for record_features): the 12 batch features and the class each head chose (-1: none). */
+   * for record_features): the 12 batch features and the class each head chose (-1: none; -2:
+   * the features were outside the scheduler's trained range, the plain schedule ran). */
   float features[12];
   int32_t schedule_classes[3];
   int64_t kernel_launches; /* kernels of this library the call launched */
@@ -356,6 +357,13 @@ dyngb200_status dyngb200_scheduler_set_params(dyngb200_context ctx, dyngb200_sch
 dyngb200_status dyngb200_scheduler_get_params(dyngb200_context ctx, dyngb200_scheduler s,
                                               float* params, float* feature_mean,
                                               float* feature_scale);
+/* The raw feature range the scheduler was trained on (12 floats each; NULL, NULL: no range).
+ * An update whose features fall outside it keeps the plain schedule (its stats report schedule
+ * classes -2): the network never extrapolates. */
+dyngb200_status dyngb200_scheduler_set_feature_range(dyngb200_scheduler s, const float* lo,
+                                                     const float* hi);
+dyngb200_status dyngb200_scheduler_get_feature_range(dyngb200_scheduler s, float* lo, float* hi,
+                                                     int32_t* has_range);
 /* Logits (n x 15, host) of raw feature rows (n x 12, host), by the device kernels. */
 dyngb200_status dyngb200_scheduler_forward(dyngb200_context ctx, dyngb200_scheduler s,
                                            const float* features, int64_t n, float* logits);

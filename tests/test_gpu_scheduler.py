@@ -169,6 +169,36 @@ def test_learned_updates_equal_plain_updates(D):
     assert len(seen) >= 3
 
 
+def test_outside_its_trained_range_the_scheduler_keeps_the_plain_schedule(D):
+    from dyng_b200 import scheduler as S
+    rng = np.random.default_rng(12)
+    n, s, d, w = random_graph(rng, "sparse", 2000)
+    g1 = D.Graph.from_edges(s, d, w, num_vertices=n)
+    g2 = D.Graph.from_edges(s, d, w, num_vertices=n)
+    t1, t2 = D.sssp.compute(g1, 0), D.sssp.compute(g2, 0)
+    sch = S.Scheduler(seed=5)
+    sch.set_params((rng.normal(size=S.num_params()) * 0.5).astype(np.float32))
+    # a range that excludes this graph's size feature (log2(1 + n) ~ 11)
+    lo = np.full(12, -100, np.float32)
+    hi = np.full(12, 100, np.float32)
+    hi[5] = 5.0
+    sch.set_feature_range(lo, hi)
+    assert np.array_equal(sch.get_feature_range()[1], hi)
+    for step in range(3):
+        b = _batch(D, random_batch(rng, n, s, d, 500, tree_parents=t1.parents))
+        st1 = D.sssp.update(g1, b, t1)
+        st2 = D.sssp.update(g2, b, t2, scheduler=sch)
+        assert tuple(st2.schedule_classes) == (-2, -2, -2)
+        assert (st2.delta, st2.grid_blocks) == (st1.delta, st1.grid_blocks)
+        assert np.array_equal(t1.distances, t2.distances)
+        assert np.array_equal(t1.parents, t2.parents)
+    # inside the range it chooses again
+    sch.set_feature_range(None, None)
+    st2 = D.sssp.update(g2, _batch(D, random_batch(rng, n, s, d, 500, tree_parents=t2.parents)),
+                        t2, scheduler=sch)
+    assert all(c >= 0 for c in st2.schedule_classes)
+
+
 def test_snapshot_restore_replays_a_batch(D):
     rng = np.random.default_rng(12)
     n, s, d, w = random_graph(rng, "hub", 2000)

@@ -61,9 +61,32 @@ def test_committed_weights_beat_the_heuristic_on_heldout_traces():
     assert times.shape[1] == 96 and (times > 0).all()
     with np.load(S.PRETRAINED) as z:
         p, m, s = z["params"], z["feature_mean"], z["feature_scale"]
-    pred = S.classes_of(S.reference_forward(p, m, s, traces["features"]))
+        lo, hi = (z["feature_lo"], z["feature_hi"]) if "feature_lo" in z.files else (None, None)
+    pred = S.within_range(S.classes_of(S.reference_forward(p, m, s, traces["features"])),
+                          traces["features"], lo, hi)
     hold = S.holdout_mask(traces)
     report = S.evaluate(pred, traces, hold)
     assert report["batches"] >= 30
     # the learned schedules are never slower in total than the fixed heuristic on unseen batches
     assert report["learned_ms"] <= report["default_ms"]
+
+
+def test_outside_the_trained_range_the_plain_schedule_runs():
+    x = np.zeros((3, 12), np.float32)
+    x[1, 5] = 30.0   # a graph far larger than any in training
+    x[2, 0] = -5.0
+    lo, hi = S.feature_range(np.zeros((4, 12)) + np.arange(4)[:, None])
+    got = S.within_range([[6, 1, 2]] * 3, x, lo, hi)
+    assert got.tolist() == [[6, 1, 2], list(S.DEFAULT_CLASSES), list(S.DEFAULT_CLASSES)]
+    assert S.within_range([[6, 1, 2]], x[:1], None, None).tolist() == [[6, 1, 2]]
+
+
+def test_merging_trace_sets_renumbers_workloads():
+    def part(names, rows):
+        return {"workload": np.arange(rows) % len(names), "size": np.ones(rows),
+                "features": np.zeros((rows, 12)), "times": np.ones((rows, 96)),
+                "settings": np.asarray(S.all_settings(), np.int32),
+                "workload_names": np.asarray(names)}
+    m = S.merge_traces([part(["a", "b"], 4), part(["c"], 2)])
+    assert m["workload"].tolist() == [0, 1, 0, 1, 2, 2]
+    assert m["workload_names"].tolist() == ["a", "b", "c"] and m["times"].shape == (6, 96)
