@@ -265,10 +265,27 @@ class Arm:
                 "p50_ms": float(np.percentile(self.lat, 50)),
                 "p99_ms": float(np.percentile(self.lat, 99)),
                 "apply_ms_mean": float(np.mean([s.apply_ms for s in self.stats])),
-                "sssp_ms_mean": float(np.mean([s.sssp_ms for s in self.stats]))}
+                "sssp_ms_mean": float(np.mean([s.sssp_ms for s in self.stats])),
+                # per timed step: the update (events around the call), its applier and sssp
+                # kernel times, and the host time of the call
+                "steps": [[round(t, 3), round(s.apply_ms, 3), round(s.sssp_ms, 3),
+                           round(1000 * h, 3)]
+                          for t, s, h in zip(self.lat, self.stats, self.host)],
+                "maintenance": getattr(self, "maintenance", None)}
 
 
 def run_arm(env, arm, next_batch, nvtx=False):
+    D, torch, g, tree, stream, args, world, local = env
+    import gc
+    gc.collect()  # no collection of leftover objects (and their device frees) inside a timed step
+    gc.disable()
+    try:
+        return _run_arm(env, arm, next_batch, nvtx)
+    finally:
+        gc.enable()
+
+
+def _run_arm(env, arm, next_batch, nvtx):
     D, torch, g, tree, stream, args, world, local = env
     for step in range(args.warmup + args.steps):
         b = next_batch(step)
@@ -282,6 +299,7 @@ def run_arm(env, arm, next_batch, nvtx=False):
             if world > 1:
                 torch.distributed.barrier()
             torch.cuda.synchronize()
+            storage0 = g.storage()
             if nvtx:
                 torch.cuda.nvtx.range_push("timed")
         e0 = torch.cuda.Event(enable_timing=True)
@@ -300,6 +318,11 @@ def run_arm(env, arm, next_batch, nvtx=False):
     torch.cuda.synchronize()
     if nvtx:
         torch.cuda.nvtx.range_pop()
+    # storage maintenance inside the timed steps (edge-index builds, arena growths, compactions)
+    storage1 = g.storage()
+    arm.maintenance = {k: round(storage1[k] - storage0[k], 3) for k in
+                       ("index_builds", "arena_growths", "compactions", "index_ms", "grow_ms",
+                        "compact_ms")}
     from dyng_b200.replicas import max_over_ranks
     arm.total_ms = max_over_ranks(float(sum(arm.lat)))
     return arm
@@ -449,7 +472,8 @@ def main():
                    "sample": f"failed: {exc}"}
 
     if rank == 0:
-        compare = {k: {kk: round(vv, 4) if kk != "value" else vv for kk, vv in v.items()}
+        compare = {k: {kk: round(vv, 4) if kk not in ("value", "steps", "maintenance") else vv
+                       for kk, vv in v.items()}
                    for k, v in summ.items()}
         if "learned" in summ:
             compare["learned_over_plain"] = summ["learned"]["value"] / summ["plain"]["value"]

@@ -121,6 +121,11 @@ struct ApplyParams {
   long long* col_written_max;
   long long* col_written_at_max;
   UpdateCtl* ctl;
+  // the learned scheduler's batch features, accumulated by k_validate when `feat` is set: the
+  // tree the update repairs (parent array, its vertex count)
+  const int32_t* feat_parent;
+  long long feat_tree_n;
+  int feat;
 };
 
 // Pair flags.
@@ -152,8 +157,27 @@ __global__ void k_validate(ApplyParams p) {
   long long top = 0;
   long long wmax = 1;
   int dropped = 0;
+  // scheduler features: tree-edge deletions, source out-degree sum / max / count
+  long long f_tree = 0, f_deg = 0, f_max = 0, f_srcs = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
+    if (p.feat) {
+      const bool del = i >= p.ni;
+      const long long j = del ? i - p.ni : i;
+      const int32_t u = del ? p.del_src[j] : p.ins_src[j];
+      if (u >= 0 && u < n) {
+        const long long deg = p.g.out_desc[u].len;
+        f_deg += deg;
+        f_max = deg > f_max ? deg : f_max;
+        ++f_srcs;
+      }
+      if (del && p.feat_parent) {
+        const int32_t v = p.del_dst[j];
+        if (u >= 0 && v >= 0 && u < p.feat_tree_n && v < p.feat_tree_n &&
+            (p.feat_parent[v] == u || (!p.props.directed && p.feat_parent[u] == v)))
+          ++f_tree;
+      }
+    }
     if (i < p.ni) {
       const int32_t u = p.ins_src[i], v = p.ins_dst[i];
       if (p.objective >= 0) {
@@ -199,6 +223,12 @@ __global__ void k_validate(ApplyParams p) {
   warp_max(top, &c->n_after, 0);
   if (p.objective >= 0) warp_max(wmax, &c->batch_ins_max, 1);
   warp_add(dropped, &c->summary[5]);
+  if (p.feat) {
+    warp_add(f_tree, &c->feat_acc[0]);
+    warp_add(f_deg, &c->feat_acc[1]);
+    warp_max(f_max, &c->feat_acc[2], 0);
+    warp_add(f_srcs, &c->feat_acc[3]);
+  }
 }
 
 // ---- the per-batch reset: an empty pair table and zero column deltas ---------------------------
@@ -1888,14 +1918,19 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
                                 cudaMemcpyHostToDevice, s));
   ApplyParams p = make_params(ctx, g, b, objective, delta_opt);
   p.touch_gen = touch_gen;
+  // the learned scheduler's batch features come from the validation pass (the batch, the old
+  // rows and the tree before anything changes); its inference follows the plan's default width
+  const bool features = tree && (learned || (sched && sched->record_features));
+  if (features) {
+    p.feat = 1;
+    p.feat_parent = tree->parent.ptr;
+    p.feat_tree_n = tree->n;
+  }
   const int grid_ops = grid_for(b.ni + b.nd, kBlock, ctx.sm_count);
   k_validate<<<grid_ops, kBlock, 0, s>>>(p);
   k_plan<<<1, 1, 0, s>>>(p);
   ctx.launches += g.props.sorted ? 5 : 8;  // validate, plan, pairs, match, resolve (+ 3 ordering)
-  // the learned scheduler reads the batch, the old rows and the tree before anything changes,
-  // and writes its schedule into the control block (after the plan's default width)
-  if (tree && (learned || (sched && sched->record_features)))
-    launch_learned_schedule(ctx, g, *tree, b, learned);
+  if (features) launch_learned_schedule(ctx, g, *tree, b, learned);
   k_pairs<<<grid_ops, kBlock, 0, s>>>(p);
   if (g.props.allow_multi) {
     k_scan_multi<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);

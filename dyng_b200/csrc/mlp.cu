@@ -244,47 +244,6 @@ __global__ void k_refresh_bf16(const float* params, uint16_t* w) {
   }
 }
 
-// Feature accumulators of one batch, read before the applier changes anything: tree-edge
-// deletions (the deleted edge is the head's parent edge), and the out-degree sum, maximum and
-// count of the batch's source vertices.
-__global__ void k_features_acc(const int32_t* ins_src, long long ni, const int32_t* del_src,
-                               const int32_t* del_dst, long long nd, const RowDesc* out_desc,
-                               long long n_valid, const int32_t* parent, long long tree_n,
-                               int directed, UpdateCtl* c) {
-  long long tree_dels = 0, deg_sum = 0, deg_max = 0, srcs = 0;
-  const long long total = ni + nd;
-  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const bool del = i >= ni;
-    const long long j = del ? i - ni : i;
-    const int32_t u = del ? del_src[j] : ins_src[j];
-    if (u >= 0 && u < n_valid) {
-      const long long deg = out_desc[u].len;
-      deg_sum += deg;
-      deg_max = deg > deg_max ? deg : deg_max;
-      ++srcs;
-    }
-    if (del && parent) {
-      const int32_t v = del_dst[j];
-      if (u >= 0 && v >= 0 && u < tree_n && v < tree_n &&
-          (parent[v] == u || (!directed && parent[u] == v)))
-        ++tree_dels;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    tree_dels += __shfl_down_sync(0xffffffffu, tree_dels, o);
-    deg_sum += __shfl_down_sync(0xffffffffu, deg_sum, o);
-    deg_max = max(deg_max, __shfl_down_sync(0xffffffffu, deg_max, o));
-    srcs += __shfl_down_sync(0xffffffffu, srcs, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (tree_dels) atomicAdd(reinterpret_cast<unsigned long long*>(&c->feat_acc[0]), tree_dels);
-    if (deg_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&c->feat_acc[1]), deg_sum);
-    if (deg_max) atomicMax(&c->feat_acc[2], deg_max);
-    if (srcs) atomicAdd(reinterpret_cast<unsigned long long*>(&c->feat_acc[3]), srcs);
-  }
-}
-
 __device__ __forceinline__ float lg(double v) { return static_cast<float>(log2(1.0 + (v > 0 ? v : 0))); }
 
 // The 12 features of one update, the MLP on them and the schedule it picks (one warp).  Runs
@@ -296,10 +255,15 @@ __global__ void k_infer_schedule(const float* params, const uint16_t* w, FeatNor
   __shared__ float f[kMlpIn];
   __shared__ float xs[kMlpIn];
   __shared__ float h1[kMlpHidden], h2[kMlpHidden], lo[kMlpOut];
-  __shared__ uint16_t sw[kBfCount];  // the bf16 weights, staged with coalesced loads
+  // the bf16 weights, staged with 16-byte loads by warps 1..3 while lane 0 of warp 0 reads the
+  // features
+  __shared__ __align__(16) uint16_t sw[kBfCount];
+  static_assert(kBfCount % 8 == 0, "bf16 weights are staged 8 at a time");
   const int lane = threadIdx.x;
-  if (params) {
-    for (int i = threadIdx.x; i < kBfCount; i += blockDim.x) sw[i] = w[i];
+  if (params && threadIdx.x >= 32) {
+    const uint4* src = reinterpret_cast<const uint4*>(w);
+    uint4* dst = reinterpret_cast<uint4*>(sw);
+    for (int i = threadIdx.x - 32; i < kBfCount / 8; i += blockDim.x - 32) dst[i] = src[i];
   }
   if (lane == 0) {
     const long long ops = ni + nd;
@@ -576,21 +540,13 @@ void scheduler_train(Context& ctx, Scheduler& s, const float* x, const int32_t* 
   if (final_loss) *final_loss = l;
 }
 
-// Queued by the applier after its plan: features of this batch and, with a scheduler, the
-// schedule the MLP picks, written into the control block that the persistent kernel reads.
+// Queued by the applier after its plan (its validation pass accumulated the batch features in
+// the control block): the features and, with a scheduler, the schedule the MLP picks, written
+// into the control block that the persistent kernel reads.
 void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch& b,
                              const Scheduler* sch) {
   cudaStream_t s = ctx.stream;
   UpdateCtl* c = ctx.ws.ctl.ptr;
-  const long long total = b.ni + b.nd;
-  if (total > 0) {
-    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(
-        (total + 255) / 256, static_cast<long long>(ctx.sm_count) * 4)));
-    k_features_acc<<<grid, 256, 0, s>>>(b.ins_src, b.ni, b.del_src, b.del_dst, b.nd,
-                                        g.out_desc.ptr, g.n, t.parent.ptr, t.n,
-                                        g.props.directed, c);
-    ++ctx.launches;
-  }
   const int blocks = ctx.update_blocks_per_sm * ctx.sm_count;
   FeatNorm nrm{};
   if (sch) nrm = norm_of(*sch);
