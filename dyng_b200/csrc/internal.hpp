@@ -176,11 +176,10 @@ struct UpdateCtl {
   int trace_len;
   unsigned pj_t[24];  // start of each pointer-jumping round (ns since the kernel began)
   unsigned pj_done[24];  // the last block's arrival at the barrier ending each round
-  // grid barrier: blocks arrive on one of kBarGroups group counters, the last of each group on
-  // bar_count, the last group flips bar_gen
-  unsigned bar_count;
-  unsigned bar_gen;
-  unsigned bar_group[32];
+  // grid barrier: one arrival counter and the generation word the blocks wait on, each on its own
+  // 128-byte line (the polling of the generation does not slow the arrivals)
+  alignas(128) unsigned bar_count;
+  alignas(128) unsigned bar_gen;
 };
 
 // Scratch memory of a context, sized on demand and reused (the reference's workspace pool).

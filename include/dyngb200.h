@@ -126,6 +126,8 @@ typedef struct dyngb200_stats {
   /* Trace of the first 64 steps of the near-far loop: light frontier size (negative: an epoch
    * with that many far vertices), heavy chunks, and the step's start in microseconds since the
    * kernel began. */
+  /* The first 64 near-far steps: light frontier entries, heavy-row chunks (bit 30 set: the step
+   * ran block-local, in the small-frontier mode), and the time since the kernel began. */
   int32_t trace_len;
   int32_t trace_light[64];
   int32_t trace_heavy[64];
