@@ -92,6 +92,7 @@ class Server {
   long long waiting_ = 0, running_ = 0;
   long long held_bytes_ = 0;  // pinned copies of queued batches (submit waits above the cap)
   static constexpr long long kHeldCap = 1LL << 30;
+  static constexpr double kLargeMaxWaitMs = 5.0;  // a large batch waits at most this long
   dyngb200_server_info info_{};
 };
 
@@ -126,11 +127,12 @@ Server::Server(const dyngb200_server_config& cfg, const Scheduler* learned)
   monitor_ = std::thread([this] { monitor(); });
 }
 
-// The free-memory query can take tens of milliseconds on a busy machine: it runs here, every
-// kMonitorMs, and the dispatcher reads the last sample minus what it admitted since.
+// The free-memory query can take tens to hundreds of milliseconds on a busy machine, and while
+// it runs the driver delays device allocations (an arena growth waited 0.3 s behind it): it runs
+// here, every kMonitorMs, and the dispatcher reads the last sample minus what it admitted since.
 void Server::monitor() {
   cudaSetDevice(cfg_.device);
-  constexpr int kMonitorMs = 20;
+  constexpr int kMonitorMs = 250;
   std::unique_lock<std::mutex> lk(mu_);
   while (!stop_) {
     monitor_cv_.wait_for(lk, std::chrono::milliseconds(kMonitorMs), [&] { return stop_; });
@@ -183,12 +185,12 @@ int Server::add_graph(Graph& g, Tree& t) {
                     std::to_string(free_b) + " free)");
   sg->ctx->ws.reserve_vertices(g.n_cap, stream_);
   DYNGB200_CUDA(cudaStreamSynchronize(stream_));
-  // room for the graph to grow (an index doubling, an arena growth) kept in the device pool, so
-  // that growth while serving does not wait for the driver
+  // room for the graph to grow (index doublings, arena growths) kept in the device pool, so that
+  // growth while serving does not wait for the driver
   const long long graph_bytes =
       2 * (g.n_cap * 16 + g.arena_cap * (4 + 4LL * g.k)) + 16 * g.ecap;
-  if (static_cast<long long>(free_b) - need - graph_bytes / 2 > 2 * cfg_.hbm_reserve_bytes)
-    device_pool_reserve(static_cast<size_t>(graph_bytes / 2));
+  if (static_cast<long long>(free_b) - need - graph_bytes > 2 * cfg_.hbm_reserve_bytes)
+    device_pool_reserve(static_cast<size_t>(graph_bytes));
   sg->g = &g;
   sg->t = &t;
   std::unique_lock<std::mutex> lk(mu_);
@@ -340,13 +342,10 @@ void Server::run() {
       const bool known = free_sample_ >= 0;
       long long free_left = known ? free_sample_ - admitted_since_ - cfg_.hbm_reserve_bytes : 0;
       const size_t ng = graphs_.size();
-      for (size_t step = 0; step < ng && static_cast<int>(group.size()) < cfg_.max_group; ++step) {
-        const size_t gi = (next_graph_ + step) % ng;
+      // take the head of graph gi into this round: admitted, or failed by admission (then done)
+      auto take = [&](size_t gi) {
         ServerGraph& sg = *graphs_[gi];
-        if (sg.queue.empty()) continue;
         ServerRequest* r = sg.queue.front();
-        const bool large = r->ops > cfg_.small_changes;
-        if (large && !group.empty()) continue;  // a large batch runs in a round of its own
         sg.queue.pop_front();
         --waiting_;
         r->start = Clock::now();
@@ -363,13 +362,37 @@ void Server::run() {
           held_bytes_ -= held_of(*r);
           if (pool_.size() < 64) pool_.push_back(std::move(r->data));
           r->data.reset();
-          continue;
+          return;
         }
         free_left -= need;
         admitted_since_ += need;
         group.push_back(r);
-        if (large) break;
+      };
+      // Small batches first: a round takes the small heads of the graphs (round-robin), so a
+      // small batch waits for at most the round in flight, not for queued large batches.  A
+      // large batch runs in a round of its own when no small head waits, or once it has waited
+      // kLargeMaxWaitMs (no starvation).  Per-graph FIFO order holds: only heads are taken.
+      const Clock::time_point now = Clock::now();
+      size_t oldest_large = ng;
+      for (size_t gi = 0; gi < ng; ++gi) {
+        const auto& q = graphs_[gi]->queue;
+        if (q.empty() || q.front()->ops <= cfg_.small_changes) continue;
+        if (oldest_large == ng ||
+            q.front()->arrival < graphs_[oldest_large]->queue.front()->arrival)
+          oldest_large = gi;
       }
+      const bool overdue =
+          oldest_large < ng &&
+          ms_between(graphs_[oldest_large]->queue.front()->arrival, now) > kLargeMaxWaitMs;
+      if (!overdue) {
+        for (size_t step = 0; step < ng && static_cast<int>(group.size()) < cfg_.max_group;
+             ++step) {
+          const size_t gi = (next_graph_ + step) % ng;
+          const auto& q = graphs_[gi]->queue;
+          if (!q.empty() && q.front()->ops <= cfg_.small_changes) take(gi);
+        }
+      }
+      if (group.empty() && oldest_large < ng) take(oldest_large);
       next_graph_ = ng ? (next_graph_ + 1) % ng : 0;
       running_ += static_cast<long long>(group.size());
     }
