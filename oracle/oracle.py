@@ -139,6 +139,8 @@ def lib():
         L.orc_packs_parents.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
         L.orc_distances_fit.restype = ctypes.c_int
         L.orc_distances_fit.argtypes = [ctypes.c_int64, ctypes.c_int64]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_get_threads.restype = ctypes.c_int
         L.orc_mosp_combine.restype = ctypes.c_int64
         L.orc_mosp_combine.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int, _i32p, _i32p,
                                        ctypes.c_int32, _i32p, _i32p, _i32p, _i64p]
@@ -390,3 +392,10 @@ def mosp_finalize(g: Graph, source: int, parents, preferences=None, cost_columns
         raise OracleError(f"the MOSP tree edge ({int(tree.parents[missing])}, {missing}) is not "
                           "an edge of the graph")
     return MospTree(tree.distances, tree.parents, costs[:n * C].reshape(n, C), m, L)
+
+
+def set_threads(threads: int) -> int:
+    """Threads of the oracle's parallel loops (CSR assembly, transposition); 1 = sequential.
+    Results are identical for every count.  Returns the count in effect."""
+    lib().orc_set_threads(int(threads))
+    return int(lib().orc_get_threads())

@@ -33,6 +33,11 @@
  * transposed CSR plus weight-increase masks, cpp/tests/data/mosp_combined: 9 combined-graph
  * cases), converted by tests/golden/make_golden.py.
  *
+ * Threads: orc_set_threads(T > 1) runs the CSR assembly and the transposition of every apply
+ * on T OpenMP threads (the reference's host path parallelises the same loops, apply_host.cpp:
+ * 264-306, 417-468); the repair itself stays sequential.  Results are identical for every T.
+ * The checker runs with one thread; the CPU-baseline timings use the host's cores.
+ *
  * Errors are returned as negative status codes with a message in the caller's buffer; nothing
  * aborts.  All memory is owned by the orc_graph handle or by the caller.
  */
@@ -40,8 +45,20 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#else
+static int omp_get_thread_num(void) { return 0; }
+#endif
 
 #define ORC_INF ((int64_t)(INT64_MAX / 4)) /* sssp_infinity, problem.hpp:340-341 */
+
+/* Threads of the parallel loops (the reference's OpenMP host path parallelises the CSR assembly
+ * and the transposition the same way, apply_host.cpp:264-306, 417-468).  1 (the default): every
+ * loop runs sequentially, as the checker does; results are identical for every thread count. */
+static int g_threads = 1;
+void orc_set_threads(int threads) { g_threads = threads > 1 ? threads : 1; }
+int orc_get_threads(void) { return g_threads; }
 
 enum {
   ORC_OK = 0,
@@ -116,19 +133,73 @@ static int transpose(orc_graph* g) {
     free(position);
     return ORC_OUT_OF_MEMORY;
   }
-  for (int64_t e = 0; e < m; ++e) g->in_row_ptr[g->col[e] + 1]++;
-  for (int64_t v = 0; v < n; ++v) g->in_row_ptr[v + 1] += g->in_row_ptr[v];
-  memcpy(cursor, g->in_row_ptr, (size_t)n * sizeof(int64_t));
-  for (int64_t u = 0; u < n; ++u) {
-    for (int64_t e = g->row_ptr[u]; e < g->row_ptr[u + 1]; ++e) {
-      const int64_t pos = cursor[g->col[e]]++;
-      position[e] = pos;
-      g->in_col[pos] = (int32_t)u;
+  if (g_threads > 1) {
+    /* A counting sort per thread: thread t owns the out-rows [u_t, u_t+1) (contiguous slots in
+     * ascending order), counts its in-degrees privately, then writes each of its slots at
+     * in_row_ptr[v] + (slots of v from threads before t) + (its own earlier slots of v): the
+     * in-row order is the out-edge order, as in the sequential loop, with no atomics and no
+     * sort (the reference sorts each in-row after an atomic scatter, apply_host.cpp:417-468). */
+    const int T = g_threads;
+    int64_t* ubound = (int64_t*)xmalloc((size_t)(T + 1) * sizeof(int64_t));
+    int32_t* cnt = (int32_t*)calloc((size_t)T * (size_t)(n > 0 ? n : 1), sizeof(int32_t));
+    ubound[0] = 0;
+    for (int t = 1; t < T; ++t) {  /* split the slots evenly, on row boundaries */
+      const int64_t target = m * t / T;
+      int64_t lo = ubound[t - 1], hi = n;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (g->row_ptr[mid] < target) lo = mid + 1;
+        else hi = mid;
+      }
+      ubound[t] = lo;
+    }
+    ubound[T] = n;
+#pragma omp parallel num_threads(T)
+    {
+      const int t = omp_get_thread_num();
+      int32_t* c = cnt + (size_t)t * (size_t)n;
+      for (int64_t e = g->row_ptr[ubound[t]]; e < g->row_ptr[ubound[t + 1]]; ++e) c[g->col[e]]++;
+#pragma omp barrier
+#pragma omp for schedule(static)
+      for (int64_t v = 0; v < n; ++v) {  /* per vertex: threads' counts become offsets */
+        int64_t sum = 0;
+        for (int q = 0; q < T; ++q) {
+          const int32_t x = cnt[(size_t)q * (size_t)n + (size_t)v];
+          cnt[(size_t)q * (size_t)n + (size_t)v] = (int32_t)sum;
+          sum += x;
+        }
+        g->in_row_ptr[v + 1] = sum;
+      }
+#pragma omp single
+      for (int64_t v = 0; v < n; ++v) g->in_row_ptr[v + 1] += g->in_row_ptr[v];
+      /* implicit barrier after single */
+      for (int64_t u = ubound[t]; u < ubound[t + 1]; ++u) {
+        for (int64_t e = g->row_ptr[u]; e < g->row_ptr[u + 1]; ++e) {
+          const int32_t v = g->col[e];
+          const int64_t pos = g->in_row_ptr[v] + c[v]++;
+          position[e] = pos;
+          g->in_col[pos] = (int32_t)u;
+        }
+      }
+    }
+    free(ubound);
+    free(cnt);
+  } else {
+    for (int64_t e = 0; e < m; ++e) g->in_row_ptr[g->col[e] + 1]++;
+    for (int64_t v = 0; v < n; ++v) g->in_row_ptr[v + 1] += g->in_row_ptr[v];
+    memcpy(cursor, g->in_row_ptr, (size_t)n * sizeof(int64_t));
+    for (int64_t u = 0; u < n; ++u) {
+      for (int64_t e = g->row_ptr[u]; e < g->row_ptr[u + 1]; ++e) {
+        const int64_t pos = cursor[g->col[e]]++;
+        position[e] = pos;
+        g->in_col[pos] = (int32_t)u;
+      }
     }
   }
   for (int k = 0; k < g->k; ++k) {
     const int32_t* in = g->w + (size_t)k * (size_t)m;
     int32_t* out = g->in_w + (size_t)k * (size_t)m;
+#pragma omp parallel for num_threads(g_threads) if (g_threads > 1) schedule(static)
     for (int64_t e = 0; e < m; ++e) out[position[e]] = in[e];
   }
   free(cursor);
@@ -551,6 +622,7 @@ int orc_graph_apply(orc_graph* g, int64_t num_inserts, const int32_t* ins_src,
     if (status == ORC_OK) {
       /* assemble the updated CSR */
       int64_t* new_row = (int64_t*)calloc((size_t)rows + 1, sizeof(int64_t));
+#pragma omp parallel for num_threads(g_threads) if (g_threads > 1) schedule(static)
       for (int64_t u = 0; u < rows; ++u) {
         int64_t deg = 0;
         if (row_off[u] >= 0) {
@@ -558,11 +630,13 @@ int orc_graph_apply(orc_graph* g, int64_t num_inserts, const int32_t* ins_src,
         } else if (u < n) {
           deg = g->row_ptr[u + 1] - g->row_ptr[u];
         }
-        new_row[u + 1] = new_row[u] + deg;
+        new_row[u + 1] = deg;
       }
+      for (int64_t u = 0; u < rows; ++u) new_row[u + 1] += new_row[u];
       const int64_t m_new = new_row[rows];
       int32_t* new_col = (int32_t*)xmalloc((size_t)m_new * sizeof(int32_t));
       int32_t* new_w = (int32_t*)xmalloc((size_t)m_new * (size_t)k * sizeof(int32_t));
+#pragma omp parallel for num_threads(g_threads) if (g_threads > 1) schedule(dynamic, 4096)
       for (int64_t u = 0; u < rows; ++u) {
         int64_t out = new_row[u];
         if (row_off[u] < 0) {

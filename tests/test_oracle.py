@@ -303,3 +303,30 @@ def test_mosp_thesis_worked_example():
         while m.parents[walk[-1]] >= 0:
             walk.append(int(m.parents[walk[-1]]))
         assert m.scale == 4 and walk == path and m.costs[6].tolist() == cost
+
+
+def test_parallel_apply_equals_sequential():
+    # the CPU-baseline timing runs the oracle's CSR assembly and transposition on several
+    # threads: graphs (out and in rows, weights) and repaired trees equal the sequential run
+    from dyng_b200 import generators as G
+    e = G.rmat(12, 16, w_max=100, seed=4)
+    rp, col, w = e.csr()
+    out = {}
+    try:
+        for threads in (1, 4):
+            O.set_threads(threads)
+            g = O.Graph.from_csr(rp, col, w, 1, O.default_props())
+            t, _ = O.compute(g, 0, rule=1)
+            stream = G.BatchStream(e, seed=5)
+            for _ in range(3):
+                b = stream.next(3000, 0.75, 0.5, parents=t.parents)
+                O.update(g, O.Batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                                    b.delete_dst), t)
+            out[threads] = (g.to_csr(), t.distances.copy(), t.parents.copy())
+    finally:
+        O.set_threads(1)
+    a, b = out[1], out[4]
+    for key in a[0]:
+        np.testing.assert_array_equal(a[0][key], b[0][key], err_msg=key)
+    np.testing.assert_array_equal(a[1], b[1])
+    np.testing.assert_array_equal(a[2], b[2])
