@@ -399,6 +399,170 @@ stats update(const resources& res, graph<V, E, W>& g, const edge_batch_view<V, W
 }
 
 }  // namespace sssp
+
+// ---- mosp (mosp.hpp:79-506) ----------------------------------------------------------------------
+namespace mosp {
+
+inline constexpr int max_objectives = 64;
+inline constexpr std::int64_t max_preference_scale = std::int64_t{1} << 20;
+
+// mosp::options (mosp.hpp:79-101).
+struct options {
+  std::vector<std::int32_t> preferences;
+  std::int64_t delta = 0;
+  engine cuda_engine = engine::automatic;
+  bool compute_path_costs = true;
+  bool validate_inputs = true;
+  int num_objectives = 0;
+  dyngb200_mosp_options native() const {
+    dyngb200_mosp_options o{};
+    o.num_objectives = num_objectives;
+    o.num_preferences = static_cast<std::int32_t>(preferences.size());
+    o.preferences = preferences.empty() ? nullptr : preferences.data();
+    o.delta = delta;
+    o.compute_path_costs = compute_path_costs ? 1 : 0;
+    o.validate_inputs = validate_inputs ? 1 : 0;
+    return o;
+  }
+};
+
+// mosp::stats (mosp.hpp:115-125): the batch, `affected`, the combined graph's edges, L and the
+// K sssp updates in objective order.
+struct stats : dyngb200_mosp_stats {
+  std::vector<sssp::stats> objectives;
+};
+
+// mosp::result (mosp.hpp:138-348): the K trees, the MOSP tree and the path costs.
+template <typename V = std::int32_t, typename D = std::int64_t>
+class result {
+  static_assert(detail::is_i32<V> && std::is_same_v<D, std::int64_t>,
+                "dyng_b200 builds mosp::result<int32, int64>");
+
+ public:
+  // result::from_arrays (mosp.hpp:300-347): K host trees of n entries each.
+  template <typename E, typename W>
+  static result from_arrays(const resources& res, const graph<V, E, W>& g, V source,
+                            const std::vector<std::vector<D>>& distances,
+                            const std::vector<std::vector<V>>& parents,
+                            bool canonicalize = true, const options& opt = {}) {
+    if (distances.size() != parents.size())
+      throw invalid_argument_error("mosp::result::from_arrays: as many distance as parent arrays");
+    std::vector<const std::int64_t*> dp;
+    std::vector<const std::int32_t*> pp;
+    std::int64_t n = distances.empty() ? 0 : static_cast<std::int64_t>(distances[0].size());
+    for (std::size_t k = 0; k < distances.size(); ++k) {
+      if (static_cast<std::int64_t>(distances[k].size()) != n ||
+          static_cast<std::int64_t>(parents[k].size()) != n)
+        throw invalid_argument_error("mosp::result::from_arrays: arrays of different lengths");
+      dp.push_back(distances[k].data());
+      pp.push_back(parents[k].data());
+    }
+    const dyngb200_mosp_options o = opt.native();
+    dyngb200_mosp m = nullptr;
+    detail::check(dyngb200_mosp_from_arrays(res.handle(), g.handle(), source,
+                                            static_cast<std::int32_t>(dp.size()), dp.data(),
+                                            pp.data(), n, DYNGB200_HOST, canonicalize ? 1 : 0, &o,
+                                            &m));
+    return result(m, opt);
+  }
+  int num_objectives() const { return info().k; }
+  V source() const { return info().source; }
+  std::int64_t preference_scale() const { return info().scale; }
+  std::uint64_t graph_version() const { return info().version; }
+  const options& get_options() const { return opt_; }
+  void set_options(const options& opt) {
+    const dyngb200_mosp_options o = opt.native();
+    detail::check(dyngb200_mosp_set_options(h_.get(), &o));
+    opt_ = opt;
+  }
+  // The trees of the objectives and the MOSP tree: device views (read with dyng::to_vector),
+  // valid until the next update of this result.
+  array_view<D> distances(int objective) const {
+    const dyngb200_tree t = tree(objective);
+    const std::int64_t* d = nullptr;
+    detail::check(dyngb200_tree_device_arrays(t, &d, nullptr));
+    auto h = h_;
+    return {d, info().n, memory_space::device, [h, t](const resources& r, D* out) {
+              detail::check(dyngb200_tree_distances(r.handle(), t, out, DYNGB200_HOST));
+            }};
+  }
+  array_view<V> parents(int objective) const {
+    const dyngb200_tree t = tree(objective);
+    const std::int32_t* p = nullptr;
+    detail::check(dyngb200_tree_device_arrays(t, nullptr, &p));
+    auto h = h_;
+    return {p, info().n, memory_space::device, [h, t](const resources& r, V* out) {
+              detail::check(dyngb200_tree_parents(r.handle(), t, out, DYNGB200_HOST));
+            }};
+  }
+  array_view<D> combined_distances() const {
+    auto h = h_;
+    return {nullptr, info().n, memory_space::device, [h](const resources&, D* out) {
+              detail::check(dyngb200_mosp_combined(h.get(), out, nullptr, DYNGB200_HOST));
+            }};
+  }
+  array_view<V> combined_parents() const {
+    auto h = h_;
+    return {nullptr, info().n, memory_space::device, [h](const resources&, V* out) {
+              detail::check(dyngb200_mosp_combined(h.get(), nullptr, out, DYNGB200_HOST));
+            }};
+  }
+  // n x K, vertex-major (costs[v * K + k]); host memory, as the reference's path_costs().
+  std::vector<D> path_costs() const {
+    const info_t i = info();
+    std::vector<D> out(static_cast<std::size_t>(i.n) * static_cast<std::size_t>(i.k));
+    detail::check(dyngb200_mosp_path_costs(h_.get(), out.data()));
+    return out;
+  }
+  dyngb200_mosp handle() const { return h_.get(); }
+  result(dyngb200_mosp m, const options& opt)
+      : h_(m, [](dyngb200_mosp p) { dyngb200_mosp_destroy(p); }), opt_(opt) {}
+
+ private:
+  struct info_t {
+    std::int32_t k;
+    std::int64_t n;
+    std::int64_t scale;
+    std::int32_t source;
+    std::uint64_t version;
+  };
+  info_t info() const {
+    info_t i{};
+    detail::check(dyngb200_mosp_info(h_.get(), &i.k, &i.n, &i.scale, &i.source, &i.version));
+    return i;
+  }
+  dyngb200_tree tree(int objective) const {
+    dyngb200_tree t = nullptr;
+    detail::check(dyngb200_mosp_tree(h_.get(), objective, &t));
+    return t;
+  }
+  std::shared_ptr<dyngb200_mosp_s> h_;
+  options opt_;
+};
+
+// mosp::compute(resources::cuda(), g, source, opt) (mosp.hpp:444-449).
+template <typename V, typename E, typename W>
+result<V> compute(const resources& res, const graph<V, E, W>& g, V source,
+                  const options& opt = {}) {
+  const dyngb200_mosp_options o = opt.native();
+  dyngb200_mosp m = nullptr;
+  detail::check(dyngb200_mosp_compute(res.handle(), g.handle(), source, &o, &m));
+  return result<V>(m, opt);
+}
+
+// mosp::update(resources::cuda(), g, batch, r) (mosp.hpp:502-506).
+template <typename V, typename E, typename W>
+stats update(const resources& res, graph<V, E, W>& g, const edge_batch_view<V, W>& batch,
+             result<V>& r) {
+  stats st{};
+  st.objectives.resize(static_cast<std::size_t>(r.num_objectives()));
+  const dyngb200_batch b = batch.native();
+  detail::check(dyngb200_mosp_update(res.handle(), g.handle(), &b, r.handle(), &st,
+                                     st.objectives.data()));
+  return st;
+}
+
+}  // namespace mosp
 }  // namespace dyng
 
 #endif  // DYNG_B200_DYNG_HPP
