@@ -74,14 +74,15 @@ class Schedule(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_group", ctypes.c_int32),
-                ("small_changes", ctypes.c_int64), ("hbm_reserve_bytes", ctypes.c_int64)]
+                ("small_changes", ctypes.c_int64), ("hbm_reserve_bytes", ctypes.c_int64),
+                ("lanes", ctypes.c_int32)]
 
 
 class RequestTimes(ctypes.Structure):
     _fields_ = [("queued_ms", ctypes.c_double), ("service_ms", ctypes.c_double),
                 ("total_ms", ctypes.c_double), ("group_size", ctypes.c_int32),
                 ("begin_ms", ctypes.c_double), ("round_ms", ctypes.c_double),
-                ("copy_ms", ctypes.c_double)]
+                ("copy_ms", ctypes.c_double), ("lane", ctypes.c_int32)]
 
 
 class GraphStorage(ctypes.Structure):
@@ -107,7 +108,8 @@ class MospStats(ctypes.Structure):
 
 class ServerInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "failed", "rounds",
-                                              "max_group", "waiting", "admission_us_max")]
+                                              "max_group", "waiting", "admission_us_max",
+                                              "lanes", "large_rounds")]
 
 
 # Every symbol of include/dyngb200.h with (restype, argtypes).

@@ -227,6 +227,9 @@ struct Context {
   long long launches = 0;  // kernels this context has launched (reported per call in the stats)
   int update_blocks_per_sm = 0;
   int compute_blocks_per_sm = 0;
+  // cap on the update's persistent grid (0: occupancy x SMs); the serving loop's lanes split the
+  // SMs' block slots between two concurrent persistent kernels with it
+  int max_update_blocks = 0;
   Workspace ws;
   // the learned scheduler's hook: when set, the next update runs with this schedule
   dyngb200_schedule schedule{};
@@ -415,6 +418,10 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
                        const dyngb200_schedule& sched, const Scheduler* learned,
                        PendingUpdate& u);
 void sssp_update_end(PendingUpdate& u, dyngb200_stats* st);
+// The update's persistent kernel: blocks an SM holds at once, and the grid an update launches
+// (occupancy x SMs, or Context::max_update_blocks when smaller).
+int update_blocks_per_sm(Context& ctx);
+int update_grid_blocks(Context& ctx);
 void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree* const* trees,
                       int count, dyngb200_stats* stats);
 void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,

@@ -547,7 +547,7 @@ void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch&
                              const Scheduler* sch) {
   cudaStream_t s = ctx.stream;
   UpdateCtl* c = ctx.ws.ctl.ptr;
-  const int blocks = ctx.update_blocks_per_sm * ctx.sm_count;
+  const int blocks = update_grid_blocks(ctx);
   FeatNorm nrm{};
   if (sch) nrm = norm_of(*sch);
   k_infer_schedule<<<1, 128, 0, s>>>(sch ? sch->params.ptr : nullptr,

@@ -1,19 +1,25 @@
 // The serving loop: several graphs resident on one GPU, each with its own shortest-path tree,
 // fed by batches that arrive at any time from any host thread.
 //
-// - One dispatcher thread owns the GPU work.  Requests wait in per-graph FIFO queues, so the
-//   batches of one graph apply in arrival order and every result is the one the same batches
-//   would give alone, one after the other.
-// - Continuous batching: each round takes the oldest waiting request of every graph that has
-//   one (round-robin over the graphs), as long as they are small, and queues all of their
-//   updates on one stream before waiting once (sssp_update_begin / sssp_update_end).  The host
-//   work of one update (staging, launches) overlaps the GPU work of the previous ones, and a
-//   round needs one host-device synchronisation instead of one per update.  A large batch runs
-//   in a round of its own.
+// - Requests wait in per-graph FIFO queues, so the batches of one graph apply in arrival order
+//   and every result is the one the same batches would give alone, one after the other.  A graph
+//   is in at most one round at a time.
+// - Two lanes, each a dispatcher thread with its own stream.  The small lane runs rounds of small
+//   batches: the oldest waiting request of every free graph (round-robin), all of their updates
+//   queued on the lane's stream before one wait (sssp_update_begin / sssp_update_end), so the
+//   host work of one update overlaps the GPU work of the previous ones and a round needs one
+//   host-device synchronisation.  The large lane runs one large batch at a time.
+// - The persistent kernel holds every SM it is given, so a small batch behind a large one would
+//   wait for all of it.  While the large lane runs, its persistent grid is capped at (occupancy -
+//   1) blocks per SM and the small lane's at one block per SM: the two grids together fill the
+//   SMs' block slots exactly, so both are co-resident whatever the order of their blocks (no grid
+//   barrier can wait on a block that has no slot).  A small round that starts while the large
+//   lane is idle takes the whole grid, and a large batch waits for such a round to end first.
 // - Admission by free HBM: a graph is registered only if its workspace fits beside the reserve,
 //   and a batch is dispatched only if its estimated scratch fits in the free device memory beyond
 //   the reserve; otherwise it fails with OUT_OF_MEMORY instead of taking the device down.
-// - Every graph has its own context (workspace, control block) on the server's one stream.
+// - Every graph has its own context (workspace, control block), pointed at the stream of the
+//   lane that runs it.
 #include "handles.hpp"
 
 #include <algorithm>
@@ -34,6 +40,8 @@ namespace dyngb200 {
 
 using Clock = std::chrono::steady_clock;
 
+struct ServerGraph;
+
 struct ServerRequest {
   uint64_t ticket = 0;
   int slot = 0;
@@ -42,6 +50,8 @@ struct ServerRequest {
   long long ops = 0;
   Clock::time_point arrival, ready, start, begun, synced, finish;
   int group_size = 0;
+  int lane = 0;
+  ServerGraph* graph = nullptr;  // set when a lane takes the request
   bool done = false;
   dyngb200_status status = DYNGB200_OK;
   std::string message;
@@ -53,6 +63,7 @@ struct ServerGraph {
   Graph* g = nullptr;
   Tree* t = nullptr;
   std::deque<ServerRequest*> queue;
+  bool busy = false;  // in a lane's round
 };
 
 class Server {
@@ -66,22 +77,23 @@ class Server {
   dyngb200_server_info info();
 
  private:
-  void run();
+  void run(int lane);
+  bool take_round(int lane, std::vector<ServerRequest*>& group, int& cap);
   void monitor();
-  void dispatch(std::vector<ServerRequest*>& group);
+  void dispatch(int lane, std::vector<ServerRequest*>& group, int cap);
   long long estimate_bytes(const ServerGraph& sg, const ServerRequest& r) const;
   std::unique_ptr<HostBuf<int32_t>> take_buffer(size_t n);
   void give_buffer(std::unique_ptr<HostBuf<int32_t>> b);
 
   dyngb200_server_config cfg_{};
   const Scheduler* learned_ = nullptr;
-  cudaStream_t stream_ = nullptr;
+  cudaStream_t streams_[2] = {nullptr, nullptr};  // the small lane's, the large lane's
   std::vector<std::unique_ptr<ServerGraph>> graphs_;
   std::unordered_map<uint64_t, std::unique_ptr<ServerRequest>> requests_;
   std::vector<std::unique_ptr<HostBuf<int32_t>>> pool_;
   std::mutex mu_;
   std::condition_variable work_cv_, done_cv_;
-  std::thread worker_;
+  std::thread workers_[2];
   std::thread monitor_;  // samples the free device memory for admission (off the dispatcher)
   std::condition_variable monitor_cv_;
   long long free_sample_ = -1;   // bytes free at the last sample (-1: none)
@@ -89,6 +101,12 @@ class Server {
   bool stop_ = false;
   uint64_t next_ticket_ = 1;
   size_t next_graph_ = 0;  // round-robin start
+  // lanes: 1 until the first graph shows the GPU holds two persistent grids side by side
+  int lanes_ = 1;
+  int full_blocks_ = 0, small_blocks_ = 0;  // persistent grid: whole, the small lane's share
+  bool large_running_ = false;  // the large lane's round is in flight
+  bool large_wants_ = false;    // a large batch waits for a whole-grid small round to end
+  bool small_full_ = false;     // a small round runs on the whole grid
   long long waiting_ = 0, running_ = 0;
   long long held_bytes_ = 0;  // pinned copies of queued batches (submit waits above the cap)
   static constexpr long long kHeldCap = 1LL << 30;
@@ -118,12 +136,13 @@ Server::Server(const dyngb200_server_config& cfg, const Scheduler* learned)
   if (cfg_.hbm_reserve_bytes <= 0) cfg_.hbm_reserve_bytes = 1LL << 30;
   expects(!learned_ || learned_->device == cfg_.device,
           "server: the scheduler belongs to another device");
+  expects(cfg_.lanes >= 0 && cfg_.lanes <= 2, "server: lanes is 0, 1 or 2");
   DYNGB200_CUDA(cudaSetDevice(cfg_.device));
-  DYNGB200_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  for (auto& st : streams_) DYNGB200_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   size_t free_b = 0, total_b = 0;
   DYNGB200_CUDA(cudaMemGetInfo(&free_b, &total_b));
   free_sample_ = static_cast<long long>(free_b);
-  worker_ = std::thread([this] { run(); });
+  for (int lane = 0; lane < 2; ++lane) workers_[lane] = std::thread([this, lane] { run(lane); });
   monitor_ = std::thread([this] { monitor(); });
 }
 
@@ -160,10 +179,12 @@ Server::~Server() {
   }
   work_cv_.notify_all();
   monitor_cv_.notify_all();
-  if (worker_.joinable()) worker_.join();
+  for (auto& w : workers_)
+    if (w.joinable()) w.join();
   if (monitor_.joinable()) monitor_.join();
   graphs_.clear();
-  if (stream_) cudaStreamDestroy(stream_);
+  for (auto& st : streams_)
+    if (st) cudaStreamDestroy(st);
 }
 
 int Server::add_graph(Graph& g, Tree& t) {
@@ -172,7 +193,7 @@ int Server::add_graph(Graph& g, Tree& t) {
   expect_tree_current(g, t, "server::add_graph");
   auto sg = std::make_unique<ServerGraph>();
   sg->ctx = std::make_unique<Context>();
-  context_init(*sg->ctx, cfg_.device, stream_);
+  context_init(*sg->ctx, cfg_.device, streams_[0]);
   // admission: the context's per-vertex workspace (~100 B per vertex of capacity) must fit
   size_t free_b = 0, total_b = 0;
   DYNGB200_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -183,8 +204,10 @@ int Server::add_graph(Graph& g, Tree& t) {
                     " bytes) does not fit beside the reserve of " +
                     std::to_string(cfg_.hbm_reserve_bytes) + " bytes (" +
                     std::to_string(free_b) + " free)");
-  sg->ctx->ws.reserve_vertices(g.n_cap, stream_);
-  DYNGB200_CUDA(cudaStreamSynchronize(stream_));
+  sg->ctx->ws.reserve_vertices(g.n_cap, streams_[0]);
+  DYNGB200_CUDA(cudaStreamSynchronize(streams_[0]));
+  // the split: the large lane's grid takes all but one block slot per SM, the small lane's one
+  const int per_sm = update_blocks_per_sm(*sg->ctx);
   // room for the graph to grow (index doublings, arena growths) kept in the device pool, so that
   // growth while serving does not wait for the driver
   const long long graph_bytes =
@@ -194,6 +217,11 @@ int Server::add_graph(Graph& g, Tree& t) {
   sg->g = &g;
   sg->t = &t;
   std::unique_lock<std::mutex> lk(mu_);
+  if (graphs_.empty()) {
+    full_blocks_ = per_sm * sg->ctx->sm_count;
+    small_blocks_ = sg->ctx->sm_count;
+    lanes_ = cfg_.lanes != 1 && per_sm >= 2 ? 2 : 1;
+  }
   graphs_.push_back(std::move(sg));
   return static_cast<int>(graphs_.size()) - 1;
 }
@@ -281,7 +309,7 @@ uint64_t Server::submit(int slot, const dyngb200_batch& b) {
     if (r && r->data && pool_.size() < 64) pool_.push_back(std::move(r->data));
     throw;
   }
-  work_cv_.notify_one();
+  work_cv_.notify_all();  // either lane may be the one that takes it
   return ticket;
 }
 
@@ -302,6 +330,7 @@ ServerRequest Server::wait(uint64_t ticket) {
   out.synced = r->synced;
   out.finish = r->finish;
   out.group_size = r->group_size;
+  out.lane = r->lane;
   out.done = true;
   out.status = r->status;
   out.message = r->message;
@@ -319,6 +348,7 @@ dyngb200_server_info Server::info() {
   std::unique_lock<std::mutex> lk(mu_);
   dyngb200_server_info i = info_;
   i.waiting = waiting_;
+  i.lanes = lanes_;
   return i;
 }
 
@@ -330,94 +360,141 @@ long long Server::estimate_bytes(const ServerGraph& sg, const ServerRequest& r) 
   return r.ops * (20 + dir * (96 + 2 * (4 + 4 * k) * 3 / 2)) + (1LL << 20);
 }
 
-void Server::run() {
+// Picks the next round of `lane` (the caller holds mu_): true when it took requests, or failed
+// some by admission (they are done); `cap` is the persistent grid of the round (0: whole).
+bool Server::take_round(int lane, std::vector<ServerRequest*>& group, int& cap) {
+  cap = 0;
+  const size_t ng = graphs_.size();
+  if (waiting_ == 0 || ng == 0 || lane >= lanes_) return false;
+  const bool known = free_sample_ >= 0;
+  long long free_left = known ? free_sample_ - admitted_since_ - cfg_.hbm_reserve_bytes : 0;
+  bool failed = false;
+  // take the head of graph gi into this round: admitted, or failed by admission (then done)
+  auto take = [&](size_t gi) {
+    ServerGraph& sg = *graphs_[gi];
+    ServerRequest* r = sg.queue.front();
+    sg.queue.pop_front();
+    --waiting_;
+    r->start = Clock::now();
+    r->lane = lane;
+    r->graph = &sg;
+    const long long need = estimate_bytes(sg, *r);
+    if (known && need > free_left) {
+      // admission: the batch's scratch does not fit beside the reserve; fail it, keep the rest
+      r->status = DYNGB200_OUT_OF_MEMORY;
+      r->message = "server: admission refused: the batch needs about " + std::to_string(need) +
+                   " bytes of device memory beyond the reserve, " +
+                   std::to_string(std::max(free_left, 0LL)) + " are free";
+      r->finish = Clock::now();
+      r->done = true;
+      ++info_.failed;
+      held_bytes_ -= held_of(*r);
+      if (pool_.size() < 64) pool_.push_back(std::move(r->data));
+      r->data.reset();
+      failed = true;
+      return;
+    }
+    free_left -= need;
+    admitted_since_ += need;
+    sg.busy = true;
+    group.push_back(r);
+  };
+  auto head = [&](size_t gi, bool large) {
+    const ServerGraph& sg = *graphs_[gi];
+    return !sg.busy && !sg.queue.empty() && (sg.queue.front()->ops > cfg_.small_changes) == large;
+  };
+  auto small_heads = [&] {
+    for (size_t step = 0; step < ng && static_cast<int>(group.size()) < cfg_.max_group; ++step) {
+      const size_t gi = (next_graph_ + step) % ng;
+      if (head(gi, false)) take(gi);
+    }
+    next_graph_ = (next_graph_ + 1) % ng;
+  };
+  size_t oldest_large = ng;
+  for (size_t gi = 0; gi < ng; ++gi)
+    if (head(gi, true) && (oldest_large == ng || graphs_[gi]->queue.front()->arrival <
+                                                     graphs_[oldest_large]->queue.front()->arrival))
+      oldest_large = gi;
+  if (lanes_ == 1) {
+    // One lane: small batches first; a large batch runs in a round of its own when no small head
+    // waits, or once it has waited kLargeMaxWaitMs (no starvation).
+    const bool overdue =
+        oldest_large < ng &&
+        ms_between(graphs_[oldest_large]->queue.front()->arrival, Clock::now()) > kLargeMaxWaitMs;
+    if (!overdue) small_heads();
+    if (group.empty() && !failed && oldest_large < ng) take(oldest_large);
+  } else if (lane == 0) {
+    small_heads();
+    if (!group.empty()) {
+      cap = large_running_ || large_wants_ ? small_blocks_ : 0;
+      small_full_ = cap == 0;
+    }
+  } else {
+    if (oldest_large == ng) {
+      large_wants_ = false;
+      return false;
+    }
+    if (small_full_) {  // a whole-grid small round is in flight: wait for it
+      large_wants_ = true;
+      return false;
+    }
+    large_wants_ = false;
+    take(oldest_large);
+    if (!group.empty()) {
+      cap = full_blocks_ - small_blocks_;
+      large_running_ = true;
+      ++info_.large_rounds;
+    }
+  }
+  return !group.empty() || failed;
+}
+
+void Server::run(int lane) {
   cudaSetDevice(cfg_.device);
   std::vector<ServerRequest*> group;
   for (;;) {
     group.clear();
+    int cap = 0;
     {
       std::unique_lock<std::mutex> lk(mu_);
-      work_cv_.wait(lk, [&] { return stop_ || waiting_ > 0; });
-      if (waiting_ == 0 && stop_) return;
-      const bool known = free_sample_ >= 0;
-      long long free_left = known ? free_sample_ - admitted_since_ - cfg_.hbm_reserve_bytes : 0;
-      const size_t ng = graphs_.size();
-      // take the head of graph gi into this round: admitted, or failed by admission (then done)
-      auto take = [&](size_t gi) {
-        ServerGraph& sg = *graphs_[gi];
-        ServerRequest* r = sg.queue.front();
-        sg.queue.pop_front();
-        --waiting_;
-        r->start = Clock::now();
-        const long long need = estimate_bytes(sg, *r);
-        if (known && need > free_left) {
-          // admission: the batch's scratch does not fit beside the reserve; fail it, keep the rest
-          r->status = DYNGB200_OUT_OF_MEMORY;
-          r->message = "server: admission refused: the batch needs about " + std::to_string(need) +
-                       " bytes of device memory beyond the reserve, " +
-                       std::to_string(std::max(free_left, 0LL)) + " are free";
-          r->finish = Clock::now();
-          r->done = true;
-          ++info_.failed;
-          held_bytes_ -= held_of(*r);
-          if (pool_.size() < 64) pool_.push_back(std::move(r->data));
-          r->data.reset();
-          return;
-        }
-        free_left -= need;
-        admitted_since_ += need;
-        group.push_back(r);
-      };
-      // Small batches first: a round takes the small heads of the graphs (round-robin), so a
-      // small batch waits for at most the round in flight, not for queued large batches.  A
-      // large batch runs in a round of its own when no small head waits, or once it has waited
-      // kLargeMaxWaitMs (no starvation).  Per-graph FIFO order holds: only heads are taken.
-      const Clock::time_point now = Clock::now();
-      size_t oldest_large = ng;
-      for (size_t gi = 0; gi < ng; ++gi) {
-        const auto& q = graphs_[gi]->queue;
-        if (q.empty() || q.front()->ops <= cfg_.small_changes) continue;
-        if (oldest_large == ng ||
-            q.front()->arrival < graphs_[oldest_large]->queue.front()->arrival)
-          oldest_large = gi;
+      for (;;) {
+        if (stop_ && waiting_ == 0) return;
+        if (take_round(lane, group, cap)) break;
+        work_cv_.wait(lk);
       }
-      const bool overdue =
-          oldest_large < ng &&
-          ms_between(graphs_[oldest_large]->queue.front()->arrival, now) > kLargeMaxWaitMs;
-      if (!overdue) {
-        for (size_t step = 0; step < ng && static_cast<int>(group.size()) < cfg_.max_group;
-             ++step) {
-          const size_t gi = (next_graph_ + step) % ng;
-          const auto& q = graphs_[gi]->queue;
-          if (!q.empty() && q.front()->ops <= cfg_.small_changes) take(gi);
-        }
-      }
-      if (group.empty() && oldest_large < ng) take(oldest_large);
-      next_graph_ = ng ? (next_graph_ + 1) % ng : 0;
       running_ += static_cast<long long>(group.size());
     }
     done_cv_.notify_all();  // admission failures are done
-    if (!group.empty()) dispatch(group);
+    if (!group.empty()) dispatch(lane, group, cap);
     {
       std::unique_lock<std::mutex> lk(mu_);
       running_ -= static_cast<long long>(group.size());
-      ++info_.rounds;
-      info_.max_group = std::max<long long>(info_.max_group, static_cast<long long>(group.size()));
+      if (!group.empty()) {
+        ++info_.rounds;
+        info_.max_group =
+            std::max<long long>(info_.max_group, static_cast<long long>(group.size()));
+        if (lanes_ == 2 && lane == 1) large_running_ = false;
+        if (lanes_ == 2 && lane == 0) small_full_ = false;
+      }
     }
+    work_cv_.notify_all();  // graphs freed, a lane's grid released: the other lane may go on
     done_cv_.notify_all();
   }
 }
 
-// One round: every update of the group queued on the shared stream, then one wait, then each
+// One round: every update of the group queued on the lane's stream, then one wait, then each
 // update's results.  Distinct graphs, distinct contexts: no scratch is shared inside a round.
-void Server::dispatch(std::vector<ServerRequest*>& group) {
+void Server::dispatch(int lane, std::vector<ServerRequest*>& group, int cap) {
   const size_t n = group.size();
+  cudaStream_t stream = streams_[lane];
   std::vector<std::unique_ptr<PendingUpdate>> pending(n);
   std::vector<char> begun(n, 0);
   for (size_t i = 0; i < n; ++i) {
     ServerRequest* r = group[i];
-    ServerGraph& sg = *graphs_[r->slot];
+    ServerGraph& sg = *r->graph;
     r->group_size = static_cast<int>(n);
+    sg.ctx->stream = stream;  // the graph's previous round, on either lane, has completed
+    sg.ctx->max_update_blocks = cap;
     try {
       expect_tree_current(*sg.g, *sg.t, "sssp::update");
       pending[i] = std::make_unique<PendingUpdate>();
@@ -433,10 +510,11 @@ void Server::dispatch(std::vector<ServerRequest*>& group) {
       r->message = e.what();
     }
   }
-  cudaStreamSynchronize(stream_);  // errors surface in sssp_update_end
+  cudaStreamSynchronize(stream);  // errors surface in sssp_update_end
   const Clock::time_point synced = Clock::now();
   for (size_t i = 0; i < n; ++i) {
     ServerRequest* r = group[i];
+    ServerGraph& sg = *r->graph;
     r->synced = synced;
     if (!begun[i]) r->begun = r->start;
     if (begun[i]) {
@@ -451,12 +529,14 @@ void Server::dispatch(std::vector<ServerRequest*>& group) {
       }
     }
     pending[i].reset();
+    sg.ctx->max_update_blocks = 0;
     const long long bytes = held_of(*r);
     give_buffer(std::move(r->data));
     r->finish = Clock::now();
     std::unique_lock<std::mutex> lk(mu_);
     held_bytes_ -= bytes;
-    r->done = true;
+    sg.busy = false;
+    r->done = true;  // a waiter may take (and free) the request from here on
     if (r->status == DYNGB200_OK) ++info_.completed;
     else ++info_.failed;
   }
@@ -521,6 +601,7 @@ dyngb200_status dyngb200_server_wait(dyngb200_server s, uint64_t ticket, dyngb20
     times->begin_ms = ran ? dyngb200::ms_between(r.start, r.begun) : 0.0;
     times->round_ms = ran ? dyngb200::ms_between(r.start, r.synced) : 0.0;
     times->copy_ms = dyngb200::ms_between(r.arrival, r.ready);
+    times->lane = r.lane;
   }
   dyngb200::last_error() = r.message;
   return r.status;

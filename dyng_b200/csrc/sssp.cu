@@ -1358,6 +1358,25 @@ __global__ void k_pack(long long n, int bits, const long long* dist, const int32
 
 }  // namespace
 
+// Blocks of the persistent kernel an SM holds at once (its occupancy, asked once per context).
+int update_blocks_per_sm(Context& ctx) {
+  if (ctx.update_blocks_per_sm == 0) {
+    int per_sm = 0;
+    DYNGB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sssp, kThreads, 0));
+    expects(per_sm >= 1, "sssp: the persistent kernel does not fit on an SM", DYNGB200_NOT_SUPPORTED);
+    ctx.update_blocks_per_sm = per_sm;
+  }
+  expects(ctx.update_blocks_per_sm * ctx.sm_count <= kPjMaxBlocks,
+          "sssp: more persistent blocks than the pointer-jumping lists support", DYNGB200_NOT_SUPPORTED);
+  return ctx.update_blocks_per_sm;
+}
+
+// The update's persistent grid: occupancy x SMs, or the context's cap when it is smaller.
+int update_grid_blocks(Context& ctx) {
+  const int full = update_blocks_per_sm(ctx) * ctx.sm_count;
+  return ctx.max_update_blocks > 0 && ctx.max_update_blocks < full ? ctx.max_update_blocks : full;
+}
+
 // Blocks of the persistent kernel (co-resident: cooperative launch).
 // The schedule's fields in the control block (0 / unset: the heuristic).
 void schedule_into(const dyngb200_schedule& sched, UpdateCtl& init) {
@@ -1371,15 +1390,7 @@ void schedule_into(const dyngb200_schedule& sched, UpdateCtl& init) {
 
 static int persistent_blocks(Context& ctx, const dyngb200_schedule& sched) {
   (void)sched;  // the schedule's grid size is applied on the device (active_blocks)
-  if (ctx.update_blocks_per_sm == 0) {
-    int per_sm = 0;
-    DYNGB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sssp, kThreads, 0));
-    expects(per_sm >= 1, "sssp: the persistent kernel does not fit on an SM", DYNGB200_NOT_SUPPORTED);
-    ctx.update_blocks_per_sm = per_sm;
-  }
-  expects(ctx.update_blocks_per_sm * ctx.sm_count <= kPjMaxBlocks,
-          "sssp: more persistent blocks than the pointer-jumping lists support", DYNGB200_NOT_SUPPORTED);
-  return ctx.update_blocks_per_sm * ctx.sm_count;
+  return update_grid_blocks(ctx);
 }
 
 static void launch(Context& ctx, SsspParams& p, int blocks) {

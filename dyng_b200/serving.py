@@ -1,9 +1,10 @@
 """dyng_b200.serving: several resident graphs updated by batches that arrive at any time.
 
-The loop itself is native (dyng_b200/csrc/serve.cu): one dispatcher thread, per-graph FIFO
-order (every result equals running the same batches alone, in order), continuous batching of
-small batches of different graphs into one round on one stream, admission by free HBM.  This
-module is its Python face and the load generator that measures it:
+The loop itself is native (dyng_b200/csrc/serve.cu): per-graph FIFO order (every result equals
+running the same batches alone, in order), continuous batching of small batches of different
+graphs into one round on one stream, large batches on a lane of their own that shares the SMs
+with the small rounds (lanes=2, the default), admission by free HBM.  This module is its Python
+face and the load generator that measures it:
 
     python -m dyng_b200.serving --rates 10,100,500,2000 --seconds 5
 
@@ -28,10 +29,10 @@ class Server:
     """A serving loop on one GPU.  Graphs and trees added to it belong to it until close()."""
 
     def __init__(self, resources: Resources | None = None, scheduler=None, max_group: int = 8,
-                 small_changes: int = 65536, hbm_reserve_bytes: int = 1 << 30):
+                 small_changes: int = 65536, hbm_reserve_bytes: int = 1 << 30, lanes: int = 2):
         self._res = resources or default_resources()
         cfg = N.ServerConfig(self._res.device, int(max_group), int(small_changes),
-                             int(hbm_reserve_bytes))
+                             int(hbm_reserve_bytes), int(lanes))
         self._h = ctypes.c_void_p()
         self._keep = [scheduler]
         check(N.lib().dyngb200_server_create(ctypes.byref(cfg),
@@ -54,7 +55,8 @@ class Server:
 
     def wait(self, ticket: int):
         """(Stats, times) of a request; raises its update's error.  times: queued_ms,
-        service_ms, total_ms, group_size."""
+        service_ms, total_ms, group_size, begin_ms, round_ms, copy_ms, lane (1: the large
+        lane)."""
         st = N.Stats()
         tm = N.RequestTimes()
         check(N.lib().dyngb200_server_wait(self._h, int(ticket), ctypes.byref(st),
@@ -62,7 +64,7 @@ class Server:
         return Stats._from_native(st), {"queued_ms": tm.queued_ms, "service_ms": tm.service_ms,
                                         "total_ms": tm.total_ms, "group_size": tm.group_size,
                                         "begin_ms": tm.begin_ms, "round_ms": tm.round_ms,
-                                        "copy_ms": tm.copy_ms}
+                                        "copy_ms": tm.copy_ms, "lane": tm.lane}
 
     def drain(self) -> None:
         check(N.lib().dyngb200_server_drain(self._h))
@@ -132,7 +134,8 @@ def run_load(server, slots, pools, rate, seconds, rng, size_range=(100, 1_000_00
         for i, tk in enumerate(iter(tickets_q.get, None)):
             st, tm = server.wait(tk[0])
             done.append((tk[1], tk[2], tm["total_ms"], tm["queued_ms"], tm["group_size"],
-                         tm["service_ms"], tm["begin_ms"], tm["round_ms"], tm["copy_ms"], tk[3]))
+                         tm["service_ms"], tm["begin_ms"], tm["round_ms"], tm["copy_ms"], tk[3],
+                         tm["lane"]))
 
     import queue
     tickets_q = queue.Queue()
@@ -188,7 +191,7 @@ STORAGE_KEYS = ("arena_growths", "compactions", "index_builds", "grow_ms", "comp
                 "index_ms", "maintenance_ms_max")
 PARTS = (("queued", 3), ("service", 5), ("begin", 6), ("round", 7), ("copy", 8))
 RECORD = ("graph", "changes", "total_ms", "queued_ms", "group_size", "service_ms", "begin_ms",
-          "round_ms", "copy_ms", "submitted_s")
+          "round_ms", "copy_ms", "submitted_s", "lane")
 
 
 def main(argv=None):
@@ -204,6 +207,10 @@ def main(argv=None):
     ap.add_argument("--learned", default="", help="scheduler weights (.npz); empty: heuristic")
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--dump", default="", help="write every request's record to this .npz")
+    ap.add_argument("--small-changes", type=int, default=65536,
+                    help="batches up to this many changes run in the small lane's rounds")
+    ap.add_argument("--lanes", type=int, default=2,
+                    help="2: large batches on their own lane beside small rounds; 1: one lane")
     a = ap.parse_args(argv)
     rng = np.random.default_rng(a.seed)
     res = Resources(0)
@@ -211,7 +218,7 @@ def main(argv=None):
     if a.learned:
         from .scheduler import Scheduler
         sched = Scheduler.load(a.learned, resources=res)
-    server = Server(res, scheduler=sched)
+    server = Server(res, scheduler=sched, lanes=a.lanes, small_changes=a.small_changes)
     slots, pools, keep = [], [], []
     for i, sc in enumerate(int(x) for x in a.scales.split(",")):
         edges = rmat(sc, 16, w_max=1000, seed=100 + i, device="cuda")

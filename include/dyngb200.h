@@ -402,6 +402,9 @@ typedef struct dyngb200_server_config {
   int32_t max_group;         /* updates queued before one wait (0: 8) */
   int64_t small_changes;     /* batches up to this many changes share a round (0: 65536) */
   int64_t hbm_reserve_bytes; /* device memory admission keeps free (0: 1 GiB) */
+  int32_t lanes;             /* 0 or 2: large batches run on their own lane, on two thirds of the
+                                SMs' block slots, beside rounds of small ones on the rest;
+                                1: one lane (a large batch holds every SM while it runs) */
 } dyngb200_server_config;
 typedef struct dyngb200_request_times {
   double queued_ms;   /* submit -> dispatch */
@@ -411,6 +414,7 @@ typedef struct dyngb200_request_times {
   double begin_ms;    /* host time queuing this update's work (staging, launches) */
   double round_ms;    /* dispatch -> the round's work complete on the GPU */
   double copy_ms;     /* inside submit: the batch copied into the server's pinned buffer */
+  int32_t lane;       /* 0: a round of small batches (or every round with one lane); 1: large */
 } dyngb200_request_times;
 typedef struct dyngb200_server_info {
   int64_t submitted;
@@ -420,6 +424,8 @@ typedef struct dyngb200_server_info {
   int64_t max_group;
   int64_t waiting;
   int64_t admission_us_max; /* longest free-memory query (a helper thread's), microseconds */
+  int64_t lanes;            /* lanes in use (2 once a graph shows the GPU holds the split) */
+  int64_t large_rounds;     /* rounds of the large lane */
 } dyngb200_server_info;
 /* learned: a scheduler used for every update (NULL: the fixed heuristic). */
 dyngb200_status dyngb200_server_create(const dyngb200_server_config* config,

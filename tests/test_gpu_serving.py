@@ -1,6 +1,7 @@
 """The serving loop on the GPU: every request's result in a mix equals the same batches run
-alone, in order, on a copy of its graph; rounds group small batches of different graphs;
-admission refuses what does not fit; a bad batch fails alone."""
+alone, in order, on a copy of its graph, with one lane and with large batches on a lane of
+their own beside the small rounds (their persistent grids sharing the SMs); rounds group small
+batches of different graphs; admission refuses what does not fit; a bad batch fails alone."""
 import threading
 
 import numpy as np
@@ -43,8 +44,9 @@ def _alone(spec, batches):
     return out, t.distances, t.parents
 
 
+@pytest.mark.parametrize("lanes", [1, 2])
 @pytest.mark.parametrize("learned", [False, True])
-def test_mix_equals_alone(learned):
+def test_mix_equals_alone(learned, lanes):
     work = _workload(3)
     sched = None
     if learned:
@@ -52,7 +54,7 @@ def test_mix_equals_alone(learned):
         sched = S.Scheduler(seed=11)
         sched.set_params((np.random.default_rng(5).normal(size=S.num_params()) * 0.5)
                          .astype(np.float32))
-    server = Server(scheduler=sched, max_group=8, small_changes=10000)
+    server = Server(scheduler=sched, max_group=8, small_changes=10000, lanes=lanes)
     handles, slots = [], []
     for spec, _ in work:
         n, s, d, w = spec
@@ -86,6 +88,15 @@ def test_mix_equals_alone(learned):
     groups = [tm["group_size"] for i in results for _, tm in results[i]]
     assert info["completed"] == sum(len(b) for _, b in work) and info["failed"] == 0
     assert max(groups) >= 2  # small batches of different graphs shared rounds
+    ran_large = [tm["lane"] for i in results for _, tm in results[i]]
+    assert info["lanes"] == lanes
+    if lanes == 2:
+        # the 20000-change batches ran on the large lane, everything else on the small one
+        sizes = [len(b["ins_src"]) + len(b["del_src"]) for _, bs in work for b in bs]
+        assert info["large_rounds"] == sum(z > 10000 for z in sizes) > 0
+        assert sum(ran_large) == info["large_rounds"]
+    else:
+        assert not any(ran_large) and info["large_rounds"] == 0
     assert all(tm["total_ms"] >= tm["service_ms"] >= 0 for i in results for _, tm in results[i])
     server.close()
 
