@@ -141,6 +141,11 @@ struct UpdateCtl {
   u64 heavy_cnt[3];     // (slots << 40 | chunks) of the heavy near-frontier lists
   u64 walk_heavy[3];
   u64 pull_heavy;       // heavy pull candidates
+  // push steps hand out medium rows and heavy chunks to warps through these cursors (per step,
+  // triple-buffered like the list counters)
+  int med_cursor[3];
+  int pad_cursor;
+  unsigned long long heavy_cursor[3];
   int touched_count;
   int active[3];
   int rounds;

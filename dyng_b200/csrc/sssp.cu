@@ -588,11 +588,14 @@ __device__ __forceinline__ int find_heavy(const int2* list, int count, long long
 
 // Expand a frontier: light rows in balanced groups of up to 32 per warp, medium rows one per warp,
 // heavy rows in kHeavyChunk-slot chunks over all warps.  push / walk expand out-rows, pull
-// expands in-rows.
+// expands in-rows.  With cursors (zero at the start of the step), medium rows and heavy chunks go
+// to whichever warp asks next, so a warp that finished its light rows early takes more of them;
+// without, warp w takes rows w, w + nwarps, ...
 template <int MODE>
 __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_count,
                        const int* med, int med_count, const int2* heavy, u64 heavy_cnt,
-                       long long gwarp, long long nwarps, long long* probe = nullptr) {
+                       long long gwarp, long long nwarps, long long* probe = nullptr,
+                       int* med_cursor = nullptr, unsigned long long* heavy_cursor = nullptr) {
   const int lane = threadIdx.x & 31;
   unsigned long long t_part = probe ? global_ns() : 0;
   // probe: the warp's time in each part, summed into probe[0..2], maxed into probe[3..5]
@@ -636,30 +639,41 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
   }
   part_done(0);
   // medium: one row per warp
-  for (long long i = gwarp; i < med_count; i += nwarps) {
+  auto medium_row = [&](long long i) {
     const int owner = ld_cg(&med[i]);
     u64 du = 0;
     if (MODE == kPush) {
       const u64 word = ld_cg(&p.packed[owner]);
-      if (word == kPackedInf) continue;
+      if (word == kPackedInf) return;
       du = X.pk.dist(word);
     }
     if (lane == 0) ++X.rows;
     const RowDesc desc = descs[owner];
     warp_slots<MODE>(p, X, owner, du, desc.start, 0, desc.len);
+  };
+  if (med_cursor) {
+    for (;;) {
+      int i = 0;
+      if (lane == 0) i = atomicAdd(med_cursor, 1);
+      i = __shfl_sync(0xffffffffu, i, 0);
+      if (i >= med_count) break;
+      medium_row(i);
+    }
+  } else {
+    for (long long i = gwarp; i < med_count; i += nwarps) medium_row(i);
   }
   part_done(1);
   // heavy: chunks
   const int hcount = static_cast<int>(heavy_cnt >> 40);
   const long long chunks = static_cast<long long>(heavy_cnt & ((1ULL << 40) - 1));
-  for (long long ch = gwarp; ch < chunks; ch += nwarps) {
+  auto heavy_chunk = [&](long long ch) {
     const int h = find_heavy(heavy, hcount, ch);
     const int owner = __ldcg(&heavy[h].x);
     const int base = __ldcg(&heavy[h].y);
     u64 du = 0;
     if (MODE == kPush) {
       const u64 word = ld_cg(&p.packed[owner]);
-      if (word == kPackedInf) continue;
+      if (word == kPackedInf) return;
       du = X.pk.dist(word);
     }
     if (ch == base && lane == 0) ++X.rows;
@@ -667,6 +681,17 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     const int e0 = static_cast<int>(ch - base) * kHeavyChunk;
     const int e1 = min(desc.len, e0 + kHeavyChunk);
     warp_slots<MODE>(p, X, owner, du, desc.start, e0, e1);
+  };
+  if (heavy_cursor) {
+    for (;;) {
+      unsigned long long ch = 0;
+      if (lane == 0) ch = atomicAdd(heavy_cursor, 1ULL);
+      ch = __shfl_sync(0xffffffffu, ch, 0);
+      if (static_cast<long long>(ch) >= chunks) break;
+      heavy_chunk(static_cast<long long>(ch));
+    }
+  } else {
+    for (long long ch = gwarp; ch < chunks; ch += nwarps) heavy_chunk(ch);
   }
   part_done(2);
 }
@@ -753,10 +778,13 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
         c->near_cnt[(S.it + 2) % 3] = 0;
         c->near_med_cnt[(S.it + 2) % 3] = 0;
         c->heavy_cnt[(S.it + 2) % 3] = 0;
+        c->med_cursor[(S.it + 2) % 3] = 0;
+        c->heavy_cursor[(S.it + 2) % 3] = 0;
       }
       const unsigned long long t_busy = (!BLOCK && step == 0) ? global_ns() : 0;
       expand<kPush>(p, X, lists[S.it & 1], nc, mlists[S.it & 1], mc, hlists[S.it & 1], hc, gwarp,
-                    nwarps, (!BLOCK && step == 0) ? &c->work[16] : nullptr);
+                    nwarps, (!BLOCK && step == 0) ? &c->work[16] : nullptr, &c->med_cursor[cs],
+                    &c->heavy_cursor[cs]);
       if (!BLOCK && step == 0) {
         // balance of the first step: the slowest warp's and the summed busy time, and warps
         const long long busy = static_cast<long long>(global_ns() - t_busy);
@@ -933,17 +961,40 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         __shared__ int s_prefix[kPjMaxBlocks + 1];
         const long long span = (n + nblk - 1) / nblk;
         const long long lo = static_cast<long long>(blockIdx.x) * span;
-        const long long hi = min(n, lo + span);
         // ancestor[] starts as the parents with the roots marked, written by a sequential pass
-        // over the block's range, so that every round gathers one random word per vertex
+        // over all vertices, so that every round gathers one random word per vertex
         // (ancestor[a]) instead of two (parent[a] and stamp[a])
-        for (long long v = lo + threadIdx.x; v < hi; v += blockDim.x) {
-          const int st = ld_cg(&p.stamp[v]);
-          const int pa = v < p.tree_n ? p.parent[v] : -1;
-          // a child of the source has no ancestor that can be a root: its chain ends at once
-          // (and nothing ever gathers ancestor[source], which every chain would reach)
-          p.ancestor[v] = st == gen_inv ? kMarked : (pa == p.source ? -1 : pa);
+        // a child of the source has no ancestor that can be a root: its chain ends at once
+        // (and nothing ever gathers ancestor[source], which every chain would reach)
+        auto first_ancestor = [&](int st, int pa) {
+          return st == gen_inv ? kMarked : (pa == p.source ? -1 : pa);
+        };
+        // 16-byte loads, two quads per thread in flight (a one-word loop was latency-bound at
+        // about a quarter of the bandwidth); the tail, and unaligned arrays, word by word
+        const bool vec = ((reinterpret_cast<uintptr_t>(p.stamp) | reinterpret_cast<uintptr_t>(p.parent) |
+                           reinterpret_cast<uintptr_t>(p.ancestor)) & 15) == 0;
+        const long long quads = vec ? min(n, p.tree_n) >> 2 : 0;
+        for (long long q0 = tid; q0 < quads; q0 += 2 * threads) {
+          int4 st[2], pa[2];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const long long q = q0 + j * threads;
+            if (q < quads) {
+              st[j] = __ldcg(reinterpret_cast<const int4*>(p.stamp) + q);
+              pa[j] = __ldcg(reinterpret_cast<const int4*>(p.parent) + q);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const long long q = q0 + j * threads;
+            if (q < quads)
+              reinterpret_cast<int4*>(p.ancestor)[q] =
+                  make_int4(first_ancestor(st[j].x, pa[j].x), first_ancestor(st[j].y, pa[j].y),
+                            first_ancestor(st[j].z, pa[j].z), first_ancestor(st[j].w, pa[j].w));
+          }
         }
+        for (long long v = 4 * quads + tid; v < n; v += threads)
+          p.ancestor[v] = first_ancestor(ld_cg(&p.stamp[v]), v < p.tree_n ? p.parent[v] : -1);
         if (tid == 0) c->work[22] = n;
         if (!grid_barrier(c, bar)) return;
         for (int round = 0; round < max_rounds; ++round) {
