@@ -652,12 +652,16 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     warp_slots<MODE>(p, X, owner, du, desc.start, 0, desc.len);
   };
   if (med_cursor) {
+    // runs of rows per grab, so that a step makes at most about 4 grabs per warp (one cursor
+    // address takes every grab of the step)
+    const int run = 1 + static_cast<int>(med_count / (4 * nwarps));
     for (;;) {
       int i = 0;
-      if (lane == 0) i = atomicAdd(med_cursor, 1);
+      if (lane == 0) i = atomicAdd(med_cursor, run);
       i = __shfl_sync(0xffffffffu, i, 0);
       if (i >= med_count) break;
-      medium_row(i);
+      const int end = min(med_count, i + run);
+      for (; i < end; ++i) medium_row(i);
     }
   } else {
     for (long long i = gwarp; i < med_count; i += nwarps) medium_row(i);
@@ -683,12 +687,14 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     warp_slots<MODE>(p, X, owner, du, desc.start, e0, e1);
   };
   if (heavy_cursor) {
+    const long long run = 1 + chunks / (4 * nwarps);
     for (;;) {
       unsigned long long ch = 0;
-      if (lane == 0) ch = atomicAdd(heavy_cursor, 1ULL);
+      if (lane == 0) ch = atomicAdd(heavy_cursor, static_cast<unsigned long long>(run));
       ch = __shfl_sync(0xffffffffu, ch, 0);
       if (static_cast<long long>(ch) >= chunks) break;
-      heavy_chunk(static_cast<long long>(ch));
+      const long long end = min(chunks, static_cast<long long>(ch) + run);
+      for (long long c = static_cast<long long>(ch); c < end; ++c) heavy_chunk(c);
     }
   } else {
     for (long long ch = gwarp; ch < chunks; ch += nwarps) heavy_chunk(ch);
