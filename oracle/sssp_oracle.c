@@ -35,8 +35,11 @@
  *
  * Threads: orc_set_threads(T > 1) runs the CSR assembly and the transposition of every apply
  * on T OpenMP threads (the reference's host path parallelises the same loops, apply_host.cpp:
- * 264-306, 417-468); the repair itself stays sequential.  Results are identical for every T.
- * The checker runs with one thread; the CPU-baseline timings use the host's cores.
+ * 264-306, 417-468), and the repair of an update whose tree packs (distance, parent) into one
+ * word on the threaded engine (openmp.cpp:223-583: invalidation by level, a pull seed, push
+ * rounds with a compare-and-swap minimum).  Trees, invalidated and affected counts are
+ * identical for every T; the schedule-dependent counters (pushes) are not.  The checker runs
+ * with one thread; the CPU-baseline timings use the host's cores.
  *
  * Errors are returned as negative status codes with a message in the caller's buffer; nothing
  * aborts.  All memory is owned by the orc_graph handle or by the caller.
@@ -997,6 +1000,196 @@ static int has_rootless_cycle(const orc_graph* g, const int32_t* parent, const i
  * dist / parent hold the old tree on entry (n_old entries) and receive the new one; their
  * capacity must cover the vertex count after growth (num_vertices_after of the summary).
  */
+/* ---------------------------------------------------------------------------------------------
+ * The threaded repair (openmp.cpp:223-583), used when the oracle runs on more than one thread
+ * (the timed CPU baseline; the checker runs the sequential engine above).  The steps are the
+ * sequential engine's, in parallel over the vertices of each step: invalidation by level over a
+ * children index, a pull seed of the invalidated vertices and the insertion heads, then push
+ * rounds over the vertices whose distance fell.  Every vertex's (distance, parent) lives in one
+ * packed word, (distance << bits) | parent, lowered by a compare-and-swap minimum, so a word
+ * only ever falls in the lexicographic (distance, parent) order and the fixed point is the
+ * canonical tree the sequential engine reaches (lowest parent id among the tight in-edges).
+ * ------------------------------------------------------------------------------------------- */
+static int atomic_min_u64(uint64_t* p, uint64_t v, uint64_t* old) {
+  uint64_t cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+  while (v < cur) {
+    if (__atomic_compare_exchange_n(p, &cur, v, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+      *old = cur;
+      return 1;
+    }
+  }
+  return 0;
+}
+
+/* Claims v for generation gen (once per generation) and appends it to list[*count]. */
+static void claim_append(int* stamp, int32_t v, int gen, int32_t* list, int64_t* count) {
+  int cur = __atomic_load_n(&stamp[v], __ATOMIC_RELAXED);
+  while (cur != gen) {
+    if (__atomic_compare_exchange_n(&stamp[v], &cur, gen, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+      list[__atomic_fetch_add(count, 1, __ATOMIC_RELAXED)] = v;
+      return;
+    }
+  }
+}
+
+/* The best packed offer of v's in-row (pull), or ORC_PACKED_NONE. */
+#define ORC_PACKED_NONE UINT64_MAX
+static uint64_t pull_offer(const orc_graph* g, const int32_t* in_w, const uint64_t* word,
+                           int bits, int64_t v) {
+  uint64_t best = ORC_PACKED_NONE;
+  for (int64_t e = g->in_row_ptr[v]; e < g->in_row_ptr[v + 1]; ++e) {
+    const int32_t u = g->in_col[e];
+    const uint64_t wu = __atomic_load_n(&word[u], __ATOMIC_RELAXED);
+    if (wu == ORC_PACKED_NONE) continue;
+    const uint64_t offer = (((wu >> bits) + (uint64_t)in_w[e]) << bits) | (uint64_t)u;
+    if (offer < best) best = offer;
+  }
+  return best;
+}
+
+static int update_threaded(orc_graph* g, int32_t source, int k, int64_t n_old,
+                           const int32_t* cfrom, const int32_t* cto, int64_t nc, int64_t* dist,
+                           int32_t* parent, orc_stats* s, char* err, size_t err_cap) {
+  const int64_t n = g->n;
+  const int bits = parent_bits(n);
+  const uint64_t none = ((uint64_t)1 << bits) - 1;
+  const int32_t* w = g->w + (size_t)k * (size_t)g->m;
+  const int32_t* in_w = g->in_w + (size_t)k * (size_t)g->m;
+  const size_t nz = (size_t)(n > 0 ? n : 1);
+  uint64_t* word = (uint64_t*)xmalloc(nz * sizeof(uint64_t));
+  int64_t* old_d = (int64_t*)xmalloc(nz * sizeof(int64_t));
+  int32_t* old_p = (int32_t*)xmalloc(nz * sizeof(int32_t));
+  int* stamp = (int*)calloc(nz, sizeof(int));
+  int32_t* list_a = (int32_t*)xmalloc((nz + 1) * sizeof(int32_t));
+  int32_t* list_b = (int32_t*)xmalloc((nz + 1) * sizeof(int32_t));
+  int64_t* cstart = (int64_t*)calloc(nz + 1, sizeof(int64_t));
+  int32_t* children = (int32_t*)xmalloc(nz * sizeof(int32_t));
+  int status = ORC_OK;
+  (void)n_old;
+  /* identify_affected: the roots (tree edges among the changes), checked for rootless cycles */
+  const int inval = 1;
+  int64_t ninv = 0;
+  for (int64_t i = 0; i < nc; ++i) {
+    const int32_t u = cfrom[i], v = cto[i];
+    if (parent[v] == u && stamp[v] != inval) {
+      stamp[v] = inval;
+      list_a[ninv++] = v;
+    }
+  }
+  if (nc > 0 && has_rootless_cycle(g, parent, stamp, inval)) {
+    set_err(err, err_cap, "sssp: the input shortest-path tree has a parent cycle");
+    status = ORC_INVALID_ARGUMENT;
+    goto done;
+  }
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+  for (int64_t v = 0; v < n; ++v) {
+    old_d[v] = dist[v];
+    old_p[v] = parent[v];
+  }
+  if (ninv > 0) {
+    /* children index: counts, a scan, then a fill (the order inside a row does not matter) */
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+    for (int64_t v = 0; v < n; ++v)
+      if (v != source && parent[v] >= 0) __atomic_fetch_add(&cstart[parent[v] + 1], 1, __ATOMIC_RELAXED);
+    for (int64_t v = 0; v < n; ++v) cstart[v + 1] += cstart[v];
+    int64_t* fill = (int64_t*)xmalloc(nz * sizeof(int64_t));
+    memcpy(fill, cstart, nz * sizeof(int64_t));
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+    for (int64_t v = 0; v < n; ++v)
+      if (v != source && parent[v] >= 0)
+        children[__atomic_fetch_add(&fill[parent[v]], 1, __ATOMIC_RELAXED)] = (int32_t)v;
+    free(fill);
+    /* the invalidated subtrees, level by level: list_a[lo, hi) is the current level */
+    int64_t lo = 0, hi = ninv;
+    while (lo < hi) {
+      int64_t top = hi;
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 256)
+      for (int64_t i = lo; i < hi; ++i) {
+        const int32_t x = list_a[i];
+        for (int64_t c = cstart[x]; c < cstart[x + 1]; ++c)
+          claim_append(stamp, children[c], inval, list_a, &top);
+      }
+      lo = hi;
+      hi = top;
+    }
+    ninv = hi;
+  }
+  s->invalidated = ninv;
+  /* packed words: the old tree, the invalidated vertices and new vertices unreached */
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+  for (int64_t v = 0; v < n; ++v) {
+    const int dead = stamp[v] == inval || dist[v] >= ORC_INF / 2;
+    word[v] = dead ? ORC_PACKED_NONE
+                   : ((uint64_t)dist[v] << bits) | (parent[v] < 0 ? none : (uint64_t)parent[v]);
+  }
+  {
+    /* seed: every invalidated vertex pulls, then every insertion head (not the source) */
+    int gen = 2;
+    int64_t nf = 0;
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 256)
+    for (int64_t i = 0; i < ninv + g->num_ins; ++i) {
+      const int32_t v = i < ninv ? list_a[i] : g->ins_dst[i - ninv];
+      if (v == source) continue;
+      const uint64_t best = pull_offer(g, in_w, word, bits, v);
+      uint64_t prev;
+      if (best != ORC_PACKED_NONE && atomic_min_u64(&word[v], best, &prev) &&
+          (prev == ORC_PACKED_NONE || (best >> bits) < (prev >> bits)))
+        claim_append(stamp, v, gen, list_b, &nf);
+    }
+    /* push rounds */
+    int32_t* cur = list_b;
+    int32_t* nxt = list_a;
+    while (nf > 0) {
+      s->iterations++;
+      if (s->iterations > n) {
+        set_err(err, err_cap, "the threaded update did not converge");
+        status = ORC_NOT_CONVERGED;
+        goto done;
+      }
+      s->pushes += nf;
+      ++gen;
+      int64_t nn = 0;
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 64)
+      for (int64_t i = 0; i < nf; ++i) {
+        const int32_t a = cur[i];
+        const uint64_t wa = __atomic_load_n(&word[a], __ATOMIC_RELAXED);
+        if (wa == ORC_PACKED_NONE) continue;
+        const uint64_t da = wa >> bits;
+        for (int64_t e = g->row_ptr[a]; e < g->row_ptr[a + 1]; ++e) {
+          const int32_t x = g->col[e];
+          if (x == source) continue;
+          const uint64_t offer = ((da + (uint64_t)w[e]) << bits) | (uint64_t)a;
+          uint64_t prev;
+          if (atomic_min_u64(&word[x], offer, &prev) &&
+              (prev == ORC_PACKED_NONE || (offer >> bits) < (prev >> bits)))
+            claim_append(stamp, x, gen, nxt, &nn);
+        }
+      }
+      int32_t* t = cur;
+      cur = nxt;
+      nxt = t;
+      nf = nn;
+    }
+  }
+  {
+    int64_t affected = 0;
+#pragma omp parallel for num_threads(g_threads) schedule(static) reduction(+ : affected)
+    for (int64_t v = 0; v < n; ++v) {
+      const uint64_t x = word[v];
+      const int64_t d = x == ORC_PACKED_NONE ? ORC_INF : (int64_t)(x >> bits);
+      const int32_t p = x == ORC_PACKED_NONE || (x & none) == none ? -1 : (int32_t)(x & none);
+      dist[v] = d;
+      parent[v] = p;
+      affected += d != old_d[v] || p != old_p[v];
+    }
+    s->affected = affected;
+  }
+done:
+  free(word); free(old_d); free(old_p); free(stamp); free(list_a); free(list_b); free(cstart);
+  free(children);
+  return status;
+}
+
 int orc_sssp_update(orc_graph* g, int32_t source, int k, int64_t delta_opt, int rule,
                     int64_t num_inserts, const int32_t* ins_src, const int32_t* ins_dst,
                     const int32_t* ins_w, int64_t num_deletes, const int32_t* del_src,
@@ -1050,6 +1243,14 @@ int orc_sssp_update(orc_graph* g, int32_t source, int k, int64_t delta_opt, int 
       cto[nc] = g->ins_dst[i];
       ++nc;
     }
+  }
+  if (g_threads > 1 && orc_packs_parents(g->n, max_w, rule)) {
+    s.packed_parents = 1;
+    status = update_threaded(g, source, k, n_old, cfrom, cto, nc, dist, parent, &s, err, err_cap);
+    free(cfrom);
+    free(cto);
+    if (st) *st = s;
+    return status;
   }
   engine E;
   status = engine_init(&E, g, k, source, dist, parent, &s);

@@ -330,3 +330,54 @@ def test_parallel_apply_equals_sequential():
         np.testing.assert_array_equal(a[0][key], b[0][key], err_msg=key)
     np.testing.assert_array_equal(a[1], b[1])
     np.testing.assert_array_equal(a[2], b[2])
+
+
+@pytest.mark.parametrize("case", ["sparse", "multigraph-k2", "undirected", "growth", "no-tree-edges"])
+def test_threaded_repair_equals_sequential(case):
+    # the CPU baseline runs the oracle's repair on several threads (openmp.cpp:223-583): the
+    # trees and the deterministic counters (invalidated, affected) equal the sequential engine's
+    # after every batch of a chain
+    from tests.helpers import random_batch, random_graph
+    rng = np.random.default_rng({"sparse": 1, "multigraph-k2": 2, "undirected": 3, "growth": 4,
+                                 "no-tree-edges": 5}[case])
+    n, src, dst, w = random_graph(rng, "sparse", 2000, multi=case == "multigraph-k2")
+    k = 2 if case == "multigraph-k2" else 1
+    objective = k - 1
+    if k == 2:
+        w = np.stack([w, rng.integers(1, 9, w.size)], axis=1).reshape(-1)
+    props = {"multigraph-k2": O.mosp_props(), "undirected": O.mosp_props(directed=0)}.get(
+        case, O.default_props())
+    batches = []
+    parents = None
+    runs = {}
+    try:
+        for threads in (1, 8):
+            O.set_threads(threads)
+            g = O.Graph.from_edges(n, src, dst, w, k, props)
+            t, _ = O.compute(g, 0, objective=objective, rule=1)
+            seen = []
+            for step in range(4):
+                if threads == 1:
+                    if case == "no-tree-edges":
+                        b = {"ins_src": rng.integers(0, n, 50).astype(np.int32),
+                             "ins_dst": rng.integers(0, n, 50).astype(np.int32),
+                             "ins_w": rng.integers(1, 9, 50).astype(np.int32),
+                             "del_src": np.zeros(0, np.int32), "del_dst": np.zeros(0, np.int32)}
+                    else:
+                        b = random_batch(rng, g.n, src, dst, 400, tree_parents=t.parents,
+                                         grow=40 if case == "growth" else 0)
+                    b["ins_w"] = np.repeat(b["ins_w"], k) if k > 1 else b["ins_w"]
+                    batches.append(b)
+                b = batches[step]
+                st, sm = O.update(g, O.Batch(b["ins_src"], b["ins_dst"], b["ins_w"], b["del_src"],
+                                             b["del_dst"], k), t)
+                seen.append((st["invalidated"], st["affected"], sm["num_vertices_after"],
+                             t.distances.copy(), t.parents.copy()))
+            runs[threads] = seen
+    finally:
+        O.set_threads(1)
+    for step, (a, b) in enumerate(zip(runs[1], runs[8])):
+        assert a[:3] == b[:3], (case, step)
+        np.testing.assert_array_equal(a[3], b[3], err_msg=f"{case} step {step}")
+        np.testing.assert_array_equal(a[4], b[4], err_msg=f"{case} step {step}")
+    assert any(s[0] > 0 for s in runs[1]) or case == "no-tree-edges"
