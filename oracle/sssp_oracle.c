@@ -1032,16 +1032,20 @@ static void claim_append(int* stamp, int32_t v, int gen, int32_t* list, int64_t*
   }
 }
 
-/* The best packed offer of v's in-row (pull), or ORC_PACKED_NONE. */
+/* The best packed offer of v's in-row (pull), or ORC_PACKED_NONE.  Offers above maxd (the
+ * largest distance a word holds; no shortest distance is above it) are dropped, as the device
+ * kernel drops them, so no shift overflows. */
 #define ORC_PACKED_NONE UINT64_MAX
 static uint64_t pull_offer(const orc_graph* g, const int32_t* in_w, const uint64_t* word,
-                           int bits, int64_t v) {
+                           int bits, uint64_t maxd, int64_t v) {
   uint64_t best = ORC_PACKED_NONE;
   for (int64_t e = g->in_row_ptr[v]; e < g->in_row_ptr[v + 1]; ++e) {
     const int32_t u = g->in_col[e];
     const uint64_t wu = __atomic_load_n(&word[u], __ATOMIC_RELAXED);
     if (wu == ORC_PACKED_NONE) continue;
-    const uint64_t offer = (((wu >> bits) + (uint64_t)in_w[e]) << bits) | (uint64_t)u;
+    const uint64_t nd = (wu >> bits) + (uint64_t)in_w[e];
+    if (nd > maxd) continue;
+    const uint64_t offer = (nd << bits) | (uint64_t)u;
     if (offer < best) best = offer;
   }
   return best;
@@ -1053,6 +1057,7 @@ static int update_threaded(orc_graph* g, int32_t source, int k, int64_t n_old,
   const int64_t n = g->n;
   const int bits = parent_bits(n);
   const uint64_t none = ((uint64_t)1 << bits) - 1;
+  const uint64_t maxd = (~0ULL >> bits) - 1;
   const int32_t* w = g->w + (size_t)k * (size_t)g->m;
   const int32_t* in_w = g->in_w + (size_t)k * (size_t)g->m;
   const size_t nz = (size_t)(n > 0 ? n : 1);
@@ -1130,7 +1135,7 @@ static int update_threaded(orc_graph* g, int32_t source, int k, int64_t n_old,
     for (int64_t i = 0; i < ninv + g->num_ins; ++i) {
       const int32_t v = i < ninv ? list_a[i] : g->ins_dst[i - ninv];
       if (v == source) continue;
-      const uint64_t best = pull_offer(g, in_w, word, bits, v);
+      const uint64_t best = pull_offer(g, in_w, word, bits, maxd, v);
       uint64_t prev;
       if (best != ORC_PACKED_NONE && atomic_min_u64(&word[v], best, &prev) &&
           (prev == ORC_PACKED_NONE || (best >> bits) < (prev >> bits)))
@@ -1157,8 +1162,9 @@ static int update_threaded(orc_graph* g, int32_t source, int k, int64_t n_old,
         const uint64_t da = wa >> bits;
         for (int64_t e = g->row_ptr[a]; e < g->row_ptr[a + 1]; ++e) {
           const int32_t x = g->col[e];
-          if (x == source) continue;
-          const uint64_t offer = ((da + (uint64_t)w[e]) << bits) | (uint64_t)a;
+          const uint64_t nd = da + (uint64_t)w[e];
+          if (x == source || nd > maxd) continue;
+          const uint64_t offer = (nd << bits) | (uint64_t)a;
           uint64_t prev;
           if (atomic_min_u64(&word[x], offer, &prev) &&
               (prev == ORC_PACKED_NONE || (offer >> bits) < (prev >> bits)))
