@@ -175,27 +175,51 @@ def batch_maker(args, stream):
     return lambda parents: churn.next(args.batch)
 
 
-def cpu_baseline_sample(edges, tree_d, tree_p, batches, budget_s=20.0, source=0):
-    """The oracle (the reference's algorithm restated in C, on every host core as the
-    reference's OpenMP host path: the batch application and the repair threaded) on the same
-    graph and batches: time sssp::update per batch until the budget is spent."""
+def oracle_replay(edges, source, init_tree, batches, gpu_stats, final_tree, budget_s=90.0):
+    """The CPU leg: the oracle (the reference's algorithm restated in C, batch application and
+    repair on every host core, as the reference's OpenMP host path) computes the initial tree of
+    the same graph itself, then replays the GPU arm's batches in order, timing each update.
+
+    It is also the full-size parity check of the GPU arm: the oracle's initial tree against the
+    GPU's compute, every batch's `invalidated` / `affected` and apply summary against the GPU's
+    stats of the same batch, and, when every batch was replayed within the budget, the final
+    tree against the GPU's (distances and parents bit for bit)."""
     from oracle import oracle as O
     cores = O.set_threads(host_cores())
     rp, col, w = edges.csr()
     og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
-    ot = O.from_arrays(og, source, tree_d, tree_p, canonicalize=False, validate=False, rule=1)
+    t0 = time.perf_counter()
+    ot, _ = O.compute(og, source, rule=1)
+    compute_s = time.perf_counter() - t0
+    check = {"compute_equal": bool(np.array_equal(ot.distances, init_tree[0]) and
+                                   np.array_equal(ot.parents, init_tree[1])),
+             "batches": len(batches), "replayed": 0, "stats_equal": True, "final_tree_equal": None,
+             "first_mismatch": None, "oracle_compute_s": round(compute_s, 1)}
     done, changes, spent = 0, 0, 0.0
-    for b in batches:
+    for i, (b, gs) in enumerate(zip(batches, gpu_stats)):
         t0 = time.perf_counter()
-        O.update(og, O.Batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
-                             b.delete_dst), ot)
+        ost, osm = O.update(og, O.Batch(b.insert_src, b.insert_dst, b.insert_weights, b.delete_src,
+                                        b.delete_dst), ot)
         spent += time.perf_counter() - t0
         done += 1
         changes += b.size
+        got = (gs.invalidated, gs.affected, gs.batch.inserted_edges, gs.batch.deleted_edges,
+               gs.batch.updated_edges)
+        want = (ost["invalidated"], ost["affected"], osm["inserted_edges"], osm["deleted_edges"],
+                osm["updated_edges"])
+        if got != want and check["stats_equal"]:
+            check["stats_equal"] = False
+            check["first_mismatch"] = {"batch": i, "gpu": list(got), "oracle": list(want)}
         if spent > budget_s:
             break
+    check["replayed"] = done
+    if done == len(batches):
+        check["final_tree_equal"] = bool(np.array_equal(ot.distances, final_tree[0]) and
+                                         np.array_equal(ot.parents, final_tree[1]))
     O.set_threads(1)
-    return changes / spent, done, spent, cores
+    check["verified"] = bool(check["compute_equal"] and check["stats_equal"] and
+                             check["final_tree_equal"])
+    return changes / spent, done, spent, cores, check
 
 
 def host_cores() -> int:
@@ -207,7 +231,11 @@ def host_cores() -> int:
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU algorithm (the oracle port) on this workload."""
+    """--impl reference: the reference's CPU algorithm (the oracle port) on this workload.
+
+    Nothing of this package's CUDA library runs here: the synthetic graph is generated with
+    torch tensor ops (on the GPU when one is present: input generation only, outside the timed
+    steps), and the oracle computes the initial tree and applies every batch."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -216,21 +244,10 @@ def run_reference(args):
     edges, _ = make_workload(args, device)
     from dyng_b200 import generators as G
     from oracle import oracle as O
+    cores = O.set_threads(host_cores())
     rp, col, w = edges.csr()
     og = O.Graph.from_csr(rp, col, w, 1, O.default_props())
-    # initial tree: from the CUDA path when a GPU is present (a compute of the oracle at this
-    # scale is not part of the update path), else from the oracle
-    if device:
-        import dyng_b200 as D
-        g = D.Graph.from_csr(rp, col, w)
-        t = D.sssp.compute(g, source_of(args))
-        d0, p0 = t.distances, t.parents
-        del t, g
-    else:
-        ot0, _ = O.compute(og, source_of(args), rule=1)
-        d0, p0 = ot0.distances, ot0.parents
-    ot = O.from_arrays(og, source_of(args), d0, p0, canonicalize=False, validate=False, rule=1)
-    cores = O.set_threads(host_cores())
+    ot, _ = O.compute(og, source_of(args), rule=1)
     stream = G.BatchStream(edges, seed=7)
     make_batch = batch_maker(args, stream)
     times, sizes = [], []
@@ -250,7 +267,10 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": workload_name(args),
+                       "vertices": int(edges.num_vertices), "edges": int(edges.src.size),
                        "batch_changes": args.batch, "insert_fraction": insert_fraction(args),
+                       "source": source_of(args), "parallelism": f"replicas{args.gpus}",
+                       "l2": "inputs larger than L2 (graph arenas ~1 GB)",
                        "p50_ms": 1000 * float(np.percentile(times, 50)),
                        "p99_ms": 1000 * float(np.percentile(times, 99))},
             "cpu_baseline": {"value": value, "unit": "changed edges/s", "cores": cores,
@@ -269,6 +289,7 @@ class Arm:
     def __init__(self, name, schedule=None, scheduler=None):
         self.name, self.schedule, self.scheduler = name, schedule, scheduler
         self.lat, self.sizes, self.stats, self.host = [], [], [], []
+        self.all_stats = []  # every step's stats, warm-up included (the oracle replay checks them)
         self.total_ms = 0.0
 
     def summary(self, world):
@@ -322,6 +343,7 @@ def _run_arm(env, arm, next_batch, nvtx):
         st = D.sssp.update(g, db, tree, schedule=arm.schedule, scheduler=arm.scheduler)
         e1.record(stream)
         e1.synchronize()
+        arm.all_stats.append(st)
         if step >= args.warmup:
             arm.host.append(time.perf_counter() - h0)
             arm.lat.append(e0.elapsed_time(e1))
@@ -368,6 +390,9 @@ def main():
     source = source_of(args)
     tree = D.sssp.compute(g, source)
     build_s = time.time() - t0
+    # the oracle replay (CPU leg, rank 0) starts from its own compute and checks it against this
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    init_tree = (tree.distances, tree.parents) if cpu_leg else None
     bs = G.BatchStream(edges, seed=7)
     make_batch = batch_maker(args, bs)
     env = (D, torch, g, tree, stream, args, world, local)
@@ -403,8 +428,9 @@ def main():
     arms["plain"] = run_arm(env, Arm("plain", schedule=fixed), generate,
                             nvtx=args.schedule == "plain")
     same = None
+    final_plain = (tree.distances, tree.parents)
     if learned is not None:
-        d_plain, p_plain = tree.distances, tree.parents
+        d_plain, p_plain = final_plain
         g.copy_from(g_snap)
         tree.copy_from(t_snap)
         del g_snap, t_snap
@@ -412,7 +438,6 @@ def main():
                                   nvtx=args.schedule == "learned")
         same = bool(np.array_equal(d_plain, tree.distances) and
                     np.array_equal(p_plain, tree.parents))
-        del d_plain, p_plain
     clocks = sampler.stop()
     head = arms[args.schedule]
     summ = {k: a.summary(world) for k, a in arms.items()}
@@ -464,26 +489,35 @@ def main():
              for k in ("iterations", "epochs", "pushes", "invalidated", "affected", "rounds",
                        "touched", "delta", "grid_blocks")}
     classes = [list(s.schedule_classes) for s in timed_stats] if args.schedule == "learned" else None
+    # the same roofline per phase of the kernel (bytes and device time of each phase, summed over
+    # the timed steps): the kernel-wide fraction blends O(n) streaming passes with the latency-
+    # bound frontier phases
+    per_step = [s.phase_bytes_ms() for s in timed_stats]
+    phase_roof = {}
+    for name in timed_stats[0].PHASE_WORK:
+        pb = float(sum(x[name][0] for x in per_step))
+        pm = float(sum(x[name][1] for x in per_step))
+        gbs = pb / (pm / 1000.0) / 1e9 if pm > 0 else None
+        phase_roof[name] = {"bytes_per_update": round(pb / len(per_step)),
+                            "ms_per_update": round(pm / len(per_step), 4),
+                            "achieved_gbs": round(gbs, 1) if gbs is not None else None,
+                            "frac": round(gbs / peak, 4) if gbs is not None and peak else None}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    oracle_check = None
+    if cpu_leg:
         try:
-            cbs = G.BatchStream(edges, seed=7)
-            cmake = batch_maker(args, cbs)
-            batches = [cmake(None) for _ in range(4)]
-            # the sample starts from the initial tree of the same graph
-            g0 = D.Graph.from_csr(rp, col, w, resources=res)
-            t_init = D.sssp.compute(g0, source)
-            d0, p0 = t_init.distances, t_init.parents
-            del t_init, g0
-            v, done, spent, cores = cpu_baseline_sample(edges, d0, p0, batches, source=source)
+            v, done, spent, cores, oracle_check = oracle_replay(
+                edges, source, init_tree, recorded, arms["plain"].all_stats, final_plain)
             cpu = {"value": v, "unit": "changed edges/s", "cores": cores, "kind": "port",
-                   "sample": f"oracle sssp::update on {done} of the workload's {args.batch}-change "
-                             f"batches ({spent:.1f} s), same graph; apply and repair on "
-                             f"{cores} threads"}
+                   "sample": f"oracle sssp::update on {done} of the GPU arm's {len(recorded)} "
+                             f"{args.batch}-change batches ({spent:.1f} s), same graph, from the "
+                             f"oracle's own compute; apply and repair on {cores} threads"}
         except Exception as exc:  # noqa: BLE001
             cpu = {"value": None, "unit": "changed edges/s", "cores": host_cores(),
                    "kind": "port", "sample": f"failed: {exc}"}
+        del init_tree
+    del final_plain
 
     if rank == 0:
         compare = {k: {kk: round(vv, 4) if kk not in ("value", "steps", "maintenance") else vv
@@ -516,6 +550,8 @@ def main():
                        "pj_rounds_us_last_update": list(timed_stats[-1].pj_rounds_us),
                        "pj_done_us_last_update": list(timed_stats[-1].pj_done_us),
                        "verified_vs_compute": verified, "compute_from_scratch": compute_info,
+                       "verified_vs_oracle": oracle_check["verified"] if oracle_check else None,
+                       "oracle_check": oracle_check,
                        "setup_s": {"generate": round(gen_s, 1), "build_and_compute": round(build_s, 1)}},
             "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": ctypes.sizeof(D._native.Stats),
@@ -524,7 +560,7 @@ def main():
             "gpu_launches": int(sum(s.kernel_launches for s in timed_stats)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic(args),
-                         "peak_kind": peak_kind, "kernel": "k_sssp"},
+                         "peak_kind": peak_kind, "kernel": "k_sssp", "phases": phase_roof},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

@@ -53,7 +53,7 @@ class Stats(ctypes.Structure):
                 ("grid_blocks", ctypes.c_int32), ("invalidation", ctypes.c_int32),
                 ("apply_ms", ctypes.c_float), ("sssp_ms", ctypes.c_float),
                 ("rounds", ctypes.c_int64), ("touched", ctypes.c_int64),
-                ("work", ctypes.c_int64 * 24), ("phase_ms", ctypes.c_float * 7),
+                ("work", ctypes.c_int64 * 32), ("phase_ms", ctypes.c_float * 7),
                 ("trace_len", ctypes.c_int32), ("trace_light", ctypes.c_int32 * 64),
                 ("trace_heavy", ctypes.c_int32 * 64), ("trace_us", ctypes.c_float * 64),
                 ("features", ctypes.c_float * 12), ("schedule_classes", ctypes.c_int32 * 3),
@@ -113,6 +113,13 @@ class ServerInfo(ctypes.Structure):
 
 
 # Every symbol of include/dyngb200.h with (restype, argtypes).
+class TestHooks(ctypes.Structure):
+    """dyngb200_test_hooks: host-side failure injection for the tests (no GPU fault)."""
+
+    _fields_ = [("barrier_timeout_ns", ctypes.c_int64), ("barrier_extra_arrivals", ctypes.c_int32),
+                ("no_cooperative_launch", ctypes.c_int32)]
+
+
 SIGNATURES = {
     "dyngb200_last_error_message": (ctypes.c_char_p, []),
     "dyngb200_status_name": (ctypes.c_char_p, [ctypes.c_int]),
@@ -120,6 +127,9 @@ SIGNATURES = {
     "dyngb200_context_create": (ctypes.c_int, [ctypes.c_int, c_void_p, ctypes.POINTER(c_void_p)]),
     "dyngb200_context_destroy": (ctypes.c_int, [c_void_p]),
     "dyngb200_context_synchronize": (ctypes.c_int, [c_void_p]),
+    "dyngb200_context_set_test_hooks": (ctypes.c_int, [c_void_p, ctypes.POINTER(TestHooks)]),
+    "dyngb200_debug_device_allocations": (ctypes.c_int, [c_i64p]),
+    "dyngb200_debug_fail_device_allocation": (ctypes.c_int, [ctypes.c_int64]),
     "dyngb200_props_default": (None, [ctypes.POINTER(Props)]),
     "dyngb200_props_mosp_compatible": (None, [ctypes.POINTER(Props)]),
     "dyngb200_graph_from_edges": (ctypes.c_int, [c_void_p, ctypes.c_int64, c_i32p, c_i32p, c_i32p,

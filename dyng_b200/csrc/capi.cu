@@ -274,6 +274,33 @@ dyngb200_status dyngb200_context_synchronize(dyngb200_context ctx) {
   });
 }
 
+dyngb200_status dyngb200_context_set_test_hooks(dyngb200_context ctx,
+                                                const dyngb200_test_hooks* hooks) {
+  return guarded([&] {
+    expects(ctx != nullptr, "context_set_test_hooks: null context");
+    const dyngb200_test_hooks h = hooks ? *hooks : dyngb200_test_hooks{0, 0, 0};
+    expects(h.barrier_timeout_ns >= 0 && h.barrier_extra_arrivals >= 0,
+            "context_set_test_hooks: negative limit or arrivals");
+    ctx->ctx.test_barrier_timeout_ns = h.barrier_timeout_ns;
+    ctx->ctx.test_barrier_extra = h.barrier_extra_arrivals;
+    ctx->ctx.test_no_cooperative = h.no_cooperative_launch != 0 ? 1 : 0;
+  });
+}
+
+dyngb200_status dyngb200_debug_device_allocations(int64_t* count) {
+  return guarded([&] {
+    expects(count != nullptr, "debug_device_allocations: null argument");
+    *count = device_alloc_count();
+  });
+}
+
+dyngb200_status dyngb200_debug_fail_device_allocation(int64_t nth) {
+  return guarded([&] {
+    expects(nth >= 0, "debug_fail_device_allocation: negative count");
+    device_alloc_fail_at(nth);
+  });
+}
+
 dyngb200_status dyngb200_graph_from_edges(dyngb200_context ctx, int64_t n, const int32_t* src,
                                           const int32_t* dst, const int32_t* weights,
                                           int64_t num_edges, int32_t num_weights, int32_t memory,

@@ -1283,7 +1283,11 @@ ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int object
 // Workspace
 // ------------------------------------------------------------------------------------------------
 void Workspace::reserve_vertices(long long n_cap, cudaStream_t s) {
+  pj_blk.reserve(2 * kPjMaxBlocks, s);
   if (n_cap <= n_sized) return;
+  // buffers are released before they are reallocated: until every one is back, the workspace
+  // counts as unsized (a failed allocation makes the next call start over, never skip)
+  n_sized = 0;
   const size_t n = static_cast<size_t>(n_cap);
   for (DevBuf<int>* b : {&touch_out_stamp, &touch_in_stamp, &stamp, &touch_stamp}) {
     b->release();
@@ -1315,6 +1319,7 @@ void Workspace::reserve_batch(long long ops, int k, cudaStream_t s) {
   while (cap < 2 * ops) cap <<= 1;
   if (cap > pairs_sized) {
     const size_t c = static_cast<size_t>(cap);
+    pairs_sized = 0;  // unsized until every table is back (see reserve_vertices)
     pair_key.release();
     pair_key.reserve(c, s);
     for (DevBuf<int>* b : {&pair_d, &pair_t, &pair_first, &pair_last, &pair_out_pos, &pair_in_pos,
@@ -1543,27 +1548,37 @@ struct MaintenanceTimer {
 }  // namespace
 
 // (Re)build the edge index with room for `extra` more edges and at least `min_cap` slots.
+// Slots of an edge index for the graph's edges plus `extra` insertions (load <= 1/2 after the
+// build), at least min_cap.
+static long long index_want(const Graph& g, long long extra, long long min_cap) {
+  long long want = 1024;
+  while (want < 2 * (g.host_counters.m + extra) + 65536 || want < min_cap) want <<= 1;
+  return want;
+}
+
 void graph_index_build(Context& ctx, Graph& g, long long extra, long long min_cap) {
   MaintenanceTimer timer(g, g.index_ms);
   ++g.index_builds;
   cudaStream_t s = ctx.stream;
-  long long want = 1024;
-  while (want < 2 * (g.host_counters.m + extra) + 65536 || want < min_cap) want <<= 1;
+  Workspace& ws = ctx.ws;
+  ws.ctl.reserve(1, s);  // before the index changes: every allocation comes first
+  const long long want = index_want(g, extra, min_cap);
   if (want != g.ecap) {
-    g.ekey.release();
-    g.eout.release();
-    g.ein.release();
-    g.ekey.reserve(static_cast<size_t>(want));
-    g.eout.reserve(static_cast<size_t>(want));
-    g.ein.reserve(static_cast<size_t>(want));
+    // the new arrays first: a failed allocation leaves the old index, whole, in place
+    DevBuf<u64> key;
+    DevBuf<unsigned> out, in;
+    key.reserve(static_cast<size_t>(want));
+    out.reserve(static_cast<size_t>(want));
+    in.reserve(static_cast<size_t>(want));
+    g.ekey.swap(key);
+    g.eout.swap(out);
+    g.ein.swap(in);
     g.ecap = want;
   }
   GraphCounters gc = g.host_counters;
   gc.idx_live = 0;
   gc.idx_dead = 0;
   DYNGB200_CUDA(cudaMemcpyAsync(g.counters.ptr, &gc, sizeof(gc), cudaMemcpyHostToDevice, s));
-  Workspace& ws = ctx.ws;
-  ws.ctl.reserve(1, s);
   DYNGB200_CUDA(cudaMemsetAsync(&ws.ctl.ptr->error, 0, sizeof(unsigned), s));
   GraphView v = g.view();
   const int grid = ctx.sm_count * 8;
@@ -1717,7 +1732,26 @@ void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in
   long long base = std::max(top[0] + demand[0], top[1] + demand[1]);
   const long long arena = round4(base + std::max(base / 2, 1LL << 16));
   expects(arena < 0xffffffffLL, "graph: the slack arena exceeds 2^32 slots", DYNGB200_CAPACITY);
-  // pass 2: side by side, so that one old and one new arena are held at a time
+  // pass 2: the new arenas of both sides are allocated before either side's rows move (the row
+  // descriptors are rewritten in place, and both sides share arena_cap): a failed allocation
+  // leaves the graph as it was
+  DevBuf<int32_t> ncol[2], nw[2];
+  for (int side = 0; side < 2; ++side) {
+    ncol[side].reserve(static_cast<size_t>(arena));
+    nw[side].reserve(static_cast<size_t>(arena) * static_cast<size_t>(k));
+  }
+  // the edge index is rebuilt over the moved slots below: its arrays (when it grows) and the
+  // control block are allocated now, so the rebuild cannot fail on an allocation after the
+  // slots moved (the old index would point at other edges' slots)
+  const long long index_cap = g.props.allow_multi ? g.ecap : index_want(g, 0, g.ecap);
+  DevBuf<u64> ikey;
+  DevBuf<unsigned> iout, iin;
+  if (index_cap != g.ecap) {
+    ikey.reserve(static_cast<size_t>(index_cap));
+    iout.reserve(static_cast<size_t>(index_cap));
+    iin.reserve(static_cast<size_t>(index_cap));
+  }
+  ctx.ws.ctl.reserve(1, s);
   for (int side = 0; side < 2; ++side) {
     DevBuf<int32_t>& col = side == 0 ? g.out_col : g.in_col;
     DevBuf<int32_t>& w = side == 0 ? g.out_w : g.in_w;
@@ -1726,20 +1760,26 @@ void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in
     ctx.launches += 2;
     k_compact_count<<<grid, kBlock, 0, s>>>(desc, col.ptr, n, g.props.headroom, cap.ptr);
     DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(temp.ptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
-    DevBuf<int32_t> ncol, nw;
-    ncol.reserve(static_cast<size_t>(arena));
-    nw.reserve(static_cast<size_t>(arena) * static_cast<size_t>(k));
-    DYNGB200_CUDA(cudaMemsetAsync(ncol.ptr, 0xff, static_cast<size_t>(arena) * sizeof(int32_t), s));
+    DYNGB200_CUDA(cudaMemsetAsync(ncol[side].ptr, 0xff,
+                                  static_cast<size_t>(arena) * sizeof(int32_t), s));
     k_compact_copy<<<grid, kBlock, 0, s>>>(desc, (side == 0 ? g.out_cap : g.in_cap).ptr,
                                            (side == 0 ? g.out_dead : g.in_dead).ptr, col.ptr,
-                                           w.ptr, g.arena_cap, start.ptr, ncol.ptr, nw.ptr, arena,
-                                           g.k, n);
+                                           w.ptr, g.arena_cap, start.ptr, ncol[side].ptr,
+                                           nw[side].ptr, arena, g.k, n);
     DYNGB200_CUDA(cudaGetLastError());
-    DYNGB200_CUDA(cudaStreamSynchronize(s));
-    col.swap(ncol);
-    w.swap(nw);
   }
+  DYNGB200_CUDA(cudaStreamSynchronize(s));
+  g.out_col.swap(ncol[0]);
+  g.out_w.swap(nw[0]);
+  g.in_col.swap(ncol[1]);
+  g.in_w.swap(nw[1]);
   g.arena_cap = arena;
+  if (index_cap != g.ecap) {
+    g.ekey.swap(ikey);
+    g.eout.swap(iout);
+    g.ein.swap(iin);
+    g.ecap = index_cap;
+  }
   ++g.compactions;
   GraphCounters& gc = g.host_counters;
   gc.out_top = static_cast<u64>(top[0]);
@@ -1775,48 +1815,47 @@ void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, lo
     expects(new_cap < (1LL << 32), "graph: the slack arena would pass 2^32 slots",
             DYNGB200_CAPACITY);
     const size_t k = static_cast<size_t>(g.k > 0 ? g.k : 1);
-    for (DevBuf<int32_t>* d : {&g.out_col, &g.in_col}) {
-      DevBuf<int32_t> fresh;
-      fresh.reserve(static_cast<size_t>(new_cap));
-      DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, static_cast<size_t>(top) * sizeof(int32_t),
-                                    cudaMemcpyDeviceToDevice, ctx.stream));
-      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      d->swap(fresh);
-    }
-    for (DevBuf<int32_t>* d : {&g.out_w, &g.in_w}) {
-      DevBuf<int32_t> fresh;
-      fresh.reserve(static_cast<size_t>(new_cap) * k);
-      for (size_t j = 0; j < k; ++j)
-        DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr + j * new_cap, d->ptr + j * g.arena_cap,
+    // all four new arrays before anything is swapped: the weight columns' stride is arena_cap,
+    // so the arrays and arena_cap change together or not at all
+    DevBuf<int32_t> fresh[4];
+    DevBuf<int32_t>* cur[4] = {&g.out_col, &g.in_col, &g.out_w, &g.in_w};
+    for (int a = 0; a < 4; ++a)
+      fresh[a].reserve(static_cast<size_t>(new_cap) * (a < 2 ? 1 : k));
+    for (int a = 0; a < 4; ++a) {
+      const size_t cols = a < 2 ? 1 : k;
+      for (size_t j = 0; j < cols; ++j)
+        DYNGB200_CUDA(cudaMemcpyAsync(fresh[a].ptr + j * new_cap, cur[a]->ptr + j * g.arena_cap,
                                       static_cast<size_t>(top) * sizeof(int32_t),
                                       cudaMemcpyDeviceToDevice, ctx.stream));
-      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      d->swap(fresh);
     }
+    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+    for (int a = 0; a < 4; ++a) cur[a]->swap(fresh[a]);
     g.arena_cap = new_cap;
     ++g.arena_growths;
   }
   if (compact) graph_compact(ctx, g, need_out, need_in);
   if (need_n > g.n_cap) {
     const long long new_cap = std::max(need_n + 1024, g.n_cap * 2);
-    for (DevBuf<RowDesc>* d : {&g.out_desc, &g.in_desc}) {
-      DevBuf<RowDesc> fresh;
-      fresh.reserve(static_cast<size_t>(new_cap));
-      DYNGB200_CUDA(cudaMemsetAsync(fresh.ptr, 0, new_cap * sizeof(RowDesc), ctx.stream));
-      DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, g.n_cap * sizeof(RowDesc),
+    // every new array before anything is swapped (a failed allocation changes nothing)
+    DevBuf<RowDesc> fdesc[2];
+    DevBuf<int32_t> fint[4];
+    DevBuf<RowDesc>* cdesc[2] = {&g.out_desc, &g.in_desc};
+    DevBuf<int32_t>* cint[4] = {&g.out_cap, &g.in_cap, &g.out_dead, &g.in_dead};
+    for (auto& f : fdesc) f.reserve(static_cast<size_t>(new_cap));
+    for (auto& f : fint) f.reserve(static_cast<size_t>(new_cap));
+    for (int a = 0; a < 2; ++a) {
+      DYNGB200_CUDA(cudaMemsetAsync(fdesc[a].ptr, 0, new_cap * sizeof(RowDesc), ctx.stream));
+      DYNGB200_CUDA(cudaMemcpyAsync(fdesc[a].ptr, cdesc[a]->ptr, g.n_cap * sizeof(RowDesc),
                                     cudaMemcpyDeviceToDevice, ctx.stream));
-      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      d->swap(fresh);
     }
-    for (DevBuf<int32_t>* d : {&g.out_cap, &g.in_cap, &g.out_dead, &g.in_dead}) {
-      DevBuf<int32_t> fresh;
-      fresh.reserve(static_cast<size_t>(new_cap));
-      DYNGB200_CUDA(cudaMemsetAsync(fresh.ptr, 0, new_cap * sizeof(int32_t), ctx.stream));
-      DYNGB200_CUDA(cudaMemcpyAsync(fresh.ptr, d->ptr, g.n_cap * sizeof(int32_t),
+    for (int a = 0; a < 4; ++a) {
+      DYNGB200_CUDA(cudaMemsetAsync(fint[a].ptr, 0, new_cap * sizeof(int32_t), ctx.stream));
+      DYNGB200_CUDA(cudaMemcpyAsync(fint[a].ptr, cint[a]->ptr, g.n_cap * sizeof(int32_t),
                                     cudaMemcpyDeviceToDevice, ctx.stream));
-      DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
-      d->swap(fresh);
     }
+    DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+    for (int a = 0; a < 2; ++a) cdesc[a]->swap(fdesc[a]);
+    for (int a = 0; a < 4; ++a) cint[a]->swap(fint[a]);
     g.n_cap = new_cap;
   }
 }
@@ -1978,11 +2017,12 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
   const StagedBatch b = stage_batch(ctx, batch, g.k);
   UpdateCtl r{};
   DevBuf<unsigned char> flags;
+  // allocated before the applier is queued: a failed allocation leaves the graph as it was
+  if (weight_increased && b.ni > 0) flags.reserve(static_cast<size_t>(b.ni) * g.k);
   for (int attempt = 0;; ++attempt) {
     apply_prepare(ctx, g, b, -1, 0, nullptr);
     apply_commit(ctx, g, b);
     if (weight_increased && b.ni > 0) {
-      flags.reserve(static_cast<size_t>(b.ni) * g.k);
       ApplyParams p = make_params(ctx, g, b, -1, 0);
       k_insert_flags<<<grid_for(b.ni, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, flags.ptr);
       ++ctx.launches;

@@ -47,6 +47,8 @@ void* device_alloc(size_t bytes, int* device);
 void device_free(void* p, int device) noexcept;
 void device_pool_reserve(size_t bytes);        // pre-fill the current device's pool
 long long device_pool_idle_bytes(int device);  // pooled bytes not in use
+long long device_alloc_count();                // device_alloc calls of this process so far
+void device_alloc_fail_at(long long nth);      // the nth device_alloc from now fails (0: none)
 
 // A device buffer that grows on demand (contents are not preserved unless asked).
 template <typename T>
@@ -172,7 +174,7 @@ struct UpdateCtl {
   long long loop_pushes;
   u64 loop_threshold;
   // work counters (algorithmic traffic) and phase timestamps of the sssp kernel
-  long long work[24];
+  long long work[32];
   unsigned long long phase_ns[8];
   // trace of the first 64 push iterations / epochs: (light count, heavy chunks, ns since start)
   int trace_n[64];
@@ -185,7 +187,13 @@ struct UpdateCtl {
   // 128-byte line (the polling of the generation does not slow the arrivals)
   alignas(128) unsigned bar_count;
   alignas(128) unsigned bar_gen;
+  // progress of a block that works alone (the small-frontier loop of block 0): the blocks waiting
+  // at a grid barrier meanwhile restart their time limit whenever it moves
+  alignas(128) unsigned heartbeat;
 };
+
+// Persistent blocks the pointer-jumping survivor lists of the sssp kernel support.
+constexpr int kPjMaxBlocks = 1024;
 
 // Scratch memory of a context, sized on demand and reused (the reference's workspace pool).
 struct Workspace {
@@ -207,6 +215,7 @@ struct Workspace {
   // sssp
   DevBuf<int> stamp, touch_stamp, flag, in_far, ancestor;
   DevBuf<int> pj_blk;  // per-block survivor counts of pointer jumping
+  DevBuf<long long> batch_extrema;  // update_each: per-objective insertion weight range, max id
   DevBuf<int> candidates, frontier, near_a, near_b, far_a, far_b, heavy_a, heavy_b, pull_heavy,
       touched, cand_med, near_med_a, near_med_b;
   DevBuf<UpdateCtl> ctl;
@@ -239,7 +248,16 @@ struct Context {
   // the learned scheduler's hook: when set, the next update runs with this schedule
   dyngb200_schedule schedule{};
   int schedule_set = 0;
+  // test hooks (dyngb200_context_set_test_hooks): the grid barrier's time limit without progress
+  // (0: kBarrierTimeoutNs), blocks every grid barrier waits for beyond the launched ones (they
+  // never arrive: the barrier's wait runs out), and a device taken as one without cooperative launch
+  long long test_barrier_timeout_ns = 0;
+  int test_barrier_extra = 0;
+  int test_no_cooperative = 0;
 };
+
+// The persistent kernels need cooperative launch; checked before anything of a call changes.
+void require_cooperative(const Context& ctx);
 
 struct Graph {
   uint64_t id = 0;

@@ -11,6 +11,7 @@
 // is never reused while a kernel on any stream may still touch it.
 #include "internal.hpp"
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <unordered_map>
@@ -58,9 +59,24 @@ int current_device() {
   return d;
 }
 
+std::atomic<long long> g_alloc_count{0};
+std::atomic<long long> g_fail_countdown{0};
+
 }  // namespace
 
+long long device_alloc_count() { return g_alloc_count.load(); }
+
+void device_alloc_fail_at(long long nth) { g_fail_countdown.store(nth > 0 ? nth : 0); }
+
 void* device_alloc(size_t bytes, int* device) {
+  g_alloc_count.fetch_add(1);
+  // the test hook of the allocation-failure sweeps: one allocation fails as cudaMalloc would
+  // (nothing is allocated, the call reports out-of-memory)
+  long long left = g_fail_countdown.load();
+  while (left > 0 && !g_fail_countdown.compare_exchange_weak(left, left - 1)) {
+  }
+  if (left == 1)
+    throw Error(DYNGB200_OUT_OF_MEMORY, "CUDA out of memory (an injected allocation failure)");
   const int d = current_device();
   DevicePool& dp = pool_of(d);
   void* p = nullptr;

@@ -26,7 +26,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kHeavyChunk = 256;
 constexpr unsigned long long kBarrierTimeoutNs = 5ULL * 1000 * 1000 * 1000;
-constexpr int kPjMaxBlocks = 1024;   // persistent blocks the pointer-jumping lists support
 
 struct SsspParams {
   GraphView g;
@@ -78,7 +77,11 @@ struct SsspParams {
   int* pj_blk;           // survivor counts of the pointer-jumping rounds: 2 x kPjMaxBlocks
   const unsigned char* inc;  // the applier's weight-increase flags (pairs x k)
   int use_inc;           // 1: changed edges of `objective` from inc[] (a batch applied for another
-                         // objective), 0: from the pair flags     // the tree's record of this run (the learned scheduler's history)
+                         // objective), 0: from the pair flags
+  // the grid barrier: its time limit without progress (0: kBarrierTimeoutNs) and blocks it waits
+  // for beyond the launched ones (0 outside tests; a phantom block makes every wait run out)
+  unsigned long long barrier_limit_ns;
+  int barrier_extra;
 };
 
 // Pair flags of the applier (graph.cu).
@@ -111,6 +114,8 @@ struct StageSet {
 
 __shared__ StageSet g_stage;
 __shared__ int g_nblk;  // blocks taking part in this launch (the schedule's grid size)
+__shared__ int g_bar_arrivals;  // arrivals a grid barrier waits for (g_nblk, plus test phantoms)
+__shared__ unsigned long long g_bar_limit;  // the barrier's time limit without progress (ns)
 
 __device__ __forceinline__ void staged_append(int id, int* list, int* count, int v) {
   const unsigned mask = __activemask();
@@ -179,21 +184,24 @@ __device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
 // released to the block that completes the barrier); the last arrival resets the counter and
 // releases the next generation, which the others poll with acquire loads.  Measured on B200 with
 // 444 blocks: 2.2 us per barrier, against 3.7 us for two-level arrival counters with full fences
-// sharing a line with the polled word.  The wait is bounded: past kBarrierTimeoutNs (or once
-// another block has timed out) it sets kErrTimeout and returns false.
+// sharing a line with the polled word.  The wait is bounded: once the barrier has seen no
+// progress for its limit (kBarrierTimeoutNs; progress = a move of the heartbeat word, which block
+// 0 bumps every step while it runs the small-frontier loop alone and the others wait here), or
+// once another block has timed out, it sets kErrTimeout and returns false.
 __device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
   stage_flush();
   __syncthreads();
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     const unsigned target = gen + 1;
-    const unsigned nblk = static_cast<unsigned>(g_nblk);
+    const unsigned arrivals = static_cast<unsigned>(g_bar_arrivals);
     int ok = 1;
-    if (atom_add_acq_rel(&c->bar_count, 1u) + 1u == nblk) {
+    if (atom_add_acq_rel(&c->bar_count, 1u) + 1u == arrivals) {
       st_relaxed(&c->bar_count, 0u);  // before the release: no block arrives again before it
       st_release(&c->bar_gen, target);
     } else {
       unsigned long long start = 0;
+      unsigned beat = 0;
       unsigned spins = 0;
       while (ld_acquire(&c->bar_gen) != target) {
         if ((++spins & 1023u) == 0) {
@@ -202,9 +210,11 @@ __device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
             break;
           }
           const unsigned long long now = global_ns();
-          if (start == 0) {
+          const unsigned hb = ld_volatile(&c->heartbeat);
+          if (start == 0 || hb != beat) {
             start = now;
-          } else if (now - start > kBarrierTimeoutNs) {
+            beat = hb;
+          } else if (now - start > g_bar_limit) {
             atomicOr(&c->error, kErrTimeout);
             ok = 0;
             break;
@@ -746,6 +756,8 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
   int2* hlists[2] = {p.heavy_a, p.heavy_b};
   const Packing pk = X.pk;
   while (true) {
+    // alone, block 0 shows the waiting blocks that it makes progress (no result is read back)
+    if (BLOCK && threadIdx.x == 0) atomicAdd(&c->heartbeat, 1u);
     const int cs = S.it % 3;
     const int nc = ld_cg(&c->near_cnt[cs]);
     const int mc = ld_cg(&c->near_med_cnt[cs]);
@@ -853,7 +865,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
                        ? c->active_blocks
                        : static_cast<int>(gridDim.x);
   if (static_cast<int>(blockIdx.x) >= nblk) return;
-  if (threadIdx.x == 0) g_nblk = nblk;
+  if (threadIdx.x == 0) {
+    g_nblk = nblk;
+    g_bar_arrivals = nblk + (p.barrier_extra > 0 ? p.barrier_extra : 0);
+    g_bar_limit = p.barrier_limit_ns > 0 ? p.barrier_limit_ns : kBarrierTimeoutNs;
+  }
   if (c->sched_heavy > 0) p.heavy_degree = c->sched_heavy;
   p.small_frontier = c->sched_small;
   p.walk = c->sched_walk && p.tree_trusted ? 1 : 0;
@@ -879,6 +895,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
   // work counters (see dyngb200_stats::work)
   long long w_visits = 0, w_jumps = 0, w_inval = 0;
   unsigned pull_slots = 0, pull_words = 0, pull_rows = 0, unpacked = 0;
+  unsigned pull_atomics = 0, pull_appends = 0, pair_visits = 0, walk_rows = 0, walk_slots = 0;
   if (tid == 0) c->phase_ns[0] = global_ns();
 
   if (p.from_scratch) {
@@ -916,6 +933,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
     const int pairs = c->pairs;
     int changed = 0;
     for (long long i = tid; i < pairs; i += threads) {
+      ++pair_visits;
       const int slot = p.pair_list[i];
       const int f = p.pair_flags[slot];
       const bool increased = p.use_inc ? p.inc[static_cast<long long>(slot) * p.k + p.objective] != 0
@@ -1152,7 +1170,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         ++level;
       }
       w_inval += X.appends;
-      X.appends = 0;
+      walk_rows = X.rows;
+      walk_slots = X.slots;
+      X.appends = X.rows = X.slots = 0;
       if (tid == 0) {
         c->levels = level;
         c->phase_ns[2] = global_ns();
@@ -1162,6 +1182,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
     if (tid == 0) c->phase_ns[3] = global_ns();
     // ---- insertion heads: pulled, or (canonical trees) offered the inserted edge ----------------
     for (long long i = tid; i < pairs; i += threads) {
+      ++pair_visits;
       const int slot = p.pair_list[i];
       const int f = p.pair_flags[slot];
       if (!(f & kPairHead)) continue;
@@ -1202,7 +1223,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
       pull_slots = Y.slots;
       pull_words = Y.words;
       pull_rows = Y.rows;
-      X.atomics += Y.atomics;
+      pull_atomics = Y.atomics;
+      pull_appends = Y.appends;
       X.tries += Y.tries;
     }
     if (!grid_barrier(c, bar)) return;
@@ -1364,8 +1386,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
   warp_sum_into_ll(static_cast<long long>(X.tries), &c->work[12]);
   warp_sum_into_ll(static_cast<long long>(X.appends), &c->work[10]);
   warp_sum_into_ll(static_cast<long long>(unpacked), &c->work[11]);
+  warp_sum_into_ll(static_cast<long long>(pull_atomics), &c->work[23]);
+  warp_sum_into_ll(static_cast<long long>(pull_appends), &c->work[24]);
+  warp_sum_into_ll(static_cast<long long>(pair_visits), &c->work[25]);
+  warp_sum_into_ll(static_cast<long long>(walk_rows), &c->work[26]);
+  warp_sum_into_ll(static_cast<long long>(walk_slots), &c->work[27]);
   if (tid == 0) {
-    c->work[2] = 0;  // invalidated vertices: reported in c->invalidated
+    c->work[2] = ld_cg(&c->invalidated);  // complete: summed before the heads' barrier
     c->phase_ns[7] = global_ns();
     c->iterations = iterations;
     c->epochs = epochs;
@@ -1450,9 +1477,15 @@ static int persistent_blocks(Context& ctx, const dyngb200_schedule& sched) {
   return update_grid_blocks(ctx);
 }
 
-static void launch(Context& ctx, SsspParams& p, int blocks) {
-  expects(ctx.coop_supported != 0, "sssp: the fused engine needs cooperative launch",
+void require_cooperative(const Context& ctx) {
+  expects(ctx.coop_supported != 0 && ctx.test_no_cooperative == 0,
+          "sssp: the fused engine needs cooperative launch, which this device does not offer "
+          "(this library has no engine without it)",
           DYNGB200_NOT_SUPPORTED);
+}
+
+static void launch(Context& ctx, SsspParams& p, int blocks) {
+  require_cooperative(ctx);
   void* args[] = {&p};
   ++ctx.launches;
   DYNGB200_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_sssp), dim3(blocks),
@@ -1488,13 +1521,18 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
   p.touched = ws.touched.ptr;
   p.ctl = ws.ctl.ptr;
   p.hist = t.hist.ptr;
-  ws.pj_blk.reserve(2 * kPjMaxBlocks);
-  p.pj_blk = ws.pj_blk.ptr;
+  expects(ws.pj_blk.ptr != nullptr, "sssp: the workspace was not reserved", DYNGB200_INTERNAL);
+  p.pj_blk = ws.pj_blk.ptr;  // reserved by Workspace::reserve_vertices
+  p.barrier_limit_ns = ctx.test_barrier_timeout_ns > 0
+                           ? static_cast<unsigned long long>(ctx.test_barrier_timeout_ns)
+                           : 0;
+  p.barrier_extra = ctx.test_barrier_extra;
   return p;
 }
 
 // compute(): the persistent kernel from the source (fused.cuh:167-176).
 void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
+  require_cooperative(ctx);
   const long long launches0 = ctx.launches;
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
@@ -1567,7 +1605,7 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
     st->sssp_ms = ms;
     st->kernel_launches = ctx.launches - launches0;
     st->affected = r.affected;
-    for (int i = 0; i < 24; ++i) st->work[i] = r.work[i];
+    for (int i = 0; i < 32; ++i) st->work[i] = r.work[i];
     st->trace_len = r.trace_len;
     for (int i = 0; i < r.trace_len && i < 64; ++i) {
       st->trace_light[i] = r.trace_n[i];
@@ -1590,6 +1628,9 @@ static void enqueue_attempt(PendingUpdate& u) {
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   tree_reserve(ctx, t, g.n_cap);
+  // every allocation of the attempt comes before the applier is queued: a failed one leaves the
+  // graph as it was
+  g.pinned.reserve(kCounterSlots + g.host_columns.size());
   DYNGB200_CUDA(cudaEventRecord(u.e0, s));
   apply_prepare(ctx, g, u.b, t.opt.objective, t.opt.delta, &u.sched, &t, u.learned);
   apply_commit(ctx, g, u.b);
@@ -1612,7 +1653,6 @@ static void enqueue_attempt(PendingUpdate& u) {
   p.heavy_degree = 256;
   launch(ctx, p, u.blocks);
   DYNGB200_CUDA(cudaEventRecord(u.e2, s));
-  g.pinned.reserve(kCounterSlots + g.host_columns.size());
   DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
                                 cudaMemcpyDeviceToHost, s));
   DYNGB200_CUDA(cudaMemcpyAsync(g.pinned.ptr, g.counters.ptr, sizeof(GraphCounters),
@@ -1640,6 +1680,7 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
   u.sched = sched;
   u.learned = learned;
   u.launches0 = ctx.launches;
+  require_cooperative(ctx);  // before the batch is staged or applied: nothing changes
   if (g.host_columns[t.opt.objective].dirty) graph_rescan_columns(ctx, g);
   graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
   u.b = stage_batch(ctx, batch, g.k);
@@ -1702,7 +1743,7 @@ static void finish_tree(Context& ctx, Graph& g, Tree& t, const UpdateCtl& r, int
     st->sssp_ms = sssp_ms;
     st->rounds = r.rounds;
     st->touched = r.affected;
-    for (int i = 0; i < 24; ++i) st->work[i] = r.work[i];
+    for (int i = 0; i < 32; ++i) st->work[i] = r.work[i];
     st->trace_len = r.trace_len;
     for (int i = 0; i < r.trace_len && i < 64; ++i) {
       st->trace_light[i] = r.trace_n[i];
@@ -1877,6 +1918,7 @@ static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied
 // first error is rethrown.
 void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree* const* trees,
                       int count, dyngb200_stats* stats) {
+  require_cooperative(ctx);
   cudaStream_t s = ctx.stream;
   for (int i = 0; i < count; ++i)
     if (g.host_columns[trees[i]->opt.objective].dirty) graph_rescan_columns(ctx, g);
@@ -1885,7 +1927,7 @@ void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree*
   const int k = g.k;
   std::vector<long long> ext(2 * k + 1, 0);
   for (int c = 0; c < k; ++c) ext[2 * c + 1] = INT64_MAX;
-  DevBuf<long long> d_ext;
+  DevBuf<long long>& d_ext = ctx.ws.batch_extrema;  // kept: steady-state calls allocate nothing
   d_ext.reserve(ext.size());
   DYNGB200_CUDA(cudaMemcpyAsync(d_ext.ptr, ext.data(), ext.size() * sizeof(long long),
                                 cudaMemcpyHostToDevice, s));

@@ -83,6 +83,13 @@ class Resources:
     def synchronize(self) -> None:
         check(N.lib().dyngb200_context_synchronize(self._h))
 
+    def set_test_hooks(self, barrier_timeout_ns: int = 0, barrier_extra_arrivals: int = 0,
+                       no_cooperative_launch: bool = False) -> None:
+        """Host-side failure injection for tests (dyngb200_test_hooks); no argument clears."""
+        h = N.TestHooks(int(barrier_timeout_ns), int(barrier_extra_arrivals),
+                        int(bool(no_cooperative_launch)))
+        check(N.lib().dyngb200_context_set_test_hooks(self._h, ctypes.byref(h)))
+
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
             N.lib().dyngb200_context_destroy(self._h)
@@ -367,3 +374,16 @@ class Graph:
             check(N.lib().dyngb200_graph_to_csr(self._res._h, self._h, _ptr64(rp), _ptr32(col),
                                                 _ptr32(w), None, None, None))
         return CSR(rp, col, w.reshape(k, m))
+
+
+def device_allocations() -> int:
+    """Device allocations the library has made in this process so far."""
+    n = ctypes.c_int64()
+    check(N.lib().dyngb200_debug_device_allocations(ctypes.byref(n)))
+    return n.value
+
+
+def fail_device_allocation(nth: int) -> None:
+    """The nth device allocation from now fails with OutOfMemoryError (0 disarms): the
+    allocation-failure sweeps of the reference's tests/support/failing_allocator.hpp."""
+    check(N.lib().dyngb200_debug_fail_device_allocation(int(nth)))

@@ -66,10 +66,25 @@ class Stats:
                   "unpacked", "atomic_attempts", "step0_max_warp_ns", "step0_sum_warp_ns",
                   "step0_warps", "step0_light_ns", "step0_medium_ns", "step0_heavy_ns",
                   "step0_max_light_ns", "step0_max_medium_ns", "step0_max_heavy_ns",
-                  "pj_seeded")
-    # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows);
-    # attempted atomics are a diagnostic, their bytes are in "atomics" (the successful ones):
-    WORK_BYTES = (8, 12, 20, 20, 8, 8, 20, 8, 8, 8, 12, 20) + (0,) * 10 + (12,)
+                  "pj_seeded", "pull_atomics", "pull_appends", "pair_visits", "walk_rows",
+                  "walk_slots")
+    # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows):
+    #   pointer-jumping visit 8 (ancestor + flag), jump 12 (ancestor[a], flag[a], write),
+    #   invalidated vertex 12 (word set to INF, candidate entry), pull candidate / pushed vertex
+    #   20 (list entry, row descriptor, own word), row slot 8 (column + weight), word read 8,
+    #   successful atomicMin 8, frontier append 12 (entry + stamp), unpacked vertex 20 (word, old
+    #   distance and parent), seeded vertex 12 (stamp, parent, ancestor written), change pair 16
+    #   (list entry, flags, key), walk row 12 (entry, descriptor), walk slot 8 (column, parent);
+    #   attempted atomics and the balance probes are diagnostics (0 bytes).
+    WORK_BYTES = ((8, 12, 12, 20, 8, 8, 20, 8, 8, 8, 12, 20) + (0,) * 10 +
+                  (12, 8, 12, 16, 12, 8) + (0,) * 4)
+    # The work counters of each phase of the kernel (indices into WORK_NAMES), and the phases'
+    # device times (indices into PHASES): the per-phase roofline.
+    PHASE_WORK = {"roots_heads": ((25,), (0, 3)),
+                  "invalidation": ((0, 1, 2, 22, 26, 27), (1, 2)),
+                  "pull": ((3, 4, 5, 23, 24), (4,)),
+                  "near_far": ((6, 7, 8, 9, 10), (5,)),
+                  "unpack": ((11,), (6,))}
     PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
     _SCALARS = ("invalidated", "affected", "iterations", "epochs", "pushes", "delta",
                 "max_weight", "grid_blocks", "invalidation", "rounds", "touched",
@@ -146,6 +161,18 @@ class Stats:
     @property
     def algorithmic_bytes(self) -> int:
         return int(sum(a * b for a, b in zip(self.work, self.WORK_BYTES)))
+
+    def phase_bytes_ms(self) -> dict:
+        """Per phase of the kernel: (algorithmic bytes, device ms).  The unpack also counts the
+        12 bytes it writes per affected vertex."""
+        work, ms = self.work, self.phase_ms
+        out = {}
+        for name, (units, phases) in self.PHASE_WORK.items():
+            b = sum(work[i] * self.WORK_BYTES[i] for i in units)
+            if name == "unpack":
+                b += 12 * self.affected
+            out[name] = (int(b), float(sum(ms[i] for i in phases)))
+        return out
 
     def __repr__(self):
         return (f"Stats(invalidated={self.invalidated}, affected={self.affected}, "

@@ -118,8 +118,11 @@ typedef struct dyngb200_stats {
    * atomicMin, [10] frontier appends, [11] vertices the commit compared, [12] atomicMin attempts (successful
    * or not); the first near-far step's balance: [13] the slowest warp's busy ns, [14] the warps'
    * summed busy ns, [15] warps, [16..18] the warps' summed ns in light / medium / heavy rows,
-   * [19..21] the slowest warp's ns in each; [22] vertices seeded for pointer jumping; [23] zero. */
-  int64_t work[24];
+   * [19..21] the slowest warp's ns in each; [22] vertices seeded for pointer jumping; [23]
+   * successful atomicMin of the pull, [24] frontier appends of the pull, [25] change pairs
+   * visited by the roots and insertion-head passes; [26] rows and [27] slots of the subtree
+   * walk (the walk invalidation); [28..31] zero.  [9] and [10] count the near-far loop only. */
+  int64_t work[32];
   /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
    * first split, near-far loop, unpack. */
   float phase_ms[7];
@@ -174,6 +177,30 @@ dyngb200_status dyngb200_context_destroy(dyngb200_context ctx);
 dyngb200_status dyngb200_context_synchronize(dyngb200_context ctx);
 void dyngb200_props_default(dyngb200_props* props);
 void dyngb200_props_mosp_compatible(dyngb200_props* props);
+
+/* ---- test support (the reference's tests/support: failing_allocator.hpp:18-143, the counting
+ * resource of sssp_cuda_test.cpp:622-655, resources_access::force_cooperative_launch used at
+ * sssp_cuda_test.cpp:106-150).  Failures made on the host: nothing here faults a GPU. ------- */
+typedef struct dyngb200_test_hooks {
+  /* A grid barrier of the persistent kernel gives up after this long without progress (0: the
+   * library's 5 s); it then records a timeout, every block leaves the kernel and the call
+   * reports INTERNAL with the tree poisoned. */
+  int64_t barrier_timeout_ns;
+  /* Blocks every grid barrier waits for beyond the launched ones (0: none).  Nothing ever
+   * arrives for them, so every barrier's wait runs out after barrier_timeout_ns. */
+  int32_t barrier_extra_arrivals;
+  /* Nonzero: the context behaves as on a device without cooperative launch (the persistent
+   * kernels are refused with NOT_SUPPORTED before anything changes). */
+  int32_t no_cooperative_launch;
+} dyngb200_test_hooks;
+/* Set (hooks) or clear (NULL) the test hooks of a context. */
+dyngb200_status dyngb200_context_set_test_hooks(dyngb200_context ctx,
+                                                const dyngb200_test_hooks* hooks);
+/* Device allocations the library has made in this process (every DevBuf growth; frees are not
+ * counted): after warm-up, a steady stream of same-size updates adds none. */
+dyngb200_status dyngb200_debug_device_allocations(int64_t* count);
+/* The nth device allocation from now fails as cudaMalloc would (OUT_OF_MEMORY); 0 disarms. */
+dyngb200_status dyngb200_debug_fail_device_allocation(int64_t nth);
 
 /* ---- graph (cpp/include/dyng/graph/graph.hpp:143-195, 332-487) ----------------------------- */
 /* graph<int32,int64,int32>::from_edges: weights insertion-major (num_weights per edge). */

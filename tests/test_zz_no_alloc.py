@@ -44,6 +44,40 @@ def test_static_scratch_matches_regular_compute_twice():
         np.testing.assert_array_equal(p, ref.parents)
 
 
+def test_static_scratch_call_allocates_nothing():
+    # after a warm-up call, a call on a fresh source leaves the library's allocation count, torch's
+    # allocator and the device's free memory exactly where they were
+    import gc
+
+    import torch
+    from dyng_b200.graph import device_allocations
+    e = G.rmat(12, 8, w_max=100, seed=5)
+    rp, col, w = e.csr()
+    g = D.Graph.from_csr(rp, col, w)
+    n = g.num_vertices()
+    D.sssp.compute(g, 0)  # column statistics current
+    dist = torch.empty(n, dtype=torch.int64, device="cuda")
+    par = torch.empty(n, dtype=torch.int32, device="cuda")
+    lib = N.lib()
+
+    def call(source):
+        return lib.dyngb200_sssp_compute_static_scratch(
+            g._h, source, 0, 0, ctypes.cast(ctypes.c_void_p(dist.data_ptr()), N.c_i64p),
+            ctypes.cast(ctypes.c_void_p(par.data_ptr()), N.c_i32p), None)
+
+    assert call(1) == 0, lib.dyngb200_last_error_message().decode()
+    gc.collect()
+    torch.cuda.synchronize()
+    before = (device_allocations(), torch.cuda.memory_allocated(), torch.cuda.mem_get_info()[0])
+    assert call(2) == 0, lib.dyngb200_last_error_message().decode()
+    torch.cuda.synchronize()
+    after = (device_allocations(), torch.cuda.memory_allocated(), torch.cuda.mem_get_info()[0])
+    assert after == before
+    ref = D.sssp.compute(g, 2)
+    np.testing.assert_array_equal(dist.cpu().numpy(), ref.distances)
+    np.testing.assert_array_equal(par.cpu().numpy(), ref.parents)
+
+
 def test_static_scratch_refuses_large_graphs():
     n = (1 << 16) + 5
     src = np.arange(n - 1, dtype=np.int32)
