@@ -58,7 +58,8 @@ class Stats(ctypes.Structure):
                 ("trace_heavy", ctypes.c_int32 * 64), ("trace_us", ctypes.c_float * 64),
                 ("features", ctypes.c_float * 12), ("schedule_classes", ctypes.c_int32 * 3),
                 ("kernel_launches", ctypes.c_int64), ("pj_round_us", ctypes.c_float * 24),
-                ("pj_done_us", ctypes.c_float * 24)]
+                ("pj_done_us", ctypes.c_float * 24), ("apply_step_us", ctypes.c_float * 12),
+                ("host_us", ctypes.c_float * 4)]
 
 
 class Options(ctypes.Structure):
@@ -117,7 +118,7 @@ class TestHooks(ctypes.Structure):
     """dyngb200_test_hooks: host-side failure injection for the tests (no GPU fault)."""
 
     _fields_ = [("barrier_timeout_ns", ctypes.c_int64), ("barrier_extra_arrivals", ctypes.c_int32),
-                ("no_cooperative_launch", ctypes.c_int32)]
+                ("no_cooperative_launch", ctypes.c_int32), ("barrier_kernel", ctypes.c_int32)]
 
 
 SIGNATURES = {

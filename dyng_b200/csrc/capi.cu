@@ -278,9 +278,12 @@ dyngb200_status dyngb200_context_set_test_hooks(dyngb200_context ctx,
                                                 const dyngb200_test_hooks* hooks) {
   return guarded([&] {
     expects(ctx != nullptr, "context_set_test_hooks: null context");
-    const dyngb200_test_hooks h = hooks ? *hooks : dyngb200_test_hooks{0, 0, 0};
+    const dyngb200_test_hooks h = hooks ? *hooks : dyngb200_test_hooks{0, 0, 0, 0};
     expects(h.barrier_timeout_ns >= 0 && h.barrier_extra_arrivals >= 0,
             "context_set_test_hooks: negative limit or arrivals");
+    expects(h.barrier_kernel >= 0 && h.barrier_kernel <= 2,
+            "context_set_test_hooks: barrier_kernel is 0, 1 or 2");
+    ctx->ctx.test_barrier_kernel = h.barrier_kernel;
     ctx->ctx.test_barrier_timeout_ns = h.barrier_timeout_ns;
     ctx->ctx.test_barrier_extra = h.barrier_extra_arrivals;
     ctx->ctx.test_no_cooperative = h.no_cooperative_launch != 0 ? 1 : 0;

@@ -18,6 +18,8 @@
 // its number of existing matches c, its deletions d and insertions t and the first / last
 // insertion, so the pairs are grouped by a hash table instead of rebuilding rows in batch order.
 #include "internal.hpp"
+#include "grid_sync.cuh"
+#include "mlp_common.cuh"
 
 #include <cub/device/device_scan.cuh>
 
@@ -53,15 +55,16 @@ __device__ __forceinline__ void warp_max(long long v, long long* target, long lo
   if ((threadIdx.x & 31) == 0 && v > floor_value) atomicMax(target, v);
 }
 
-// Per-thread column statistics deltas of the first kLocalColumns objectives (the rest go to the
-// global counters directly); flushed once per warp at the end of a kernel.
-constexpr int kLocalColumns = 4;
+// Per-thread column statistics deltas of weight column 0, in registers (the other columns go to
+// the global counters directly); flushed once per warp at the end of a step.  Scalars, not
+// arrays indexed by the column: every thread of the persistent grid carries them, and an array
+// indexed at run time would live in local memory.
 struct ColumnAcc {
-  long long sum[kLocalColumns];
-  long long removed_at_max[kLocalColumns];
-  long long written_max[kLocalColumns];
-  long long written_at_max[kLocalColumns];
-  int bad[kLocalColumns];
+  long long sum;
+  long long removed_at_max;
+  long long written_max;
+  long long written_at_max;
+  int bad;
 };
 
 struct ApplyParams {
@@ -121,6 +124,9 @@ struct ApplyParams {
   long long* col_written_max;
   long long* col_written_at_max;
   UpdateCtl* ctl;
+  // append-order rows: each touched out row's segment and the pairs appended to it, in order
+  int* seg_offsets;
+  int* seg;
   // the learned scheduler's batch features, accumulated by k_validate when `feat` is set: the
   // tree the update repairs (parent array, its vertex count)
   const int32_t* feat_parent;
@@ -150,7 +156,7 @@ __device__ __forceinline__ int find_pair(const ApplyParams& p, u64 k) {
 }
 
 // ---- A: Step 0 checks, vertex growth, largest insertion weight --------------------------------
-__global__ void k_validate(ApplyParams p) {
+__device__ void ph_validate(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const long long total = p.ni + p.nd;
   const long long n = c->n_old;
@@ -159,8 +165,7 @@ __global__ void k_validate(ApplyParams p) {
   int dropped = 0;
   // scheduler features: tree-edge deletions, source out-degree sum / max / count
   long long f_tree = 0, f_deg = 0, f_max = 0, f_srcs = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = tid; i < total; i += threads) {
     if (p.feat) {
       const bool del = i >= p.ni;
       const long long j = del ? i - p.ni : i;
@@ -232,27 +237,26 @@ __global__ void k_validate(ApplyParams p) {
 }
 
 // ---- the per-batch reset: an empty pair table and zero column deltas ---------------------------
-__global__ void k_clear_tables(u64* key, int* d, int* t, int* first, int* last, long long cap,
-                               long long* sum_delta, long long* removed_at_max,
-                               long long* written_max, long long* written_at_max, int k) {
-  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < cap;
-       i += static_cast<long long>(gridDim.x) * blockDim.x) {
-    key[i] = ~0ULL;
-    d[i] = 0;
-    t[i] = 0;
-    first[i] = 0x7f7f7f7f;
-    last[i] = -1;
+__device__ void ph_clear(const ApplyParams& p, long long tid, long long threads) {
+  const long long cap = static_cast<long long>(p.mask) + 1;
+  const int k = p.k > 0 ? p.k : 1;
+  for (long long i = tid; i < cap; i += threads) {
+    p.key[i] = ~0ULL;
+    p.d[i] = 0;
+    p.t[i] = 0;
+    p.first[i] = 0x7f7f7f7f;
+    p.last[i] = -1;
     if (i < k) {
-      sum_delta[i] = 0;
-      removed_at_max[i] = 0;
-      written_max[i] = 0;
-      written_at_max[i] = 0;
+      p.col_sum_delta[i] = 0;
+      p.col_removed_at_max[i] = 0;
+      p.col_written_max[i] = 0;
+      p.col_written_at_max[i] = 0;
     }
   }
 }
 
 // ---- B: the plan (one thread): capacity, packing bound, near-far width ------------------------
-__global__ void k_plan(ApplyParams p) {
+__device__ void ph_plan(const ApplyParams& p) {
   UpdateCtl* c = p.ctl;
   const GraphCounters* gc = p.g.counters;
   c->n_after = max(c->n_after, c->n_old);
@@ -355,17 +359,14 @@ __device__ void add_op(PairStage& st, const ApplyParams& p, int32_t u, int32_t v
 }
 
 // ---- C: group the effective operations by (u, v) pair ------------------------------------------
-__global__ void k_pairs(ApplyParams p) {
-  __shared__ PairStage st;
+__device__ void ph_pairs(const ApplyParams& p, PairStage& st, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   if (threadIdx.x < 3) st.cnt[threadIdx.x] = 0;
   __syncthreads();
   const long long total = p.ni + p.nd;
   const long long n_after = c->n_after;
   long long missing = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = tid; i < total; i += threads) {
     if (i < p.ni) {
       const int32_t u = p.ins_src[i], v = p.ins_dst[i];
       if (u == v && p.props.on_self_loop != 0) continue;
@@ -408,11 +409,10 @@ __global__ void k_pairs(ApplyParams p) {
 
 // ---- D: match existing slots (simple graphs: at most one slot per pair, found in the edge
 // index; positions are absolute arena slots) ------------------------------------------------------
-__global__ void k_match(ApplyParams p) {
+__device__ void ph_match(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     const long long e = index_find(p.g, p.key[slot]);
     if (e >= 0) {
@@ -427,11 +427,10 @@ __global__ void k_match(ApplyParams p) {
 
 // Multi-edge graphs: one thread per pair walks its rows in order (the first alive matches).
 // Records c, the first match and the match the insertions address (see resolve).
-__global__ void k_scan_multi(ApplyParams p) {
+__device__ void ph_scan_multi(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
@@ -467,14 +466,13 @@ __global__ void k_scan_multi(ApplyParams p) {
 
 
 // ---- E: resolve every pair (counts, policies, classification, per-row slot demand) -------------
-__global__ void k_resolve(ApplyParams p) {
+__device__ void ph_resolve(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
   const int policy = p.props.on_existing_insert;
   long long acc[5] = {0, 0, 0, 0, 0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
@@ -588,15 +586,13 @@ __device__ __forceinline__ u64 warp_reserve(u64 amount, u64* counter) {
 // ---- F: per touched row: stay in place or move to the top of the arena -------------------------
 // A row that overflows its slack (or is mostly tombstones) gets a new place at the arena top.  The warps iterate together so that the arena
 // space of a warp's relocated rows is reserved with one atomic per side.
-__global__ void k_alloc(ApplyParams p) {
+__device__ void ph_alloc(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
   const int total = rows_out + rows_in;
   const double headroom = p.props.headroom;
   const int lane = threadIdx.x & 31;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < total; i0 += stride) {
+  for (long long i0 = tid & ~31LL; i0 < total; i0 += threads) {
     const int i = i0 + lane;
     const bool active = i < total;
     const int side = i < rows_out ? 0 : 1;
@@ -648,20 +644,15 @@ __global__ void k_alloc(ApplyParams p) {
 }
 
 __device__ __forceinline__ void acc_init(ColumnAcc& a) {
-  for (int j = 0; j < kLocalColumns; ++j) {
-    a.sum[j] = 0;
-    a.removed_at_max[j] = 0;
-    a.written_max[j] = 0;
-    a.written_at_max[j] = 0;
-    a.bad[j] = 0;
-  }
+  a.sum = a.removed_at_max = a.written_max = a.written_at_max = 0;
+  a.bad = 0;
 }
 __device__ __forceinline__ void column_out(const ApplyParams& p, ColumnAcc& a, int j, long long w,
                                            long long old_max) {
-  if (j < kLocalColumns) {
-    a.sum[j] -= w;
-    a.removed_at_max[j] += w == old_max;
-    a.bad[j] -= w < 1;
+  if (j == 0) {
+    a.sum -= w;
+    a.removed_at_max += w == old_max;
+    a.bad -= w < 1;
     return;
   }
   atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_sum_delta[j]),
@@ -670,10 +661,10 @@ __device__ __forceinline__ void column_out(const ApplyParams& p, ColumnAcc& a, i
   if (w < 1) atomicSub(&p.g.columns[j].bad, 1);
 }
 __device__ __forceinline__ void column_in(const ApplyParams& p, ColumnAcc& a, int j, long long w) {
-  if (j < kLocalColumns) {
-    a.sum[j] += w;
-    a.written_max[j] = max(a.written_max[j], w);
-    a.bad[j] += w < 1;
+  if (j == 0) {
+    a.sum += w;
+    a.written_max = max(a.written_max, w);
+    a.bad += w < 1;
     return;
   }
   atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_sum_delta[j]),
@@ -683,28 +674,24 @@ __device__ __forceinline__ void column_in(const ApplyParams& p, ColumnAcc& a, in
 }
 // Flush a warp's accumulators (all lanes must call).
 __device__ __forceinline__ void acc_flush(const ApplyParams& p, ColumnAcc& a) {
-  const int k = p.k < kLocalColumns ? p.k : kLocalColumns;
-  for (int j = 0; j < k; ++j) {
-    warp_add(a.sum[j], &p.col_sum_delta[j]);
-    warp_add(a.removed_at_max[j], &p.col_removed_at_max[j]);
-    warp_max(a.written_max[j], &p.col_written_max[j], 0);
-    warp_add(a.written_at_max[j], &p.col_written_at_max[j]);
-    long long bad = a.bad[j];
-    for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
-    if ((threadIdx.x & 31) == 0 && bad != 0) atomicAdd(&p.g.columns[j].bad, static_cast<int>(bad));
-  }
+  warp_add(a.sum, &p.col_sum_delta[0]);
+  warp_add(a.removed_at_max, &p.col_removed_at_max[0]);
+  warp_max(a.written_max, &p.col_written_max[0], 0);
+  warp_add(a.written_at_max, &p.col_written_at_max[0]);
+  long long bad = a.bad;
+  for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
+  if ((threadIdx.x & 31) == 0 && bad != 0) atomicAdd(&p.g.columns[0].bad, static_cast<int>(bad));
 }
 
 // ---- G: tombstones and upserts in place -------------------------------------------------------
-__global__ void k_mutate(ApplyParams p) {
+__device__ void ph_mutate(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
   ColumnAcc acc;
   acc_init(acc);
   long long idx_deleted = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
@@ -783,14 +770,13 @@ __global__ void k_mutate(ApplyParams p) {
 }
 
 // ---- H: move relocated rows (live slots, in order) ---------------------------------------------
-__global__ void k_move(ApplyParams p) {
+__device__ void ph_move(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const long long warp = tid >> 5;
+  const long long warps = threads >> 5;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
-  for (int i = warp; i < rows_out + rows_in; i += warps) {
+  for (long long i = warp; i < rows_out + rows_in; i += warps) {
     const int side = i < rows_out ? 0 : 1;
     const int s = side == 0 ? i : i - rows_out;
     if (!(side == 0 ? p.reloc_out : p.reloc_in)[s]) continue;
@@ -823,14 +809,13 @@ __global__ void k_move(ApplyParams p) {
 }
 
 // ---- I: append the new slots ---------------------------------------------------------------------
-__global__ void k_append(ApplyParams p) {
+__device__ void ph_append(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
   ColumnAcc acc;
   acc_init(acc);
   long long idx_new = 0, idx_reused = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     const int flags = p.flags[slot];
     if (!(flags & kPairAppend)) continue;
@@ -877,13 +862,11 @@ __global__ void k_append(ApplyParams p) {
 }
 
 // ---- J: new row descriptors ----------------------------------------------------------------------
-__global__ void k_rows_final(ApplyParams p) {
+__device__ void ph_rows_final(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
   long long garbage_out = 0, garbage_in = 0, dead_delta_out = 0, dead_delta_in = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows_out + rows_in;
-       i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < rows_out + rows_in; i += threads) {
     const int side = i < rows_out ? 0 : 1;
     const int s = side == 0 ? i : i - rows_out;
     const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
@@ -920,13 +903,12 @@ __global__ void k_rows_final(ApplyParams p) {
 }
 
 // Count the weights written by the batch that equal the new maximum (for count_at_max).
-__global__ void k_count_written_max(ApplyParams p) {
+__device__ void ph_count_written_max(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
   ColumnAcc acc;
   acc_init(acc);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     const int flags = p.flags[slot];
     if (!(flags & (kPairAppend | kPairUpsert))) continue;
@@ -935,19 +917,17 @@ __global__ void k_count_written_max(ApplyParams p) {
       const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
       const long long target = max(p.col_written_max[j], p.g.columns[j].max_w);
       if (nw == target) {
-        if (j < kLocalColumns) ++acc.written_at_max[j];
+        if (j == 0) ++acc.written_at_max;
         else atomicAdd(reinterpret_cast<unsigned long long*>(&p.col_written_at_max[j]), 1ULL);
       }
     }
   }
-  const int k = p.k < kLocalColumns ? p.k : kLocalColumns;
-  for (int j = 0; j < k; ++j) warp_add(acc.written_at_max[j], &p.col_written_at_max[j]);
+  warp_add(acc.written_at_max, &p.col_written_at_max[0]);
 }
 
 // One thread: graph counters and column statistics after the batch.
-__global__ void k_finalize(ApplyParams p) {
+__device__ void ph_finalize(const ApplyParams& p) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   GraphCounters* gc = p.g.counters;
   gc->n = c->n_after;
   gc->m += c->summary[0] - c->summary[1];
@@ -955,6 +935,7 @@ __global__ void k_finalize(ApplyParams p) {
   gc->in_top = c->top_in;
   c->summary[6] = c->n_after - c->n_old;
   c->summary[7] = c->n_after;
+  c->applied = 1;
   for (int j = 0; j < p.k; ++j) {
     ColumnStats cs = p.g.columns[j];
     cs.sum_w += p.col_sum_delta[j];
@@ -1018,36 +999,25 @@ __global__ void k_rescan_count(GraphView g, long long n, long long* out) {
 // Append order (row_order::append): the new slots of a row follow the batch order of their first
 // insertion, as the reference appends them (apply_host.cpp:214-246).  The atomic ranks of
 // k_resolve are replaced by the rank among the row's appended pairs ordered by first insertion.
-__global__ void k_row_offsets(ApplyParams p, int* offsets) {
-  // one block: exclusive scan of apps_out over the touched out rows
-  __shared__ int s_carry;
-  __shared__ int s_part[1024];
-  const int rows = p.ctl->rows_out;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
-  for (int base = 0; base < rows; base += 1024) {
-    const int i = base + threadIdx.x;
-    const int v = i < rows ? p.apps_out[i] : 0;
-    s_part[threadIdx.x] = v;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-      const int add = threadIdx.x >= o ? s_part[threadIdx.x - o] : 0;
-      __syncthreads();
-      s_part[threadIdx.x] += add;
-      __syncthreads();
-    }
-    if (i < rows) offsets[i] = s_carry + s_part[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) s_carry += s_part[1023];
-    __syncthreads();
+// Append-order rows: a segment of the segment array per touched out row, sized by its appended
+// pairs.  The segments only have to be disjoint (each row sorts its own), so a warp reserves its
+// rows' segments with one atomic instead of a scan in row order.
+__device__ void ph_row_offsets(const ApplyParams& p, int* offsets, long long tid, long long threads) {
+  UpdateCtl* c = p.ctl;
+  const int rows = c->rows_out;
+  const int lane = threadIdx.x & 31;
+  for (long long i0 = tid & ~31LL; i0 < rows; i0 += threads) {
+    const long long i = i0 + lane;
+    const u64 a = i < rows ? static_cast<u64>(p.apps_out[i]) : 0;
+    const u64 at = warp_reserve(a, &c->seg_top);
+    if (i < rows) offsets[i] = static_cast<int>(at);
   }
 }
 
-__global__ void k_fill_segments(ApplyParams p, const int* offsets, int* seg) {
+__device__ void ph_fill_segments(const ApplyParams& p, const int* offsets, int* seg, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int pairs = c->pairs;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += gridDim.x * blockDim.x) {
+  for (long long i = tid; i < pairs; i += threads) {
     const int slot = p.list[i];
     if (!(p.flags[slot] & kPairAppend)) continue;
     const int32_t u = static_cast<int32_t>(p.key[slot] >> 32);
@@ -1055,11 +1025,10 @@ __global__ void k_fill_segments(ApplyParams p, const int* offsets, int* seg) {
   }
 }
 
-__global__ void k_sort_segments(ApplyParams p, const int* offsets, int* seg) {
+__device__ void ph_sort_segments(const ApplyParams& p, const int* offsets, int* seg, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
-  if (c->error) return;
   const int rows = c->rows_out;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < rows; s += gridDim.x * blockDim.x) {
+  for (long long s = tid; s < rows; s += threads) {
     const int a = p.apps_out[s];
     if (a <= 0) continue;
     int* base = seg + offsets[s];
@@ -1198,6 +1167,116 @@ __global__ void k_compact_copy(RowDesc* desc, int32_t* cap_out, int32_t* dead,
       cap_out[v] = static_cast<int32_t>(start[v + 1] - to);
       dead[v] = 0;
     }
+  }
+}
+
+// ---- the applier as one cooperative persistent kernel -------------------------------------------
+// Steps A-J of the batch applier (apply_host.cpp:57-395 restated per pair, above) in one launch:
+// each step is a grid-stride pass of every block, and a grid barrier separates the steps that
+// depend on one another (grid_sync.cuh).  Every block leaves a barrier with the same snapshot of
+// the error word, so an error (an invalid batch, a capacity shortfall) stops all blocks at the same
+// point, before anything of the graph changes: the steps that mutate the graph (G-J) run only after
+// the allocation step found room for the whole batch.  Block 0 computes the plan and, for the
+// learned scheduler, the batch features and the schedule while the other blocks group the pairs.
+//
+// The block footprint (256 threads, at most 80 registers by the launch bounds, the shared memory
+// below) stays within the sssp kernel's, so the grids the serving loop's lanes size for the sssp
+// kernel's block slots are co-resident for this kernel too.
+struct ApplyLaunch {
+  InferArgs infer;
+  int infer_on;   // block 0 computes the batch features (and, with weights, the schedule)
+  unsigned long long barrier_limit_ns;  // 0: kBarrierTimeoutNs
+  int barrier_extra;                    // test hook: arrivals that never come (0 outside tests)
+};
+
+union ApplySmem {
+  PairStage pairs;
+  InferShared infer;
+};
+
+__global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch L) {
+  __shared__ ApplySmem sm;
+  UpdateCtl* c = p.ctl;
+  const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long threads = static_cast<long long>(gridDim.x) * blockDim.x;
+  const unsigned arrivals = gridDim.x + static_cast<unsigned>(L.barrier_extra > 0 ? L.barrier_extra : 0);
+  const unsigned long long limit = L.barrier_limit_ns > 0 ? L.barrier_limit_ns : kBarrierTimeoutNs;
+  unsigned gen = gs_ld_volatile(&c->bar_gen);
+  unsigned err = 0;
+  // step timestamps (block 0's view): apply_ns[0] the start, then the end of each step
+  int stamp = 0;
+  auto mark = [&]() {
+    ++stamp;
+    if (tid == 0 && stamp < 12) c->apply_ns[stamp] = global_ns();
+  };
+  if (tid == 0) c->apply_ns[0] = global_ns();
+  // A: Step 0 checks (and the scheduler's feature sums); this batch's pair table cleared
+  ph_clear(p, tid, threads);
+  ph_validate(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err)) return;
+  mark();
+  // B: the plan, then the features and schedule, by block 0
+  if (blockIdx.x == 0) {
+    if (threadIdx.x == 0) ph_plan(p);
+    if (L.infer_on) {
+      __syncthreads();
+      infer_schedule_block(L.infer, c, p.g.counters, p.ni, p.nd, sm.infer);
+    }
+    __syncthreads();  // the pair stage below reuses the inference's shared memory
+  }
+  // an invalid batch or a vertex capacity shortfall ends the call here (nothing has changed; the
+  // host reads the plan for the retry): every block decides on the same values
+  if (err != 0 || max(c->n_after, c->n_old) > p.g.n_cap) return;
+  // C: the operations grouped by (u, v) pair; while block 0 runs the inference the other blocks
+  // share the pairs among themselves (the inference is then off the critical path)
+  const long long skip = L.infer_on ? blockDim.x : 0;
+  const long long ptid = (L.infer_on && blockIdx.x == 0) ? (1LL << 62) : tid - skip;
+  ph_pairs(p, sm.pairs, ptid, threads - skip);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  // D: the live slot of each pair
+  if (p.g.allow_multi) ph_scan_multi(p, tid, threads);
+  else ph_match(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  // E: the outcome of each pair, its weight-increase class, the rows' demand
+  ph_resolve(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  if (!p.props.sorted) {
+    // append order: the order of the pairs appended to each row
+    ph_row_offsets(p, p.seg_offsets, tid, threads);
+    if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+    ph_fill_segments(p, p.seg_offsets, p.seg, tid, threads);
+    if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+    ph_sort_segments(p, p.seg_offsets, p.seg, tid, threads);
+    if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  }
+  // F: room for every touched row (the last point where an error leaves the graph untouched)
+  ph_alloc(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  // G: tombstones and upserts in place
+  if (threadIdx.x == 0) c->committing = 1;  // from here on a stop leaves the graph incomplete
+  ph_mutate(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  // H, I: relocated rows moved and new slots appended (disjoint slots)
+  ph_move(p, tid, threads);
+  ph_append(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  // J: row descriptors, the written maxima, then counters and column statistics
+  ph_rows_final(p, tid, threads);
+  ph_count_written_max(p, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  mark();
+  if (tid == 0) {
+    ph_finalize(p);
+    c->apply_ns[11] = global_ns();
   }
 }
 
@@ -1675,6 +1754,7 @@ void side_to_csr(long long n, int k, const std::vector<RowDesc>& desc,
 
 void graph_export(Context& ctx, Graph& g, int64_t* row_ptr, int32_t* col, int32_t* w,
                   int64_t* in_row_ptr, int32_t* in_col, int32_t* in_w) {
+  require_intact(g);
   graph_refresh_host(ctx, g);
   const long long n = g.n;
   for (int side = 0; side < 2; ++side) {
@@ -1797,7 +1877,6 @@ void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in
 // Grow the vertex capacity and/or the arenas.  Heavily fragmented arenas are compacted instead.
 void graph_grow(Context& ctx, Graph& g, long long need_n, long long need_out, long long need_in) {
   graph_refresh_host(ctx, g);
-  const long long n = g.n;
   const long long m = g.m;
   const long long garbage = static_cast<long long>(
       std::max(g.host_counters.out_garbage, g.host_counters.in_garbage));
@@ -1927,24 +2006,40 @@ StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k) {
   return b;
 }
 
-// Steps A-E (nothing in the graph changes): checks, plan, grouping, matching, resolution.
-void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
-                   long long delta_opt, const dyngb200_schedule* sched, Tree* tree,
-                   const Scheduler* learned) {
+// Blocks of the applier kernel per SM (asked once per context).
+static int apply_blocks_per_sm(Context& ctx) {
+  if (ctx.apply_blocks_per_sm == 0) {
+    int per_sm = 0;
+    DYNGB200_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply, kBlock, 0));
+    expects(per_sm >= 1, "graph::apply: the applier kernel does not fit on an SM",
+            DYNGB200_NOT_SUPPORTED);
+    ctx.apply_blocks_per_sm = per_sm;
+  }
+  return ctx.apply_blocks_per_sm;
+}
+
+// The batch applier (Steps A-J), queued on ctx.stream as one cooperative launch; the caller reads
+// the control block once at the end.  `objective` >= 0 also records the sssp change
+// classification for that weight column and the plan (packing, default width); tree arrays are
+// not touched.  With `tree` and a scheduler (or a schedule asking for features), block 0 of the
+// launch computes the batch features and the schedule into the control block.
+void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective, long long delta_opt,
+                  const dyngb200_schedule* sched, Tree* tree, const Scheduler* learned) {
+  require_cooperative(ctx);
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   const long long dir = g.props.directed ? 1 : 2;
   const long long ops = (b.ni + b.nd) * dir;
+  // every allocation first: a failed one leaves the graph as it was
   ws.reserve_vertices(g.n_cap, s);
   ws.reserve_batch(ops, g.k, s);
+  if (!g.props.sorted) {
+    const size_t cap = static_cast<size_t>(ws.pairs_sized);
+    ws.row_seg_offsets.reserve(cap);
+    ws.row_seg.reserve(cap);
+  }
+  const int blocks = std::min(apply_blocks_per_sm(ctx) * ctx.sm_count, update_grid_blocks(ctx));
   const int touch_gen = ws.next_touch_generation(s);
-  const size_t cap = static_cast<size_t>(ws.pairs_sized);
-  // the pair table of this batch (pairs_active entries) and the column deltas, in one launch
-  k_clear_tables<<<grid_for(ws.pairs_active, kBlock, ctx.sm_count), kBlock, 0, s>>>(
-      ws.pair_key.ptr, ws.pair_d.ptr, ws.pair_t.ptr, ws.pair_first.ptr, ws.pair_last.ptr,
-      ws.pairs_active, ws.col_sum_delta.ptr, ws.col_removed_at_max.ptr, ws.col_written_max.ptr,
-      ws.col_written_at_max.ptr, g.k > 0 ? g.k : 1);
-  ++ctx.launches;
   UpdateCtl init{};
   init.err_index = INT64_MAX;
   init.n_old = g.n;
@@ -1957,6 +2052,9 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
                                 cudaMemcpyHostToDevice, s));
   ApplyParams p = make_params(ctx, g, b, objective, delta_opt);
   p.touch_gen = touch_gen;
+  p.seg_offsets = ws.row_seg_offsets.ptr;
+  p.seg = ws.row_seg.ptr;
+  ApplyLaunch L{};
   // the learned scheduler's batch features come from the validation pass (the batch, the old
   // rows and the tree before anything changes); its inference follows the plan's default width
   const bool features = tree && (learned || (sched && sched->record_features));
@@ -1964,48 +2062,17 @@ void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
     p.feat = 1;
     p.feat_parent = tree->parent.ptr;
     p.feat_tree_n = tree->n;
+    L.infer_on = 1;
+    learned_infer_args(ctx, *tree, learned, &L.infer);
   }
-  const int grid_ops = grid_for(b.ni + b.nd, kBlock, ctx.sm_count);
-  k_validate<<<grid_ops, kBlock, 0, s>>>(p);
-  k_plan<<<1, 1, 0, s>>>(p);
-  ctx.launches += g.props.sorted ? 5 : 8;  // validate, plan, pairs, match, resolve (+ 3 ordering)
-  if (features) launch_learned_schedule(ctx, g, *tree, b, learned);
-  k_pairs<<<grid_ops, kBlock, 0, s>>>(p);
-  if (g.props.allow_multi) {
-    k_scan_multi<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
-  } else {
-    k_match<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
-  }
-  k_resolve<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p);
-  if (!g.props.sorted) {
-    ws.row_seg_offsets.reserve(cap);
-    ws.row_seg.reserve(cap);
-    k_row_offsets<<<1, 1024, 0, s>>>(p, ws.row_seg_offsets.ptr);
-    k_fill_segments<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, ws.row_seg_offsets.ptr,
-                                                                           ws.row_seg.ptr);
-    k_sort_segments<<<grid_for(ops, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, ws.row_seg_offsets.ptr,
-                                                                           ws.row_seg.ptr);
-  }
-  DYNGB200_CUDA(cudaGetLastError());
-}
-
-// Steps F-J: allocation (the last point where a capacity error leaves the graph untouched), then
-// the mutation of the slack rows and the counters.
-void apply_commit(Context& ctx, Graph& g, const StagedBatch& b) {
-  cudaStream_t s = ctx.stream;
-  const long long dir = g.props.directed ? 1 : 2;
-  const long long ops = (b.ni + b.nd) * dir;
-  ApplyParams p = make_params(ctx, g, b, -1, 0);
-  const int grid = grid_for(2 * ops, kBlock, ctx.sm_count);
-  ctx.launches += 7;
-  k_alloc<<<grid, kBlock, 0, s>>>(p);
-  k_mutate<<<grid, kBlock, 0, s>>>(p);
-  k_move<<<ctx.sm_count * 4, kBlock, 0, s>>>(p);
-  k_append<<<grid, kBlock, 0, s>>>(p);
-  k_rows_final<<<grid, kBlock, 0, s>>>(p);
-  k_count_written_max<<<grid, kBlock, 0, s>>>(p);
-  k_finalize<<<1, 1, 0, s>>>(p);
-  DYNGB200_CUDA(cudaGetLastError());
+  L.barrier_limit_ns = ctx.test_barrier_timeout_ns > 0
+                           ? static_cast<unsigned long long>(ctx.test_barrier_timeout_ns)
+                           : 0;
+  L.barrier_extra = ctx.test_barrier_kernel == 2 ? 0 : ctx.test_barrier_extra;
+  void* args[] = {&p, &L};
+  ++ctx.launches;
+  DYNGB200_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_apply), dim3(blocks),
+                                            dim3(kBlock), args, 0, s));
 }
 
 // graph::apply on its own (no tree): the applier, one read-back, growth and retry on capacity.
@@ -2013,6 +2080,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
                  dyngb200_apply_summary* summary, unsigned char* weight_increased) {
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
+  require_intact(g);
   graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
   const StagedBatch b = stage_batch(ctx, batch, g.k);
   UpdateCtl r{};
@@ -2020,8 +2088,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
   // allocated before the applier is queued: a failed allocation leaves the graph as it was
   if (weight_increased && b.ni > 0) flags.reserve(static_cast<size_t>(b.ni) * g.k);
   for (int attempt = 0;; ++attempt) {
-    apply_prepare(ctx, g, b, -1, 0, nullptr);
-    apply_commit(ctx, g, b);
+    apply_launch(ctx, g, b, -1, 0, nullptr);
     if (weight_increased && b.ni > 0) {
       ApplyParams p = make_params(ctx, g, b, -1, 0);
       k_insert_flags<<<grid_for(b.ni, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, flags.ptr);
@@ -2045,6 +2112,12 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
       continue;
     }
     break;
+  }
+  if (r.committing && !r.applied) {
+    g.broken = true;
+    throw Error(DYNGB200_INTERNAL,
+                "graph::apply: the batch applier stopped part-way through applying the batch; "
+                "the graph is incomplete");
   }
   if (r.error & kErrCapacity) throw Error(DYNGB200_CAPACITY, "graph::apply: capacity exceeded");
   if (r.error & kErrInvalidBatch) {

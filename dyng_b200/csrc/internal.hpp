@@ -127,6 +127,9 @@ struct UpdateCtl {
   int relocated_out, relocated_in;
   int pad1;
   u64 top_out, top_in;  // tentative arena tops
+  u64 seg_top;          // append-order rows: segments reserved so far
+  int committing;       // the applier passed its allocation step: the graph is being changed
+  int applied;          // the applier finished: the graph holds the batch
   long long summary[8];  // apply_summary fields in dyngb200_apply_summary order
   // sssp
   int packing_bits;
@@ -181,12 +184,14 @@ struct UpdateCtl {
   int trace_h[64];
   unsigned trace_t[64];
   int trace_len;
+  unsigned long long apply_ns[12];  // the applier kernel: start, then the end of each step
   unsigned pj_t[24];  // start of each pointer-jumping round (ns since the kernel began)
   unsigned pj_done[24];  // the last block's arrival at the barrier ending each round
   // grid barrier: one arrival counter and the generation word the blocks wait on, each on its own
   // 128-byte line (the polling of the generation does not slow the arrivals)
   alignas(128) unsigned bar_count;
   alignas(128) unsigned bar_gen;
+  unsigned bar_err;  // the error word as the last arrival saw it (read after bar_gen moves)
   // progress of a block that works alone (the small-frontier loop of block 0): the blocks waiting
   // at a grid barrier meanwhile restart their time limit whenever it moves
   alignas(128) unsigned heartbeat;
@@ -240,6 +245,7 @@ struct Context {
   int coop_supported = 0;
   long long launches = 0;  // kernels this context has launched (reported per call in the stats)
   int update_blocks_per_sm = 0;
+  int apply_blocks_per_sm = 0;
   int compute_blocks_per_sm = 0;
   // cap on the update's persistent grid (0: occupancy x SMs); the serving loop's lanes split the
   // SMs' block slots between two concurrent persistent kernels with it
@@ -253,15 +259,22 @@ struct Context {
   // never arrive: the barrier's wait runs out), and a device taken as one without cooperative launch
   long long test_barrier_timeout_ns = 0;
   int test_barrier_extra = 0;
+  int test_barrier_kernel = 0;  // the phantom arrivals: 0 every kernel, 1 the applier, 2 sssp
   int test_no_cooperative = 0;
 };
 
 // The persistent kernels need cooperative launch; checked before anything of a call changes.
 void require_cooperative(const Context& ctx);
+// A graph an update left incomplete refuses further use.
+struct Graph;
+void require_intact(const Graph& g);
 
 struct Graph {
   uint64_t id = 0;
   uint64_t version = 0;
+  // an update stopped part-way through changing the graph (a grid barrier of the applier timed
+  // out after its first change): the graph refuses further use
+  bool broken = false;
   dyngb200_props props{};
   int k = 1;
   long long n = 0, m = 0;  // host mirrors after the last completed call
@@ -378,9 +391,10 @@ void scheduler_gradients(Context& ctx, Scheduler& s, const float* x, const int32
                          float* grads, double* loss);
 void scheduler_train(Context& ctx, Scheduler& s, const float* x, const int32_t* y, long long n,
                      int epochs, int batch, float lr, uint64_t seed, double* final_loss);
-// features of the batch (and, with a scheduler, its schedule) into the control block
-void launch_learned_schedule(Context& ctx, Graph& g, Tree& t, const StagedBatch& b,
-                             const Scheduler* sch);
+// What the batch applier's first block needs to compute the batch features (and, with a
+// scheduler, its schedule) into the control block (mlp_common.cuh)
+struct InferArgs;
+void learned_infer_args(Context& ctx, Tree& t, const Scheduler* sch, InferArgs* out);
 
 // graph.cu
 void graph_build(Context& ctx, Graph& g, long long n, const int64_t* row_ptr, const int32_t* col,
@@ -407,11 +421,10 @@ struct StagedBatch {
   const int32_t* del_dst;
   long long nd;
 };
-void apply_prepare(Context& ctx, Graph& g, const StagedBatch& b, int objective,
-                   long long delta_opt, const dyngb200_schedule* sched, Tree* tree = nullptr,
-                   const Scheduler* learned = nullptr);
+void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective,
+                  long long delta_opt, const dyngb200_schedule* sched, Tree* tree = nullptr,
+                  const Scheduler* learned = nullptr);
 void schedule_into(const dyngb200_schedule& sched, UpdateCtl& init);
-void apply_commit(Context& ctx, Graph& g, const StagedBatch& b);
 StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k);
 
 // sssp.cu
@@ -432,6 +445,7 @@ struct PendingUpdate {
   int blocks = 0;
   long long launches0 = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+  double host_us[4] = {};  // see dyngb200_stats::host_us
   PendingUpdate() = default;
   PendingUpdate(const PendingUpdate&) = delete;
   PendingUpdate& operator=(const PendingUpdate&) = delete;

@@ -13,8 +13,10 @@
 //   - the grid barrier is this file's own, with a time limit after which it records kErrTimeout
 //     and every block leaves the kernel (no unbounded spin).
 #include "internal.hpp"
+#include "grid_sync.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -25,7 +27,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHeavyChunk = 256;
-constexpr unsigned long long kBarrierTimeoutNs = 5ULL * 1000 * 1000 * 1000;
 
 struct SsspParams {
   GraphView g;
@@ -90,9 +91,7 @@ constexpr int kPairDelete = 1, kPairIncreased = 2, kPairHead = 4, kPairAppend = 
 
 enum Mode { kPush = 0, kPull = 1, kWalk = 2 };
 
-__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) {
-  return *reinterpret_cast<const volatile unsigned*>(p);
-}
+__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return gs_ld_volatile(p); }
 
 // Shared-memory staging of list appends.  A lane appends into its block's stage with a
 // warp-aggregated shared-memory atomic (ballot + popc); at the end of the phase the block copies
@@ -159,75 +158,20 @@ __device__ __forceinline__ void stage_flush() {
   if (threadIdx.x < kStages) g_stage.cnt[threadIdx.x] = 0;
 }
 
-// Grid-wide barrier over co-resident blocks (cooperative launch).  Flushes the block's stages
-// first.  Returns false once any block has recorded a timeout; the caller then leaves the kernel.
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
-  unsigned old;
-  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
-               : "memory");
-  return old;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// Grid-wide barrier over co-resident blocks (cooperative launch, grid_sync.cuh).  Flushes the
+// block's stages first.  Returns false once any block has recorded a timeout; the caller then
+// leaves the kernel.  *err (optional) receives the error word as every block sees it.
+__device__ __forceinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen, unsigned* err = nullptr) {
+  stage_flush();
+  unsigned e = 0;
+  const bool ok = grid_sync(c, gen, static_cast<unsigned>(g_bar_arrivals), g_bar_limit, &e);
+  if (err) *err = e;
+  return ok;
 }
 
-// The grid-wide barrier of the persistent kernel.  Thread 0 of every block arrives on one counter
-// with an acquire-release add (the block's writes, ordered before it by __syncthreads, are
-// released to the block that completes the barrier); the last arrival resets the counter and
-// releases the next generation, which the others poll with acquire loads.  Measured on B200 with
-// 444 blocks: 2.2 us per barrier, against 3.7 us for two-level arrival counters with full fences
-// sharing a line with the polled word.  The wait is bounded: once the barrier has seen no
-// progress for its limit (kBarrierTimeoutNs; progress = a move of the heartbeat word, which block
-// 0 bumps every step while it runs the small-frontier loop alone and the others wait here), or
-// once another block has timed out, it sets kErrTimeout and returns false.
-__device__ __noinline__ bool grid_barrier(UpdateCtl* c, unsigned& gen) {
-  stage_flush();
-  __syncthreads();
-  __shared__ int s_ok;
-  if (threadIdx.x == 0) {
-    const unsigned target = gen + 1;
-    const unsigned arrivals = static_cast<unsigned>(g_bar_arrivals);
-    int ok = 1;
-    if (atom_add_acq_rel(&c->bar_count, 1u) + 1u == arrivals) {
-      st_relaxed(&c->bar_count, 0u);  // before the release: no block arrives again before it
-      st_release(&c->bar_gen, target);
-    } else {
-      unsigned long long start = 0;
-      unsigned beat = 0;
-      unsigned spins = 0;
-      while (ld_acquire(&c->bar_gen) != target) {
-        if ((++spins & 1023u) == 0) {
-          if (ld_volatile(&c->error) & kErrTimeout) {
-            ok = 0;
-            break;
-          }
-          const unsigned long long now = global_ns();
-          const unsigned hb = ld_volatile(&c->heartbeat);
-          if (start == 0 || hb != beat) {
-            start = now;
-            beat = hb;
-          } else if (now - start > g_bar_limit) {
-            atomicOr(&c->error, kErrTimeout);
-            ok = 0;
-            break;
-          }
-        }
-      }
-    }
-    s_ok = ok;
-  }
-  __syncthreads();
-  ++gen;
-  return s_ok != 0;
-}
+// A vertex whose packed word this update changed: the commit compares only these with the stored
+// (distance, parent) (a plain store: every writer stores the same value).
+__device__ __forceinline__ void touch(const SsspParams& p, int v) { p.touch_stamp[v] = p.touch_gen; }
 
 __device__ __forceinline__ bool claim(int* stamp, int v, int generation) {
   return atomicExch(&stamp[v], generation) != generation;
@@ -304,6 +248,7 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
   if (MODE == kWalk) {
     if (y < p.tree_n && p.parent[y] == owner && claim(p.stamp, y, X.gen)) {
       p.packed[y] = kPackedInf;
+      touch(p, y);
       add_candidate(p, y);
       ++X.appends;
       list_append(X.next, y, p.g.out_desc[y].len, p.heavy_degree);
@@ -333,7 +278,10 @@ __device__ __forceinline__ void visit(const SsspParams& p, Ctx& X, int owner, u6
   if (cand >= ld_cg(&p.packed[dst])) return;
   ++X.tries;
   const u64 old = atomicMin(&p.packed[dst], cand);
-  if (cand < old) ++X.atomics;
+  if (cand < old) {
+    ++X.atomics;
+    touch(p, dst);
+  }
   if (nd < X.pk.dist(old)) {
     if (MODE == kPull) {
       if (claim(p.stamp, dst, X.gen)) {
@@ -374,7 +322,10 @@ __device__ __forceinline__ void offer_owner(const SsspParams& p, Ctx& X, int own
   // atomicMin and claim together (see push_commit): a lost race appends the owner anyway
   const u64 old = atomicMin(&p.packed[owner], cand);
   const bool claimed = claim(p.stamp, owner, X.gen);
-  if (cand < old) ++X.atomics;
+  if (cand < old) {
+    ++X.atomics;
+    touch(p, owner);
+  }
   if (claimed) {
     ++X.appends;
     staged_append(kStNext, X.next.light, X.next.light_cnt, owner);
@@ -418,7 +369,10 @@ __device__ __forceinline__ void push_commit(const SsspParams& p, Ctx& X, const O
   const int len = near ? p.g.out_desc[dst].len : 0;
   const u64 old = atomicMin(&p.packed[dst], r.cand);
   const bool claimed = near ? claim(p.stamp, dst, X.gen) : atomicExch(&p.in_far[dst], 1) == 0;
-  if (r.cand < old) ++X.atomics;
+  if (r.cand < old) {
+    ++X.atomics;
+    touch(p, dst);
+  }
   if (!claimed) return;
   ++X.appends;
   if (near) list_append(X.next, dst, len, p.heavy_degree);
@@ -608,14 +562,18 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
                        int* med_cursor = nullptr, unsigned long long* heavy_cursor = nullptr) {
   const int lane = threadIdx.x & 31;
   unsigned long long t_part = probe ? global_ns() : 0;
-  // probe: the warp's time in each part, summed into probe[0..2], maxed into probe[3..5]
+  // probe: the warp's time in each part, summed into probe[0..2], maxed into probe[3..5]; the
+  // block's warps meet in shared memory first (one global atomic per block and value)
+  __shared__ long long s_part[6];
+  if (probe && threadIdx.x < 6) s_part[threadIdx.x] = 0;
+  if (probe) __syncthreads();
   auto part_done = [&](int part) {
     if (!probe) return;
     const unsigned long long now = global_ns();
     if (lane == 0) {
       const long long d = static_cast<long long>(now - t_part);
-      atomicAdd(reinterpret_cast<unsigned long long*>(&probe[part]), static_cast<unsigned long long>(d));
-      atomicMax(&probe[3 + part], d);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s_part[part]), static_cast<unsigned long long>(d));
+      atomicMax(&s_part[3 + part], d);
     }
     t_part = now;
   };
@@ -634,14 +592,12 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
       if (lane < per && i < light_count) {
         owner = ld_cg(&light[i]);
         ++X.rows;
+        // the descriptor is loaded beside the owner's word, not after it (one round trip)
+        desc = descs[owner];
         if (MODE == kPush) {
           const u64 word = ld_cg(&p.packed[owner]);
-          if (word != kPackedInf) {
-            du = X.pk.dist(word);
-            desc = descs[owner];
-          }
-        } else {
-          desc = descs[owner];
+          if (word != kPackedInf) du = X.pk.dist(word);
+          else desc.len = 0;
         }
       }
       warp_rows<MODE>(p, X, owner, du, desc.start, desc.len);
@@ -651,6 +607,7 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
   // medium: one row per warp
   auto medium_row = [&](long long i) {
     const int owner = ld_cg(&med[i]);
+    const RowDesc desc = descs[owner];  // beside the owner's word
     u64 du = 0;
     if (MODE == kPush) {
       const u64 word = ld_cg(&p.packed[owner]);
@@ -658,10 +615,11 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
       du = X.pk.dist(word);
     }
     if (lane == 0) ++X.rows;
-    const RowDesc desc = descs[owner];
     warp_slots<MODE>(p, X, owner, du, desc.start, 0, desc.len);
   };
-  if (med_cursor) {
+  // the cursors balance many rows or chunks over the warps; with at most one per warp the fixed
+  // split is as balanced and spares every warp an atomic on one shared address
+  if (med_cursor && med_count > nwarps) {
     // runs of rows per grab, so that a step makes at most about 4 grabs per warp (one cursor
     // address takes every grab of the step)
     const int run = 1 + static_cast<int>(med_count / (4 * nwarps));
@@ -684,6 +642,7 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     const int h = find_heavy(heavy, hcount, ch);
     const int owner = __ldcg(&heavy[h].x);
     const int base = __ldcg(&heavy[h].y);
+    const RowDesc desc = descs[owner];  // beside the owner's word
     u64 du = 0;
     if (MODE == kPush) {
       const u64 word = ld_cg(&p.packed[owner]);
@@ -691,12 +650,11 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
       du = X.pk.dist(word);
     }
     if (ch == base && lane == 0) ++X.rows;
-    const RowDesc desc = descs[owner];
     const int e0 = static_cast<int>(ch - base) * kHeavyChunk;
     const int e1 = min(desc.len, e0 + kHeavyChunk);
     warp_slots<MODE>(p, X, owner, du, desc.start, e0, e1);
   };
-  if (heavy_cursor) {
+  if (heavy_cursor && chunks > nwarps) {
     const long long run = 1 + chunks / (4 * nwarps);
     for (;;) {
       unsigned long long ch = 0;
@@ -710,11 +668,20 @@ __device__ void expand(const SsspParams& p, Ctx& X, const int* light, int light_
     for (long long ch = gwarp; ch < chunks; ch += nwarps) heavy_chunk(ch);
   }
   part_done(2);
+  if (probe) {
+    __syncthreads();
+    if (threadIdx.x < 3)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&probe[threadIdx.x]),
+                static_cast<unsigned long long>(s_part[threadIdx.x]));
+    else if (threadIdx.x < 6)
+      atomicMax(&probe[threadIdx.x], s_part[threadIdx.x]);
+  }
 }
 
 
 __device__ __forceinline__ void invalidate(const SsspParams& p, int v) {
   p.packed[v] = kPackedInf;
+  touch(p, v);
   add_candidate(p, v);
 }
 
@@ -805,12 +772,23 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
                     &c->heavy_cursor[cs]);
       if (!BLOCK && step == 0) {
         // balance of the first step: the slowest warp's and the summed busy time, and warps
+        // (met per block in shared memory: one global atomic per block and value)
+        __shared__ long long s_busy[2];
+        if (threadIdx.x == 0) s_busy[0] = s_busy[1] = 0;
+        __syncthreads();
         const long long busy = static_cast<long long>(global_ns() - t_busy);
         if ((threadIdx.x & 31) == 0) {
-          atomicMax(&c->work[13], busy);
-          atomicAdd(reinterpret_cast<unsigned long long*>(&c->work[14]),
+          atomicMax(&s_busy[0], busy);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&s_busy[1]),
                     static_cast<unsigned long long>(busy));
-          atomicAdd(reinterpret_cast<unsigned long long*>(&c->work[15]), 1ULL);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          atomicMax(&c->work[13], s_busy[0]);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&c->work[14]),
+                    static_cast<unsigned long long>(s_busy[1]));
+          atomicAdd(reinterpret_cast<unsigned long long*>(&c->work[15]),
+                    static_cast<unsigned long long>(blockDim.x >> 5));
         }
       }
       if (BLOCK) block_barrier();
@@ -875,7 +853,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
   p.walk = c->sched_walk && p.tree_trusted ? 1 : 0;
   if (c->sched_delta > 0) p.delta_override = c->sched_delta;
   stage_init();
-  unsigned bar = 0;
+  // the barrier generation continues from the previous kernel on this control block (the applier)
+  unsigned bar = ld_volatile(&c->bar_gen);
   const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   const long long threads = static_cast<long long>(nblk) * blockDim.x;
   const int lane = threadIdx.x & 31;
@@ -958,8 +937,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
     }
     if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(&c->changed, 1);
     if (__any_sync(0xffffffffu, changed == 2) && lane == 0) atomicOr(&c->changed, 2);
-    if (!grid_barrier(c, bar)) return;
-    if (ld_volatile(&c->error)) return;
+    unsigned roots_err = 0;
+    if (!grid_barrier(c, bar, &roots_err)) return;
+    if (roots_err) return;  // every block sees the same snapshot: all leave together
     if (tid == 0) c->phase_ns[1] = global_ns();
     // pointer jumping runs when roots exist, or (a tree imported without validation) when any
     // edge changed, so that a parent cycle is still reported as the reference reports it
@@ -987,7 +967,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         const long long lo = static_cast<long long>(blockIdx.x) * span;
         // ancestor[] starts as the parents with the roots marked, written by a sequential pass
         // over all vertices, so that every round gathers one random word per vertex
-        // (ancestor[a]) instead of two (parent[a] and stamp[a])
+        // (ancestor[a]) instead of two (parent[a] and stamp[a]; a round 0 that gathered both
+        // instead of this pass measured 18 % slower at R-MAT scale 22)
         // a child of the source has no ancestor that can be a root: its chain ends at once
         // (and nothing ever gathers ancestor[source], which every chain would reach)
         auto first_ancestor = [&](int st, int pa) {
@@ -1205,6 +1186,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
       const u64 cand = pk.pack(nd, u);
       if (cand >= ld_cg(&p.packed[v])) continue;
       const u64 old = atomicMin(&p.packed[v], cand);
+      if (cand < old) touch(p, v);
       if (nd < pk.dist(old) && claim(p.stamp, v, gen_pull))
         staged_append(kStNext, p.frontier, &c->frontier_count, v);
     }
@@ -1312,35 +1294,42 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         p.parent[v] = word == kPackedInf ? -1 : pk.parent(word);
       }
     } else {
-      // every vertex's word against its (distance, parent): the changed ones are written and
-      // counted (no list of written words is kept during the update)
-      // four vertices per thread and step, all loads issued before any compare
-      for (long long v0 = tid; v0 < n; v0 += 4 * threads) {
-        u64 word[4];
-        long long od[4];
-        int32_t op[4];
+      // only a vertex whose packed word this update changed can change its (distance, parent):
+      // the stamps of every vertex are scanned (4 bytes each, 16-byte loads) and the stamped
+      // ones compared with the stored pair; the changed ones are written and counted
+      const bool vec = (reinterpret_cast<uintptr_t>(p.touch_stamp) & 15) == 0;
+      const long long quads = vec ? n >> 2 : 0;
+      auto commit = [&](long long v) {
+        ++unpacked;
+        const u64 word = ld_cg(&p.packed[v]);
+        const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word));
+        const int32_t par = word == kPackedInf ? -1 : pk.parent(word);
+        if (p.dist[v] != d || p.parent[v] != par) {
+          p.dist[v] = d;
+          p.parent[v] = par;
+          ++affected;
+        }
+      };
+      for (long long q0 = tid; q0 < quads; q0 += 2 * threads) {
+        int4 ts[2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const long long v = v0 + q * threads;
-          word[q] = v < n ? ld_cg(&p.packed[v]) : kPackedInf;
-          od[q] = v < n ? p.dist[v] : kInfinity;
-          op[q] = v < n ? p.parent[v] : -1;
+        for (int j = 0; j < 2; ++j) {
+          const long long q = q0 + j * threads;
+          ts[j] = q < quads ? __ldcg(reinterpret_cast<const int4*>(p.touch_stamp) + q)
+                            : make_int4(0, 0, 0, 0);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const long long v = v0 + q * threads;
-          if (v >= n) continue;
-          ++unpacked;
-          const long long d =
-              word[q] == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word[q]));
-          const int32_t par = word[q] == kPackedInf ? -1 : pk.parent(word[q]);
-          if (od[q] != d || op[q] != par) {
-            p.dist[v] = d;
-            p.parent[v] = par;
-            ++affected;
-          }
+        for (int j = 0; j < 2; ++j) {
+          const long long v = 4 * (q0 + j * threads);
+          if (ts[j].x == p.touch_gen) commit(v);
+          if (ts[j].y == p.touch_gen) commit(v + 1);
+          if (ts[j].z == p.touch_gen) commit(v + 2);
+          if (ts[j].w == p.touch_gen) commit(v + 3);
         }
       }
+      for (long long v = 4 * quads + tid; v < n; v += threads)
+        if (ld_cg(&p.touch_stamp[v]) == p.touch_gen) commit(v);
+      if (tid == 0) c->work[28] = n;  // stamps scanned
     }
   } else {
     // distance-only words: recover the lowest-id tight parent of every vertex
@@ -1477,6 +1466,13 @@ static int persistent_blocks(Context& ctx, const dyngb200_schedule& sched) {
   return update_grid_blocks(ctx);
 }
 
+void require_intact(const Graph& g) {
+  expects(!g.broken,
+          "graph: an earlier update stopped part-way through applying its batch (a grid barrier "
+          "of the batch applier timed out), so the graph is incomplete; build it again",
+          DYNGB200_INTERNAL);
+}
+
 void require_cooperative(const Context& ctx) {
   expects(ctx.coop_supported != 0 && ctx.test_no_cooperative == 0,
           "sssp: the fused engine needs cooperative launch, which this device does not offer "
@@ -1526,12 +1522,13 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
   p.barrier_limit_ns = ctx.test_barrier_timeout_ns > 0
                            ? static_cast<unsigned long long>(ctx.test_barrier_timeout_ns)
                            : 0;
-  p.barrier_extra = ctx.test_barrier_extra;
+  p.barrier_extra = ctx.test_barrier_kernel == 1 ? 0 : ctx.test_barrier_extra;
   return p;
 }
 
 // compute(): the persistent kernel from the source (fused.cuh:167-176).
 void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
+  require_intact(g);
   require_cooperative(ctx);
   const long long launches0 = ctx.launches;
   Workspace& ws = ctx.ws;
@@ -1621,7 +1618,12 @@ constexpr size_t kCounterSlots = (sizeof(GraphCounters) + sizeof(ColumnStats) - 
 
 // One attempt of an update, queued on the context's stream: the applier, the persistent kernel,
 // and the read-back of the control block, counters and column statistics into pinned memory.
+static double us_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+}
+
 static void enqueue_attempt(PendingUpdate& u) {
+  const auto h0 = std::chrono::steady_clock::now();
   Context& ctx = *u.ctx;
   Graph& g = *u.g;
   Tree& t = *u.t;
@@ -1632,9 +1634,10 @@ static void enqueue_attempt(PendingUpdate& u) {
   // graph as it was
   g.pinned.reserve(kCounterSlots + g.host_columns.size());
   DYNGB200_CUDA(cudaEventRecord(u.e0, s));
-  apply_prepare(ctx, g, u.b, t.opt.objective, t.opt.delta, &u.sched, &t, u.learned);
-  apply_commit(ctx, g, u.b);
+  apply_launch(ctx, g, u.b, t.opt.objective, t.opt.delta, &u.sched, &t, u.learned);
   DYNGB200_CUDA(cudaEventRecord(u.e1, s));
+  u.host_us[1] += us_since(h0);
+  const auto h1 = std::chrono::steady_clock::now();
   SsspParams p = base_params(ctx, g, t);
   p.from_scratch = 0;
   p.tree_n = t.n;
@@ -1660,6 +1663,7 @@ static void enqueue_attempt(PendingUpdate& u) {
   DYNGB200_CUDA(cudaMemcpyAsync(g.pinned.ptr + kCounterSlots, g.columns.ptr,
                                 g.host_columns.size() * sizeof(ColumnStats),
                                 cudaMemcpyDeviceToHost, s));
+  u.host_us[2] += us_since(h1);
 }
 
 PendingUpdate::~PendingUpdate() {
@@ -1674,12 +1678,14 @@ PendingUpdate::~PendingUpdate() {
 void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& batch,
                        const dyngb200_schedule& sched, const Scheduler* learned,
                        PendingUpdate& u) {
+  const auto h0 = std::chrono::steady_clock::now();
   u.ctx = &ctx;
   u.g = &g;
   u.t = &t;
   u.sched = sched;
   u.learned = learned;
   u.launches0 = ctx.launches;
+  require_intact(g);
   require_cooperative(ctx);  // before the batch is staged or applied: nothing changes
   if (g.host_columns[t.opt.objective].dirty) graph_rescan_columns(ctx, g);
   graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
@@ -1688,6 +1694,7 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
   DYNGB200_CUDA(cudaEventCreate(&u.e0));
   DYNGB200_CUDA(cudaEventCreate(&u.e1));
   DYNGB200_CUDA(cudaEventCreate(&u.e2));
+  u.host_us[0] = us_since(h0);
   enqueue_attempt(u);
 }
 
@@ -1756,6 +1763,10 @@ static void finish_tree(Context& ctx, Graph& g, Tree& t, const UpdateCtl& r, int
     st->kernel_launches = ctx.launches - launches0;
     for (int i = 0; i < 24 && i < r.rounds; ++i) st->pj_round_us[i] = r.pj_t[i] * 1e-3f;
     for (int i = 0; i < 24 && i < r.rounds; ++i) st->pj_done_us[i] = r.pj_done[i] * 1e-3f;
+    for (int i = 1; i < 12; ++i)
+      st->apply_step_us[i] = r.apply_ns[i] > r.apply_ns[0]
+                                 ? static_cast<float>((r.apply_ns[i] - r.apply_ns[0]) * 1e-3)
+                                 : 0.0f;
     for (int i = 0; i < 7; ++i)
       st->phase_ms[i] = r.phase_ns[i + 1] > r.phase_ns[i]
                             ? static_cast<float>((r.phase_ns[i + 1] - r.phase_ns[i]) * 1e-6)
@@ -1774,7 +1785,9 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
   const long long launches0 = u.launches0;
   UpdateCtl r{};
   for (int attempt = 0;; ++attempt) {
+    const auto w0 = std::chrono::steady_clock::now();
     DYNGB200_CUDA(cudaStreamSynchronize(ctx.stream));
+    u.host_us[3] += us_since(w0);
     r = *ws.host_ctl.ptr;
     g.host_counters = *reinterpret_cast<const GraphCounters*>(g.pinned.ptr);
     std::memcpy(g.host_columns.data(), g.pinned.ptr + kCounterSlots,
@@ -1792,13 +1805,31 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
   float apply_ms = 0, sssp_ms = 0;
   cudaEventElapsedTime(&apply_ms, u.e0, u.e1);
   cudaEventElapsedTime(&sssp_ms, u.e1, u.e2);
-  if (r.error & (kErrInvalidBatch | kErrCapacity)) {
+  if (!r.applied) {
+    if (r.committing) {
+      // the applier stopped between its first change and its last: the graph is incomplete
+      g.broken = true;
+      t.poisoned = true;
+      throw Error(DYNGB200_INTERNAL,
+                  (r.error & kErrTimeout)
+                      ? "sssp::update: a grid barrier of the batch applier timed out part-way "
+                        "through applying the batch; the graph is incomplete"
+                      : "sssp::update: the batch applier found the in-edge mirror inconsistent "
+                        "part-way through applying the batch; the graph is incomplete");
+    }
     // found before the commit: the graph and the tree are unchanged
     std::string msg = "sssp::update: invalid batch";
     if (r.err_index == -2) msg = "sssp::update: distances do not fit in 62 bits";
     else if (r.err_index != INT64_MAX) msg += " (operation " + std::to_string(r.err_index) + ")";
     if (r.error & kErrCapacity) throw Error(DYNGB200_CAPACITY, "sssp::update: capacity exceeded");
-    throw Error(DYNGB200_INVALID_ARGUMENT, msg);
+    if (r.error & kErrInvalidBatch) throw Error(DYNGB200_INVALID_ARGUMENT, msg);
+    if (r.error & kErrTimeout)
+      throw Error(DYNGB200_INTERNAL,
+                  "sssp::update: a grid barrier of the batch applier timed out before the batch "
+                  "was applied; the graph and the tree are unchanged");
+    throw Error(DYNGB200_INTERNAL,
+                "sssp::update: the batch applier found the in-edge mirror inconsistent with the "
+                "rows; the graph and the tree are unchanged");
   }
   // the batch is committed from here on
   g.version += 1;
@@ -1806,6 +1837,8 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
   g.m = g.host_counters.m;
   t.version = g.version;
   finish_tree(ctx, g, t, r, blocks, apply_ms, sssp_ms, learned, sched, launches0, st);
+  if (st)
+    for (int i = 0; i < 4; ++i) st->host_us[i] = static_cast<float>(u.host_us[i]);
 }
 
 // update(): sssp::update(resources::cuda(), g, batch, tree) (sssp.hpp:484-489).
@@ -1918,6 +1951,7 @@ static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied
 // first error is rethrown.
 void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree* const* trees,
                       int count, dyngb200_stats* stats) {
+  require_intact(g);
   require_cooperative(ctx);
   cudaStream_t s = ctx.stream;
   for (int i = 0; i < count; ++i)
@@ -2080,6 +2114,7 @@ unsigned char* static_scratch_for(int device) {
 
 void sssp_compute_static(Graph& g, int32_t source, int objective, long long delta,
                          int64_t* distances, int32_t* parents, cudaStream_t s) {
+  require_intact(g);
   const long long n = g.n;
   expects(n <= kStaticMaxVertices,
           "sssp::compute (static scratch): the graph has " + std::to_string(n) +

@@ -84,10 +84,12 @@ class Resources:
         check(N.lib().dyngb200_context_synchronize(self._h))
 
     def set_test_hooks(self, barrier_timeout_ns: int = 0, barrier_extra_arrivals: int = 0,
-                       no_cooperative_launch: bool = False) -> None:
-        """Host-side failure injection for tests (dyngb200_test_hooks); no argument clears."""
+                       no_cooperative_launch: bool = False, barrier_kernel: int = 0) -> None:
+        """Host-side failure injection for tests (dyngb200_test_hooks); no argument clears.
+        barrier_kernel: the kernel the phantom arrivals hold up (0 both, 1 the batch applier,
+        2 the sssp kernel)."""
         h = N.TestHooks(int(barrier_timeout_ns), int(barrier_extra_arrivals),
-                        int(bool(no_cooperative_launch)))
+                        int(bool(no_cooperative_launch)), int(barrier_kernel))
         check(N.lib().dyngb200_context_set_test_hooks(self._h, ctypes.byref(h)))
 
     def close(self) -> None:

@@ -67,24 +67,24 @@ class Stats:
                   "step0_warps", "step0_light_ns", "step0_medium_ns", "step0_heavy_ns",
                   "step0_max_light_ns", "step0_max_medium_ns", "step0_max_heavy_ns",
                   "pj_seeded", "pull_atomics", "pull_appends", "pair_visits", "walk_rows",
-                  "walk_slots")
+                  "walk_slots", "stamps_scanned")
     # Algorithmic bytes per unit of work (4-byte ids / weights, 8-byte packed words and rows):
     #   pointer-jumping visit 8 (ancestor + flag), jump 12 (ancestor[a], flag[a], write),
     #   invalidated vertex 12 (word set to INF, candidate entry), pull candidate / pushed vertex
     #   20 (list entry, row descriptor, own word), row slot 8 (column + weight), word read 8,
-    #   successful atomicMin 8, frontier append 12 (entry + stamp), unpacked vertex 20 (word, old
+    #   successful atomicMin 8, frontier append 12 (entry + stamp), compared vertex 20 (word, old
     #   distance and parent), seeded vertex 12 (stamp, parent, ancestor written), change pair 16
-    #   (list entry, flags, key), walk row 12 (entry, descriptor), walk slot 8 (column, parent);
-    #   attempted atomics and the balance probes are diagnostics (0 bytes).
+    #   (list entry, flags, key), walk row 12 (entry, descriptor), walk slot 8 (column, parent),
+    #   scanned change stamp 4; attempted atomics and the balance probes are diagnostics (0 bytes).
     WORK_BYTES = ((8, 12, 12, 20, 8, 8, 20, 8, 8, 8, 12, 20) + (0,) * 10 +
-                  (12, 8, 12, 16, 12, 8) + (0,) * 4)
+                  (12, 8, 12, 16, 12, 8, 4) + (0,) * 3)
     # The work counters of each phase of the kernel (indices into WORK_NAMES), and the phases'
     # device times (indices into PHASES): the per-phase roofline.
     PHASE_WORK = {"roots_heads": ((25,), (0, 3)),
                   "invalidation": ((0, 1, 2, 22, 26, 27), (1, 2)),
                   "pull": ((3, 4, 5, 23, 24), (4,)),
                   "near_far": ((6, 7, 8, 9, 10), (5,)),
-                  "unpack": ((11,), (6,))}
+                  "unpack": ((11, 28), (6,))}
     PHASES = ("roots", "invalidation", "invalidate_scan", "heads", "pull", "near_far", "unpack")
     _SCALARS = ("invalidated", "affected", "iterations", "epochs", "pushes", "delta",
                 "max_weight", "grid_blocks", "invalidation", "rounds", "touched",
@@ -149,6 +149,17 @@ class Stats:
     def pj_done_us(self) -> tuple:
         """The last block's arrival at the barrier ending each pointer-jumping round (us)."""
         return tuple(float(self._s.pj_done_us[i]) for i in range(min(int(self._s.rounds), 24)))
+
+    @property
+    def apply_step_us(self) -> tuple:
+        """The batch applier kernel: the end of each step (us since it began; 0: not reached)."""
+        return tuple(float(x) for x in self._s.apply_step_us)
+
+    @property
+    def host_us(self) -> tuple:
+        """Host time of the call (us): checks and staging, queuing the applier, queuing the sssp
+        kernel and the read-back, waiting for the device."""
+        return tuple(float(x) for x in self._s.host_us)
 
     @property
     def features(self) -> tuple:

@@ -121,7 +121,8 @@ typedef struct dyngb200_stats {
    * [19..21] the slowest warp's ns in each; [22] vertices seeded for pointer jumping; [23]
    * successful atomicMin of the pull, [24] frontier appends of the pull, [25] change pairs
    * visited by the roots and insertion-head passes; [26] rows and [27] slots of the subtree
-   * walk (the walk invalidation); [28..31] zero.  [9] and [10] count the near-far loop only. */
+   * walk (the walk invalidation); [28] change stamps the commit scanned ([11] then counts the
+   * stamped vertices it compared); [29..31] zero.  [9] and [10] count the near-far loop only. */
   int64_t work[32];
   /* Device time of the kernel's phases (ms): setup+roots, pointer jumping, invalidation, pull,
    * first split, near-far loop, unpack. */
@@ -143,6 +144,13 @@ typedef struct dyngb200_stats {
   int64_t kernel_launches; /* kernels of this library the call launched */
   float pj_round_us[24];    /* start of each pointer-jumping round, us since the kernel began */
   float pj_done_us[24];     /* the last block's arrival at the barrier ending each round */
+  /* The batch applier kernel: the end of each of its steps (us since it began; 0: not reached):
+   * [1] checks, [2] pairs, [3] matching, [4] resolution, then (append-order rows) three ordering
+   * steps, then allocation, mutation, moves and appends, row descriptors; [11] the finalize. */
+  float apply_step_us[12];
+  /* Host time of the call (us): [0] checks, index room and batch staging, [1] queuing the batch
+   * applier, [2] queuing the sssp kernel and the read-back, [3] waiting for the device. */
+  float host_us[4];
 } dyngb200_stats;
 
 /* sssp::options (cpp/include/dyng/sssp.hpp:78-94). */
@@ -192,6 +200,10 @@ typedef struct dyngb200_test_hooks {
   /* Nonzero: the context behaves as on a device without cooperative launch (the persistent
    * kernels are refused with NOT_SUPPORTED before anything changes). */
   int32_t no_cooperative_launch;
+  /* Which persistent kernel the phantom arrivals hold up: 0 both, 1 the batch applier (its first
+   * barrier comes before any change: the call fails with the graph and the tree unchanged), 2 the
+   * sssp kernel (after the batch is applied: the tree is poisoned). */
+  int32_t barrier_kernel;
 } dyngb200_test_hooks;
 /* Set (hooks) or clear (NULL) the test hooks of a context. */
 dyngb200_status dyngb200_context_set_test_hooks(dyngb200_context ctx,

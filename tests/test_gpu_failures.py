@@ -1,8 +1,9 @@
 """Failures made on the host, and what the library leaves behind (no GPU fault is made).
 
   - a grid barrier that never completes (a phantom block that never arrives, with a short
-    test-only time limit): every block leaves the kernel, the call reports INTERNAL, the tree is
-    poisoned and the context keeps working (the bounded waits of the persistent kernel);
+    test-only time limit): every block leaves the kernel and the call reports INTERNAL; in the
+    batch applier before any change (graph and tree unchanged), in the sssp kernel after the
+    batch was applied (the tree poisoned); the context keeps working either way;
   - a long loop run by one block while the others wait at a grid barrier outlives that limit
     without a timeout: the waiting blocks restart their limit whenever the working block shows
     progress;
@@ -42,7 +43,33 @@ def _case(seed=3, n=3000):
     return rng, n, s, d, w
 
 
-def test_a_barrier_that_never_completes_times_out_and_poisons():
+def test_a_barrier_of_the_applier_that_never_completes_changes_nothing():
+    # the batch applier's first grid barrier comes before any change: its timeout leaves the
+    # graph and the tree as they were (strong guarantee), and the same update then succeeds
+    rng, n, s, d, w = _case()
+    res = D.Resources(0)
+    g = D.Graph.from_edges(s, d, w, n, resources=res)
+    og = O.Graph.from_edges(n, s, d, w, 1)
+    t = D.sssp.compute(g, 0)
+    ot, _ = O.compute(og, 0, rule=1)
+    d0, p0, m0 = t.distances, t.parents, g.num_edges()
+    b = random_batch(rng, n, s, d, 400, tree_parents=ot.parents)
+    res.set_test_hooks(barrier_timeout_ns=2_000_000, barrier_extra_arrivals=1, barrier_kernel=1)
+    try:
+        with pytest.raises(D.InternalError, match="timed out before the batch was applied"):
+            D.sssp.update(g, _batch(b), t)
+    finally:
+        res.set_test_hooks()
+    assert g.version() == 0 and g.num_edges() == m0 and not t.poisoned
+    np.testing.assert_array_equal(t.distances, d0)
+    np.testing.assert_array_equal(t.parents, p0)
+    D.sssp.update(g, _batch(b), t)
+    O.update(og, _obatch(b), ot)
+    np.testing.assert_array_equal(t.distances, ot.distances)
+    np.testing.assert_array_equal(t.parents, ot.parents)
+
+
+def test_a_barrier_of_the_sssp_kernel_that_never_completes_times_out_and_poisons():
     rng, n, s, d, w = _case()
     res = D.Resources(0)
     g = D.Graph.from_edges(s, d, w, n, resources=res)
@@ -50,11 +77,11 @@ def test_a_barrier_that_never_completes_times_out_and_poisons():
     t = D.sssp.compute(g, 0)
     ot, _ = O.compute(og, 0, rule=1)
     b = random_batch(rng, n, s, d, 400, tree_parents=ot.parents)
-    res.set_test_hooks(barrier_timeout_ns=2_000_000, barrier_extra_arrivals=1)
+    res.set_test_hooks(barrier_timeout_ns=2_000_000, barrier_extra_arrivals=1, barrier_kernel=2)
     try:
         with pytest.raises(D.InternalError, match="timed out"):
             D.sssp.update(g, _batch(b), t)
-        assert g.version() == 1  # the batch was applied before the kernel ran
+        assert g.version() == 1  # the batch was applied before the sssp kernel ran
         with pytest.raises(D.StaleResultError):
             t.distances
         with pytest.raises(D.InternalError, match="timed out"):
