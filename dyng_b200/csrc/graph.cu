@@ -156,7 +156,7 @@ __device__ __forceinline__ int find_pair(const ApplyParams& p, u64 k) {
 }
 
 // ---- A: Step 0 checks, vertex growth, largest insertion weight --------------------------------
-__device__ void ph_validate(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_validate(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const long long total = p.ni + p.nd;
   const long long n = c->n_old;
@@ -225,14 +225,24 @@ __device__ void ph_validate(const ApplyParams& p, long long tid, long long threa
       }
     }
   }
-  warp_max(top, &c->n_after, 0);
-  if (p.objective >= 0) warp_max(wmax, &c->batch_ins_max, 1);
-  warp_add(dropped, &c->summary[5]);
-  if (p.feat) {
-    warp_add(f_tree, &c->feat_acc[0]);
-    warp_add(f_deg, &c->feat_acc[1]);
-    warp_max(f_max, &c->feat_acc[2], 0);
-    warp_add(f_srcs, &c->feat_acc[3]);
+  red_max(R, 0, top);
+  red_max(R, 1, wmax);
+  red_sum(R, 2, dropped);
+  red_sum(R, 3, f_tree);
+  red_sum(R, 4, f_deg);
+  red_max(R, 5, f_max);
+  red_sum(R, 6, f_srcs);
+  __syncthreads();
+  long long t;
+  switch (threadIdx.x) {
+    case 0: if ((t = red_maximum(R, 0, 0)) > 0) atomicMax(&c->n_after, t); break;
+    case 1: if (p.objective >= 0 && (t = red_maximum(R, 1, 1)) > 1) atomicMax(&c->batch_ins_max, t); break;
+    case 2: if ((t = red_total(R, 2)) != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[5]), static_cast<unsigned long long>(t)); break;
+    case 3: if (p.feat && (t = red_total(R, 3)) != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&c->feat_acc[0]), static_cast<unsigned long long>(t)); break;
+    case 4: if (p.feat && (t = red_total(R, 4)) != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&c->feat_acc[1]), static_cast<unsigned long long>(t)); break;
+    case 5: if (p.feat && (t = red_maximum(R, 5, 0)) > 0) atomicMax(&c->feat_acc[2], t); break;
+    case 6: if (p.feat && (t = red_total(R, 6)) != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&c->feat_acc[3]), static_cast<unsigned long long>(t)); break;
+    default: break;
   }
 }
 
@@ -359,7 +369,7 @@ __device__ void add_op(PairStage& st, const ApplyParams& p, int32_t u, int32_t v
 }
 
 // ---- C: group the effective operations by (u, v) pair ------------------------------------------
-__device__ void ph_pairs(const ApplyParams& p, PairStage& st, long long tid, long long threads) {
+__device__ void ph_pairs(const ApplyParams& p, PairStage& st, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   if (threadIdx.x < 3) st.cnt[threadIdx.x] = 0;
   __syncthreads();
@@ -388,13 +398,17 @@ __device__ void ph_pairs(const ApplyParams& p, PairStage& st, long long tid, lon
       if (!p.props.directed && u != v) add_op(st, p, v, u, 0, static_cast<int>(j));
     }
   }
-  warp_add(missing, &c->summary[4]);
+  red_sum(R, 0, missing);
   // flush the stages: one global atomic per list and block
   __syncthreads();
   if (threadIdx.x < 3) {
     const int n = min(st.cnt[threadIdx.x], kPairStageCap);
     int* counter = threadIdx.x == 0 ? &c->pairs : (threadIdx.x == 1 ? &c->rows_out : &c->rows_in);
     st.base[threadIdx.x] = n > 0 ? atomicAdd(counter, n) : 0;
+  } else if (threadIdx.x == 3) {
+    const long long t = red_total(R, 0);
+    if (t != 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[4]), static_cast<unsigned long long>(t));
   }
   __syncthreads();
   for (int list = 0; list < 3; ++list) {
@@ -466,7 +480,7 @@ __device__ void ph_scan_multi(const ApplyParams& p, long long tid, long long thr
 
 
 // ---- E: resolve every pair (counts, policies, classification, per-row slot demand) -------------
-__device__ void ph_resolve(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_resolve(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
@@ -563,7 +577,13 @@ __device__ void ph_resolve(const ApplyParams& p, long long tid, long long thread
       }
     }
   }
-  for (int f = 0; f < 5; ++f) warp_add(acc[f], &c->summary[f]);
+  for (int f = 0; f < 5; ++f) red_sum(R, f, acc[f]);
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    const long long t = red_total(R, threadIdx.x);
+    if (t != 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&c->summary[threadIdx.x]), static_cast<unsigned long long>(t));
+  }
 }
 
 // Warp-wide reservation on a shared counter: every lane asks for `amount` (0: none), one atomic
@@ -586,12 +606,13 @@ __device__ __forceinline__ u64 warp_reserve(u64 amount, u64* counter) {
 // ---- F: per touched row: stay in place or move to the top of the arena -------------------------
 // A row that overflows its slack (or is mostly tombstones) gets a new place at the arena top.  The warps iterate together so that the arena
 // space of a warp's relocated rows is reserved with one atomic per side.
-__device__ void ph_alloc(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_alloc(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
   const int total = rows_out + rows_in;
   const double headroom = p.props.headroom;
   const int lane = threadIdx.x & 31;
+  long long moved_out = 0, moved_in = 0;  // relocated rows (lane 0 of each warp counts)
   for (long long i0 = tid & ~31LL; i0 < total; i0 += threads) {
     const int i = i0 + lane;
     const bool active = i < total;
@@ -625,8 +646,8 @@ __device__ void ph_alloc(const ApplyParams& p, long long tid, long long threads)
     const unsigned n_out = __popc(__ballot_sync(0xffffffffu, reloc && side == 0));
     const unsigned n_in = __popc(__ballot_sync(0xffffffffu, reloc && side == 1));
     if (lane == 0) {
-      if (n_out) atomicAdd(&c->relocated_out, static_cast<int>(n_out));
-      if (n_in) atomicAdd(&c->relocated_in, static_cast<int>(n_in));
+      moved_out += n_out;
+      moved_in += n_in;
     }
     if (!active) continue;
     if (reloc) {
@@ -640,6 +661,13 @@ __device__ void ph_alloc(const ApplyParams& p, long long tid, long long threads)
     (side == 0 ? p.new_start_out : p.new_start_in)[s] = start;
     (side == 0 ? p.new_cap_out : p.new_cap_in)[s] = new_cap;
     (side == 0 ? p.live_out : p.live_in)[s] = live;
+  }
+  red_sum(R, 0, moved_out);
+  red_sum(R, 1, moved_in);
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const long long t = red_total(R, threadIdx.x);
+    if (t != 0) atomicAdd(threadIdx.x == 0 ? &c->relocated_out : &c->relocated_in, static_cast<int>(t));
   }
 }
 
@@ -672,19 +700,41 @@ __device__ __forceinline__ void column_in(const ApplyParams& p, ColumnAcc& a, in
   atomicMax(&p.col_written_max[j], w);
   if (w < 1) atomicAdd(&p.g.columns[j].bad, 1);
 }
-// Flush a warp's accumulators (all lanes must call).
-__device__ __forceinline__ void acc_flush(const ApplyParams& p, ColumnAcc& a) {
-  warp_add(a.sum, &p.col_sum_delta[0]);
-  warp_add(a.removed_at_max, &p.col_removed_at_max[0]);
-  warp_max(a.written_max, &p.col_written_max[0], 0);
-  warp_add(a.written_at_max, &p.col_written_at_max[0]);
-  long long bad = a.bad;
-  for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
-  if ((threadIdx.x & 31) == 0 && bad != 0) atomicAdd(&p.g.columns[0].bad, static_cast<int>(bad));
+// The block's column-0 accumulators into reduction slots base .. base + 4 (all threads call).
+__device__ __forceinline__ void acc_stage(BlockRed& R, const ColumnAcc& a, int base) {
+  red_sum(R, base, a.sum);
+  red_sum(R, base + 1, a.removed_at_max);
+  red_max(R, base + 2, a.written_max);
+  red_sum(R, base + 3, a.written_at_max);
+  red_sum(R, base + 4, a.bad);
+}
+// After the barrier that follows acc_stage: thread `base + i` commits value i (one atomic per
+// block and value).
+__device__ __forceinline__ void acc_commit(const ApplyParams& p, const BlockRed& R, int base) {
+  const int i = static_cast<int>(threadIdx.x) - base;
+  if (i < 0 || i > 4) return;
+  if (i == 2) {
+    const long long t = red_maximum(R, base + 2, 0);
+    if (t > 0) atomicMax(&p.col_written_max[0], t);
+    return;
+  }
+  const long long t = red_total(R, base + i);
+  if (t == 0) return;
+  if (i == 4) {
+    atomicAdd(&p.g.columns[0].bad, static_cast<int>(t));
+    return;
+  }
+  long long* target = i == 0 ? &p.col_sum_delta[0]
+                             : (i == 1 ? &p.col_removed_at_max[0] : &p.col_written_at_max[0]);
+  atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(t));
+}
+// A block's signed counter into one global atomic (called by the committing thread).
+__device__ __forceinline__ void commit_add(long long t, long long* target) {
+  if (t != 0) atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(t));
 }
 
 // ---- G: tombstones and upserts in place -------------------------------------------------------
-__device__ void ph_mutate(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_mutate(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
@@ -764,9 +814,15 @@ __device__ void ph_mutate(const ApplyParams& p, long long tid, long long threads
       }
     }
   }
-  acc_flush(p, acc);
-  warp_add(-idx_deleted, &p.g.counters->idx_live);
-  warp_add(idx_deleted, &p.g.counters->idx_dead);
+  acc_stage(R, acc, 0);
+  red_sum(R, 5, idx_deleted);
+  __syncthreads();
+  acc_commit(p, R, 0);
+  if (threadIdx.x == 5) {
+    const long long t = red_total(R, 5);
+    commit_add(-t, &p.g.counters->idx_live);
+    commit_add(t, &p.g.counters->idx_dead);
+  }
 }
 
 // ---- H: move relocated rows (live slots, in order) ---------------------------------------------
@@ -809,7 +865,7 @@ __device__ void ph_move(const ApplyParams& p, long long tid, long long threads) 
 }
 
 // ---- I: append the new slots ---------------------------------------------------------------------
-__device__ void ph_append(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_append(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int pairs = c->pairs;
   ColumnAcc acc;
@@ -856,13 +912,17 @@ __device__ void ph_append(const ApplyParams& p, long long tid, long long threads
       p.g.ein[ie] = placed[1];
     }
   }
-  acc_flush(p, acc);
-  warp_add(idx_new, &p.g.counters->idx_live);
-  warp_add(-idx_reused, &p.g.counters->idx_dead);
+  acc_stage(R, acc, 0);
+  red_sum(R, 5, idx_new);
+  red_sum(R, 6, idx_reused);
+  __syncthreads();
+  acc_commit(p, R, 0);
+  if (threadIdx.x == 5) commit_add(red_total(R, 5), &p.g.counters->idx_live);
+  if (threadIdx.x == 6) commit_add(-red_total(R, 6), &p.g.counters->idx_dead);
 }
 
 // ---- J: new row descriptors ----------------------------------------------------------------------
-__device__ void ph_rows_final(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_rows_final(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
   long long garbage_out = 0, garbage_in = 0, dead_delta_out = 0, dead_delta_in = 0;
@@ -896,14 +956,21 @@ __device__ void ph_rows_final(const ApplyParams& p, long long tid, long long thr
     descs[r] = nd;
   }
   GraphCounters* gc = p.g.counters;
-  warp_add_u(static_cast<u64>(garbage_out), &gc->out_garbage);
-  warp_add_u(static_cast<u64>(garbage_in), &gc->in_garbage);
-  warp_add(dead_delta_out, &gc->dead_out);
-  warp_add(dead_delta_in, &gc->dead_in);
+  red_sum(R, 8, garbage_out);
+  red_sum(R, 9, garbage_in);
+  red_sum(R, 10, dead_delta_out);
+  red_sum(R, 11, dead_delta_in);
+  __syncthreads();
+  if (threadIdx.x == 8 || threadIdx.x == 9) {
+    const long long t = red_total(R, threadIdx.x);
+    if (t != 0) atomicAdd(threadIdx.x == 8 ? &gc->out_garbage : &gc->in_garbage, static_cast<u64>(t));
+  }
+  if (threadIdx.x == 10) commit_add(red_total(R, 10), &gc->dead_out);
+  if (threadIdx.x == 11) commit_add(red_total(R, 11), &gc->dead_in);
 }
 
 // Count the weights written by the batch that equal the new maximum (for count_at_max).
-__device__ void ph_count_written_max(const ApplyParams& p, long long tid, long long threads) {
+__device__ void ph_count_written_max(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int pairs = c->pairs;
   ColumnAcc acc;
@@ -922,7 +989,9 @@ __device__ void ph_count_written_max(const ApplyParams& p, long long tid, long l
       }
     }
   }
-  warp_add(acc.written_at_max, &p.col_written_at_max[0]);
+  red_sum(R, 12, acc.written_at_max);
+  __syncthreads();
+  if (threadIdx.x == 12) commit_add(red_total(R, 12), &p.col_written_at_max[0]);
 }
 
 // One thread: graph counters and column statistics after the batch.
@@ -1196,6 +1265,7 @@ union ApplySmem {
 
 __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch L) {
   __shared__ ApplySmem sm;
+  __shared__ BlockRed red;
   UpdateCtl* c = p.ctl;
   const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   const long long threads = static_cast<long long>(gridDim.x) * blockDim.x;
@@ -1212,7 +1282,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch 
   if (tid == 0) c->apply_ns[0] = global_ns();
   // A: Step 0 checks (and the scheduler's feature sums); this batch's pair table cleared
   ph_clear(p, tid, threads);
-  ph_validate(p, tid, threads);
+  ph_validate(p, red, tid, threads);
   if (!grid_sync(c, gen, arrivals, limit, &err)) return;
   mark();
   // B: the plan, then the features and schedule, by block 0
@@ -1231,7 +1301,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch 
   // share the pairs among themselves (the inference is then off the critical path)
   const long long skip = L.infer_on ? blockDim.x : 0;
   const long long ptid = (L.infer_on && blockIdx.x == 0) ? (1LL << 62) : tid - skip;
-  ph_pairs(p, sm.pairs, ptid, threads - skip);
+  ph_pairs(p, sm.pairs, red, ptid, threads - skip);
   if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   // D: the live slot of each pair
@@ -1240,7 +1310,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch 
   if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   // E: the outcome of each pair, its weight-increase class, the rows' demand
-  ph_resolve(p, tid, threads);
+  ph_resolve(p, red, tid, threads);
   if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   if (!p.props.sorted) {
@@ -1255,23 +1325,24 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch 
     if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   }
-  // F: room for every touched row (the last point where an error leaves the graph untouched)
-  ph_alloc(p, tid, threads);
-  if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
+  // F: room for every touched row (the last point where an error leaves the graph untouched);
+  // the barrier's last arrival records that the graph is about to change (any block past it
+  // sees `committing` set, so a stop from here on is reported as leaving the graph incomplete)
+  ph_alloc(p, red, tid, threads);
+  if (!grid_sync(c, gen, arrivals, limit, &err, &c->committing) || err != 0) return;
   mark();
   // G: tombstones and upserts in place
-  if (threadIdx.x == 0) c->committing = 1;  // from here on a stop leaves the graph incomplete
-  ph_mutate(p, tid, threads);
+  ph_mutate(p, red, tid, threads);
   if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   // H, I: relocated rows moved and new slots appended (disjoint slots)
   ph_move(p, tid, threads);
-  ph_append(p, tid, threads);
+  ph_append(p, red, tid, threads);
   if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   // J: row descriptors, the written maxima, then counters and column statistics
-  ph_rows_final(p, tid, threads);
-  ph_count_written_max(p, tid, threads);
+  ph_rows_final(p, red, tid, threads);
+  ph_count_written_max(p, red, tid, threads);
   if (!grid_sync(c, gen, arrivals, limit, &err) || err != 0) return;
   mark();
   if (tid == 0) {

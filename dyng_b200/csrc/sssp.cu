@@ -177,15 +177,33 @@ __device__ __forceinline__ bool claim(int* stamp, int v, int generation) {
   return atomicExch(&stamp[v], generation) != generation;
 }
 
-__device__ __forceinline__ void warp_min_into(u64 v, u64* target) {
+// The block's minimum into *target with one atomic per block (every thread of the block calls).
+__device__ __forceinline__ void block_min_into(u64 v, u64* target) {
+  __shared__ u64 s_min[kThreads / 32];
   for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0 && v != kPackedInf) atomicMin(target, v);
+  if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u64 m = kPackedInf;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = min(m, s_min[w]);
+    if (m != kPackedInf) atomicMin(target, m);
+  }
+  __syncthreads();
 }
 
-__device__ __forceinline__ void warp_sum_into_ll(long long v, long long* target) {
+// The block's sum into *target with one atomic per block (every thread of the block calls).
+__device__ __forceinline__ void block_sum_into(long long v, long long* target) {
+  __shared__ long long s_sum[kThreads / 32];
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0)
-    atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(v));
+  if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += s_sum[w];
+    if (t != 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(t));
+  }
+  __syncthreads();
 }
 
 // Rows are sorted into three classes when they join a frontier: light (up to 32 slots: their
@@ -803,7 +821,7 @@ __device__ int near_far(const SsspParams& p, Ctx& X, LoopState& S, unsigned& bar
       const u64 word = ld_cg(&p.packed[ld_cg(&far[i])]);
       if (word != kPackedInf) local = min(local, pk.dist(word));
     }
-    warp_min_into(local, &c->minimum);
+    block_min_into(local, &c->minimum);
     if (BLOCK) block_barrier();
     else if (!grid_barrier(c, bar)) return -1;
     S.threshold = max(S.threshold, ld_cg(reinterpret_cast<const u64*>(&c->minimum))) + delta;
@@ -935,8 +953,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         }
       }
     }
-    if (__any_sync(0xffffffffu, changed) && lane == 0) atomicOr(&c->changed, 1);
-    if (__any_sync(0xffffffffu, changed == 2) && lane == 0) atomicOr(&c->changed, 2);
+    {
+      // one atomic per block (not per warp) into the shared flag word
+      const int any1 = __syncthreads_or(changed != 0);
+      const int any2 = __syncthreads_or(changed == 2);
+      if (threadIdx.x == 0 && any1) atomicOr(&c->changed, any2 ? 3 : 1);
+    }
     unsigned roots_err = 0;
     if (!grid_barrier(c, bar, &roots_err)) return;
     if (roots_err) return;  // every block sees the same snapshot: all leave together
@@ -1004,7 +1026,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         if (!grid_barrier(c, bar)) return;
         for (int round = 0; round < max_rounds; ++round) {
           if (tid == 0) {
-            c->active[(round + 1) % 3] = 0;
             c->rounds = round + 1;
             if (round < 24) c->pj_t[round] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
           }
@@ -1109,14 +1130,21 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
             }
           }
           __syncthreads();
-          if (threadIdx.x == 0) {
-            p.pj_blk[(round & 1) * kPjMaxBlocks + blockIdx.x] = s_pj_cnt;
-            if (round < 24)
-              atomicMax(&c->pj_done[round], static_cast<unsigned>(global_ns() - c->phase_ns[0]));
-          }
-          if (__any_sync(0xffffffffu, jumping) && lane == 0) c->active[round % 3] = 1;
+          if (threadIdx.x == 0) p.pj_blk[(round & 1) * kPjMaxBlocks + blockIdx.x] = s_pj_cnt;
+          (void)jumping;
           if (!grid_barrier(c, bar)) return;
-          if (ld_cg(&c->active[round % 3]) == 0) break;
+          if (tid == 0 && round < 24)
+            c->pj_done[round] = static_cast<unsigned>(global_ns() - c->phase_ns[0]);
+          // every block reads the survivor counts itself: none left, the rounds are done (no
+          // flag that every warp with a survivor would store)
+          {
+            const int* cnt = p.pj_blk + (round & 1) * kPjMaxBlocks;
+            int mine = 0;
+            for (int q = threadIdx.x; q < nblk; q += blockDim.x) mine |= ld_cg(&cnt[q]);
+            const int any = __syncthreads_or(mine != 0);
+            if (tid == 0) c->active[round % 3] = any;  // the host's parent-cycle check
+            if (!any) break;
+          }
         }
       }
       if (tid == 0) c->phase_ns[2] = global_ns();
@@ -1190,7 +1218,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
       if (nd < pk.dist(old) && claim(p.stamp, v, gen_pull))
         staged_append(kStNext, p.frontier, &c->frontier_count, v);
     }
-    warp_sum_into_ll(w_inval, &c->invalidated);
+    block_sum_into(w_inval, &c->invalidated);
     if (!grid_barrier(c, bar)) return;
     if (tid == 0) c->phase_ns[4] = global_ns();
     // ---- pull pass (fused.cuh:258-285): every candidate takes its best in-neighbour ----------
@@ -1220,7 +1248,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
     const u64 word = ld_cg(&p.packed[ld_cg(&p.frontier[i])]);
     if (word != kPackedInf) local = min(local, pk.dist(word));
   }
-  warp_min_into(local, &c->minimum);
+  block_min_into(local, &c->minimum);
   if (!grid_barrier(c, bar)) return;
   const u64 smallest = ld_cg(reinterpret_cast<const u64*>(&c->minimum));
   X.threshold = (smallest == kPackedInf ? 0 : smallest) + delta;
@@ -1362,24 +1390,38 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
         affected += (ld_cg(&p.candidates[v]) != 0 || ld_cg(&p.ancestor[v]) != ld_cg(&p.parent[v]));
     }
   }
-  warp_sum_into_ll(affected, &c->affected);
-  warp_sum_into_ll(w_visits, &c->work[0]);
-  warp_sum_into_ll(w_jumps, &c->work[1]);
-  warp_sum_into_ll(static_cast<long long>(pull_rows), &c->work[3]);
-  warp_sum_into_ll(static_cast<long long>(pull_slots), &c->work[4]);
-  warp_sum_into_ll(static_cast<long long>(pull_words), &c->work[5]);
-  warp_sum_into_ll(static_cast<long long>(X.rows), &c->work[6]);
-  warp_sum_into_ll(static_cast<long long>(X.slots), &c->work[7]);
-  warp_sum_into_ll(static_cast<long long>(X.words), &c->work[8]);
-  warp_sum_into_ll(static_cast<long long>(X.atomics), &c->work[9]);
-  warp_sum_into_ll(static_cast<long long>(X.tries), &c->work[12]);
-  warp_sum_into_ll(static_cast<long long>(X.appends), &c->work[10]);
-  warp_sum_into_ll(static_cast<long long>(unpacked), &c->work[11]);
-  warp_sum_into_ll(static_cast<long long>(pull_atomics), &c->work[23]);
-  warp_sum_into_ll(static_cast<long long>(pull_appends), &c->work[24]);
-  warp_sum_into_ll(static_cast<long long>(pair_visits), &c->work[25]);
-  warp_sum_into_ll(static_cast<long long>(walk_rows), &c->work[26]);
-  warp_sum_into_ll(static_cast<long long>(walk_slots), &c->work[27]);
+  // the work counters, one atomic per block and counter
+  {
+    __shared__ BlockRed red;
+    red_sum(red, 0, affected);
+    red_sum(red, 1, w_visits);
+    red_sum(red, 2, w_jumps);
+    red_sum(red, 3, pull_rows);
+    red_sum(red, 4, pull_slots);
+    red_sum(red, 5, pull_words);
+    red_sum(red, 6, X.rows);
+    red_sum(red, 7, X.slots);
+    red_sum(red, 8, X.words);
+    red_sum(red, 9, X.atomics);
+    red_sum(red, 10, X.tries);
+    red_sum(red, 11, X.appends);
+    red_sum(red, 12, unpacked);
+    red_sum(red, 13, pull_atomics);
+    red_sum(red, 14, pull_appends);
+    red_sum(red, 15, pair_visits);
+    red_sum(red, 16, walk_rows);
+    red_sum(red, 17, walk_slots);
+    __syncthreads();
+    if (threadIdx.x < 18) {
+      // reduction slot -> work counter (slot 0: affected)
+      const int w = threadIdx.x < 10 ? static_cast<int>(threadIdx.x) - 1 + (threadIdx.x >= 3 ? 1 : 0)
+                                     : (threadIdx.x == 10 ? 12 : (threadIdx.x == 11 ? 10 : (threadIdx.x == 12 ? 11 : static_cast<int>(threadIdx.x) + 10)));
+      const long long t = red_total(red, threadIdx.x);
+      long long* target = threadIdx.x == 0 ? &c->affected : &c->work[w];
+      if (t != 0)
+        atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(t));
+    }
+  }
   if (tid == 0) {
     c->work[2] = ld_cg(&c->invalidated);  // complete: summed before the heads' barrier
     c->phase_ns[7] = global_ns();
