@@ -485,6 +485,8 @@ def main():
             for i, name in enumerate(timed_stats[0].WORK_NAMES)}
     phases = {name: round(float(np.mean([s.phase_ms[i] for s in timed_stats])), 3)
               for i, name in enumerate(timed_stats[0].PHASES)}
+    stages = {name: round(float(np.mean([s.stages_ms()[name] for s in timed_stats])), 4)
+              for name in timed_stats[0].stages_ms()}
     shape = {k: float(np.mean([getattr(s, k) for s in timed_stats]))
              for k in ("iterations", "epochs", "pushes", "invalidated", "affected", "rounds",
                        "touched", "delta", "grid_blocks")}
@@ -544,7 +546,8 @@ def main():
                        "sssp_ms_mean": summ[args.schedule]["sssp_ms_mean"],
                        "host_ms_p50": 1000 * float(np.percentile(head.host, 50)),
                        "schedules": compare, "learned_classes": classes,
-                       "sssp_phases_ms": phases, "sssp_work": work, "update_shape": shape,
+                       "sssp_phases_ms": phases, "stages_ms": stages, "sssp_work": work,
+                       "update_shape": shape,
                        "alg_bytes_per_update": float(np.mean(alg)),
                        "trace_last_update": [list(t) for t in timed_stats[-1].trace],
                        "pj_rounds_us_last_update": list(timed_stats[-1].pj_rounds_us),

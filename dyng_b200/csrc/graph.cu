@@ -20,8 +20,8 @@
 #include "internal.hpp"
 #include "grid_sync.cuh"
 #include "mlp_common.cuh"
+#include "scan.cuh"
 
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -1860,10 +1860,8 @@ void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in
   cap.reserve(static_cast<size_t>(n) + 1);
   start.reserve(static_cast<size_t>(n) + 1);
   long long top[2] = {0, 0};
-  size_t temp_bytes = 0;
-  DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
-  DevBuf<unsigned char> temp;
-  temp.reserve(temp_bytes);
+  DevBuf<long long> temp;
+  temp.reserve(static_cast<size_t>(scan_scratch(n + 1)));
   const long long demand[2] = {
       std::max(0LL, need_out - static_cast<long long>(g.host_counters.out_top)),
       std::max(0LL, need_in - static_cast<long long>(g.host_counters.in_top))};
@@ -1875,7 +1873,7 @@ void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in
                                             (side == 0 ? g.out_col : g.in_col).ptr, n,
                                             g.props.headroom, cap.ptr);
     DYNGB200_CUDA(cudaGetLastError());
-    DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(temp.ptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
+    ctx.launches += exclusive_scan(cap.ptr, start.ptr, n + 1, temp.ptr, s);
     DYNGB200_CUDA(cudaMemcpyAsync(&top[side], start.ptr + n, sizeof(long long),
                                   cudaMemcpyDeviceToHost, s));
     DYNGB200_CUDA(cudaStreamSynchronize(s));
@@ -1910,7 +1908,7 @@ void graph_compact(Context& ctx, Graph& g, long long need_out, long long need_in
     DYNGB200_CUDA(cudaMemsetAsync(cap.ptr + n, 0, sizeof(long long), s));
     ctx.launches += 2;
     k_compact_count<<<grid, kBlock, 0, s>>>(desc, col.ptr, n, g.props.headroom, cap.ptr);
-    DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(temp.ptr, temp_bytes, cap.ptr, start.ptr, n + 1, s));
+    ctx.launches += exclusive_scan(cap.ptr, start.ptr, n + 1, temp.ptr, s);
     DYNGB200_CUDA(cudaMemsetAsync(ncol[side].ptr, 0xff,
                                   static_cast<size_t>(arena) * sizeof(int32_t), s));
     k_compact_copy<<<grid, kBlock, 0, s>>>(desc, (side == 0 ? g.out_cap : g.in_cap).ptr,

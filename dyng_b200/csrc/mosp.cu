@@ -21,8 +21,8 @@
 //      copied into the caller's host buffer when read (path_costs() is host memory, as in the
 //      reference).
 #include "handles.hpp"
+#include "scan.cuh"
 
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -265,7 +265,7 @@ struct Mosp {
   // scratch of the finalize step
   DevBuf<int> out_count, fill, anc[2], missing;
   DevBuf<long long> cap, start;
-  DevBuf<unsigned char> scan_temp;
+  DevBuf<long long> scan_temp;  // tile totals of the out-row scan
   DevBuf<unsigned long long> totals;
   DevBuf<unsigned> first;
   DevBuf<int64_t> acc[2];
@@ -428,10 +428,7 @@ FinalizeCounts mosp_finalize(Context& ctx, Graph& g, Mosp& m, bool count_affecte
   m.cap.reserve(static_cast<size_t>(n_cap) + 1);
   m.start.reserve(static_cast<size_t>(n_cap) + 1);
   m.totals.reserve(2);
-  size_t temp_bytes = 0;
-  DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, m.cap.ptr, m.start.ptr,
-                                              n_cap + 1, s));
-  m.scan_temp.reserve(std::max<size_t>(temp_bytes, 1));
+  m.scan_temp.reserve(static_cast<size_t>(scan_scratch(n_cap + 1)));
   DYNGB200_CUDA(cudaMemsetAsync(m.out_count.ptr, 0, n_cap * sizeof(int), s));
   DYNGB200_CUDA(cudaMemsetAsync(m.totals.ptr, 0, 2 * sizeof(unsigned long long), s));
   DYNGB200_CUDA(cudaMemsetAsync(m.cap.ptr + n_cap, 0, sizeof(long long), s));
@@ -449,8 +446,7 @@ FinalizeCounts mosp_finalize(Context& ctx, Graph& g, Mosp& m, bool count_affecte
   const GraphView cv = cg.view();
   k_mosp_in_rows<<<grid, kMospBlock, 0, s>>>(in, cv, stride, n_cap, m.out_count.ptr, m.totals.ptr);
   k_mosp_out_caps<<<grid, kMospBlock, 0, s>>>(m.out_count.ptr, n_cap, m.cap.ptr);
-  DYNGB200_CUDA(cub::DeviceScan::ExclusiveSum(m.scan_temp.ptr, temp_bytes, m.cap.ptr, m.start.ptr,
-                                              n_cap + 1, s));
+  ctx.launches += exclusive_scan(m.cap.ptr, m.start.ptr, n_cap + 1, m.scan_temp.ptr, s);
   k_mosp_out_desc<<<grid, kMospBlock, 0, s>>>(cv, m.out_count.ptr, m.start.ptr, n_cap, m.fill.ptr);
   k_mosp_out_fill<<<grid, kMospBlock, 0, s>>>(cv, n, m.fill.ptr);
   ctx.launches += 5;

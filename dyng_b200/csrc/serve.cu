@@ -4,17 +4,22 @@
 // - Requests wait in per-graph FIFO queues, so the batches of one graph apply in arrival order
 //   and every result is the one the same batches would give alone, one after the other.  A graph
 //   is in at most one round at a time.
-// - Two lanes, each a dispatcher thread with its own stream.  The small lane runs rounds of small
-//   batches: the oldest waiting request of every free graph (round-robin), all of their updates
-//   queued on the lane's stream before one wait (sssp_update_begin / sssp_update_end), so the
-//   host work of one update overlaps the GPU work of the previous ones and a round needs one
-//   host-device synchronisation.  The large lane runs one large batch at a time.
+// - Lanes, each a dispatcher thread with its own stream: one large lane and one or more small
+//   lanes.  A small lane runs rounds of small batches: the oldest waiting request of every free
+//   graph (round-robin), all of their updates queued on the lane's stream before one wait
+//   (sssp_update_begin / sssp_update_end), so the host work of one update overlaps the GPU work of
+//   the previous ones and a round needs one host-device synchronisation.  The large lane runs one
+//   large batch at a time.
 // - The persistent kernel holds every SM it is given, so a small batch behind a large one would
 //   wait for all of it.  While the large lane runs, its persistent grid is capped at (occupancy -
 //   1) blocks per SM and the small lane's at one block per SM: the two grids together fill the
 //   SMs' block slots exactly, so both are co-resident whatever the order of their blocks (no grid
-//   barrier can wait on a block that has no slot).  A small round that starts while the large
-//   lane is idle takes the whole grid, and a large batch waits for such a round to end first.
+//   barrier can wait on a block that has no slot).  With one small lane, a small round that
+//   starts while the large lane is idle takes the whole grid, and a large batch waits for such a
+//   round to end first.  With several small lanes the one-block-per-SM layer is split between
+//   them in fixed shares: small batches of different graphs run side by side, each on the same
+//   grid whatever else runs (a steady service time), and the grids of all lanes still sum to the
+//   block slots.
 // - Admission by free HBM: a graph is registered only if its workspace fits beside the reserve,
 //   and a batch is dispatched only if its estimated scratch fits in the free device memory beyond
 //   the reserve; otherwise it fails with OUT_OF_MEMORY instead of taking the device down.
@@ -27,6 +32,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -42,10 +48,60 @@ using Clock = std::chrono::steady_clock;
 
 struct ServerGraph;
 
+// Page-locked host memory for the copies of queued batches: one slab of the back-pressure cap,
+// allocated when the server starts and carved first-fit (free extents kept sorted and merged), so
+// serving never asks the driver for host memory: a cudaMallocHost under load took milliseconds
+// and held up the other lanes' CUDA calls meanwhile.
+class PinnedSlab {
+ public:
+  void init(size_t ints) {
+    mem_.reserve(ints);
+    free_.clear();
+    free_[0] = mem_.count;
+  }
+  // Room for n int32 values (nullptr: no free extent is large enough).
+  int32_t* take(size_t n) {
+    n = round(n);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      const size_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > n) free_[off + n] = len - n;
+      return mem_.ptr + off;
+    }
+    return nullptr;
+  }
+  void give(int32_t* p, size_t n) {
+    n = round(n);
+    size_t off = static_cast<size_t>(p - mem_.ptr);
+    auto next = free_.lower_bound(off);
+    if (next != free_.end() && off + n == next->first) {  // merge with the extent after
+      n += next->second;
+      next = free_.erase(next);
+    }
+    if (next != free_.begin()) {  // merge with the extent before
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += n;
+        return;
+      }
+    }
+    free_[off] = n;
+  }
+  bool owns(const int32_t* p) const { return p >= mem_.ptr && p < mem_.ptr + mem_.count; }
+
+ private:
+  static size_t round(size_t n) { return (std::max<size_t>(n, 1) + 63) & ~static_cast<size_t>(63); }
+  HostBuf<int32_t> mem_;
+  std::map<size_t, size_t> free_;  // offset -> length, in int32 values
+};
+
 struct ServerRequest {
   uint64_t ticket = 0;
   int slot = 0;
-  std::unique_ptr<HostBuf<int32_t>> data;  // pinned copy of the batch's five arrays
+  int32_t* data = nullptr;   // pinned copy of the batch's five arrays (in the slab, or in `own`)
+  size_t data_n = 0;
+  std::unique_ptr<HostBuf<int32_t>> own;  // a batch larger than the slab: its own pinned copy
   dyngb200_batch batch{};
   long long ops = 0;
   Clock::time_point arrival, ready, start, begun, synced, finish;
@@ -82,18 +138,17 @@ class Server {
   void monitor();
   void dispatch(int lane, std::vector<ServerRequest*>& group, int cap);
   long long estimate_bytes(const ServerGraph& sg, const ServerRequest& r) const;
-  std::unique_ptr<HostBuf<int32_t>> take_buffer(size_t n);
-  void give_buffer(std::unique_ptr<HostBuf<int32_t>> b);
+  void release_copy(ServerRequest& r);  // the caller holds mu_
 
   dyngb200_server_config cfg_{};
   const Scheduler* learned_ = nullptr;
-  cudaStream_t streams_[2] = {nullptr, nullptr};  // the small lane's, the large lane's
+  std::vector<cudaStream_t> streams_;  // one per lane: the small lanes', then the large lane's
   std::vector<std::unique_ptr<ServerGraph>> graphs_;
   std::unordered_map<uint64_t, std::unique_ptr<ServerRequest>> requests_;
-  std::vector<std::unique_ptr<HostBuf<int32_t>>> pool_;
+  PinnedSlab slab_;
   std::mutex mu_;
   std::condition_variable work_cv_, done_cv_;
-  std::thread workers_[2];
+  std::vector<std::thread> workers_;
   std::thread monitor_;  // samples the free device memory for admission (off the dispatcher)
   std::condition_variable monitor_cv_;
   long long free_sample_ = -1;   // bytes free at the last sample (-1: none)
@@ -103,7 +158,9 @@ class Server {
   size_t next_graph_ = 0;  // round-robin start
   // lanes: 1 until the first graph shows the GPU holds two persistent grids side by side
   int lanes_ = 1;
-  int full_blocks_ = 0, small_blocks_ = 0;  // persistent grid: whole, the small lane's share
+  int want_lanes_ = 2;  // the configured lanes (small ones plus the large one)
+  int full_blocks_ = 0, small_blocks_ = 0;  // persistent grid: whole, the small lanes' layer
+  std::vector<int> small_cap_;  // with several small lanes: each one's share of the layer
   bool large_running_ = false;  // the large lane's round is in flight
   bool large_wants_ = false;    // a large batch waits for a whole-grid small round to end
   bool small_full_ = false;     // a small round runs on the whole grid
@@ -111,6 +168,7 @@ class Server {
   long long held_bytes_ = 0;  // pinned copies of queued batches (submit waits above the cap)
   static constexpr long long kHeldCap = 1LL << 30;
   static constexpr double kLargeMaxWaitMs = 5.0;  // a large batch waits at most this long
+  static constexpr int kMaxLanes = 8;
   dyngb200_server_info info_{};
 };
 
@@ -136,13 +194,18 @@ Server::Server(const dyngb200_server_config& cfg, const Scheduler* learned)
   if (cfg_.hbm_reserve_bytes <= 0) cfg_.hbm_reserve_bytes = 1LL << 30;
   expects(!learned_ || learned_->device == cfg_.device,
           "server: the scheduler belongs to another device");
-  expects(cfg_.lanes >= 0 && cfg_.lanes <= 2, "server: lanes is 0, 1 or 2");
+  expects(cfg_.lanes >= 0 && cfg_.lanes <= kMaxLanes,
+          "server: lanes is 0 (two), 1 or up to " + std::to_string(kMaxLanes));
+  want_lanes_ = cfg_.lanes == 0 ? 2 : cfg_.lanes;
   DYNGB200_CUDA(cudaSetDevice(cfg_.device));
+  streams_.assign(static_cast<size_t>(want_lanes_), nullptr);
+  slab_.init(static_cast<size_t>(kHeldCap / sizeof(int32_t)));
   for (auto& st : streams_) DYNGB200_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   size_t free_b = 0, total_b = 0;
   DYNGB200_CUDA(cudaMemGetInfo(&free_b, &total_b));
   free_sample_ = static_cast<long long>(free_b);
-  for (int lane = 0; lane < 2; ++lane) workers_[lane] = std::thread([this, lane] { run(lane); });
+  for (int lane = 0; lane < want_lanes_; ++lane)
+    workers_.emplace_back([this, lane] { run(lane); });
   monitor_ = std::thread([this] { monitor(); });
 }
 
@@ -220,34 +283,22 @@ int Server::add_graph(Graph& g, Tree& t) {
   if (graphs_.empty()) {
     full_blocks_ = per_sm * sg->ctx->sm_count;
     small_blocks_ = sg->ctx->sm_count;
-    lanes_ = cfg_.lanes != 1 && per_sm >= 2 ? 2 : 1;
+    lanes_ = want_lanes_ >= 2 && per_sm >= 2 ? want_lanes_ : 1;
+    // several small lanes share the one-block-per-SM layer in equal parts
+    const int small_lanes = lanes_ - 1;
+    small_cap_.assign(static_cast<size_t>(std::max(small_lanes, 1)), small_blocks_);
+    if (small_lanes > 1)
+      for (int l = 0; l < small_lanes; ++l)
+        small_cap_[l] = small_blocks_ / small_lanes + (l < small_blocks_ % small_lanes ? 1 : 0);
   }
   graphs_.push_back(std::move(sg));
   return static_cast<int>(graphs_.size()) - 1;
 }
 
-std::unique_ptr<HostBuf<int32_t>> Server::take_buffer(size_t n) {
-  std::unique_lock<std::mutex> lk(mu_);
-  size_t best = pool_.size();
-  for (size_t i = 0; i < pool_.size(); ++i)
-    if (pool_[i]->count >= n && (best == pool_.size() || pool_[i]->count < pool_[best]->count))
-      best = i;
-  if (best < pool_.size()) {
-    auto b = std::move(pool_[best]);
-    pool_.erase(pool_.begin() + static_cast<long>(best));
-    return b;
-  }
-  lk.unlock();
-  auto b = std::make_unique<HostBuf<int32_t>>();
-  size_t cap = 1024;
-  while (cap < n) cap *= 2;
-  b->reserve(cap);
-  return b;
-}
-
-void Server::give_buffer(std::unique_ptr<HostBuf<int32_t>> b) {
-  std::unique_lock<std::mutex> lk(mu_);
-  if (pool_.size() < 64) pool_.push_back(std::move(b));
+void Server::release_copy(ServerRequest& r) {
+  if (r.data && slab_.owns(r.data)) slab_.give(r.data, r.data_n);
+  r.data = nullptr;
+  r.own.reset();
 }
 
 uint64_t Server::submit(int slot, const dyngb200_batch& b) {
@@ -263,18 +314,28 @@ uint64_t Server::submit(int slot, const dyngb200_batch& b) {
   const long long ni = b.num_insertions, nd = b.num_deletions;
   const int k = b.num_weights > 0 ? b.num_weights : 0;
   const size_t total = static_cast<size_t>(2 * ni + ni * k + 2 * nd);
-  {
-    // backpressure: queued batches hold at most kHeldCap bytes of pinned copies
-    std::unique_lock<std::mutex> lk(mu_);
-    const long long want = static_cast<long long>(total * sizeof(int32_t));
-    done_cv_.wait(lk, [&] { return held_bytes_ == 0 || held_bytes_ + want <= kHeldCap; });
-    held_bytes_ += want;
-  }
   const long long bytes = static_cast<long long>(total * sizeof(int32_t));
+  {
+    // backpressure: queued batches hold at most kHeldCap bytes of pinned copies, all in the
+    // slab (waiting for room when the free extents are too small); a batch larger than the slab
+    // gets a copy of its own once nothing else is held
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] {
+      if (held_bytes_ > 0 && held_bytes_ + bytes > kHeldCap) return false;
+      r->data = slab_.take(total);
+      return r->data != nullptr || held_bytes_ == 0;
+    });
+    held_bytes_ += bytes;
+  }
   uint64_t ticket = 0;
   try {
-    r->data = take_buffer(total);
-    int32_t* p = r->data->ptr;
+    if (!r->data) {
+      r->own = std::make_unique<HostBuf<int32_t>>();
+      r->own->reserve(total);
+      r->data = r->own->ptr;
+    }
+    r->data_n = total;
+    int32_t* p = r->data;
     auto put = [&](const int32_t* src, long long count) {
       if (count > 0) {
         if (b.memory == DYNGB200_DEVICE)
@@ -306,7 +367,8 @@ uint64_t Server::submit(int slot, const dyngb200_batch& b) {
   } catch (...) {
     std::unique_lock<std::mutex> lk(mu_);
     held_bytes_ -= bytes;
-    if (r && r->data && pool_.size() < 64) pool_.push_back(std::move(r->data));
+    if (r) release_copy(*r);
+    done_cv_.notify_all();
     throw;
   }
   work_cv_.notify_all();  // either lane may be the one that takes it
@@ -389,8 +451,7 @@ bool Server::take_round(int lane, std::vector<ServerRequest*>& group, int& cap) 
       r->done = true;
       ++info_.failed;
       held_bytes_ -= held_of(*r);
-      if (pool_.size() < 64) pool_.push_back(std::move(r->data));
-      r->data.reset();
+      release_copy(*r);
       failed = true;
       return;
     }
@@ -423,11 +484,15 @@ bool Server::take_round(int lane, std::vector<ServerRequest*>& group, int& cap) 
         ms_between(graphs_[oldest_large]->queue.front()->arrival, Clock::now()) > kLargeMaxWaitMs;
     if (!overdue) small_heads();
     if (group.empty() && !failed && oldest_large < ng) take(oldest_large);
-  } else if (lane == 0) {
+  } else if (lane < lanes_ - 1) {
     small_heads();
     if (!group.empty()) {
-      cap = large_running_ || large_wants_ ? small_blocks_ : 0;
-      small_full_ = cap == 0;
+      if (lanes_ == 2) {
+        cap = large_running_ || large_wants_ ? small_blocks_ : 0;
+        small_full_ = cap == 0;
+      } else {
+        cap = small_cap_[lane];
+      }
     }
   } else {
     if (oldest_large == ng) {
@@ -473,7 +538,7 @@ void Server::run(int lane) {
         ++info_.rounds;
         info_.max_group =
             std::max<long long>(info_.max_group, static_cast<long long>(group.size()));
-        if (lanes_ == 2 && lane == 1) large_running_ = false;
+        if (lanes_ >= 2 && lane == lanes_ - 1) large_running_ = false;
         if (lanes_ == 2 && lane == 0) small_full_ = false;
       }
     }
@@ -531,9 +596,9 @@ void Server::dispatch(int lane, std::vector<ServerRequest*>& group, int cap) {
     pending[i].reset();
     sg.ctx->max_update_blocks = 0;
     const long long bytes = held_of(*r);
-    give_buffer(std::move(r->data));
     r->finish = Clock::now();
     std::unique_lock<std::mutex> lk(mu_);
+    release_copy(*r);
     held_bytes_ -= bytes;
     sg.busy = false;
     r->done = true;  // a waiter may take (and free) the request from here on

@@ -55,8 +55,8 @@ class Server:
 
     def wait(self, ticket: int):
         """(Stats, times) of a request; raises its update's error.  times: queued_ms,
-        service_ms, total_ms, group_size, begin_ms, round_ms, copy_ms, lane (1: the large
-        lane)."""
+        service_ms, total_ms, group_size, begin_ms, round_ms, copy_ms, lane (lanes - 1: the
+        large lane)."""
         st = N.Stats()
         tm = N.RequestTimes()
         check(N.lib().dyngb200_server_wait(self._h, int(ticket), ctypes.byref(st),
@@ -175,15 +175,43 @@ def summarize(done, wall, rate):
             "by_size": by_size(done)}
 
 
+def graph_waits(done):
+    """Per request: how long it waited for its own graph's earlier requests to finish (the
+    batches of one graph apply in arrival order, so a request cannot start before its
+    predecessor on the same graph is done).  Records are in completion order; submission times
+    (submitted_s) order them per graph."""
+    wait = [0.0] * len(done)
+    by_graph = {}
+    for i, d in enumerate(done):
+        by_graph.setdefault(d[0], []).append(i)
+    for idx in by_graph.values():
+        idx.sort(key=lambda i: done[i][9])
+        prev_finish = -1.0
+        for i in idx:
+            submit_ms = done[i][9] * 1000.0
+            wait[i] = max(0.0, prev_finish - submit_ms)
+            prev_finish = max(prev_finish, submit_ms + done[i][2])
+    return wait
+
+
 def by_size(done):
     """p50 / p99 latency per decade of batch size (the load mixes 100 .. 1M changes, whose own
-    service times differ by 10x, so the overall p99 / p50 mostly measures the mix)."""
+    service times differ by 10x, so the overall p99 / p50 mostly measures the mix); `own_*`
+    leaves out the wait for the same graph's earlier requests (graph_waits): the latency the
+    serving loop adds to the order it must keep."""
     out = {}
+    gw = graph_waits(done)
     for lo in (100, 1_000, 10_000, 100_000):
-        lat = [d[2] for d in done if lo <= d[1] < lo * 10 or (lo == 100_000 and d[1] >= lo)]
-        if lat:
+        sel = [i for i, d in enumerate(done)
+               if lo <= d[1] < lo * 10 or (lo == 100_000 and d[1] >= lo)]
+        if sel:
+            lat = [done[i][2] for i in sel]
+            own = [done[i][2] - gw[i] for i in sel]
             out[f"{lo}+"] = {"n": len(lat), "p50_ms": float(np.percentile(lat, 50)),
-                             "p99_ms": float(np.percentile(lat, 99))}
+                             "p99_ms": float(np.percentile(lat, 99)),
+                             "own_p50_ms": float(np.percentile(own, 50)),
+                             "own_p99_ms": float(np.percentile(own, 99)),
+                             "graph_wait_p99_ms": float(np.percentile([gw[i] for i in sel], 99))}
     return out
 
 
@@ -210,7 +238,8 @@ def main(argv=None):
     ap.add_argument("--small-changes", type=int, default=65536,
                     help="batches up to this many changes run in the small lane's rounds")
     ap.add_argument("--lanes", type=int, default=2,
-                    help="2: large batches on their own lane beside small rounds; 1: one lane")
+                    help="2: large batches on their own lane beside small rounds; 1: one lane; "
+                         "3..8: lanes - 1 small lanes side by side beside the large one")
     a = ap.parse_args(argv)
     rng = np.random.default_rng(a.seed)
     res = Resources(0)

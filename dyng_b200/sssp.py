@@ -173,6 +173,23 @@ class Stats:
     def algorithmic_bytes(self) -> int:
         return int(sum(a * b for a, b in zip(self.work, self.WORK_BYTES)))
 
+    # The reference's profiler stages (parity/timed_regions/sssp.toml) -> this update's device
+    # times: the commit is the batch applier (the in-edge mirror is kept in place inside it, so
+    # graph.transpose has no time of its own), and the sssp kernel's phases map onto the stages
+    # of the update's Steps 1 and 2.
+    STAGES = {"sssp.identify_affected": (0, 1, 2), "sssp.seed": (3, 4), "sssp.loop": (5,),
+              "sssp.finalize": (6,)}
+
+    def stages_ms(self) -> dict:
+        """Device time (ms) under the reference's profiler stage names (sssp.update >
+        sssp.commit > graph.apply, sssp.identify_affected, sssp.seed, sssp.loop, sssp.finalize)."""
+        ms = self.phase_ms
+        out = {"sssp.update": self.apply_ms + self.sssp_ms, "sssp.commit": self.apply_ms,
+               "graph.apply": self.apply_ms, "graph.transpose": 0.0}
+        for name, phases in self.STAGES.items():
+            out[name] = float(sum(ms[i] for i in phases))
+        return out
+
     def phase_bytes_ms(self) -> dict:
         """Per phase of the kernel: (algorithmic bytes, device ms).  The unpack also counts the
         12 bytes it writes per affected vertex."""

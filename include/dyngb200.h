@@ -443,7 +443,10 @@ typedef struct dyngb200_server_config {
   int64_t hbm_reserve_bytes; /* device memory admission keeps free (0: 1 GiB) */
   int32_t lanes;             /* 0 or 2: large batches run on their own lane, on two thirds of the
                                 SMs' block slots, beside rounds of small ones on the rest;
-                                1: one lane (a large batch holds every SM while it runs) */
+                                1: one lane (a large batch holds every SM while it runs);
+                                3..8: lanes - 1 small lanes share the rest in fixed parts, so
+                                small batches of different graphs run side by side (the large
+                                lane is lane lanes - 1) */
 } dyngb200_server_config;
 typedef struct dyngb200_request_times {
   double queued_ms;   /* submit -> dispatch */

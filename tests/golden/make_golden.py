@@ -175,4 +175,8 @@ def combined(data):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DYNG_REFERENCE")
+    if not root:
+        sys.exit("usage: python tests/golden/make_golden.py <dynG source tree> "
+                 "(or set DYNG_REFERENCE)")
+    main(root)

@@ -44,7 +44,7 @@ def _alone(spec, batches):
     return out, t.distances, t.parents
 
 
-@pytest.mark.parametrize("lanes", [1, 2])
+@pytest.mark.parametrize("lanes", [1, 2, 4])
 @pytest.mark.parametrize("learned", [False, True])
 def test_mix_equals_alone(learned, lanes):
     work = _workload(3)
@@ -87,16 +87,25 @@ def test_mix_equals_alone(learned, lanes):
         assert np.array_equal(t.distances, dist) and np.array_equal(t.parents, par)
     groups = [tm["group_size"] for i in results for _, tm in results[i]]
     assert info["completed"] == sum(len(b) for _, b in work) and info["failed"] == 0
-    assert max(groups) >= 2  # small batches of different graphs shared rounds
-    ran_large = [tm["lane"] for i in results for _, tm in results[i]]
+    lanes_used = [tm["lane"] for i in results for _, tm in results[i]]
+    if lanes <= 2:
+        assert max(groups) >= 2  # small batches of different graphs shared rounds
+    else:
+        # small batches of different graphs ran side by side on the small lanes
+        assert len({ln for ln in lanes_used if ln < lanes - 1}) >= 2
     assert info["lanes"] == lanes
-    if lanes == 2:
-        # the 20000-change batches ran on the large lane, everything else on the small one
+    if lanes >= 2:
+        # the 20000-change batches ran on the large lane (the last), everything else on the
+        # small ones
         sizes = [len(b["ins_src"]) + len(b["del_src"]) for _, bs in work for b in bs]
         assert info["large_rounds"] == sum(z > 10000 for z in sizes) > 0
-        assert sum(ran_large) == info["large_rounds"]
+        assert sum(ln == lanes - 1 for ln in lanes_used) == info["large_rounds"]
+        assert all((ln == lanes - 1) == (z > 10000) for ln, z in
+                   zip([tm["lane"] for i in sorted(results) for _, tm in results[i]],
+                       [len(b["ins_src"]) + len(b["del_src"]) for i in sorted(results)
+                        for b in work[i][1]]))
     else:
-        assert not any(ran_large) and info["large_rounds"] == 0
+        assert not any(lanes_used) and info["large_rounds"] == 0
     assert all(tm["total_ms"] >= tm["service_ms"] >= 0 for i in results for _, tm in results[i])
     server.close()
 

@@ -14,7 +14,8 @@ import pytest
 from dyng_b200 import mosp_io as io
 from tests.helpers import combined_case, fixture_case
 
-REFERENCE_DATA = os.path.join(os.environ.get("DYNG_REFERENCE", "/root/reference"),
+# the reference's fixture tree, when DYNG_REFERENCE names a dynG source tree (else skipped)
+REFERENCE_DATA = os.path.join(os.environ.get("DYNG_REFERENCE", "/nonexistent"),
                               "cpp", "tests", "data")
 REFERENCE_FIXTURES = os.path.join(REFERENCE_DATA, "mosp_sssp")
 
