@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--grid-blocks", type=int, default=0)
     ap.add_argument("--heavy-degree", type=int, default=0)
     ap.add_argument("--small", type=int, default=0, help="small-frontier size (0 default, -1 off)")
+    ap.add_argument("--engine", default="automatic", choices=["automatic", "fused", "operators"],
+                    help="sssp options.cuda_engine (automatic: fused with cooperative launch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-verify", action="store_true")
     return ap.parse_args()
@@ -388,7 +390,8 @@ def main():
     t0 = time.time()
     g = D.Graph.from_csr(rp, col, w, resources=res)
     source = source_of(args)
-    tree = D.sssp.compute(g, source)
+    options = D.sssp.Options(cuda_engine=args.engine)
+    tree = D.sssp.compute(g, source, options)
     build_s = time.time() - t0
     # the oracle replay (CPU leg, rank 0) starts from its own compute and checks it against this
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
@@ -464,7 +467,7 @@ def main():
     verified = None
     compute_info = None
     if not args.no_verify:
-        fresh, cst = D.sssp.compute(g, source, stats=True)
+        fresh, cst = D.sssp.compute(g, source, options, stats=True)
         verified = bool(np.array_equal(fresh.distances, tree.distances) and
                         np.array_equal(fresh.parents, tree.parents))
         # the same kernel on bulk work: a from-scratch solve of the final graph
@@ -478,6 +481,7 @@ def main():
     # roofline of the dominant kernel (the sssp persistent kernel): algorithmic bytes counted by
     # the kernel (Stats.work x Stats.WORK_BYTES) over its CUDA-event time on the launching stream
     sssp_ms = [s.sssp_ms for s in timed_stats]
+    engine = timed_stats[0].engine_used
     peak, peak_kind = peaks()
     alg = [s.algorithmic_bytes + 12 * s.affected for s in timed_stats]
     achieved = float(np.sum(alg) / (np.sum(sssp_ms) / 1000.0) / 1e9) if sssp_ms else 0.0
@@ -538,7 +542,8 @@ def main():
                        "vertices": int(edges.num_vertices), "edges": int(edges.src.size),
                        "batch_changes": args.batch, "insert_fraction": insert_fraction(args),
                        "source": source,
-                       "schedule": args.schedule, "parallelism": f"replicas{world}",
+                       "schedule": args.schedule, "engine": engine,
+                       "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (graph arenas ~1 GB)",
                        "p50_ms": summ[args.schedule]["p50_ms"],
                        "p99_ms": summ[args.schedule]["p99_ms"],
@@ -562,8 +567,12 @@ def main():
                     "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
             "gpu_launches": int(sum(s.kernel_launches for s in timed_stats)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if peak else None, "traffic": traffic(args),
-                         "peak_kind": peak_kind, "kernel": "k_sssp", "phases": phase_roof},
+                         "frac": achieved / peak if peak else None,
+                         "traffic": traffic(args) if engine == "fused" else None,
+                         "peak_kind": peak_kind,
+                         "kernel": "k_sssp" if engine == "fused" else
+                                   "k_op_* (the operators engine's launches and host steps)",
+                         "phases": phase_roof},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

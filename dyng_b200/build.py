@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdyngb200.so")
-SOURCES = ["memory.cu", "graph.cu", "sssp.cu", "mlp.cu", "capi.cu", "serve.cu", "mosp.cu"]
+SOURCES = ["memory.cu", "graph.cu", "sssp.cu", "operators.cu", "mlp.cu", "capi.cu", "serve.cu", "mosp.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

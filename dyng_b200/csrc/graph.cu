@@ -1351,6 +1351,75 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch 
   }
 }
 
+// ---- the applier as ordinary launches, one per step ----------------------------------------------
+// The same steps A-J for a device without cooperative launch and for the operators engine: the
+// end of a launch stands in for each grid barrier.  Every launch but the first two starts by
+// reading the error word and the capacity check of the plan, which all its blocks see alike (the
+// previous launch has finished), so an error stops the sequence at the same step as the fused
+// kernel's barrier snapshot does.  The plan (and the scheduler's inference) runs as a launch of
+// one block; `mark` >= 0 records the end of the previous step in apply_ns[mark].
+enum ApplyStep {
+  kStepValidate, kStepPlan, kStepPairs, kStepMatch, kStepResolve, kStepRowOffsets,
+  kStepFillSegments, kStepSortSegments, kStepAlloc, kStepMutate, kStepMoveAppend, kStepRows,
+  kStepFinalize
+};
+
+__global__ void __launch_bounds__(kBlock, 3) k_apply_step(ApplyParams p, ApplyLaunch L, int step,
+                                                          int mark) {
+  __shared__ ApplySmem sm;
+  __shared__ BlockRed red;
+  UpdateCtl* c = p.ctl;
+  const long long tid = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long threads = static_cast<long long>(gridDim.x) * blockDim.x;
+  if (tid == 0 && mark >= 0 && mark < 12) c->apply_ns[mark] = global_ns();
+  if (step == kStepValidate) {
+    ph_clear(p, tid, threads);
+    ph_validate(p, red, tid, threads);
+    return;
+  }
+  if (step == kStepPlan) {
+    if (threadIdx.x == 0) ph_plan(p);
+    if (L.infer_on) {
+      __syncthreads();
+      infer_schedule_block(L.infer, c, p.g.counters, p.ni, p.nd, sm.infer);
+    }
+    return;
+  }
+  if (gs_ld_volatile(&c->error) != 0 || max(c->n_after, c->n_old) > p.g.n_cap) return;
+  switch (step) {
+    case kStepPairs: ph_pairs(p, sm.pairs, red, tid, threads); break;
+    case kStepMatch:
+      if (p.g.allow_multi) ph_scan_multi(p, tid, threads);
+      else ph_match(p, tid, threads);
+      break;
+    case kStepResolve: ph_resolve(p, red, tid, threads); break;
+    case kStepRowOffsets: ph_row_offsets(p, p.seg_offsets, tid, threads); break;
+    case kStepFillSegments: ph_fill_segments(p, p.seg_offsets, p.seg, tid, threads); break;
+    case kStepSortSegments: ph_sort_segments(p, p.seg_offsets, p.seg, tid, threads); break;
+    case kStepAlloc: ph_alloc(p, red, tid, threads); break;
+    case kStepMutate:
+      // past the allocation step with no error: the graph is about to change
+      if (tid == 0) c->committing = 1;
+      ph_mutate(p, red, tid, threads);
+      break;
+    case kStepMoveAppend:
+      ph_move(p, tid, threads);
+      ph_append(p, red, tid, threads);
+      break;
+    case kStepRows:
+      ph_rows_final(p, red, tid, threads);
+      ph_count_written_max(p, red, tid, threads);
+      break;
+    case kStepFinalize:
+      if (tid == 0) {
+        ph_finalize(p);
+        c->apply_ns[11] = global_ns();
+      }
+      break;
+    default: break;
+  }
+}
+
 int grid_for(long long work, int block, int sm_count) {
   long long g = (work + block - 1) / block;
   const long long cap = static_cast<long long>(sm_count) * 8;
@@ -1434,6 +1503,8 @@ ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int object
 // ------------------------------------------------------------------------------------------------
 void Workspace::reserve_vertices(long long n_cap, cudaStream_t s) {
   pj_blk.reserve(2 * kPjMaxBlocks, s);
+  op_counts.reserve(4, s);
+  op_host.reserve(4);
   if (n_cap <= n_sized) return;
   // buffers are released before they are reallocated: until every one is back, the workspace
   // counts as unsized (a failed allocation makes the next call start over, never skip)
@@ -2087,14 +2158,16 @@ static int apply_blocks_per_sm(Context& ctx) {
   return ctx.apply_blocks_per_sm;
 }
 
-// The batch applier (Steps A-J), queued on ctx.stream as one cooperative launch; the caller reads
-// the control block once at the end.  `objective` >= 0 also records the sssp change
-// classification for that weight column and the plan (packing, default width); tree arrays are
-// not touched.  With `tree` and a scheduler (or a schedule asking for features), block 0 of the
-// launch computes the batch features and the schedule into the control block.
+// The batch applier (Steps A-J), queued on ctx.stream as one cooperative launch (or, `stepped`,
+// as one ordinary launch per step); the caller reads the control block once at the end.
+// `objective` >= 0 also records the sssp change classification for that weight column and the
+// plan (packing, default width); tree arrays are not touched.  With `tree` and a scheduler (or a
+// schedule asking for features), block 0 of the launch computes the batch features and the
+// schedule into the control block.
 void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective, long long delta_opt,
-                  const dyngb200_schedule* sched, Tree* tree, const Scheduler* learned) {
-  require_cooperative(ctx);
+                  const dyngb200_schedule* sched, Tree* tree, const Scheduler* learned,
+                  bool stepped) {
+  if (!stepped) require_cooperative(ctx);
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   const long long dir = g.props.directed ? 1 : 2;
@@ -2138,6 +2211,34 @@ void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective, l
                            ? static_cast<unsigned long long>(ctx.test_barrier_timeout_ns)
                            : 0;
   L.barrier_extra = ctx.test_barrier_kernel == 2 ? 0 : ctx.test_barrier_extra;
+  if (stepped) {
+    // the steps in the fused kernel's order; apply_ns gets the same marks (the start of the
+    // applier, then the end of each step; the plan is timed with the pairs, as in the fused
+    // kernel, where the two overlap)
+    int mark = 0;
+    auto step = [&](int which, int grid) {
+      k_apply_step<<<grid, kBlock, 0, s>>>(p, L, which, which == kStepPairs ? -1 : mark);
+      if (which != kStepPairs) ++mark;
+      ++ctx.launches;
+      DYNGB200_CUDA(cudaGetLastError());
+    };
+    step(kStepValidate, blocks);
+    step(kStepPlan, 1);
+    step(kStepPairs, blocks);
+    step(kStepMatch, blocks);
+    step(kStepResolve, blocks);
+    if (!g.props.sorted) {
+      step(kStepRowOffsets, blocks);
+      step(kStepFillSegments, blocks);
+      step(kStepSortSegments, blocks);
+    }
+    step(kStepAlloc, blocks);
+    step(kStepMutate, blocks);
+    step(kStepMoveAppend, blocks);
+    step(kStepRows, blocks);
+    step(kStepFinalize, 1);
+    return;
+  }
   void* args[] = {&p, &L};
   ++ctx.launches;
   DYNGB200_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_apply), dim3(blocks),
@@ -2157,7 +2258,7 @@ void graph_apply(Context& ctx, Graph& g, const dyngb200_batch& batch,
   // allocated before the applier is queued: a failed allocation leaves the graph as it was
   if (weight_increased && b.ni > 0) flags.reserve(static_cast<size_t>(b.ni) * g.k);
   for (int attempt = 0;; ++attempt) {
-    apply_launch(ctx, g, b, -1, 0, nullptr);
+    apply_launch(ctx, g, b, -1, 0, nullptr, nullptr, nullptr, !cooperative_available(ctx));
     if (weight_increased && b.ni > 0) {
       ApplyParams p = make_params(ctx, g, b, -1, 0);
       k_insert_flags<<<grid_for(b.ni, kBlock, ctx.sm_count), kBlock, 0, s>>>(p, flags.ptr);

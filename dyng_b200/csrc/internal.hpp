@@ -225,6 +225,8 @@ struct Workspace {
       touched, cand_med, near_med_a, near_med_b;
   DevBuf<UpdateCtl> ctl;
   HostBuf<UpdateCtl> host_ctl;
+  DevBuf<unsigned long long> op_counts;  // the operators engine's step counters
+  HostBuf<unsigned long long> op_host;
   int generation = 0;     // stamp generations (sssp)
   int touch_generation = 0;  // row-touch generations (applier)
   long long n_sized = 0;
@@ -265,6 +267,13 @@ struct Context {
 
 // The persistent kernels need cooperative launch; checked before anything of a call changes.
 void require_cooperative(const Context& ctx);
+// The engines (sssp.cpp:195-226 of the reference): the fused persistent kernels need cooperative
+// launch; the operators engine (ordinary launches, the loop on the host) runs anywhere;
+// `automatic` takes the fused engine where the device offers cooperative launch.
+bool cooperative_available(const Context& ctx);
+// Throws NOT_SUPPORTED for the fused engine on a device without cooperative launch (before
+// anything changes); returns whether the call runs the operators engine.
+bool select_engine(const Context& ctx, int requested);
 // A graph an update left incomplete refuses further use.
 struct Graph;
 void require_intact(const Graph& g);
@@ -423,7 +432,7 @@ struct StagedBatch {
 };
 void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective,
                   long long delta_opt, const dyngb200_schedule* sched, Tree* tree = nullptr,
-                  const Scheduler* learned = nullptr);
+                  const Scheduler* learned = nullptr, bool stepped = false);
 void schedule_into(const dyngb200_schedule& sched, UpdateCtl& init);
 StagedBatch stage_batch(Context& ctx, const dyngb200_batch& batch, int k);
 
@@ -443,6 +452,7 @@ struct PendingUpdate {
   const Scheduler* learned = nullptr;
   StagedBatch b{};
   int blocks = 0;
+  bool operators = false;  // the operators engine (ordinary launches, the loop on the host)
   long long launches0 = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
   double host_us[4] = {};  // see dyngb200_stats::host_us

@@ -1,0 +1,603 @@
+// The operators engine of sssp::update and sssp::compute: the same algorithm as the fused
+// persistent kernel (sssp.cu), as a sequence of ordinary kernel launches whose loop is driven
+// from the host, which reads a few counters after each step (the reference's engine::operators,
+// cpp/src/algorithms/sssp/operators.cuh and its host loop in operators.cu: one synchronisation
+// per push iteration and per threshold raise).
+//
+// It needs no cooperative launch, so it is what engine::automatic runs on a device without one
+// (as the reference does, sssp.cpp:195-226), and what options::cuda_engine = operators asks for.
+// Every kernel is a grid-stride pass over its list or over the vertices (any grid size); rows are
+// read by one warp each (the lanes over the row's slots, their minimum or their offers combined
+// in the warp).  The fixed point is the fused kernel's: one 64-bit atomicMin per offer on the
+// packed (distance << b | parent) word, so the distances, parents, `invalidated` and `affected`
+// equal the fused engine's (and the oracle's) bit for bit.  Invalidation runs pointer jumping
+// over every vertex (full passes, at most ceil(log2 n) + 1, a parent cycle reported past that),
+// or, when the schedule asks for it on a tree that cannot hold a cycle, walks the invalidated
+// subtrees level by level over the out-rows.
+#include "internal.hpp"
+#include "sssp_params.cuh"
+
+#include <algorithm>
+#include <cstddef>
+#include <string>
+
+namespace dyngb200 {
+
+namespace {
+
+constexpr int kOpBlock = 256;
+constexpr int kMarked = -2;  // pointer jumping: an invalidated ancestor was reached
+
+// The counters one step leaves for the host.
+struct OpCounts {
+  int next;        // entries appended to the next list (near frontier, walk level, pull frontier)
+  int far;         // entries on the far pile being appended to
+  int candidates;  // vertices the pull re-evaluates
+  int jumped;      // pointer jumping: a chain moved on this round and goes on
+  unsigned long long minimum;  // smallest distance of a list (kPackedInf: none)
+};
+
+__device__ __forceinline__ Packing packing_of(int bits) {
+  Packing pk;
+  pk.bits = bits;
+  pk.no_parent = bits ? (1ULL << bits) - 1 : 0;
+  return pk;
+}
+
+__device__ __forceinline__ bool op_claim(int* stamp, int v, int generation) {
+  return atomicExch(&stamp[v], generation) != generation;
+}
+
+__device__ __forceinline__ void op_invalidate(const SsspParams& p, int v, OpCounts* oc) {
+  p.packed[v] = kPackedInf;
+  p.touch_stamp[v] = p.touch_gen;
+  p.candidates[append_slot(&oc->candidates)] = v;
+}
+
+__device__ __forceinline__ long long op_tid() {
+  return blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+}
+__device__ __forceinline__ long long op_threads() {
+  return static_cast<long long>(gridDim.x) * blockDim.x;
+}
+
+// Sum of a per-thread count over the block, added to a global counter by one atomic.
+__device__ __forceinline__ void op_block_add(long long v, long long* target) {
+  __shared__ unsigned long long s_sum;
+  if (threadIdx.x == 0) s_sum = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(&s_sum, static_cast<unsigned long long>(v));
+  __syncthreads();
+  if (threadIdx.x == 0 && s_sum != 0)
+    atomicAdd(reinterpret_cast<unsigned long long*>(target), s_sum);
+}
+
+// The persistent words in this call's format and the vertices the batch added (update); every
+// word INF but the source's (compute).
+__global__ void k_op_setup(SsspParams p, int bits, u64 maxd, long long n) {
+  const Packing pk = packing_of(bits);
+  UpdateCtl* c = p.ctl;
+  for (long long v = op_tid(); v < n; v += op_threads()) {
+    if (p.from_scratch) {
+      p.packed[v] = v == p.source ? pk.pack(0, -1) : kPackedInf;
+      continue;
+    }
+    if (v >= p.tree_n) {
+      p.dist[v] = kInfinity;
+      p.parent[v] = -1;
+      p.packed[v] = kPackedInf;
+      continue;
+    }
+    if (p.tree_bits != bits) {
+      const long long d = p.dist[v];
+      u64 word = kPackedInf;
+      if (d < kInfinity / 2) {
+        if (d < 0 || static_cast<u64>(d) > maxd) atomicOr(&c->error, kErrOverflow);
+        else word = pk.pack(static_cast<u64>(d), p.parent[v]);
+      }
+      p.packed[v] = word;
+    }
+  }
+}
+
+// Roots (fused.cuh:178-197): the heads v of deleted or weight-increased tree edges (u, v) are
+// invalidated; for the walk they are also its first level.  `changed` records whether the batch
+// holds a changed edge (1) and a root (2).
+__global__ void k_op_roots(SsspParams p, int gen_inv, int* level, int walk, OpCounts* oc) {
+  UpdateCtl* c = p.ctl;
+  const int pairs = c->pairs;
+  long long inval = 0;
+  int changed = 0;
+  for (long long i = op_tid(); i < pairs; i += op_threads()) {
+    const int slot = p.pair_list[i];
+    const int f = p.pair_flags[slot];
+    const bool increased = p.use_inc ? p.inc[static_cast<long long>(slot) * p.k + p.objective] != 0
+                                     : (f & kPairIncreased) != 0;
+    if (!(f & kPairDelete) && !increased) continue;
+    changed |= 1;
+    const u64 key = p.pair_key[slot];
+    const int32_t u = static_cast<int32_t>(key >> 32);
+    const int32_t v = static_cast<int32_t>(key & 0xffffffffu);
+    if (v < p.tree_n && p.parent[v] == u && op_claim(p.stamp, v, gen_inv)) {
+      changed |= 2;
+      op_invalidate(p, v, oc);
+      ++inval;
+      if (walk) level[append_slot(&oc->next)] = v;
+    }
+  }
+  const int any = __syncthreads_or(changed & 1);
+  const int roots = __syncthreads_or(changed & 2);
+  if (threadIdx.x == 0 && any) atomicOr(&c->changed, roots ? 3 : 1);
+  op_block_add(inval, &c->invalidated);
+}
+
+// One level of the subtree walk: every child y of a level vertex u (parent[y] == u) is
+// invalidated and joins the next level.  One warp per level vertex, its lanes over the out-row.
+__global__ void k_op_walk(SsspParams p, int gen_inv, const int* level, int count, int* next,
+                          OpCounts* oc) {
+  const int lane = threadIdx.x & 31;
+  long long inval = 0;
+  for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
+    const int u = level[i];
+    const RowDesc d = p.g.out_desc[u];
+    for (int e = lane; e < d.len; e += 32) {
+      const int y = p.g.out_col[d.start + e];
+      if (y < 0 || y >= p.tree_n || p.parent[y] != u) continue;
+      if (!op_claim(p.stamp, y, gen_inv)) continue;
+      op_invalidate(p, y, oc);
+      ++inval;
+      next[append_slot(&oc->next)] = y;
+    }
+  }
+  op_block_add(inval, &p.ctl->invalidated);
+}
+
+// Pointer jumping (fused.cuh:199-234): the first ancestors (kMarked for a root, -1 for a child of
+// the source, whose chain ends at once), then rounds over every vertex until no chain moves.
+// Invariant: ancestor[x] >= 0 implies no root on the tree path from x up to ancestor[x]; a
+// vertex whose ancestor is invalidated is invalidated on the spot.  A round may read an ancestor
+// word another thread of the same round writes: either value keeps the invariant.
+__global__ void k_op_pj_start(SsspParams p, int gen_inv, long long n) {
+  for (long long v = op_tid(); v < n; v += op_threads()) {
+    const int pa = v < p.tree_n ? p.parent[v] : -1;
+    p.ancestor[v] = p.stamp[v] == gen_inv ? kMarked : (pa == p.source ? -1 : pa);
+  }
+}
+
+__global__ void k_op_pj_round(SsspParams p, int gen_inv, long long n, OpCounts* oc) {
+  long long inval = 0;
+  int jumped = 0;
+  for (long long v = op_tid(); v < n; v += op_threads()) {
+    const int a = ld_cg(&p.ancestor[v]);
+    if (a < 0) continue;
+    int na = ld_cg(&p.ancestor[a]);
+    if (na == p.source) na = -1;  // reaching the source ends a chain
+    if (na == kMarked) {
+      p.ancestor[v] = kMarked;
+      p.stamp[v] = gen_inv;
+      op_invalidate(p, static_cast<int>(v), oc);
+      ++inval;
+    } else {
+      p.ancestor[v] = na;
+      jumped |= na >= 0;
+    }
+  }
+  if (__syncthreads_or(jumped) && threadIdx.x == 0) oc->jumped = 1;
+  op_block_add(inval, &p.ctl->invalidated);
+}
+
+// Insertion heads (fused.cuh:236-256): pulled, or (canonical trees) offered the inserted edge.
+__global__ void k_op_heads(SsspParams p, int bits, u64 maxd, int gen_inv, int gen_pull,
+                           OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  const int pairs = p.ctl->pairs;
+  for (long long i = op_tid(); i < pairs; i += op_threads()) {
+    const int slot = p.pair_list[i];
+    const int f = p.pair_flags[slot];
+    if (!(f & kPairHead)) continue;
+    const u64 key = p.pair_key[slot];
+    const int32_t v = static_cast<int32_t>(key & 0xffffffffu);
+    if (v == p.source) continue;
+    if (!p.offer_heads) {
+      if (op_claim(p.stamp, v, gen_inv)) p.candidates[append_slot(&oc->candidates)] = v;
+      continue;
+    }
+    if (!(f & (kPairAppend | kPairUpsert))) continue;  // no new weight on (u,v)
+    if (ld_cg(&p.stamp[v]) == gen_inv) continue;       // invalidated: pulled anyway
+    const int32_t u = static_cast<int32_t>(key >> 32);
+    const u64 word = ld_cg(&p.packed[u]);
+    if (word == kPackedInf) continue;
+    const int ins = (f & kPairUseFirst) ? p.pair_first[slot] : p.pair_last[slot];
+    const u64 nd = pk.dist(word) +
+                   static_cast<u64>(p.ins_w[static_cast<long long>(ins) * p.k + p.objective]);
+    if (nd > maxd) continue;
+    const u64 cand = pk.pack(nd, u);
+    if (cand >= ld_cg(&p.packed[v])) continue;
+    const u64 old = atomicMin(&p.packed[v], cand);
+    if (cand < old) p.touch_stamp[v] = p.touch_gen;
+    if (nd < pk.dist(old) && op_claim(p.stamp, v, gen_pull))
+      p.frontier[append_slot(&oc->next)] = v;
+  }
+}
+
+// The pull (fused.cuh:258-285): every candidate takes the minimum over its in-row of
+// pack(d(y) + w, y); with an offer it joins the frontier.  One warp per candidate.
+__global__ void k_op_pull(SsspParams p, int bits, u64 maxd, int gen_pull, int count,
+                          OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  const int lane = threadIdx.x & 31;
+  const int32_t* wcol = p.g.in_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+  for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
+    const int v = p.candidates[i];
+    const RowDesc d = p.g.in_desc[v];
+    u64 best = kPackedInf;
+    for (int e = lane; e < d.len; e += 32) {
+      const int y = p.g.in_col[d.start + e];
+      if (y < 0) continue;
+      // the source's word is distance 0 for good
+      const u64 word = y == p.source ? 0 : ld_cg(&p.packed[y]);
+      if (word == kPackedInf) continue;
+      const u64 nd = (y == p.source ? 0 : pk.dist(word)) + static_cast<u64>(wcol[d.start + e]);
+      if (nd > maxd) continue;
+      best = min(best, pk.pack(nd, y));
+    }
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0 && best != kPackedInf) {
+      const u64 old = atomicMin(&p.packed[v], best);
+      if (best < old) p.touch_stamp[v] = p.touch_gen;
+      if (op_claim(p.stamp, v, gen_pull)) p.frontier[append_slot(&oc->next)] = v;
+    }
+  }
+}
+
+// The smallest distance of a list's vertices (none: kPackedInf).
+__global__ void k_op_min(SsspParams p, int bits, const int* list, int count, OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  u64 local = kPackedInf;
+  for (long long i = op_tid(); i < count; i += op_threads()) {
+    const u64 word = ld_cg(&p.packed[list[i]]);
+    if (word != kPackedInf) local = min(local, pk.dist(word));
+  }
+  for (int o = 16; o > 0; o >>= 1) local = min(local, __shfl_down_sync(0xffffffffu, local, o));
+  if ((threadIdx.x & 31) == 0 && local != kPackedInf) atomicMin(&oc->minimum, local);
+}
+
+// A list split at the threshold: below it into the near frontier (claimed once per step), the
+// rest onto the far pile (the first split: once, by the vertex's flag; a split of the far pile:
+// the entries that stay).  Entries taken off the far pile lose the flag.
+__global__ void k_op_split(SsspParams p, int bits, u64 threshold, int gen, const int* list,
+                           int count, int from_far, int* near, int* far, OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  for (long long i = op_tid(); i < count; i += op_threads()) {
+    const int v = list[i];
+    const u64 word = ld_cg(&p.packed[v]);
+    const u64 d = word == kPackedInf ? kPackedInf : pk.dist(word);
+    if (d < threshold) {
+      if (from_far) p.in_far[v] = 0;
+      if (op_claim(p.stamp, v, gen)) near[append_slot(&oc->next)] = v;
+    } else if (from_far || atomicExch(&p.in_far[v], 1) == 0) {
+      far[append_slot(&oc->far)] = v;
+    }
+  }
+}
+
+// One push step of the near-far loop (fused.cuh:288-417): every near vertex u offers
+// pack(d(u) + w, u) to its out-neighbours; an improved neighbour joins the next near frontier
+// (below the threshold) or the far pile.  One warp per near vertex.
+__global__ void k_op_push(SsspParams p, int bits, u64 maxd, u64 threshold, int gen,
+                          const int* near, int count, int* next, int* far, OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  const int lane = threadIdx.x & 31;
+  const int32_t* wcol = p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+  for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
+    const int u = near[i];
+    const u64 wu = ld_cg(&p.packed[u]);
+    if (wu == kPackedInf) continue;
+    const u64 du = pk.dist(wu);
+    const RowDesc d = p.g.out_desc[u];
+    for (int e = lane; e < d.len; e += 32) {
+      const int y = p.g.out_col[d.start + e];
+      if (y < 0 || y == p.source) continue;
+      const u64 nd = du + static_cast<u64>(wcol[d.start + e]);
+      if (nd > maxd) continue;
+      const u64 cand = pk.pack(nd, u);
+      if (cand >= ld_cg(&p.packed[y])) continue;
+      const u64 old = atomicMin(&p.packed[y], cand);
+      if (cand < old) p.touch_stamp[y] = p.touch_gen;
+      if (nd >= pk.dist(old)) continue;
+      if (nd < threshold) {
+        if (op_claim(p.stamp, y, gen)) next[append_slot(&oc->next)] = y;
+      } else if (atomicExch(&p.in_far[y], 1) == 0) {
+        far[append_slot(&oc->far)] = y;
+      }
+    }
+  }
+}
+
+// The commit (fused.cuh:419-494), packed words: every vertex (compute) or every vertex whose word
+// this call changed (update) gets its (distance, parent); the changed ones are counted.
+__global__ void k_op_unpack(SsspParams p, int bits, long long n) {
+  const Packing pk = packing_of(bits);
+  long long affected = 0;
+  for (long long v = op_tid(); v < n; v += op_threads()) {
+    if (!p.from_scratch && ld_cg(&p.touch_stamp[v]) != p.touch_gen) continue;
+    const u64 word = ld_cg(&p.packed[v]);
+    const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(pk.dist(word));
+    const int32_t par = word == kPackedInf ? -1 : pk.parent(word);
+    if (p.dist[v] != d || p.parent[v] != par) {
+      p.dist[v] = d;
+      p.parent[v] = par;
+      ++affected;
+    }
+  }
+  if (!p.from_scratch) op_block_add(affected, &p.ctl->affected);
+}
+
+// The commit, distance-only words: the distances written, the parents recovered as the lowest-id
+// tight in-neighbour (three passes, as in the fused kernel).
+__global__ void k_op_dist_prepare(SsspParams p, long long n) {
+  for (long long v = op_tid(); v < n; v += op_threads()) {
+    const u64 word = ld_cg(&p.packed[v]);
+    const long long d = word == kPackedInf ? kInfinity : static_cast<long long>(word);
+    if (!p.from_scratch) {
+      p.ancestor[v] = p.parent[v];
+      p.candidates[v] = d != p.dist[v] ? 1 : 0;
+    }
+    p.dist[v] = d;
+    p.parent[v] = (word == kPackedInf || v == p.source) ? -1 : INT32_MAX;
+  }
+}
+
+__global__ void k_op_dist_parents(SsspParams p, long long n) {
+  const int32_t* wcol = p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+  const int lane = threadIdx.x & 31;
+  for (long long u = op_tid() >> 5; u < n; u += op_threads() >> 5) {
+    const u64 du = ld_cg(&p.packed[u]);
+    if (du == kPackedInf) continue;
+    const RowDesc d = p.g.out_desc[u];
+    for (int e = lane; e < d.len; e += 32) {
+      const int x = p.g.out_col[d.start + e];
+      if (x < 0 || x == p.source) continue;
+      if (du + static_cast<u64>(wcol[d.start + e]) == ld_cg(&p.packed[x]))
+        atomicMin(&p.parent[x], static_cast<int32_t>(u));
+    }
+  }
+}
+
+__global__ void k_op_dist_count(SsspParams p, long long n) {
+  long long affected = 0;
+  for (long long v = op_tid(); v < n; v += op_threads())
+    affected += (ld_cg(&p.candidates[v]) != 0 || ld_cg(&p.ancestor[v]) != ld_cg(&p.parent[v]));
+  op_block_add(affected, &p.ctl->affected);
+}
+
+// The run's counters and the tree's history into the control block (what the fused kernel
+// writes at its end).
+struct OpSummary {
+  int iterations, epochs, rounds, active, levels, last_generation, error;
+  long long pushes;
+  int frontier[4];
+};
+
+__global__ void k_op_finish(SsspParams p, OpSummary s) {
+  UpdateCtl* c = p.ctl;
+  c->iterations = s.iterations;
+  c->epochs = s.epochs;
+  c->pushes = s.pushes;
+  c->rounds = s.rounds;
+  c->levels = s.levels;
+  if (s.rounds > 0) c->active[(s.rounds - 1) % 3] = s.active;
+  c->last_generation = s.last_generation;
+  if (s.error) atomicOr(&c->error, static_cast<unsigned>(s.error));
+  c->work[2] = c->invalidated;
+  if (p.hist) {
+    TreeHistory h{};
+    h.invalidated = c->invalidated;
+    for (int i = 0; i < 4; ++i) h.frontier[i] = s.frontier[i];
+    h.iterations = s.iterations + s.epochs;
+    h.rounds = s.rounds;
+    *p.hist = h;
+  }
+}
+
+}  // namespace
+
+int operators_grid(const Context& ctx) { return std::max(1, ctx.sm_count * 8); }
+
+void run_operators(Context& ctx, const SsspParams& p) {
+  cudaStream_t s = ctx.stream;
+  Workspace& ws = ctx.ws;
+  UpdateCtl* c = p.ctl;
+  expects(ws.op_counts.ptr != nullptr && ws.op_host.ptr != nullptr,
+          "sssp: the workspace was not reserved", DYNGB200_INTERNAL);
+  static_assert(sizeof(OpCounts) <= 4 * sizeof(unsigned long long), "the step counters fit");
+  OpCounts* oc = reinterpret_cast<OpCounts*>(ws.op_counts.ptr);
+  OpCounts* hc = reinterpret_cast<OpCounts*>(ws.op_host.ptr);
+  const int grid = operators_grid(ctx);
+  auto read_ctl = [&]() {
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, c, sizeof(UpdateCtl), cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    return *ws.host_ctl.ptr;
+  };
+  // the plan (the applier's, or compute's upload) and any error found before the engine: an
+  // error leaves the control block to the caller as it is
+  const UpdateCtl plan = read_ctl();
+  if (plan.error != 0) return;
+  const long long n = plan.n_after;
+  const int bits = plan.packing_bits;
+  const u64 maxd = plan.max_distance;
+  const long long delta_sel = plan.sched_delta > 0
+                                  ? plan.sched_delta
+                                  : (p.delta_override > 0 ? p.delta_override : plan.delta);
+  const u64 delta = static_cast<u64>(delta_sel > 0 ? delta_sel : 1);
+  // the counters of the next step: `candidates` carried over (the pull's list grows through the
+  // roots, the invalidation and the heads), `far` the pile's current length, the rest cleared
+  auto reset = [&](int candidates, int far) {
+    hc->next = 0;
+    hc->far = far;
+    hc->candidates = candidates;
+    hc->jumped = 0;
+    hc->minimum = kPackedInf;
+    DYNGB200_CUDA(cudaMemcpyAsync(oc, hc, sizeof(OpCounts), cudaMemcpyHostToDevice, s));
+  };
+  auto counts = [&]() {
+    DYNGB200_CUDA(cudaMemcpyAsync(hc, oc, sizeof(OpCounts), cudaMemcpyDeviceToHost, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    return *hc;
+  };
+  auto launched = [&](int k) {
+    ctx.launches += k;
+    DYNGB200_CUDA(cudaGetLastError());
+  };
+  OpSummary sum{};
+  int gen = p.generation;
+  int frontier_count = 0;
+  int* lists[2] = {p.near_a, p.near_b};
+  int* fars[2] = {p.far_a, p.far_b};
+  if (n > 0) {
+    k_op_setup<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, n);
+    launched(1);
+  }
+  if (p.from_scratch) {
+    hc->next = p.source;  // staged in pinned memory: the copy is queued, then waited for
+    DYNGB200_CUDA(cudaMemcpyAsync(p.frontier, &hc->next, sizeof(int), cudaMemcpyHostToDevice, s));
+    DYNGB200_CUDA(cudaStreamSynchronize(s));
+    frontier_count = n > 0 ? 1 : 0;
+  } else {
+    const int gen_inv = ++gen;
+    const int gen_pull = ++gen;
+    const bool walk = plan.sched_walk != 0 && p.tree_trusted != 0;
+    // ---- roots, and the repack's overflow check ----------------------------------------------
+    reset(0, 0);
+    k_op_roots<<<grid, kOpBlock, 0, s>>>(p, gen_inv, lists[0], walk ? 1 : 0, oc);
+    launched(1);
+    OpCounts r = counts();
+    const UpdateCtl after_roots = read_ctl();
+    if (after_roots.error != 0) return;  // an input distance that does not fit: nothing written
+    if (walk) {
+      // ---- invalidation by a walk down the old tree, level by level --------------------------
+      int level = r.next, cur = 0;
+      while (level > 0) {
+        if (sum.levels > n + 1) {
+          sum.error |= kErrNotConverged;
+          break;
+        }
+        reset(r.candidates, 0);
+        k_op_walk<<<grid, kOpBlock, 0, s>>>(p, gen_inv, lists[cur], level, lists[cur ^ 1], oc);
+        launched(1);
+        r = counts();
+        level = r.next;
+        cur ^= 1;
+        ++sum.levels;
+      }
+    } else {
+      // ---- invalidation by pointer jumping: when roots exist, or (a tree imported without
+      // validation) when any edge changed, so that a parent cycle is still reported -------------
+      const int changed = after_roots.changed;
+      if ((changed & 2) || (!p.tree_trusted && (changed & 1))) {
+        int max_rounds = 0;
+        while ((1LL << max_rounds) < n) ++max_rounds;
+        ++max_rounds;
+        k_op_pj_start<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n);
+        launched(1);
+        for (int round = 0; round < max_rounds; ++round) {
+          reset(r.candidates, 0);
+          k_op_pj_round<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n, oc);
+          launched(1);
+          r = counts();
+          sum.rounds = round + 1;
+          sum.active = r.jumped;
+          if (!r.jumped) break;
+        }
+      }
+    }
+    // ---- insertion heads, then the pull over every candidate --------------------------------
+    if (sum.error == 0) {
+      reset(r.candidates, 0);
+      k_op_heads<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_inv, gen_pull, oc);
+      launched(1);
+      r = counts();
+      if (r.candidates > 0) {
+        k_op_pull<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, r.candidates, oc);
+        launched(1);
+        r = counts();
+      }
+      frontier_count = r.next;
+    }
+  }
+  // ---- the near-far loop: one host synchronisation per push step or threshold raise -----------
+  const long long iteration_cap = 4 * n + 64;
+  if (frontier_count > 0 && sum.error == 0) {
+    int cur = 0, far_cur = 0;
+    reset(0, 0);
+    k_op_min<<<grid, kOpBlock, 0, s>>>(p, bits, p.frontier, frontier_count, oc);
+    launched(1);
+    const OpCounts m = counts();
+    u64 threshold = (m.minimum == kPackedInf ? 0 : m.minimum) + delta;
+    ++gen;
+    reset(0, 0);
+    k_op_split<<<grid, kOpBlock, 0, s>>>(p, bits, threshold, gen, p.frontier, frontier_count, 0,
+                                         lists[cur], fars[far_cur], oc);
+    launched(1);
+    OpCounts r = counts();
+    int near_count = r.next, far_count = r.far;
+    while (near_count > 0 || far_count > 0) {
+      const int step = sum.iterations + sum.epochs;
+      if (step < 4) sum.frontier[step] = near_count > 0 ? near_count : -far_count;
+      if (near_count > 0) {
+        if (++sum.iterations > iteration_cap) {
+          sum.error |= kErrNotConverged;
+          break;
+        }
+        sum.pushes += near_count;
+        ++gen;
+        reset(0, far_count);
+        k_op_push<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, threshold, gen, lists[cur], near_count,
+                                            lists[cur ^ 1], fars[far_cur], oc);
+        launched(1);
+        r = counts();
+        cur ^= 1;
+        near_count = r.next;
+        far_count = r.far;
+        continue;
+      }
+      // the near frontier is empty: raise the threshold past the far pile and split the pile
+      ++sum.epochs;
+      reset(0, 0);
+      k_op_min<<<grid, kOpBlock, 0, s>>>(p, bits, fars[far_cur], far_count, oc);
+      launched(1);
+      const OpCounts fm = counts();
+      threshold = std::max(threshold, fm.minimum == kPackedInf ? threshold : fm.minimum) + delta;
+      ++gen;
+      reset(0, 0);
+      k_op_split<<<grid, kOpBlock, 0, s>>>(p, bits, threshold, gen, fars[far_cur], far_count, 1,
+                                           lists[cur], fars[far_cur ^ 1], oc);
+      launched(1);
+      r = counts();
+      far_cur ^= 1;
+      near_count = r.next;
+      far_count = r.far;
+    }
+  }
+  // ---- commit ---------------------------------------------------------------------------------
+  if (n > 0 && sum.error == 0) {
+    if (bits > 0) {
+      k_op_unpack<<<grid, kOpBlock, 0, s>>>(p, bits, n);
+      launched(1);
+    } else {
+      k_op_dist_prepare<<<grid, kOpBlock, 0, s>>>(p, n);
+      k_op_dist_parents<<<grid, kOpBlock, 0, s>>>(p, n);
+      launched(2);
+      if (!p.from_scratch) {
+        k_op_dist_count<<<grid, kOpBlock, 0, s>>>(p, n);
+        launched(1);
+      }
+    }
+  }
+  sum.last_generation = gen;
+  k_op_finish<<<1, 1, 0, s>>>(p, sum);
+  launched(1);
+}
+
+}  // namespace dyngb200

@@ -14,6 +14,7 @@
 //     and every block leaves the kernel (no unbounded spin).
 #include "internal.hpp"
 #include "grid_sync.cuh"
+#include "sssp_params.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -27,67 +28,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHeavyChunk = 256;
-
-struct SsspParams {
-  GraphView g;
-  int objective;
-  int32_t source;
-  int from_scratch;
-  long long* dist;
-  int32_t* parent;
-  u64* packed;
-  int tree_bits;         // format of the persistent words (-1: none); another format is rebuilt
-  long long tree_n;      // vertices the tree held before this call (growth fills the rest)
-  int walk;              // invalidation by a subtree walk instead of pointer jumping
-  int tree_trusted;      // computed or validated: no parent cycle possible
-  int offer_heads;       // canonical tree: insertion heads take the inserted edge's offer
-  // pairs of the applier (update only) and the batch weights
-  const u64* pair_key;
-  const int* pair_list;
-  const int* pair_flags;
-  const int* pair_first;
-  const int* pair_last;
-  const int32_t* ins_w;
-  int k;
-  // scratch
-  int* stamp;
-  int* touch_stamp;
-  int* flag;
-  int* in_far;
-  int* ancestor;
-  int* candidates;
-  int* frontier;
-  int* near_a;
-  int* near_b;
-  int* far_a;
-  int* far_b;
-  int2* heavy_a;
-  int2* heavy_b;
-  int2* pull_heavy;
-  int* cand_med;
-  int* near_med_a;
-  int* near_med_b;
-  int* touched;
-  int generation;
-  int touch_gen;
-  int heavy_degree;
-  long long delta_override;
-  int small_frontier;    // frontiers up to this size run on block 0 alone (0: never)
-  UpdateCtl* ctl;
-  TreeHistory* hist;
-  int* pj_blk;           // survivor counts of the pointer-jumping rounds: 2 x kPjMaxBlocks
-  const unsigned char* inc;  // the applier's weight-increase flags (pairs x k)
-  int use_inc;           // 1: changed edges of `objective` from inc[] (a batch applied for another
-                         // objective), 0: from the pair flags
-  // the grid barrier: its time limit without progress (0: kBarrierTimeoutNs) and blocks it waits
-  // for beyond the launched ones (0 outside tests; a phantom block makes every wait run out)
-  unsigned long long barrier_limit_ns;
-  int barrier_extra;
-};
-
-// Pair flags of the applier (graph.cu).
-constexpr int kPairDelete = 1, kPairIncreased = 2, kPairHead = 4, kPairAppend = 8,
-              kPairUpsert = 16, kPairUseFirst = 32;
 
 enum Mode { kPush = 0, kPull = 1, kWalk = 2 };
 
@@ -1515,11 +1455,23 @@ void require_intact(const Graph& g) {
           DYNGB200_INTERNAL);
 }
 
+bool cooperative_available(const Context& ctx) {
+  return ctx.coop_supported != 0 && ctx.test_no_cooperative == 0;
+}
+
 void require_cooperative(const Context& ctx) {
-  expects(ctx.coop_supported != 0 && ctx.test_no_cooperative == 0,
-          "sssp: the fused engine needs cooperative launch, which this device does not offer "
-          "(this library has no engine without it)",
+  expects(cooperative_available(ctx),
+          "sssp: the fused engine needs cooperative launch, which this device does not offer; "
+          "use cuda_engine automatic or operators (the multi-kernel engine runs without it)",
           DYNGB200_NOT_SUPPORTED);
+}
+
+bool select_engine(const Context& ctx, int requested) {
+  expects(requested >= DYNGB200_ENGINE_AUTOMATIC && requested <= DYNGB200_ENGINE_OPERATORS,
+          "sssp: unknown cuda_engine " + std::to_string(requested));
+  if (requested == DYNGB200_ENGINE_FUSED) require_cooperative(ctx);
+  return requested == DYNGB200_ENGINE_OPERATORS ||
+         (requested == DYNGB200_ENGINE_AUTOMATIC && !cooperative_available(ctx));
 }
 
 static void launch(Context& ctx, SsspParams& p, int blocks) {
@@ -1571,7 +1523,7 @@ static SsspParams base_params(Context& ctx, Graph& g, Tree& t) {
 // compute(): the persistent kernel from the source (fused.cuh:167-176).
 void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
   require_intact(g);
-  require_cooperative(ctx);
+  const bool operators = select_engine(ctx, t.opt.cuda_engine);
   const long long launches0 = ctx.launches;
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
@@ -1614,7 +1566,10 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
   DYNGB200_CUDA(cudaEventCreate(&e0));
   DYNGB200_CUDA(cudaEventCreate(&e1));
   DYNGB200_CUDA(cudaEventRecord(e0, s));
-  if (n > 0) launch(ctx, p, blocks);
+  if (n > 0) {
+    if (operators) run_operators(ctx, p);
+    else launch(ctx, p, blocks);
+  }
   DYNGB200_CUDA(cudaEventRecord(e1, s));
   DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
                                 cudaMemcpyDeviceToHost, s));
@@ -1636,11 +1591,13 @@ void sssp_compute(Context& ctx, Graph& g, Tree& t, dyngb200_stats* st) {
     st->epochs = r.epochs;
     st->pushes = r.pushes;
     st->packed_parents = pk.bits > 0;
-    st->engine_used = DYNGB200_ENGINE_FUSED;
+    st->engine_used = operators ? DYNGB200_ENGINE_OPERATORS : DYNGB200_ENGINE_FUSED;
     st->delta = init.delta;
     st->max_weight = cs.max_w;
-    st->grid_blocks = init.active_blocks > 0 && init.active_blocks < blocks ? init.active_blocks
-                                                                             : blocks;
+    st->grid_blocks = operators ? operators_grid(ctx)
+                                : (init.active_blocks > 0 && init.active_blocks < blocks
+                                       ? init.active_blocks
+                                       : blocks);
     st->sssp_ms = ms;
     st->kernel_launches = ctx.launches - launches0;
     st->affected = r.affected;
@@ -1676,7 +1633,7 @@ static void enqueue_attempt(PendingUpdate& u) {
   // graph as it was
   g.pinned.reserve(kCounterSlots + g.host_columns.size());
   DYNGB200_CUDA(cudaEventRecord(u.e0, s));
-  apply_launch(ctx, g, u.b, t.opt.objective, t.opt.delta, &u.sched, &t, u.learned);
+  apply_launch(ctx, g, u.b, t.opt.objective, t.opt.delta, &u.sched, &t, u.learned, u.operators);
   DYNGB200_CUDA(cudaEventRecord(u.e1, s));
   u.host_us[1] += us_since(h0);
   const auto h1 = std::chrono::steady_clock::now();
@@ -1696,7 +1653,8 @@ static void enqueue_attempt(PendingUpdate& u) {
   p.generation = ws.next_generation(1, s);
   p.touch_gen = p.generation;
   p.heavy_degree = 256;
-  launch(ctx, p, u.blocks);
+  if (u.operators) run_operators(ctx, p);
+  else launch(ctx, p, u.blocks);
   DYNGB200_CUDA(cudaEventRecord(u.e2, s));
   DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
                                 cudaMemcpyDeviceToHost, s));
@@ -1728,7 +1686,8 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
   u.learned = learned;
   u.launches0 = ctx.launches;
   require_intact(g);
-  require_cooperative(ctx);  // before the batch is staged or applied: nothing changes
+  // before the batch is staged or applied: nothing changes
+  u.operators = select_engine(ctx, t.opt.cuda_engine);
   if (g.host_columns[t.opt.objective].dirty) graph_rescan_columns(ctx, g);
   graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
   u.b = stage_batch(ctx, batch, g.k);
@@ -1744,7 +1703,7 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
 // (nothing was changed), then the error translation, the commit bookkeeping and the stats.
 // After the commit: the tree's errors (poisoning it), its new state and the stats.
 static void finish_tree(Context& ctx, Graph& g, Tree& t, const UpdateCtl& r, int blocks,
-                        float apply_ms, float sssp_ms, const Scheduler* learned,
+                        bool operators, float apply_ms, float sssp_ms, const Scheduler* learned,
                         const dyngb200_schedule& sched, long long launches0,
                         dyngb200_stats* st) {
   if (r.error & kErrInternal) {
@@ -1783,10 +1742,12 @@ static void finish_tree(Context& ctx, Graph& g, Tree& t, const UpdateCtl& r, int
     st->epochs = r.epochs;
     st->pushes = r.pushes;
     st->packed_parents = r.packing_bits > 0;
-    st->engine_used = DYNGB200_ENGINE_FUSED;
+    st->engine_used = operators ? DYNGB200_ENGINE_OPERATORS : DYNGB200_ENGINE_FUSED;
     st->delta = r.sched_delta > 0 ? r.sched_delta : r.delta;
     st->max_weight = r.max_w;
-    st->grid_blocks = r.active_blocks > 0 && r.active_blocks < blocks ? r.active_blocks : blocks;
+    st->grid_blocks = operators ? operators_grid(ctx)
+                                : (r.active_blocks > 0 && r.active_blocks < blocks ? r.active_blocks
+                                                                                   : blocks);
     st->invalidation = (r.sched_walk && t.trusted) ? 1 : 0;
     st->apply_ms = apply_ms;
     st->sssp_ms = sssp_ms;
@@ -1878,7 +1839,8 @@ void sssp_update_end(PendingUpdate& u, dyngb200_stats* st) {
   g.n = g.host_counters.n;
   g.m = g.host_counters.m;
   t.version = g.version;
-  finish_tree(ctx, g, t, r, blocks, apply_ms, sssp_ms, learned, sched, launches0, st);
+  finish_tree(ctx, g, t, r, blocks, u.operators, apply_ms, sssp_ms, learned, sched, launches0,
+              st);
   if (st)
     for (int i = 0; i < 4; ++i) st->host_us[i] = static_cast<float>(u.host_us[i]);
 }
@@ -1927,6 +1889,7 @@ static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied
   Workspace& ws = ctx.ws;
   cudaStream_t s = ctx.stream;
   const int obj = t.opt.objective;
+  const bool operators = select_engine(ctx, t.opt.cuda_engine);
   UpdateCtl init{};
   init.err_index = INT64_MAX;
   init.n_old = applied.n_old;
@@ -1972,7 +1935,8 @@ static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied
   p.touch_gen = p.generation;
   p.heavy_degree = 256;
   DYNGB200_CUDA(cudaEventRecord(e1, s));
-  launch(ctx, p, blocks);
+  if (operators) run_operators(ctx, p);
+  else launch(ctx, p, blocks);
   DYNGB200_CUDA(cudaEventRecord(e2, s));
   DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, ws.ctl.ptr, sizeof(UpdateCtl),
                                 cudaMemcpyDeviceToHost, s));
@@ -1984,7 +1948,7 @@ static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
   t.version = g.version;
-  finish_tree(ctx, g, t, r, blocks, 0.0f, sssp_ms, nullptr, sched, launches0, st);
+  finish_tree(ctx, g, t, r, blocks, operators, 0.0f, sssp_ms, nullptr, sched, launches0, st);
 }
 
 // update_each (update.hpp:331): the batch is applied once; every tree is brought up to date.
@@ -1994,7 +1958,7 @@ static void sssp_rerun(Context& ctx, Graph& g, Tree& t, const UpdateCtl& applied
 void sssp_update_each(Context& ctx, Graph& g, const dyngb200_batch& batch, Tree* const* trees,
                       int count, dyngb200_stats* stats) {
   require_intact(g);
-  require_cooperative(ctx);
+  for (int i = 0; i < count; ++i) select_engine(ctx, trees[i]->opt.cuda_engine);
   cudaStream_t s = ctx.stream;
   for (int i = 0; i < count; ++i)
     if (g.host_columns[trees[i]->opt.objective].dirty) graph_rescan_columns(ctx, g);

@@ -41,7 +41,14 @@ typedef enum dyngb200_status {
 
 typedef enum dyngb200_memory { DYNGB200_HOST = 0, DYNGB200_DEVICE = 1 } dyngb200_memory;
 
-/* dyng::engine (cpp/include/dyng/core/types.hpp): a tunable that never changes the result. */
+/* dyng::engine (cpp/include/dyng/core/types.hpp): a tunable that never changes the result
+ * (sssp.cpp:195-226).  FUSED: one cooperative persistent kernel for the applier and one for the
+ * sssp step, every loop decision on the device, one host synchronization per call; refused with
+ * NOT_SUPPORTED, before anything changes, on a device without cooperative launch.  OPERATORS:
+ * ordinary launches (one per applier step, one per sssp phase and per near-far step) with the
+ * loop on the host, which reads a few counters after each step; runs on any device.  AUTOMATIC:
+ * FUSED where the device offers cooperative launch, OPERATORS otherwise.  The stats report the
+ * engine that ran (engine_used). */
 typedef enum dyngb200_engine {
   DYNGB200_ENGINE_AUTOMATIC = 0,
   DYNGB200_ENGINE_FUSED = 1,
@@ -197,8 +204,9 @@ typedef struct dyngb200_test_hooks {
   /* Blocks every grid barrier waits for beyond the launched ones (0: none).  Nothing ever
    * arrives for them, so every barrier's wait runs out after barrier_timeout_ns. */
   int32_t barrier_extra_arrivals;
-  /* Nonzero: the context behaves as on a device without cooperative launch (the persistent
-   * kernels are refused with NOT_SUPPORTED before anything changes). */
+  /* Nonzero: the context behaves as on a device without cooperative launch: calls asking for
+   * the fused engine are refused with NOT_SUPPORTED before anything changes, automatic ones run
+   * the operators engine (graph_apply its applier as one launch per step). */
   int32_t no_cooperative_launch;
   /* Which persistent kernel the phantom arrivals hold up: 0 both, 1 the batch applier (its first
    * barrier comes before any change: the call fails with the graph and the tree unchanged), 2 the

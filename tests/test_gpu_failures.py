@@ -7,8 +7,8 @@
   - a long loop run by one block while the others wait at a grid barrier outlives that limit
     without a timeout: the waiting blocks restart their limit whenever the working block shows
     progress;
-  - a device without cooperative launch (sssp_cuda_test.cpp:106-150): the calls are refused
-    before anything changes;
+  - a device without cooperative launch (sssp_cuda_test.cpp:106-150): calls that ask for the fused
+    engine are refused before anything changes, automatic ones run the operators engine;
   - every device allocation of an update failed in turn (the sweep of the reference's
     tests/support/failing_allocator.hpp:18-143): the call reports OUT_OF_MEMORY and leaves the
     graph and the tree either unchanged or, after the batch was applied, the tree poisoned; the
@@ -112,28 +112,33 @@ def test_progress_keeps_a_long_single_block_loop_alive():
     np.testing.assert_array_equal(t.distances, 3 * np.arange(n, dtype=np.int64))
 
 
-def test_without_cooperative_launch_nothing_changes():
+def test_without_cooperative_launch_the_fused_engine_is_refused():
+    # cuda_engine="fused" on a device without cooperative launch is refused before anything
+    # changes; "automatic" then runs the operators engine
     rng, n, s, d, w = _case(5)
     res = D.Resources(0)
     g = D.Graph.from_edges(s, d, w, n, resources=res)
-    t = D.sssp.compute(g, 0)
+    fused = D.sssp.Options(cuda_engine="fused")
+    t = D.sssp.compute(g, 0, fused)
     d0, p0 = t.distances, t.parents
     b = random_batch(rng, n, s, d, 300, tree_parents=p0)
     m0 = g.num_edges()  # duplicate pairs of the random edge list were merged
     res.set_test_hooks(no_cooperative_launch=True)
     try:
         with pytest.raises(D.NotSupportedError, match="cooperative launch"):
-            D.sssp.compute(g, 0)
+            D.sssp.compute(g, 0, fused)
         with pytest.raises(D.NotSupportedError, match="cooperative launch"):
             D.sssp.update(g, _batch(b), t)
         assert g.version() == 0 and g.num_edges() == m0  # refused before the batch was applied
         np.testing.assert_array_equal(t.distances, d0)
         np.testing.assert_array_equal(t.parents, p0)
+        t.set_options(D.sssp.Options())
+        og = O.Graph.from_edges(n, s, d, w, 1)
+        ot, _ = O.compute(og, 0, rule=1)
+        st = D.sssp.update(g, _batch(b), t)
+        assert st.engine_used == "operators"
     finally:
         res.set_test_hooks()
-    og = O.Graph.from_edges(n, s, d, w, 1)
-    ot, _ = O.compute(og, 0, rule=1)
-    D.sssp.update(g, _batch(b), t)
     O.update(og, _obatch(b), ot)
     np.testing.assert_array_equal(t.distances, ot.distances)
     np.testing.assert_array_equal(t.parents, ot.parents)
