@@ -491,6 +491,9 @@ def main():
               for i, name in enumerate(timed_stats[0].PHASES)}
     stages = {name: round(float(np.mean([s.stages_ms()[name] for s in timed_stats])), 4)
               for name in timed_stats[0].stages_ms()}
+    # the batch applier's steps: the end of each (us since it began; 0: not reached)
+    apply_steps = [round(float(np.mean([s.apply_step_us[i] for s in timed_stats])), 1)
+                   for i in range(1, 12)]
     shape = {k: float(np.mean([getattr(s, k) for s in timed_stats]))
              for k in ("iterations", "epochs", "pushes", "invalidated", "affected", "rounds",
                        "touched", "delta", "grid_blocks")}
@@ -552,6 +555,7 @@ def main():
                        "host_ms_p50": 1000 * float(np.percentile(head.host, 50)),
                        "schedules": compare, "learned_classes": classes,
                        "sssp_phases_ms": phases, "stages_ms": stages, "sssp_work": work,
+                       "apply_steps_end_us": apply_steps,
                        "update_shape": shape,
                        "alg_bytes_per_update": float(np.mean(alg)),
                        "trace_last_update": [list(t) for t in timed_stats[-1].trace],
