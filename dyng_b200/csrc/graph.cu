@@ -442,14 +442,15 @@ __device__ void ph_match(const ApplyParams& p, long long tid, long long threads)
 // Multi-edge graphs: one thread per pair walks its rows in order (the first alive matches).
 // Records c, the first match and the match the insertions address (see resolve).
 __device__ void ph_scan_multi(const ApplyParams& p, long long tid, long long threads) {
+  // one warp per pair: the lanes read a row 32 slots at a time, the matches ranked by a ballot
   UpdateCtl* c = p.ctl;
   const int pairs = c->pairs;
-  for (long long i = tid; i < pairs; i += threads) {
+  const int lane = threadIdx.x & 31;
+  for (long long i = tid >> 5; i < pairs; i += threads >> 5) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
     const int d = p.d[slot];
-    const int t = p.t[slot];
     for (int side = 0; side < 2; ++side) {
       const int32_t r = side == 0 ? u : v;
       const int32_t want = side == 0 ? v : u;
@@ -458,21 +459,29 @@ __device__ void ph_scan_multi(const ApplyParams& p, long long tid, long long thr
       const int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
       // first match, and match number d (the first survivor of the deletions); absolute slots
       int count = 0, first = -1, target = -1;
-      for (int e = 0; e < desc.len; ++e) {
-        if (col[e] != want) continue;
-        if (count == 0) first = static_cast<int>(desc.start) + e;
-        if (count == d) target = static_cast<int>(desc.start) + e;
-        ++count;
+      for (int base = 0; base < desc.len; base += 32) {
+        const int e = base + lane;
+        const unsigned ballot = __ballot_sync(0xffffffffu, e < desc.len && col[e] == want);
+        if (ballot == 0) continue;
+        if (first < 0) first = static_cast<int>(desc.start) + base + __ffs(ballot) - 1;
+        const int found = __popc(ballot);
+        if (target < 0 && d >= count && d < count + found) {
+          unsigned rest = ballot;
+          for (int k = d - count; k > 0; --k) rest &= rest - 1;  // drop the lower matches
+          target = static_cast<int>(desc.start) + base + __ffs(rest) - 1;
+        }
+        count += found;
       }
-      (void)t;
-      if (side == 0) {
-        p.out_count[slot] = count;
-        p.out_pos[slot] = first;
-        p.out_pos2[slot] = target;
-      } else {
-        p.in_count[slot] = count;
-        p.in_pos[slot] = first;
-        p.in_pos2[slot] = target;
+      if (lane == 0) {
+        if (side == 0) {
+          p.out_count[slot] = count;
+          p.out_pos[slot] = first;
+          p.out_pos2[slot] = target;
+        } else {
+          p.in_count[slot] = count;
+          p.in_pos[slot] = first;
+          p.in_pos2[slot] = target;
+        }
       }
     }
   }
@@ -734,14 +743,21 @@ __device__ __forceinline__ void commit_add(long long t, long long* target) {
 }
 
 // ---- G: tombstones and upserts in place -------------------------------------------------------
+// Simple graphs: one thread per pair, the matching slots from the edge index.  Multigraphs: one
+// warp per pair walking both rows in order (lanes over 32 slots at a time, the matches ranked by
+// a ballot), so a hub row is read once, coalesced, instead of slot by slot by one thread.
 __device__ void ph_mutate(const ApplyParams& p, BlockRed& R, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int pairs = c->pairs;
   const bool del_first = p.props.deletions_first != 0;
+  const bool multi = p.g.allow_multi != 0;
+  const int lane = threadIdx.x & 31;
   ColumnAcc acc;
   acc_init(acc);
   long long idx_deleted = 0;
-  for (long long i = tid; i < pairs; i += threads) {
+  const long long first_i = multi ? tid >> 5 : tid;
+  const long long step = multi ? threads >> 5 : threads;
+  for (long long i = first_i; i < pairs; i += step) {
     const int slot = p.list[i];
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
@@ -756,7 +772,7 @@ __device__ void ph_mutate(const ApplyParams& p, BlockRed& R, long long tid, long
     const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
     if (!tomb && !(flags & kPairUpsert)) continue;
     const int target = del_first ? d : 0;  // the original match an upsert addresses
-    if (!p.g.allow_multi) {
+    if (!multi) {
       // simple graphs: the single matching slot, absolute positions from the edge index
       for (int side = 0; side < 2; ++side) {
         int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
@@ -791,26 +807,32 @@ __device__ void ph_mutate(const ApplyParams& p, BlockRed& R, long long tid, long
       const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
       int32_t* col = (side == 0 ? p.g.out_col : p.g.in_col) + desc.start;
       int32_t* w = (side == 0 ? p.g.out_w : p.g.in_w) + desc.start;
-      // multi-edge graphs: walk the row in order
+      // multi-edge graphs: the row in order, 32 slots per step; a match's rank is the number of
+      // matches before it (the first `tomb` become tombstones, rank `target` takes the upsert)
       int seen = 0;
-      for (int e = 0; e < desc.len && seen < cnt; ++e) {
-        if (col[e] != want) continue;
-        if (seen < tomb) {
-          col[e] = kDead;
-          if (side == 0)
-            for (int j = 0; j < p.k; ++j)
-              column_out(p, acc, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
-        } else if ((flags & kPairUpsert) && seen == target) {
-          for (int j = 0; j < p.k; ++j) {
-            const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
-            if (side == 0) {
-              column_out(p, acc, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
-              column_in(p, acc, j, nw);
+      for (int base = 0; base < desc.len && seen < cnt; base += 32) {
+        const int e = base + lane;
+        const bool match = e < desc.len && col[e] == want;
+        const unsigned ballot = __ballot_sync(0xffffffffu, match);
+        if (match) {
+          const int rank = seen + __popc(ballot & ((1u << lane) - 1));
+          if (rank < tomb) {
+            col[e] = kDead;
+            if (side == 0)
+              for (int j = 0; j < p.k; ++j)
+                column_out(p, acc, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
+          } else if (rank < cnt && (flags & kPairUpsert) && rank == target) {
+            for (int j = 0; j < p.k; ++j) {
+              const long long nw = p.ins_w[static_cast<long long>(ins_index) * p.k + j];
+              if (side == 0) {
+                column_out(p, acc, j, w[j * p.g.arena_cap + e], p.g.columns[j].max_w);
+                column_in(p, acc, j, nw);
+              }
+              w[j * p.g.arena_cap + e] = static_cast<int32_t>(nw);
             }
-            w[j * p.g.arena_cap + e] = static_cast<int32_t>(nw);
           }
         }
-        ++seen;
+        seen += __popc(ballot);
       }
     }
   }
@@ -826,40 +848,55 @@ __device__ void ph_mutate(const ApplyParams& p, BlockRed& R, long long tid, long
 }
 
 // ---- H: move relocated rows (live slots, in order) ---------------------------------------------
+// A warp takes the touched rows 32 at a time, each lane reading one row's relocation flag; the
+// warp then moves the flagged rows one after another (lanes over the row's slots).  Most touched
+// rows are not relocated, so a warp passes over 32 rows per step instead of one.
 __device__ void ph_move(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int lane = threadIdx.x & 31;
   const long long warp = tid >> 5;
   const long long warps = threads >> 5;
   const int rows_out = c->rows_out, rows_in = c->rows_in;
-  for (long long i = warp; i < rows_out + rows_in; i += warps) {
-    const int side = i < rows_out ? 0 : 1;
-    const int s = side == 0 ? i : i - rows_out;
-    if (!(side == 0 ? p.reloc_out : p.reloc_in)[s]) continue;
-    const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
-    if (r >= c->n_old) continue;
-    const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
-    const unsigned dst = (side == 0 ? p.new_start_out : p.new_start_in)[s];
-    int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
-    int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
-    int written = 0;
-    for (int base = 0; base < desc.len; base += 32) {
-      const int e = base + lane;
-      const int32_t x = e < desc.len ? col[desc.start + e] : kDead;
-      const bool live = x >= 0;
-      const unsigned ballot = __ballot_sync(0xffffffffu, live);
-      const int pos = written + __popc(ballot & ((1u << lane) - 1));
-      if (live) {
-        col[dst + pos] = x;
-        for (int j = 0; j < p.k; ++j)
-          w[j * p.g.arena_cap + dst + pos] = w[j * p.g.arena_cap + desc.start + e];
-        if (!p.g.allow_multi) {
-          const long long ie = index_find(p.g, side == 0 ? edge_key(r, x) : edge_key(x, r));
-          if (ie >= 0) (side == 0 ? p.g.eout : p.g.ein)[ie] = dst + pos;
-          else set_error(&c->error, kErrInternal);
+  const long long total = static_cast<long long>(rows_out) + rows_in;
+  for (long long g0 = warp * 32; g0 < total; g0 += warps * 32) {
+    const long long mine = g0 + lane;
+    bool flagged = false;
+    if (mine < total) {
+      const int side = mine < rows_out ? 0 : 1;
+      const int s = side == 0 ? static_cast<int>(mine) : static_cast<int>(mine - rows_out);
+      flagged = (side == 0 ? p.reloc_out : p.reloc_in)[s] != 0 &&
+                (side == 0 ? p.rows_out : p.rows_in)[s] < c->n_old;
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, flagged);
+    while (todo) {
+      const long long i = g0 + __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int side = i < rows_out ? 0 : 1;
+      const int s = side == 0 ? static_cast<int>(i) : static_cast<int>(i - rows_out);
+      const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
+      const RowDesc desc = (side == 0 ? p.g.out_desc : p.g.in_desc)[r];
+      const unsigned dst = (side == 0 ? p.new_start_out : p.new_start_in)[s];
+      int32_t* col = side == 0 ? p.g.out_col : p.g.in_col;
+      int32_t* w = side == 0 ? p.g.out_w : p.g.in_w;
+      int written = 0;
+      for (int base = 0; base < desc.len; base += 32) {
+        const int e = base + lane;
+        const int32_t x = e < desc.len ? col[desc.start + e] : kDead;
+        const bool live = x >= 0;
+        const unsigned ballot = __ballot_sync(0xffffffffu, live);
+        const int pos = written + __popc(ballot & ((1u << lane) - 1));
+        if (live) {
+          col[dst + pos] = x;
+          for (int j = 0; j < p.k; ++j)
+            w[j * p.g.arena_cap + dst + pos] = w[j * p.g.arena_cap + desc.start + e];
+          if (!p.g.allow_multi) {
+            const long long ie = index_find(p.g, side == 0 ? edge_key(r, x) : edge_key(x, r));
+            if (ie >= 0) (side == 0 ? p.g.eout : p.g.ein)[ie] = dst + pos;
+            else set_error(&c->error, kErrInternal);
+          }
         }
+        written += __popc(ballot);
       }
-      written += __popc(ballot);
     }
   }
 }
@@ -1027,41 +1064,55 @@ __device__ void ph_finalize(const ApplyParams& p) {
   }
 }
 
-// Column statistics by a full pass over the live slots (after a maximum edge was deleted).
+// Column statistics by a full pass over the live slots (after a maximum edge was deleted): one
+// warp per row, its lanes over the row's slots (coalesced; a hub row does not hold up a thread).
 __global__ void k_rescan_columns(GraphView g, long long n, long long* out) {
   // out: per objective [max, count, sum]
+  const int lane = threadIdx.x & 31;
+  const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
   for (int j = 0; j < g.k; ++j) {
     long long mx = 0, sum = 0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n;
-         v += (long long)gridDim.x * blockDim.x) {
+    for (long long v = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; v < n;
+         v += warps) {
       const RowDesc desc = g.out_desc[v];
-      for (int e = 0; e < desc.len; ++e) {
+      for (int e = lane; e < desc.len; e += 32) {
         if (g.out_col[desc.start + e] < 0) continue;
         const long long w = g.out_w[j * g.arena_cap + desc.start + e];
         mx = max(mx, w);
         sum += w;
       }
     }
-    atomicMax(&out[3 * j], mx);
-    atomicAdd(reinterpret_cast<unsigned long long*>(&out[3 * j + 2]),
-              static_cast<unsigned long long>(sum));
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    if (lane == 0) {
+      if (mx > 0) atomicMax(&out[3 * j], mx);
+      if (sum != 0)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&out[3 * j + 2]),
+                  static_cast<unsigned long long>(sum));
+    }
   }
 }
 
 __global__ void k_rescan_count(GraphView g, long long n, long long* out) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
   for (int j = 0; j < g.k; ++j) {
     const long long mx = out[3 * j];
     long long cnt = 0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n;
-         v += (long long)gridDim.x * blockDim.x) {
+    for (long long v = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; v < n;
+         v += warps) {
       const RowDesc desc = g.out_desc[v];
-      for (int e = 0; e < desc.len; ++e) {
+      for (int e = lane; e < desc.len; e += 32) {
         if (g.out_col[desc.start + e] < 0) continue;
         cnt += g.out_w[j * g.arena_cap + desc.start + e] == mx;
       }
     }
-    atomicAdd(reinterpret_cast<unsigned long long*>(&out[3 * j + 1]),
-              static_cast<unsigned long long>(cnt));
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt != 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&out[3 * j + 1]),
+                static_cast<unsigned long long>(cnt));
   }
 }
 
@@ -2084,7 +2135,7 @@ void graph_rescan_columns(Context& ctx, Graph& g) {
   const size_t k = static_cast<size_t>(g.k > 0 ? g.k : 1);
   out.reserve(3 * k);
   DYNGB200_CUDA(cudaMemsetAsync(out.ptr, 0, 3 * k * sizeof(long long), ctx.stream));
-  const int grid = grid_for(g.n, kBlock, ctx.sm_count);
+  const int grid = grid_for(32 * g.n, kBlock, ctx.sm_count);  // a warp per row
   ctx.launches += 2;
   k_rescan_columns<<<grid, kBlock, 0, ctx.stream>>>(g.view(), g.n, out.ptr);
   k_rescan_count<<<grid, kBlock, 0, ctx.stream>>>(g.view(), g.n, out.ptr);

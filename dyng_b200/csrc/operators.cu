@@ -27,6 +27,10 @@ namespace {
 
 constexpr int kOpBlock = 256;
 constexpr int kMarked = -2;  // pointer jumping: an invalidated ancestor was reached
+// Rows longer than kOpHeavy slots are not read by one warp: the warp that meets one lists its
+// kOpChunk-slot chunks, and a second launch reads every chunk with its own warp.
+constexpr int kOpHeavy = 2048;
+constexpr int kOpChunk = 1024;
 
 // The counters one step leaves for the host.
 struct OpCounts {
@@ -34,8 +38,24 @@ struct OpCounts {
   int far;         // entries on the far pile being appended to
   int candidates;  // vertices the pull re-evaluates
   int jumped;      // pointer jumping: a chain moved on this round and goes on
+  int heavy;       // chunks listed for the heavy-row launch
   unsigned long long minimum;  // smallest distance of a list (kPackedInf: none)
 };
+
+// Lists the chunks of a heavy row as (vertex, first slot) entries and returns how many it listed:
+// all of them, or those that fit below `cap` (the caller reads the rest of the row itself).  Every
+// entry below min(oc->heavy, cap) is written by the warp that reserved it.  Called by a whole warp.
+__device__ __forceinline__ int op_list_chunks(int v, int len, int2* heavy, long long cap,
+                                              OpCounts* oc) {
+  const int chunks = (len + kOpChunk - 1) / kOpChunk;
+  int base = 0;
+  if ((threadIdx.x & 31) == 0) base = atomicAdd(&oc->heavy, chunks);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const long long room = cap - base;
+  const int listed = room <= 0 ? 0 : static_cast<int>(min(static_cast<long long>(chunks), room));
+  for (int q = threadIdx.x & 31; q < listed; q += 32) heavy[base + q] = make_int2(v, q * kOpChunk);
+  return listed;
+}
 
 __device__ __forceinline__ Packing packing_of(int bits) {
   Packing pk;
@@ -222,32 +242,52 @@ __global__ void k_op_heads(SsspParams p, int bits, u64 maxd, int gen_inv, int ge
 }
 
 // The pull (fused.cuh:258-285): every candidate takes the minimum over its in-row of
-// pack(d(y) + w, y); with an offer it joins the frontier.  One warp per candidate.
-__global__ void k_op_pull(SsspParams p, int bits, u64 maxd, int gen_pull, int count,
-                          OpCounts* oc) {
-  const Packing pk = packing_of(bits);
+// pack(d(y) + w, y); with an offer it joins the frontier.  One warp per candidate; heavy rows
+// are listed by chunks for k_op_pull_heavy.
+__device__ __forceinline__ void op_pull_range(const SsspParams& p, const Packing& pk, u64 maxd,
+                                              int gen_pull, int v, const RowDesc& d, int e0,
+                                              int e1, OpCounts* oc) {
   const int lane = threadIdx.x & 31;
   const int32_t* wcol = p.g.in_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+  u64 best = kPackedInf;
+  for (int e = e0 + lane; e < e1; e += 32) {
+    const int y = p.g.in_col[d.start + e];
+    if (y < 0) continue;
+    // the source's word is distance 0 for good
+    const u64 word = y == p.source ? 0 : ld_cg(&p.packed[y]);
+    if (word == kPackedInf) continue;
+    const u64 nd = (y == p.source ? 0 : pk.dist(word)) + static_cast<u64>(wcol[d.start + e]);
+    if (nd > maxd) continue;
+    best = min(best, pk.pack(nd, y));
+  }
+  for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if (lane == 0 && best != kPackedInf) {
+    const u64 old = atomicMin(&p.packed[v], best);
+    if (best < old) p.touch_stamp[v] = p.touch_gen;
+    if (op_claim(p.stamp, v, gen_pull)) p.frontier[append_slot(&oc->next)] = v;
+  }
+}
+
+__global__ void k_op_pull(SsspParams p, int bits, u64 maxd, int gen_pull, int count, int2* heavy,
+                          long long heavy_cap, OpCounts* oc) {
+  const Packing pk = packing_of(bits);
   for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
     const int v = p.candidates[i];
     const RowDesc d = p.g.in_desc[v];
-    u64 best = kPackedInf;
-    for (int e = lane; e < d.len; e += 32) {
-      const int y = p.g.in_col[d.start + e];
-      if (y < 0) continue;
-      // the source's word is distance 0 for good
-      const u64 word = y == p.source ? 0 : ld_cg(&p.packed[y]);
-      if (word == kPackedInf) continue;
-      const u64 nd = (y == p.source ? 0 : pk.dist(word)) + static_cast<u64>(wcol[d.start + e]);
-      if (nd > maxd) continue;
-      best = min(best, pk.pack(nd, y));
-    }
-    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if (lane == 0 && best != kPackedInf) {
-      const u64 old = atomicMin(&p.packed[v], best);
-      if (best < old) p.touch_stamp[v] = p.touch_gen;
-      if (op_claim(p.stamp, v, gen_pull)) p.frontier[append_slot(&oc->next)] = v;
-    }
+    const int listed = d.len > kOpHeavy ? op_list_chunks(v, d.len, heavy, heavy_cap, oc) : 0;
+    if (listed * kOpChunk < d.len)
+      op_pull_range(p, pk, maxd, gen_pull, v, d, listed * kOpChunk, d.len, oc);
+  }
+}
+
+__global__ void k_op_pull_heavy(SsspParams p, int bits, u64 maxd, int gen_pull, const int2* heavy,
+                                long long heavy_cap, OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  const long long count = min(static_cast<long long>(ld_cg(&oc->heavy)), heavy_cap);
+  for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
+    const int2 h = heavy[i];
+    const RowDesc d = p.g.in_desc[h.x];
+    op_pull_range(p, pk, maxd, gen_pull, h.x, d, h.y, min(d.len, h.y + kOpChunk), oc);
   }
 }
 
@@ -284,34 +324,58 @@ __global__ void k_op_split(SsspParams p, int bits, u64 threshold, int gen, const
 
 // One push step of the near-far loop (fused.cuh:288-417): every near vertex u offers
 // pack(d(u) + w, u) to its out-neighbours; an improved neighbour joins the next near frontier
-// (below the threshold) or the far pile.  One warp per near vertex.
-__global__ void k_op_push(SsspParams p, int bits, u64 maxd, u64 threshold, int gen,
-                          const int* near, int count, int* next, int* far, OpCounts* oc) {
-  const Packing pk = packing_of(bits);
-  const int lane = threadIdx.x & 31;
+// (below the threshold) or the far pile.  One warp per near vertex; heavy rows are listed by
+// chunks for k_op_push_heavy.
+__device__ __forceinline__ void op_push_range(const SsspParams& p, const Packing& pk, u64 maxd,
+                                              u64 threshold, int gen, int u, u64 du,
+                                              const RowDesc& d, int e0, int e1, int* next,
+                                              int* far, OpCounts* oc) {
   const int32_t* wcol = p.g.out_w + static_cast<long long>(p.objective) * p.g.arena_cap;
+  for (int e = e0 + (threadIdx.x & 31); e < e1; e += 32) {
+    const int y = p.g.out_col[d.start + e];
+    if (y < 0 || y == p.source) continue;
+    const u64 nd = du + static_cast<u64>(wcol[d.start + e]);
+    if (nd > maxd) continue;
+    const u64 cand = pk.pack(nd, u);
+    if (cand >= ld_cg(&p.packed[y])) continue;
+    const u64 old = atomicMin(&p.packed[y], cand);
+    if (cand < old) p.touch_stamp[y] = p.touch_gen;
+    if (nd >= pk.dist(old)) continue;
+    if (nd < threshold) {
+      if (op_claim(p.stamp, y, gen)) next[append_slot(&oc->next)] = y;
+    } else if (atomicExch(&p.in_far[y], 1) == 0) {
+      far[append_slot(&oc->far)] = y;
+    }
+  }
+}
+
+__global__ void k_op_push(SsspParams p, int bits, u64 maxd, u64 threshold, int gen,
+                          const int* near, int count, int* next, int* far, int2* heavy,
+                          long long heavy_cap, OpCounts* oc) {
+  const Packing pk = packing_of(bits);
   for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
     const int u = near[i];
     const u64 wu = ld_cg(&p.packed[u]);
     if (wu == kPackedInf) continue;
-    const u64 du = pk.dist(wu);
     const RowDesc d = p.g.out_desc[u];
-    for (int e = lane; e < d.len; e += 32) {
-      const int y = p.g.out_col[d.start + e];
-      if (y < 0 || y == p.source) continue;
-      const u64 nd = du + static_cast<u64>(wcol[d.start + e]);
-      if (nd > maxd) continue;
-      const u64 cand = pk.pack(nd, u);
-      if (cand >= ld_cg(&p.packed[y])) continue;
-      const u64 old = atomicMin(&p.packed[y], cand);
-      if (cand < old) p.touch_stamp[y] = p.touch_gen;
-      if (nd >= pk.dist(old)) continue;
-      if (nd < threshold) {
-        if (op_claim(p.stamp, y, gen)) next[append_slot(&oc->next)] = y;
-      } else if (atomicExch(&p.in_far[y], 1) == 0) {
-        far[append_slot(&oc->far)] = y;
-      }
-    }
+    const int listed = d.len > kOpHeavy ? op_list_chunks(u, d.len, heavy, heavy_cap, oc) : 0;
+    if (listed * kOpChunk < d.len)
+      op_push_range(p, pk, maxd, threshold, gen, u, pk.dist(wu), d, listed * kOpChunk, d.len,
+                    next, far, oc);
+  }
+}
+
+__global__ void k_op_push_heavy(SsspParams p, int bits, u64 maxd, u64 threshold, int gen,
+                                int* next, int* far, const int2* heavy, long long heavy_cap,
+                                OpCounts* oc) {
+  const Packing pk = packing_of(bits);
+  const long long count = min(static_cast<long long>(ld_cg(&oc->heavy)), heavy_cap);
+  for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
+    const int2 h = heavy[i];
+    const u64 wu = ld_cg(&p.packed[h.x]);  // the word the listing warp read, or a smaller one
+    const RowDesc d = p.g.out_desc[h.x];
+    op_push_range(p, pk, maxd, threshold, gen, h.x, pk.dist(wu), d, h.y,
+                  min(d.len, h.y + kOpChunk), next, far, oc);
   }
 }
 
@@ -415,6 +479,8 @@ void run_operators(Context& ctx, const SsspParams& p) {
   OpCounts* oc = reinterpret_cast<OpCounts*>(ws.op_counts.ptr);
   OpCounts* hc = reinterpret_cast<OpCounts*>(ws.op_host.ptr);
   const int grid = operators_grid(ctx);
+  int2* heavy = p.heavy_a;  // (vertex, first slot) chunks of the heavy rows of one launch
+  const long long heavy_cap = static_cast<long long>(ws.heavy_a.count / 2);
   auto read_ctl = [&]() {
     DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, c, sizeof(UpdateCtl), cudaMemcpyDeviceToHost, s));
     DYNGB200_CUDA(cudaStreamSynchronize(s));
@@ -438,6 +504,7 @@ void run_operators(Context& ctx, const SsspParams& p) {
     hc->far = far;
     hc->candidates = candidates;
     hc->jumped = 0;
+    hc->heavy = 0;
     hc->minimum = kPackedInf;
     DYNGB200_CUDA(cudaMemcpyAsync(oc, hc, sizeof(OpCounts), cudaMemcpyHostToDevice, s));
   };
@@ -519,8 +586,10 @@ void run_operators(Context& ctx, const SsspParams& p) {
       launched(1);
       r = counts();
       if (r.candidates > 0) {
-        k_op_pull<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, r.candidates, oc);
-        launched(1);
+        k_op_pull<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, r.candidates, heavy,
+                                            heavy_cap, oc);
+        k_op_pull_heavy<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, heavy, heavy_cap, oc);
+        launched(2);
         r = counts();
       }
       frontier_count = r.next;
@@ -554,8 +623,10 @@ void run_operators(Context& ctx, const SsspParams& p) {
         ++gen;
         reset(0, far_count);
         k_op_push<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, threshold, gen, lists[cur], near_count,
-                                            lists[cur ^ 1], fars[far_cur], oc);
-        launched(1);
+                                            lists[cur ^ 1], fars[far_cur], heavy, heavy_cap, oc);
+        k_op_push_heavy<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, threshold, gen, lists[cur ^ 1],
+                                                  fars[far_cur], heavy, heavy_cap, oc);
+        launched(2);
         r = counts();
         cur ^= 1;
         near_count = r.next;

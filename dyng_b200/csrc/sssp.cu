@@ -1383,15 +1383,18 @@ __global__ void __launch_bounds__(kThreads, 3) k_sssp(SsspParams p) {
 
 // Canonicalise an imported tree (sssp.cpp:377-396): for every edge (u,v) with
 // dist[u] + w == dist[v] and u < parent[v], parent[v] becomes u.  Lowest id wins via atomicMin.
+// One warp per row, its lanes over the row's slots.
 __global__ void k_canonicalize(GraphView g, int objective, int32_t source, long long n,
                                const long long* dist, int32_t* parent) {
   const int32_t* wcol = g.out_w + static_cast<long long>(objective) * g.arena_cap;
-  for (long long u = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; u < n;
-       u += static_cast<long long>(gridDim.x) * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  for (long long u = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; u < n;
+       u += warps) {
     const long long du = dist[u];
     if (du >= kInfinity / 2) continue;
     const RowDesc desc = g.out_desc[u];
-    for (int e = 0; e < desc.len; ++e) {
+    for (int e = lane; e < desc.len; e += 32) {
       const int v = g.out_col[desc.start + e];
       if (v < 0 || v == source) continue;
       if (du + wcol[desc.start + e] == dist[v]) atomicMin(&parent[v], static_cast<int32_t>(u));
