@@ -1411,8 +1411,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply(ApplyParams p, ApplyLaunch 
 // one block; `mark` >= 0 records the end of the previous step in apply_ns[mark].
 enum ApplyStep {
   kStepValidate, kStepPlan, kStepPairs, kStepMatch, kStepResolve, kStepRowOffsets,
-  kStepFillSegments, kStepSortSegments, kStepAlloc, kStepMutate, kStepMoveAppend, kStepRows,
-  kStepFinalize
+  kStepFillSegments, kStepSortSegments, kStepAlloc, kStepMutate, kStepMove, kStepAppend,
+  kStepRows, kStepFinalize
 };
 
 __global__ void __launch_bounds__(kBlock, 3) k_apply_step(ApplyParams p, ApplyLaunch L, int step,
@@ -1453,10 +1453,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_apply_step(ApplyParams p, ApplyLa
       if (tid == 0) c->committing = 1;
       ph_mutate(p, red, tid, threads);
       break;
-    case kStepMoveAppend:
-      ph_move(p, tid, threads);
-      ph_append(p, red, tid, threads);
-      break;
+    case kStepMove: ph_move(p, tid, threads); break;  // H and I touch disjoint slots
+    case kStepAppend: ph_append(p, red, tid, threads); break;
     case kStepRows:
       ph_rows_final(p, red, tid, threads);
       ph_count_written_max(p, red, tid, threads);
@@ -2264,12 +2262,14 @@ void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective, l
   L.barrier_extra = ctx.test_barrier_kernel == 2 ? 0 : ctx.test_barrier_extra;
   if (stepped) {
     // the steps in the fused kernel's order; apply_ns gets the same marks (the start of the
-    // applier, then the end of each step; the plan is timed with the pairs, as in the fused
-    // kernel, where the two overlap)
+    // applier, then the end of each step of the fused kernel)
     int mark = 0;
     auto step = [&](int which, int grid) {
-      k_apply_step<<<grid, kBlock, 0, s>>>(p, L, which, which == kStepPairs ? -1 : mark);
-      if (which != kStepPairs) ++mark;
+      // the plan and the pairs, and the moves and the appends, are one step each in the fused
+      // kernel: the second of each pair records no mark
+      const bool second = which == kStepPairs || which == kStepAppend;
+      k_apply_step<<<grid, kBlock, 0, s>>>(p, L, which, second ? -1 : mark);
+      if (!second) ++mark;
       ++ctx.launches;
       DYNGB200_CUDA(cudaGetLastError());
     };
@@ -2285,7 +2285,8 @@ void apply_launch(Context& ctx, Graph& g, const StagedBatch& b, int objective, l
     }
     step(kStepAlloc, blocks);
     step(kStepMutate, blocks);
-    step(kStepMoveAppend, blocks);
+    step(kStepMove, blocks);
+    step(kStepAppend, blocks);
     step(kStepRows, blocks);
     step(kStepFinalize, 1);
     return;
