@@ -848,9 +848,11 @@ __device__ void ph_mutate(const ApplyParams& p, BlockRed& R, long long tid, long
 }
 
 // ---- H: move relocated rows (live slots, in order) ---------------------------------------------
-// A warp takes the touched rows 32 at a time, each lane reading one row's relocation flag; the
-// warp then moves the flagged rows one after another (lanes over the row's slots).  Most touched
-// rows are not relocated, so a warp passes over 32 rows per step instead of one.
+// A warp takes the touched rows 32 at a time, each lane reading one row's relocation flag and
+// length; the warp then moves the flagged rows that hold slots one after another (lanes over the
+// row's slots).  Most relocated rows are empty (a vertex without edges has no slack: its first
+// edge relocates it, at R-MAT scale 22 about 70k rows per 100k-change batch), and they have
+// nothing to move, so they take no warp step.
 __device__ void ph_move(const ApplyParams& p, long long tid, long long threads) {
   UpdateCtl* c = p.ctl;
   const int lane = threadIdx.x & 31;
@@ -864,8 +866,9 @@ __device__ void ph_move(const ApplyParams& p, long long tid, long long threads) 
     if (mine < total) {
       const int side = mine < rows_out ? 0 : 1;
       const int s = side == 0 ? static_cast<int>(mine) : static_cast<int>(mine - rows_out);
-      flagged = (side == 0 ? p.reloc_out : p.reloc_in)[s] != 0 &&
-                (side == 0 ? p.rows_out : p.rows_in)[s] < c->n_old;
+      const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
+      if ((side == 0 ? p.reloc_out : p.reloc_in)[s] != 0 && r < c->n_old)
+        flagged = (side == 0 ? p.g.out_desc : p.g.in_desc)[r].len > 0;
     }
     unsigned todo = __ballot_sync(0xffffffffu, flagged);
     while (todo) {
@@ -1818,11 +1821,13 @@ struct MaintenanceTimer {
 }  // namespace
 
 // (Re)build the edge index with room for `extra` more edges and at least `min_cap` slots.
-// Slots of an edge index for the graph's edges plus `extra` insertions (load <= 1/2 after the
-// build), at least min_cap.
+// Slots of an edge index for the graph's edges plus `extra` insertions (load <= 1/3 after the
+// build), at least min_cap.  A rebuild comes when live plus deleted keys pass 60 %: with a third
+// the graph can grow by 80 % of its edges before the next one (at R-MAT scale 22 a rebuild takes
+// 60-85 ms; at a half, 1M-change batches met one every 15 batches).
 static long long index_want(const Graph& g, long long extra, long long min_cap) {
   long long want = 1024;
-  while (want < 2 * (g.host_counters.m + extra) + 65536 || want < min_cap) want <<= 1;
+  while (want < 3 * (g.host_counters.m + extra) + 65536 || want < min_cap) want <<= 1;
   return want;
 }
 
