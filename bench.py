@@ -447,8 +447,9 @@ def main():
     value = summ[args.schedule]["value"]
     timed_stats = head.stats
     # end to end: batches in pinned host memory through the public call, headline schedule
-    e2e_lat, e2e_sizes = [], []
+    e2e_lat, e2e_sizes, e2e_stats = [], [], []
     h2d = 0
+    import gc
     for step in range(args.steps):
         b = make_batch(tree.parents)
         pinned = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in
@@ -456,12 +457,23 @@ def main():
         arrs = [p.numpy() for p in pinned]
         hb = D.EdgeBatch.from_arrays(*arrs)
         torch.cuda.synchronize()
+        gc.collect()  # as in the arms: no collection (and device free) inside the timed call
+        gc.disable()
         t0 = time.perf_counter()
-        D.sssp.update(g, hb, tree, schedule=head.schedule, scheduler=head.scheduler)
+        st = D.sssp.update(g, hb, tree, schedule=head.schedule, scheduler=head.scheduler)
         e2e_lat.append(time.perf_counter() - t0)
+        gc.enable()
         e2e_sizes.append(b.size)
+        e2e_stats.append(st)
         h2d = sum(a.nbytes for a in arrs)
     e2e_value = world * sum(e2e_sizes) / sum(e2e_lat)
+    # where an end-to-end call's time goes (us, means): the library's host phases (checks and
+    # staging with the batch copies queued, queuing the applier, queuing the sssp kernel and the
+    # read-back, waiting for the device) and the two kernels' device times
+    e2e_parts = {"host_us": [round(float(np.mean([s.host_us[i] for s in e2e_stats])), 1)
+                             for i in range(4)],
+                 "apply_us": round(1000 * float(np.mean([s.apply_ms for s in e2e_stats])), 1),
+                 "sssp_us": round(1000 * float(np.mean([s.sssp_ms for s in e2e_stats])), 1)}
 
     # correctness at full size: the updated tree equals a from-scratch compute on the new graph
     verified = None
@@ -492,8 +504,9 @@ def main():
     stages = {name: round(float(np.mean([s.stages_ms()[name] for s in timed_stats])), 4)
               for name in timed_stats[0].stages_ms()}
     # the batch applier's steps: the end of each (us since it began; 0: not reached)
-    apply_steps = [round(float(np.mean([s.apply_step_us[i] for s in timed_stats])), 1)
-                   for i in range(1, 12)]
+    apply_steps = {name: [round(float(np.mean([s.apply_step_us[i] for s in a.stats])), 1)
+                          for i in range(1, 12)]
+                   for name, a in arms.items()}
     shape = {k: float(np.mean([getattr(s, k) for s in timed_stats]))
              for k in ("iterations", "epochs", "pushes", "invalidated", "affected", "rounds",
                        "touched", "delta", "grid_blocks")}
@@ -568,7 +581,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "changed edges/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": ctypes.sizeof(D._native.Stats),
                     "p50_ms": 1000 * float(np.percentile(e2e_lat, 50)),
-                    "p99_ms": 1000 * float(np.percentile(e2e_lat, 99))},
+                    "p99_ms": 1000 * float(np.percentile(e2e_lat, 99)), "parts": e2e_parts},
             "gpu_launches": int(sum(s.kernel_launches for s in timed_stats)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None,

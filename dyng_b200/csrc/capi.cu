@@ -262,6 +262,8 @@ dyngb200_status dyngb200_context_destroy(dyngb200_context ctx) {
     if (!ctx) return;
     DeviceGuard guard(ctx->ctx.device);
     cudaStreamSynchronize(ctx->ctx.stream);
+    for (cudaEvent_t e : ctx->ctx.update_events)
+      if (e) cudaEventDestroy(e);
     if (ctx->ctx.own_stream) cudaStreamDestroy(ctx->ctx.stream);
     delete ctx;
   });

@@ -263,6 +263,10 @@ struct Context {
   int test_barrier_extra = 0;
   int test_barrier_kernel = 0;  // the phantom arrivals: 0 every kernel, 1 the applier, 2 sssp
   int test_no_cooperative = 0;
+  // the timing events of an update (before the applier, between the kernels, after the sssp
+  // kernel): created at the first update and reused (a context has one update in flight at a
+  // time), destroyed with the context
+  cudaEvent_t update_events[3] = {nullptr, nullptr, nullptr};
 };
 
 // The persistent kernels need cooperative launch; checked before anything of a call changes.
@@ -454,7 +458,7 @@ struct PendingUpdate {
   int blocks = 0;
   bool operators = false;  // the operators engine (ordinary launches, the loop on the host)
   long long launches0 = 0;
-  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;  // the context's update events
   double host_us[4] = {};  // see dyngb200_stats::host_us
   PendingUpdate() = default;
   PendingUpdate(const PendingUpdate&) = delete;

@@ -1669,11 +1669,7 @@ static void enqueue_attempt(PendingUpdate& u) {
   u.host_us[2] += us_since(h1);
 }
 
-PendingUpdate::~PendingUpdate() {
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
-  if (e2) cudaEventDestroy(e2);
-}
+PendingUpdate::~PendingUpdate() = default;  // the events belong to the context
 
 // update(), first half: host checks that need no device result, the batch staged on the device
 // and the first attempt queued.  Nothing waits for the GPU here (batches in pinned host memory
@@ -1695,9 +1691,11 @@ void sssp_update_begin(Context& ctx, Graph& g, Tree& t, const dyngb200_batch& ba
   graph_index_reserve(ctx, g, batch.num_insertions * (g.props.directed ? 1 : 2));
   u.b = stage_batch(ctx, batch, g.k);
   u.blocks = persistent_blocks(ctx, sched);
-  DYNGB200_CUDA(cudaEventCreate(&u.e0));
-  DYNGB200_CUDA(cudaEventCreate(&u.e1));
-  DYNGB200_CUDA(cudaEventCreate(&u.e2));
+  for (cudaEvent_t& e : ctx.update_events)
+    if (!e) DYNGB200_CUDA(cudaEventCreate(&e));
+  u.e0 = ctx.update_events[0];
+  u.e1 = ctx.update_events[1];
+  u.e2 = ctx.update_events[2];
   u.host_us[0] = us_since(h0);
   enqueue_attempt(u);
 }
