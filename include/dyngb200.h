@@ -110,10 +110,10 @@ typedef struct dyngb200_stats {
   int64_t epochs;      /* schedule-dependent */
   int64_t pushes;      /* schedule-dependent */
   int32_t packed_parents;
-  int32_t engine_used;
+  int32_t engine_used; /* dyngb200_engine that ran: FUSED or OPERATORS */
   int64_t delta;       /* near-far width that ran */
   int64_t max_weight;  /* bound weight of the packing */
-  int32_t grid_blocks; /* persistent grid that ran */
+  int32_t grid_blocks; /* persistent grid that ran (operators engine: its launches' grid) */
   int32_t invalidation; /* 0 pointer jumping, 1 subtree walk */
   float apply_ms;      /* device time of the batch applier */
   float sssp_ms;       /* device time of the sssp kernel */
