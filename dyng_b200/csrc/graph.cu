@@ -1555,8 +1555,8 @@ ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int object
 // ------------------------------------------------------------------------------------------------
 void Workspace::reserve_vertices(long long n_cap, cudaStream_t s) {
   pj_blk.reserve(2 * kPjMaxBlocks, s);
-  op_counts.reserve(4, s);
-  op_host.reserve(4);
+  op_counts.reserve(8, s);
+  op_host.reserve(8);
   if (n_cap <= n_sized) return;
   // buffers are released before they are reallocated: until every one is back, the workspace
   // counts as unsized (a failed allocation makes the next call start over, never skip)

@@ -2,7 +2,10 @@
 // persistent kernel (sssp.cu), as a sequence of ordinary kernel launches whose loop is driven
 // from the host, which reads a few counters after each step (the reference's engine::operators,
 // cpp/src/algorithms/sssp/operators.cuh and its host loop in operators.cu: one synchronisation
-// per push iteration and per threshold raise).
+// per push iteration and per threshold raise).  Between the roots and the first push the counts
+// stay on the device (the heads, the pull, the first threshold and split read them there), so an
+// update synchronises once for the roots, once per invalidation round or walk level, once for
+// the first split, and once per push step or threshold raise.
 //
 // It needs no cooperative launch, so it is what engine::automatic runs on a device without one
 // (as the reference does, sssp.cpp:195-226), and what options::cuda_engine = operators asks for.
@@ -39,7 +42,10 @@ struct OpCounts {
   int candidates;  // vertices the pull re-evaluates
   int jumped;      // pointer jumping: a chain moved on this round and goes on
   int heavy;       // chunks listed for the heavy-row launch
-  unsigned long long minimum;  // smallest distance of a list (kPackedInf: none)
+  int in_count;    // length of the list a split reads (set by k_op_threshold)
+  int source;      // compute: the source, staged for its copy into the frontier
+  unsigned long long minimum;    // smallest distance of a list (kPackedInf: none)
+  unsigned long long threshold;  // the near-far threshold of the current split and pushes
 };
 
 // Lists the chunks of a heavy row as (vertex, first slot) entries and returns how many it listed:
@@ -268,9 +274,10 @@ __device__ __forceinline__ void op_pull_range(const SsspParams& p, const Packing
   }
 }
 
-__global__ void k_op_pull(SsspParams p, int bits, u64 maxd, int gen_pull, int count, int2* heavy,
+__global__ void k_op_pull(SsspParams p, int bits, u64 maxd, int gen_pull, int2* heavy,
                           long long heavy_cap, OpCounts* oc) {
   const Packing pk = packing_of(bits);
+  const int count = ld_cg(&oc->candidates);  // left by the roots, the invalidation and the heads
   for (long long i = op_tid() >> 5; i < count; i += op_threads() >> 5) {
     const int v = p.candidates[i];
     const RowDesc d = p.g.in_desc[v];
@@ -292,8 +299,10 @@ __global__ void k_op_pull_heavy(SsspParams p, int bits, u64 maxd, int gen_pull, 
 }
 
 // The smallest distance of a list's vertices (none: kPackedInf).
-__global__ void k_op_min(SsspParams p, int bits, const int* list, int count, OpCounts* oc) {
+__global__ void k_op_min(SsspParams p, int bits, const int* list, const int* count_at,
+                         OpCounts* oc) {
   const Packing pk = packing_of(bits);
+  const int count = ld_cg(count_at);
   u64 local = kPackedInf;
   for (long long i = op_tid(); i < count; i += op_threads()) {
     const u64 word = ld_cg(&p.packed[list[i]]);
@@ -306,9 +315,28 @@ __global__ void k_op_min(SsspParams p, int bits, const int* list, int count, OpC
 // A list split at the threshold: below it into the near frontier (claimed once per step), the
 // rest onto the far pile (the first split: once, by the vertex's flag; a split of the far pile:
 // the entries that stay).  Entries taken off the far pile lose the flag.
-__global__ void k_op_split(SsspParams p, int bits, u64 threshold, int gen, const int* list,
-                           int count, int from_far, int* near, int* far, OpCounts* oc) {
+// The threshold of a split, on the device: the first one min + delta, each later one
+// max(threshold, min) + delta (fused.cuh:288-417); the list to split moves to `in_count`, and the
+// near frontier and the far pile it fills start empty.  One thread.
+__global__ void k_op_threshold(OpCounts* oc, u64 delta, int first, int from_far) {
+  const u64 m = oc->minimum;
+  if (first) {
+    oc->threshold = (m == kPackedInf ? 0 : m) + delta;
+  } else {
+    const u64 t = oc->threshold;
+    oc->threshold = (m == kPackedInf ? t : max(t, m)) + delta;
+  }
+  oc->minimum = kPackedInf;
+  oc->in_count = from_far ? oc->far : oc->next;
+  oc->next = 0;
+  oc->far = 0;
+}
+
+__global__ void k_op_split(SsspParams p, int bits, int gen, const int* list, int from_far,
+                           int* near, int* far, OpCounts* oc) {
   const Packing pk = packing_of(bits);
+  const u64 threshold = ld_cg(&oc->threshold);
+  const int count = ld_cg(&oc->in_count);
   for (long long i = op_tid(); i < count; i += op_threads()) {
     const int v = list[i];
     const u64 word = ld_cg(&p.packed[v]);
@@ -475,7 +503,7 @@ void run_operators(Context& ctx, const SsspParams& p) {
   UpdateCtl* c = p.ctl;
   expects(ws.op_counts.ptr != nullptr && ws.op_host.ptr != nullptr,
           "sssp: the workspace was not reserved", DYNGB200_INTERNAL);
-  static_assert(sizeof(OpCounts) <= 4 * sizeof(unsigned long long), "the step counters fit");
+  static_assert(sizeof(OpCounts) <= 8 * sizeof(unsigned long long), "the step counters fit");
   OpCounts* oc = reinterpret_cast<OpCounts*>(ws.op_counts.ptr);
   OpCounts* hc = reinterpret_cast<OpCounts*>(ws.op_host.ptr);
   const int grid = operators_grid(ctx);
@@ -497,64 +525,67 @@ void run_operators(Context& ctx, const SsspParams& p) {
                                   ? plan.sched_delta
                                   : (p.delta_override > 0 ? p.delta_override : plan.delta);
   const u64 delta = static_cast<u64>(delta_sel > 0 ? delta_sel : 1);
-  // the counters of the next step: `candidates` carried over (the pull's list grows through the
-  // roots, the invalidation and the heads), `far` the pile's current length, the rest cleared
-  auto reset = [&](int candidates, int far) {
-    hc->next = 0;
-    hc->far = far;
-    hc->candidates = candidates;
-    hc->jumped = 0;
-    hc->heavy = 0;
-    hc->minimum = kPackedInf;
+  // the step counters live in pinned memory (hc) and on the device (oc); the host changes hc
+  // and copies it over oc before a step, and copies oc back into hc after the steps it reads
+  auto put = [&]() {
     DYNGB200_CUDA(cudaMemcpyAsync(oc, hc, sizeof(OpCounts), cudaMemcpyHostToDevice, s));
   };
-  auto counts = [&]() {
+  auto get = [&]() {
     DYNGB200_CUDA(cudaMemcpyAsync(hc, oc, sizeof(OpCounts), cudaMemcpyDeviceToHost, s));
-    DYNGB200_CUDA(cudaStreamSynchronize(s));
-    return *hc;
   };
+  auto wait = [&]() { DYNGB200_CUDA(cudaStreamSynchronize(s)); };
   auto launched = [&](int k) {
     ctx.launches += k;
     DYNGB200_CUDA(cudaGetLastError());
   };
   OpSummary sum{};
   int gen = p.generation;
-  int frontier_count = 0;
   int* lists[2] = {p.near_a, p.near_b};
   int* fars[2] = {p.far_a, p.far_b};
+  *hc = OpCounts{};
+  hc->minimum = kPackedInf;
   if (n > 0) {
     k_op_setup<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, n);
     launched(1);
   }
+  bool frontier = false;  // the pull's frontier (p.frontier, oc->next entries) is ready
   if (p.from_scratch) {
-    hc->next = p.source;  // staged in pinned memory: the copy is queued, then waited for
-    DYNGB200_CUDA(cudaMemcpyAsync(p.frontier, &hc->next, sizeof(int), cudaMemcpyHostToDevice, s));
-    DYNGB200_CUDA(cudaStreamSynchronize(s));
-    frontier_count = n > 0 ? 1 : 0;
+    if (n > 0) {
+      hc->source = p.source;  // staged in pinned memory: copied in stream order
+      DYNGB200_CUDA(cudaMemcpyAsync(p.frontier, &hc->source, sizeof(int), cudaMemcpyHostToDevice,
+                                    s));
+      hc->next = 1;
+      put();
+      frontier = true;
+    }
   } else {
     const int gen_inv = ++gen;
     const int gen_pull = ++gen;
     const bool walk = plan.sched_walk != 0 && p.tree_trusted != 0;
-    // ---- roots, and the repack's overflow check ----------------------------------------------
-    reset(0, 0);
+    // ---- roots, and the repack's overflow check: one synchronisation for both ----------------
+    put();
     k_op_roots<<<grid, kOpBlock, 0, s>>>(p, gen_inv, lists[0], walk ? 1 : 0, oc);
     launched(1);
-    OpCounts r = counts();
-    const UpdateCtl after_roots = read_ctl();
+    get();
+    DYNGB200_CUDA(cudaMemcpyAsync(ws.host_ctl.ptr, c, sizeof(UpdateCtl), cudaMemcpyDeviceToHost, s));
+    wait();
+    const UpdateCtl after_roots = *ws.host_ctl.ptr;
     if (after_roots.error != 0) return;  // an input distance that does not fit: nothing written
     if (walk) {
       // ---- invalidation by a walk down the old tree, level by level --------------------------
-      int level = r.next, cur = 0;
+      int level = hc->next, cur = 0;
       while (level > 0) {
         if (sum.levels > n + 1) {
           sum.error |= kErrNotConverged;
           break;
         }
-        reset(r.candidates, 0);
+        hc->next = 0;
+        put();
         k_op_walk<<<grid, kOpBlock, 0, s>>>(p, gen_inv, lists[cur], level, lists[cur ^ 1], oc);
         launched(1);
-        r = counts();
-        level = r.next;
+        get();
+        wait();
+        level = hc->next;
         cur ^= 1;
         ++sum.levels;
       }
@@ -569,48 +600,44 @@ void run_operators(Context& ctx, const SsspParams& p) {
         k_op_pj_start<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n);
         launched(1);
         for (int round = 0; round < max_rounds; ++round) {
-          reset(r.candidates, 0);
+          hc->jumped = 0;
+          put();
           k_op_pj_round<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n, oc);
           launched(1);
-          r = counts();
+          get();
+          wait();
           sum.rounds = round + 1;
-          sum.active = r.jumped;
-          if (!r.jumped) break;
+          sum.active = hc->jumped;
+          if (!hc->jumped) break;
         }
       }
     }
-    // ---- insertion heads, then the pull over every candidate --------------------------------
+    // ---- insertion heads, then the pull over every candidate (its count read on the device) --
     if (sum.error == 0) {
-      reset(r.candidates, 0);
+      hc->next = 0;
+      hc->heavy = 0;
+      put();
       k_op_heads<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_inv, gen_pull, oc);
-      launched(1);
-      r = counts();
-      if (r.candidates > 0) {
-        k_op_pull<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, r.candidates, heavy,
-                                            heavy_cap, oc);
-        k_op_pull_heavy<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, heavy, heavy_cap, oc);
-        launched(2);
-        r = counts();
-      }
-      frontier_count = r.next;
+      k_op_pull<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, heavy, heavy_cap, oc);
+      k_op_pull_heavy<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, gen_pull, heavy, heavy_cap, oc);
+      launched(3);
+      frontier = true;
     }
   }
   // ---- the near-far loop: one host synchronisation per push step or threshold raise -----------
   const long long iteration_cap = 4 * n + 64;
-  if (frontier_count > 0 && sum.error == 0) {
+  if (frontier && sum.error == 0) {
     int cur = 0, far_cur = 0;
-    reset(0, 0);
-    k_op_min<<<grid, kOpBlock, 0, s>>>(p, bits, p.frontier, frontier_count, oc);
-    launched(1);
-    const OpCounts m = counts();
-    u64 threshold = (m.minimum == kPackedInf ? 0 : m.minimum) + delta;
+    // the first threshold and split, with the frontier's length and minimum on the device
+    k_op_min<<<grid, kOpBlock, 0, s>>>(p, bits, p.frontier, &oc->next, oc);
+    k_op_threshold<<<1, 1, 0, s>>>(oc, delta, 1, 0);
     ++gen;
-    reset(0, 0);
-    k_op_split<<<grid, kOpBlock, 0, s>>>(p, bits, threshold, gen, p.frontier, frontier_count, 0,
-                                         lists[cur], fars[far_cur], oc);
-    launched(1);
-    OpCounts r = counts();
-    int near_count = r.next, far_count = r.far;
+    k_op_split<<<grid, kOpBlock, 0, s>>>(p, bits, gen, p.frontier, 0, lists[cur], fars[far_cur],
+                                         oc);
+    launched(3);
+    get();
+    wait();
+    int near_count = hc->next, far_count = hc->far;
     while (near_count > 0 || far_count > 0) {
       const int step = sum.iterations + sum.epochs;
       if (step < 4) sum.frontier[step] = near_count > 0 ? near_count : -far_count;
@@ -621,34 +648,35 @@ void run_operators(Context& ctx, const SsspParams& p) {
         }
         sum.pushes += near_count;
         ++gen;
-        reset(0, far_count);
+        hc->next = 0;
+        hc->heavy = 0;
+        put();
+        const u64 threshold = hc->threshold;
         k_op_push<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, threshold, gen, lists[cur], near_count,
                                             lists[cur ^ 1], fars[far_cur], heavy, heavy_cap, oc);
         k_op_push_heavy<<<grid, kOpBlock, 0, s>>>(p, bits, maxd, threshold, gen, lists[cur ^ 1],
                                                   fars[far_cur], heavy, heavy_cap, oc);
         launched(2);
-        r = counts();
+        get();
+        wait();
         cur ^= 1;
-        near_count = r.next;
-        far_count = r.far;
+        near_count = hc->next;
+        far_count = hc->far;
         continue;
       }
       // the near frontier is empty: raise the threshold past the far pile and split the pile
       ++sum.epochs;
-      reset(0, 0);
-      k_op_min<<<grid, kOpBlock, 0, s>>>(p, bits, fars[far_cur], far_count, oc);
-      launched(1);
-      const OpCounts fm = counts();
-      threshold = std::max(threshold, fm.minimum == kPackedInf ? threshold : fm.minimum) + delta;
+      k_op_min<<<grid, kOpBlock, 0, s>>>(p, bits, fars[far_cur], &oc->far, oc);
+      k_op_threshold<<<1, 1, 0, s>>>(oc, delta, 0, 1);
       ++gen;
-      reset(0, 0);
-      k_op_split<<<grid, kOpBlock, 0, s>>>(p, bits, threshold, gen, fars[far_cur], far_count, 1,
-                                           lists[cur], fars[far_cur ^ 1], oc);
-      launched(1);
-      r = counts();
+      k_op_split<<<grid, kOpBlock, 0, s>>>(p, bits, gen, fars[far_cur], 1, lists[cur],
+                                           fars[far_cur ^ 1], oc);
+      launched(3);
+      get();
+      wait();
       far_cur ^= 1;
-      near_count = r.next;
-      far_count = r.far;
+      near_count = hc->next;
+      far_count = hc->far;
     }
   }
   // ---- commit ---------------------------------------------------------------------------------
