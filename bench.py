@@ -41,8 +41,8 @@ METRIC = "changed edges/s and p50/p99 update latency, learned vs plain schedule,
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=100_000)
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--graph", default="rmat", choices=["rmat", "grid"],
