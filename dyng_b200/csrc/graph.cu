@@ -114,6 +114,8 @@ struct ApplyParams {
   int* reloc_in;
   unsigned* new_start_out;
   unsigned* new_start_in;
+  unsigned* append_at_out;  // the arena slot of the row's first appended edge
+  unsigned* append_at_in;
   int* new_cap_out;
   int* new_cap_in;
   int* live_out;
@@ -250,12 +252,20 @@ __device__ void ph_validate(const ApplyParams& p, BlockRed& R, long long tid, lo
 __device__ void ph_clear(const ApplyParams& p, long long tid, long long threads) {
   const long long cap = static_cast<long long>(p.mask) + 1;
   const int k = p.k > 0 ? p.k : 1;
+  // every field a new pair starts from, written here by coalesced passes over the table rather
+  // than by the thread that inserts the pair (one scattered 32-byte sector per field and pair)
   for (long long i = tid; i < cap; i += threads) {
     p.key[i] = ~0ULL;
     p.d[i] = 0;
     p.t[i] = 0;
     p.first[i] = 0x7f7f7f7f;
     p.last[i] = -1;
+    p.out_pos[i] = -1;
+    p.in_pos[i] = -1;
+    p.out_pos2[i] = -1;
+    p.in_pos2[i] = -1;
+    p.out_count[i] = 0;
+    p.in_count[i] = 0;
     if (i < k) {
       p.col_sum_delta[i] = 0;
       p.col_removed_at_max[i] = 0;
@@ -337,13 +347,7 @@ __device__ void add_op(PairStage& st, const ApplyParams& p, int32_t u, int32_t v
   for (int probe = 0; probe <= p.mask; ++probe) {
     const u64 prev = atomicCAS(&p.key[h], kEmptyKey, k);
     if (prev == kEmptyKey) {
-      slot = static_cast<int>(h);
-      p.out_pos[slot] = -1;
-      p.in_pos[slot] = -1;
-      p.out_pos2[slot] = -1;
-      p.in_pos2[slot] = -1;
-      p.out_count[slot] = 0;
-      p.in_count[slot] = 0;
+      slot = static_cast<int>(h);  // its fields were set by the clear step
       stage_put(st, p, 0, slot);
       touch_row(st, p, 0, u);
       touch_row(st, p, 1, v);
@@ -628,7 +632,7 @@ __device__ void ph_alloc(const ApplyParams& p, BlockRed& R, long long tid, long 
     const int side = i < rows_out ? 0 : 1;
     const int s = side == 0 ? i : i - rows_out;
     int reloc = 0, new_cap = 0, live = 0;
-    unsigned start = 0;
+    unsigned start = 0, tail = 0;
     if (active) {
       const int32_t r = (side == 0 ? p.rows_out : p.rows_in)[s];
       const bool existing = r < c->n_old;
@@ -641,6 +645,7 @@ __device__ void ph_alloc(const ApplyParams& p, BlockRed& R, long long tid, long 
       const int tomb = dead + dels;
       const bool compact = tomb > 8 && tomb * 4 > desc.len;
       start = desc.start;
+      tail = desc.start + desc.len;
       new_cap = cap;
       if (desc.len + apps > cap || compact) {
         reloc = 1;
@@ -665,9 +670,11 @@ __device__ void ph_alloc(const ApplyParams& p, BlockRed& R, long long tid, long 
         set_error(&c->error, kErrCapacity);
       }
       start = static_cast<unsigned>(at);
+      tail = start + live;
     }
     (side == 0 ? p.reloc_out : p.reloc_in)[s] = reloc;
     (side == 0 ? p.new_start_out : p.new_start_in)[s] = start;
+    (side == 0 ? p.append_at_out : p.append_at_in)[s] = tail;
     (side == 0 ? p.new_cap_out : p.new_cap_in)[s] = new_cap;
     (side == 0 ? p.live_out : p.live_in)[s] = live;
   }
@@ -918,16 +925,12 @@ __device__ void ph_append(const ApplyParams& p, BlockRed& R, long long tid, long
     const u64 key = p.key[slot];
     const int32_t u = static_cast<int32_t>(key >> 32), v = static_cast<int32_t>(key & 0xffffffffu);
     const int ins_index = (flags & kPairUseFirst) ? p.first[slot] : p.last[slot];
-    // both sides' loads first (they are independent), then the stores
+    // both sides' loads first (they are independent), then the stores; the row's first append
+    // slot (after its live slots if it moved, after its old length if not) was set by the alloc
+    // step, so one scattered row field is read per side
     const int s0 = p.row_slot_out[u], s1 = p.row_slot_in[v];
     const int rk0 = p.out_rank[slot], rk1 = p.in_rank[slot];
-    const int reloc0 = p.reloc_out[s0], reloc1 = p.reloc_in[s1];
-    const RowDesc d0 = u < c->n_old ? p.g.out_desc[u] : RowDesc{0, 0};
-    const RowDesc d1 = v < c->n_old ? p.g.in_desc[v] : RowDesc{0, 0};
-    const unsigned ns0 = p.new_start_out[s0], ns1 = p.new_start_in[s1];
-    const int lv0 = p.live_out[s0], lv1 = p.live_in[s1];
-    const unsigned placed[2] = {(reloc0 ? ns0 + lv0 : d0.start + d0.len) + rk0,
-                                (reloc1 ? ns1 + lv1 : d1.start + d1.len) + rk1};
+    const unsigned placed[2] = {p.append_at_out[s0] + rk0, p.append_at_in[s1] + rk1};
     p.g.out_col[placed[0]] = v;
     p.g.in_col[placed[1]] = u;
     for (int j = 0; j < p.k; ++j) {
@@ -1536,6 +1539,8 @@ ApplyParams make_params(Context& ctx, Graph& g, const StagedBatch& b, int object
   p.reloc_in = ws.row_reloc_in.ptr;
   p.new_start_out = ws.row_new_start_out.ptr;
   p.new_start_in = ws.row_new_start_in.ptr;
+  p.append_at_out = ws.row_append_at_out.ptr;
+  p.append_at_in = ws.row_append_at_in.ptr;
   p.new_cap_out = ws.row_new_cap_out.ptr;
   p.new_cap_in = ws.row_new_cap_in.ptr;
   p.live_out = ws.row_live_out.ptr;
@@ -1611,6 +1616,10 @@ void Workspace::reserve_batch(long long ops, int k, cudaStream_t s) {
     row_new_start_out.reserve(c, s);
     row_new_start_in.release();
     row_new_start_in.reserve(c, s);
+    row_append_at_out.release();
+    row_append_at_out.reserve(c, s);
+    row_append_at_in.release();
+    row_append_at_in.reserve(c, s);
     pairs_sized = cap;
   }
   pairs_active = cap;

@@ -211,6 +211,7 @@ struct Workspace {
   DevBuf<int> rows_out, rows_in;  // touched row ids
   DevBuf<int> row_dels_out, row_dels_in, row_apps_out, row_apps_in, row_reloc_out, row_reloc_in;
   DevBuf<unsigned> row_new_start_out, row_new_start_in;
+  DevBuf<unsigned> row_append_at_out, row_append_at_in;  // first append slot of each touched row
   DevBuf<int> row_new_cap_out, row_new_cap_in, row_live_out, row_live_in;
   DevBuf<int> row_seg_offsets, row_seg;  // append order: appended pairs per row
   DevBuf<long long> col_ins_max, col_sum_delta, col_removed_at_max, col_written_max,

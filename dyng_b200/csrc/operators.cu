@@ -4,8 +4,8 @@
 // cpp/src/algorithms/sssp/operators.cuh and its host loop in operators.cu: one synchronisation
 // per push iteration and per threshold raise).  Between the roots and the first push the counts
 // stay on the device (the heads, the pull, the first threshold and split read them there), so an
-// update synchronises once for the roots, once per invalidation round or walk level, once for
-// the first split, and once per push step or threshold raise.
+// update synchronises once for the roots, once per four pointer-jumping rounds or per walk level,
+// once for the first split, and once per push step or threshold raise.
 //
 // It needs no cooperative launch, so it is what engine::automatic runs on a device without one
 // (as the reference does, sssp.cpp:195-226), and what options::cuda_engine = operators asks for.
@@ -34,13 +34,15 @@ constexpr int kMarked = -2;  // pointer jumping: an invalidated ancestor was rea
 // kOpChunk-slot chunks, and a second launch reads every chunk with its own warp.
 constexpr int kOpHeavy = 2048;
 constexpr int kOpChunk = 1024;
+// Pointer-jumping rounds launched between two host synchronisations.
+constexpr int kOpRoundsPerSync = 4;
 
 // The counters one step leaves for the host.
 struct OpCounts {
   int next;        // entries appended to the next list (near frontier, walk level, pull frontier)
   int far;         // entries on the far pile being appended to
   int candidates;  // vertices the pull re-evaluates
-  int jumped;      // pointer jumping: a chain moved on this round and goes on
+  unsigned moved;  // pointer jumping: bit r set when a chain moved on in round r and goes on
   int heavy;       // chunks listed for the heavy-row launch
   int in_count;    // length of the list a split reads (set by k_op_threshold)
   int source;      // compute: the source, staged for its copy into the frontier
@@ -191,7 +193,11 @@ __global__ void k_op_pj_start(SsspParams p, int gen_inv, long long n) {
   }
 }
 
-__global__ void k_op_pj_round(SsspParams p, int gen_inv, long long n, OpCounts* oc) {
+// Round `round` returns at once when no chain moved on in the round before it (the rounds are
+// launched a few at a time between host synchronisations; a round after the last one that moved
+// would change nothing anyway, every ancestor being negative by then).
+__global__ void k_op_pj_round(SsspParams p, int gen_inv, long long n, OpCounts* oc, int round) {
+  if (round > 0 && !((oc->moved >> (round - 1)) & 1u)) return;
   long long inval = 0;
   int jumped = 0;
   for (long long v = op_tid(); v < n; v += op_threads()) {
@@ -209,7 +215,7 @@ __global__ void k_op_pj_round(SsspParams p, int gen_inv, long long n, OpCounts* 
       jumped |= na >= 0;
     }
   }
-  if (__syncthreads_or(jumped) && threadIdx.x == 0) oc->jumped = 1;
+  if (__syncthreads_or(jumped) && threadIdx.x == 0) atomicOr(&oc->moved, 1u << round);
   op_block_add(inval, &p.ctl->invalidated);
 }
 
@@ -599,16 +605,22 @@ void run_operators(Context& ctx, const SsspParams& p) {
         ++max_rounds;
         k_op_pj_start<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n);
         launched(1);
-        for (int round = 0; round < max_rounds; ++round) {
-          hc->jumped = 0;
-          put();
-          k_op_pj_round<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n, oc);
-          launched(1);
+        hc->moved = 0;
+        put();
+        // kOpRoundsPerSync rounds per host synchronisation; sum.rounds counts the rounds up to
+        // and including the first in which no chain moved on (all of them if every one moved)
+        for (int first = 0; first < max_rounds; first += kOpRoundsPerSync) {
+          const int last = std::min(max_rounds, first + kOpRoundsPerSync);
+          for (int round = first; round < last; ++round)
+            k_op_pj_round<<<grid, kOpBlock, 0, s>>>(p, gen_inv, n, oc, round);
+          launched(last - first);
           get();
           wait();
-          sum.rounds = round + 1;
-          sum.active = hc->jumped;
-          if (!hc->jumped) break;
+          int round = first;
+          while (round < last && ((hc->moved >> round) & 1u)) ++round;
+          sum.rounds = std::min(round + 1, last);
+          sum.active = (hc->moved >> (sum.rounds - 1)) & 1u;
+          if (round < last) break;
         }
       }
     }
