@@ -40,21 +40,6 @@ __device__ __forceinline__ u64 pair_key(int32_t u, int32_t v) {
   return (static_cast<u64>(static_cast<uint32_t>(u)) << 32) | static_cast<uint32_t>(v);
 }
 
-// Warp-level sums and maxima folded into one atomic per warp (all 32 lanes must call).
-__device__ __forceinline__ void warp_add(long long v, long long* target) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0)
-    atomicAdd(reinterpret_cast<unsigned long long*>(target), static_cast<unsigned long long>(v));
-}
-__device__ __forceinline__ void warp_add_u(unsigned long long v, unsigned long long* target) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(target, v);
-}
-__device__ __forceinline__ void warp_max(long long v, long long* target, long long floor_value) {
-  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0 && v > floor_value) atomicMax(target, v);
-}
-
 // Per-thread column statistics deltas of weight column 0, in registers (the other columns go to
 // the global counters directly); flushed once per warp at the end of a step.  Scalars, not
 // arrays indexed by the column: every thread of the persistent grid carries them, and an array
