@@ -19,8 +19,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared if not hasattr(lib, s)]
     assert not missing, missing
     # the ctypes table covers the header exactly
-    assert sorted(set(declared) & set(N.SIGNATURES)) == sorted(
-        s for s in declared if s in N.SIGNATURES)
+    assert set(declared) == set(N.SIGNATURES)
 
 
 def test_host_only_entry_points():
@@ -45,3 +44,17 @@ def test_generators_are_deterministic():
     assert np.all(np.diff(key) > 0)  # sorted, no duplicate pairs
     g = G.grid(16, seed=2)
     assert g.num_vertices == 256 and g.weights.min() >= 1
+
+
+def test_null_handles_are_argument_errors_on_the_host():
+    """A null handle is refused before anything reaches the device (so this runs without a GPU):
+    INVALID_ARGUMENT with a message naming the reference's call; destroying null is a no-op."""
+    L = N.lib()
+    st = N.Stats()
+    status = L.dyngb200_sssp_update(None, None, None, None, ctypes.byref(st))
+    assert L.dyngb200_status_name(status) == b"invalid_argument"
+    assert L.dyngb200_last_error_message().startswith(b"sssp::update")
+    assert L.dyngb200_status_name(L.dyngb200_context_synchronize(None)) == b"invalid_argument"
+    for destroy in (L.dyngb200_graph_destroy, L.dyngb200_tree_destroy,
+                    L.dyngb200_context_destroy):
+        assert destroy(None) == 0
